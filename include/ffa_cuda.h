@@ -1,0 +1,236 @@
+/*
+ * ffa_cuda.h -- C ABI of libffa_cuda.so, the sm_100a tracking hot path.
+ *
+ * PyFFA (the reference) is pure Python + Numba and exposes no FFI; its
+ * hot-path boundary is the Python call interface of the tracking loop.
+ * Each entry point below replaces one group of those calls (cited per
+ * function, paths relative to the reference project).
+ *
+ * Conventions
+ *  - Every pointer named "device" is caller-owned device memory (typically a
+ *    torch tensor's data_ptr()).  Objects created here (field maps, space-charge
+ *    plans) own only their packed tables and scratch.
+ *  - Every call returns an int error code (FFA_OK = 0).  Argument errors are
+ *    reported before any work is enqueued.
+ *  - Calls are stream-ordered on the cudaStream_t passed as `stream` (NULL =
+ *    legacy default stream), never synchronise implicitly, and are not
+ *    thread-safe per object.  Kernels never trap: problems are counted in the
+ *    caller's device status words (ffa_status_index).
+ *  - Particle state is structure-of-arrays, float64, with the reference's
+ *    meaning per array (src/FFAG_Bunch.py:23-74 column map).
+ */
+#ifndef FFA_CUDA_H
+#define FFA_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFA_ABI_VERSION 1
+
+#define FFA_MAX_POLY 16
+#define FFA_MAX_SEG 16
+#define FFA_MAX_GAPS 8
+#define FFA_MAX_ORDER 4
+
+enum ffa_error {
+    FFA_OK = 0,
+    FFA_ERR_INVALID = 1,     /* bad argument (null pointer, size, flag) */
+    FFA_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    FFA_ERR_NOMEM = 3,       /* device allocation failed */
+    FFA_ERR_UNSUPPORTED = 4  /* valid but not built (e.g. order > FFA_MAX_ORDER) */
+};
+
+/* ffa_push flags */
+enum ffa_push_flags {
+    FFA_BORIS = 0,                /* relativistic Boris (solver_type 1) */
+    FFA_RK4 = 1,                  /* 4th-order Runge-Kutta (solver_type 0) */
+    FFA_FP64 = 0,                 /* all arithmetic in float64 */
+    FFA_FP32C = 2,                /* float32 fields/push, compensated r, fi, phase */
+    FFA_RF_PHYSICAL_SUM = 4       /* sum every RF gap (reference: last gap wins) */
+};
+
+/* Device status words, int64 each, accumulated with atomics. */
+enum ffa_status_index {
+    FFA_STATUS_LOST = 0,          /* particles lost at the aperture */
+    FFA_STATUS_NAN = 1,           /* non-finite coordinates seen after a push */
+    FFA_STATUS_OUT_OF_MAP = 2,    /* high-order map lookups clamped at the edge */
+    FFA_STATUS_SC_DEGENERATE = 3, /* space-charge updates with an empty grid */
+    FFA_STATUS_WORDS = 8
+};
+
+/* Mid-plane field: analytic orders 0/1 (src/FFAG_Field.py:1333-1426) and the
+ * z-Taylor maps of orders 1..max_order (src/FFAG_MathTools.py:1139-1188). */
+typedef struct ffa_field_desc {
+    int32_t nsectors;
+    int32_t n_spoly;              /* s(r) coefficients, highest degree first */
+    int32_t n_spolyp;             /* s'(r) coefficients */
+    int32_t n_convex;             /* flutter segments */
+    int32_t max_order;            /* 0..FFA_MAX_ORDER */
+    int32_t pad0;
+    double B0, k;                 /* B0 * r^k */
+    double spoly[FFA_MAX_POLY];
+    double spolyp[FFA_MAX_POLY];
+    double convex[FFA_MAX_SEG * 5];  /* x0, x1, W0, y01, y02 (rad) */
+    double r_min, r_step;
+    int64_t r_size;
+    double fi_min, fi_step;
+    int64_t fi_size;
+    /* device, float64, shape (max_order+1, r_size, fi_size), row-major;
+     * order 0 is not read */
+    const double *bz_stack;
+    const double *bfi_stack;
+    const double *br_stack;
+} ffa_field_desc;
+
+/* Fixed RF gaps (src/FFAG_Field.py:167-306, src/FFAG_Utils.py:984-1036). */
+typedef struct ffa_rf_desc {
+    int32_t enable;               /* Emap EnableFlag */
+    int32_t ngaps;                /* 1..FFA_MAX_GAPS */
+    int32_t pad0, pad1;
+    double poly_x[FFA_MAX_GAPS][4];
+    double poly_y[FFA_MAX_GAPS][4];
+    double box[FFA_MAX_GAPS][4];  /* x_min, x_max, y_min, y_max */
+    double theta_n[FFA_MAX_GAPS]; /* gap azimuth + pi/2 */
+    double rf_shift[FFA_MAX_GAPS];
+} ffa_rf_desc;
+
+typedef struct ffa_aperture {
+    int32_t enable;
+    int32_t pad0;
+    double rmin, rmax, zmin, zmax;
+} ffa_aperture;
+
+typedef struct ffa_consts {
+    double q, c, m0, E0;          /* C, m/s, kg, J */
+} ffa_consts;
+
+/* Particle state (device SoA).  f5 is dfi/dt for Boris, Etot [J] for RK4.
+ * inj/surv are 0/1 bytes (cols 7/8).  inj_step[i] is the absolute step index
+ * at which particle i is injected (-1: never), precomputed by the host from
+ * the reference's InjectParticles rule (src/FFAG_Bunch.py:265-303).
+ * The e_pre / e_pp arrays and the sc_pre / sc_pp masks hold the two most
+ * recent space-charge endpoints used by the per-step linear extrapolation
+ * (src/FFAG_track.py:449-478); they may be NULL when sc_step == 0. */
+typedef struct ffa_state_soa {
+    double *r, *vr, *z, *vz, *fi, *f5, *rf;
+    double *esc_r, *esc_z, *esc_fi;
+    uint8_t *inj, *surv;
+    const int32_t *inj_step;
+    double *e_pre_r, *e_pre_z, *e_pre_fi;
+    double *e_pp_r, *e_pp_z, *e_pp_fi;
+    uint8_t *sc_pre, *sc_pp;
+    /* FP32C mode: low words of the double-float r and fi (device, float32);
+     * the RF phase stays float64 in `rf`. */
+    float *r_lo, *fi_lo;
+} ffa_state_soa;
+
+/* Per-step host-precomputed scalars (device arrays indexed by absolute step).
+ * Boris: drf[s] = f_rf(t_s) * pi * 2 * dt, acc[s] = V0(t_s) / gap_width.
+ * RK4:   drf[4s+k], acc[4s+k] for the stage times t, t+h/2, t+h/2, t+h, with
+ *        drf the phase rate f_rf * pi * 2. */
+typedef struct ffa_step_table {
+    const double *drf;
+    const double *acc;
+    int64_t nsteps;               /* entries (Boris) or stage quadruples (RK4) */
+} ffa_step_table;
+
+typedef struct ffa_fieldmap ffa_fieldmap;
+
+/* Packs the z-Taylor stacks into the interleaved node layout the push kernels
+ * read (float64 and float32 copies).  Replaces FFAG_Bfield_analytical map
+ * loading (src/FFAG_Field.py:636-711). */
+int ffa_fieldmap_create(const ffa_field_desc *desc, void *stream, ffa_fieldmap **out);
+int ffa_fieldmap_destroy(ffa_fieldmap *fm);
+
+/* Applies the injection of absolute step `step` (flags only).
+ * Replaces FFAG_Bunch.InjectParticles (src/FFAG_Bunch.py:265-303). */
+int ffa_inject(ffa_state_soa *st, int64_t n, int64_t step, void *stream);
+
+/* Advances n particles by nsteps fixed steps starting at absolute step
+ * step0: per step injection, space-charge extrapolation (sc_step > 0), field
+ * evaluation and the Boris or RK4 update, fused in one launch with the state
+ * held in registers.  Replaces one iteration of the step loop of
+ * rk4_solve_dt_bunch3_withSC_boris / _withSC per step
+ * (src/FFAG_track.py:297-579, 65-294): Boris_solve (:948-1049) or
+ * rk4_step_malloc + RK4_Post_Step_njit (:51-61, src/FFAG_MathTools.py:2269).
+ * status: device int64[FFA_STATUS_WORDS]. */
+int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap,
+             const ffa_consts *cs, const ffa_step_table *tab, ffa_state_soa *st,
+             int64_t n, int64_t step0, int32_t nsteps, double dt, int32_t sc_step,
+             int32_t flags, void *stream, int64_t *status);
+
+/* Converts between the reference's N x 16 row-major matrix (device) and the
+ * SoA state.  soa_to_aos writes cols 0-5 and 7-12 and leaves 6, 13-15.
+ * Replaces the LocalBunch column views used throughout src/FFAG_track.py. */
+int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream);
+int ffa_soa_to_aos(const ffa_state_soa *st, int64_t n, double *aos, void *stream);
+
+/* Loads (lo words = 0) or stores the FP32C double-float words from / to the
+ * float64 state arrays. */
+int ffa_fp32c_split(ffa_state_soa *st, int64_t n, void *stream);
+int ffa_fp32c_merge(ffa_state_soa *st, int64_t n, void *stream);
+
+/* Sum of fi over the particles whose fi is not NaN, written to *out (device
+ * double), and their count to *count (device int64); the host divides.
+ * Replaces the mean in the stop test of src/FFAG_track.py:559-577. */
+int ffa_mean_fi(const ffa_state_soa *st, int64_t n, double *out, int64_t *count, void *stream);
+
+/* ------------------------------------------------------- space charge */
+
+/* 2.5D slice-by-slice space charge (src/FFAG_Bunch.py:1157-1352). */
+typedef struct ffa_sc_desc {
+    int32_t ns, nx, nz;           /* slices, transverse grid */
+    int32_t hockney;              /* 0: periodic kernel (reference); 1: open boundary */
+    int32_t boris;                /* 1: gamma from |v|; 0: gamma = Etot / E0 */
+    int32_t pad0;
+    int64_t n_max;                /* particle capacity of the scratch */
+    double sigma_ratio;           /* grid half-width in rms sizes */
+    double q_macro;               /* marcosize * q [C] */
+    double speed_c, E0_rest_MeV, E0_J;
+    /* closed-orbit tables (device, float64): r0 and pr0 of shape (nE, nfi),
+     * perimeter (nE); Ek axis [MeV] and fi axis [rad] uniform */
+    int64_t nE, nfi;
+    double Ek0, dEk, fi0, dfi;
+    const double *seo_Ek;         /* device, nE (for the perimeter interpolation) */
+    const double *seo_r;
+    const double *seo_pr;
+    const double *seo_perimeter;
+} ffa_sc_desc;
+
+/* Diagnostics of the last update (device struct written by ffa_sc_step). */
+typedef struct ffa_sc_diag {
+    double fi_s, fi_e, slice_step, mean_gamma_m1;
+    double mean_x, mean_z, sigma_x, sigma_z;
+    double xmin, xmax, zmin, zmax, dx, dz;
+    double bunch_length, q_density;
+    int64_t count, degenerate;
+} ffa_sc_diag;
+
+typedef struct ffa_sc_plan ffa_sc_plan;
+
+int ffa_sc_plan_create(const ffa_sc_desc *desc, void *stream, ffa_sc_plan **out);
+int ffa_sc_plan_destroy(ffa_sc_plan *plan);
+
+/* One space-charge update over the particles with surv != 0: coordinates,
+ * slice arc and moments, CIC deposit, Poisson solve per slice, field and
+ * gather into esc_*.  Replaces Build_2_5D_SliceGrid_sbs.  When `roll` is
+ * nonzero the extrapolation endpoints are rolled afterwards as the step loop
+ * does (first != 0 at step 0).  diag: device ffa_sc_diag or NULL. */
+int ffa_sc_step(ffa_sc_plan *plan, ffa_state_soa *st, int64_t n, int32_t roll, int32_t first,
+                void *stream, int64_t *status, ffa_sc_diag *diag);
+
+/* Device views of the plan's last charge, potential and field cubes
+ * (float32, (ns, nz, nx)), and of the per-particle slice / cell indices
+ * (int32 slice, int64 cell = (s*nz + iz)*nx + ix, -1 when not deposited). */
+int ffa_sc_buffers(const ffa_sc_plan *plan, const float **rho, const float **phi,
+                   const float **ex, const float **ez, const int32_t **slice_idx,
+                   const int64_t **cell_idx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFA_CUDA_H */

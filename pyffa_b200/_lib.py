@@ -1,0 +1,155 @@
+"""ctypes binding of libffa_cuda.so (include/ffa_cuda.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+the shared object is missing or fails to load, every GPU entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB_PATH
+
+MAX_POLY = 16
+MAX_SEG = 16
+MAX_GAPS = 8
+MAX_ORDER = 4
+
+FFA_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA runtime error", 3: "out of device memory", 4: "unsupported"}
+
+FFA_BORIS = 0
+FFA_RK4 = 1
+FFA_FP64 = 0
+FFA_FP32C = 2
+FFA_RF_PHYSICAL_SUM = 4
+
+STATUS_LOST = 0
+STATUS_NAN = 1
+STATUS_OUT_OF_MAP = 2
+STATUS_SC_DEGENERATE = 3
+STATUS_WORDS = 8
+
+d_p = C.c_void_p  # device pointers travel as integers
+
+
+class FieldDesc(C.Structure):
+    _fields_ = [
+        ("nsectors", C.c_int32), ("n_spoly", C.c_int32), ("n_spolyp", C.c_int32),
+        ("n_convex", C.c_int32), ("max_order", C.c_int32), ("pad0", C.c_int32),
+        ("B0", C.c_double), ("k", C.c_double),
+        ("spoly", C.c_double * MAX_POLY), ("spolyp", C.c_double * MAX_POLY),
+        ("convex", C.c_double * (MAX_SEG * 5)),
+        ("r_min", C.c_double), ("r_step", C.c_double), ("r_size", C.c_int64),
+        ("fi_min", C.c_double), ("fi_step", C.c_double), ("fi_size", C.c_int64),
+        ("bz_stack", d_p), ("bfi_stack", d_p), ("br_stack", d_p),
+    ]
+
+
+class RFDesc(C.Structure):
+    _fields_ = [
+        ("enable", C.c_int32), ("ngaps", C.c_int32), ("pad0", C.c_int32), ("pad1", C.c_int32),
+        ("poly_x", (C.c_double * 4) * MAX_GAPS), ("poly_y", (C.c_double * 4) * MAX_GAPS),
+        ("box", (C.c_double * 4) * MAX_GAPS),
+        ("theta_n", C.c_double * MAX_GAPS), ("rf_shift", C.c_double * MAX_GAPS),
+    ]
+
+
+class Aperture(C.Structure):
+    _fields_ = [("enable", C.c_int32), ("pad0", C.c_int32),
+                ("rmin", C.c_double), ("rmax", C.c_double), ("zmin", C.c_double), ("zmax", C.c_double)]
+
+
+class Consts(C.Structure):
+    _fields_ = [("q", C.c_double), ("c", C.c_double), ("m0", C.c_double), ("E0", C.c_double)]
+
+
+class StateSoA(C.Structure):
+    _fields_ = [
+        ("r", d_p), ("vr", d_p), ("z", d_p), ("vz", d_p), ("fi", d_p), ("f5", d_p), ("rf", d_p),
+        ("esc_r", d_p), ("esc_z", d_p), ("esc_fi", d_p),
+        ("inj", d_p), ("surv", d_p), ("inj_step", d_p),
+        ("e_pre_r", d_p), ("e_pre_z", d_p), ("e_pre_fi", d_p),
+        ("e_pp_r", d_p), ("e_pp_z", d_p), ("e_pp_fi", d_p),
+        ("sc_pre", d_p), ("sc_pp", d_p),
+        ("r_lo", d_p), ("fi_lo", d_p),
+    ]
+
+
+class StepTable(C.Structure):
+    _fields_ = [("drf", d_p), ("acc", d_p), ("nsteps", C.c_int64)]
+
+
+class SCDesc(C.Structure):
+    _fields_ = [
+        ("ns", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32), ("hockney", C.c_int32),
+        ("boris", C.c_int32), ("pad0", C.c_int32), ("n_max", C.c_int64),
+        ("sigma_ratio", C.c_double), ("q_macro", C.c_double),
+        ("speed_c", C.c_double), ("E0_rest_MeV", C.c_double), ("E0_J", C.c_double),
+        ("nE", C.c_int64), ("nfi", C.c_int64),
+        ("Ek0", C.c_double), ("dEk", C.c_double), ("fi0", C.c_double), ("dfi", C.c_double),
+        ("seo_Ek", d_p), ("seo_r", d_p), ("seo_pr", d_p), ("seo_perimeter", d_p),
+    ]
+
+
+class SCDiag(C.Structure):
+    _fields_ = [(name, C.c_double) for name in (
+        "fi_s", "fi_e", "slice_step", "mean_gamma_m1", "mean_x", "mean_z", "sigma_x", "sigma_z",
+        "xmin", "xmax", "zmin", "zmax", "dx", "dz", "bunch_length", "q_density")] + [
+        ("count", C.c_int64), ("degenerate", C.c_int64)]
+
+
+EXPORTS = {
+    "ffa_fieldmap_create": [C.POINTER(FieldDesc), d_p, C.POINTER(d_p)],
+    "ffa_fieldmap_destroy": [d_p],
+    "ffa_inject": [C.POINTER(StateSoA), C.c_int64, C.c_int64, d_p],
+    "ffa_push": [d_p, C.POINTER(RFDesc), C.POINTER(Aperture), C.POINTER(Consts), C.POINTER(StepTable),
+                 C.POINTER(StateSoA), C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                 d_p, d_p],
+    "ffa_aos_to_soa": [d_p, C.c_int64, C.POINTER(StateSoA), d_p],
+    "ffa_soa_to_aos": [C.POINTER(StateSoA), C.c_int64, d_p, d_p],
+    "ffa_fp32c_split": [C.POINTER(StateSoA), C.c_int64, d_p],
+    "ffa_fp32c_merge": [C.POINTER(StateSoA), C.c_int64, d_p],
+    "ffa_mean_fi": [C.POINTER(StateSoA), C.c_int64, d_p, d_p, d_p],
+    "ffa_sc_plan_create": [C.POINTER(SCDesc), d_p, C.POINTER(d_p)],
+    "ffa_sc_plan_destroy": [d_p],
+    "ffa_sc_step": [d_p, C.POINTER(StateSoA), C.c_int64, C.c_int32, C.c_int32, d_p, d_p, d_p],
+    "ffa_sc_buffers": [d_p, C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p),
+                       C.POINTER(d_p), C.POINTER(d_p)],
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded libffa_cuda.so; raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"libffa_cuda.so not found at {LIB_PATH}: build it with `python -m pyffa_b200.build` "
+                "(the tracking path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, argtypes in EXPORTS.items():
+            fn = getattr(L, name)
+            fn.argtypes = argtypes
+            fn.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+class FFAError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str) -> None:
+    if rc != FFA_OK:
+        raise FFAError(f"{what} failed: {ERRORS.get(rc, rc)}")
+
+
+def stream_ptr(stream) -> int:
+    """cudaStream_t of a torch.cuda.Stream (0 = legacy default stream)."""
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(getattr(stream, "cuda_stream", stream))

@@ -1,0 +1,277 @@
+// ffa_capi.cu -- extern "C" entry points of libffa_cuda.so (see include/ffa_cuda.h).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ffa_internal.cuh"
+
+using namespace ffa;
+
+namespace {
+
+cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+bool state_ok(const ffa_state_soa *st)
+{
+    return st && st->r && st->vr && st->z && st->vz && st->fi && st->f5 && st->rf && st->esc_r &&
+           st->esc_z && st->esc_fi && st->inj && st->surv;
+}
+
+// ---------------------------------------------------------------- kernels
+
+__global__ void inject_kernel(ffa_state_soa st, int64_t n, int64_t step)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (st.inj_step[i] == step) {
+        st.inj[i] = 1;
+        st.surv[i] = 1;
+    }
+}
+
+// AoS rows of 16 doubles -> SoA.  Flags are stored as bytes: a column value
+// equal to 1.0 maps to 1; the reference only ever stores 0 or 1 there.
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, int64_t n, ffa_state_soa st)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double *row = aos + i * 16;
+    st.r[i] = row[0];
+    st.vr[i] = row[1];
+    st.z[i] = row[2];
+    st.vz[i] = row[3];
+    st.fi[i] = row[4];
+    st.f5[i] = row[5];
+    st.inj[i] = row[7] == 1.0 ? 1 : (row[7] != 0.0 ? 2 : 0);
+    st.surv[i] = row[8] == 1.0 ? 1 : (row[8] != 0.0 ? 2 : 0);
+    st.rf[i] = row[9];
+    st.esc_r[i] = row[10];
+    st.esc_z[i] = row[11];
+    st.esc_fi[i] = row[12];
+}
+
+__global__ void soa_to_aos_kernel(ffa_state_soa st, int64_t n, double *__restrict__ aos)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double *row = aos + i * 16;
+    row[0] = st.r[i];
+    row[1] = st.vr[i];
+    row[2] = st.z[i];
+    row[3] = st.vz[i];
+    row[4] = st.fi[i];
+    row[5] = st.f5[i];
+    row[7] = st.inj[i] == 2 ? row[7] : (double)st.inj[i];
+    row[8] = st.surv[i] == 2 ? row[8] : (double)st.surv[i];
+    row[9] = st.rf[i];
+    row[10] = st.esc_r[i];
+    row[11] = st.esc_z[i];
+    row[12] = st.esc_fi[i];
+}
+
+__global__ void mean_fi_kernel(const double *__restrict__ fi, int64_t n, double *out, int64_t *count)
+{
+    __shared__ double ssum[32];
+    __shared__ long long scnt[32];
+    double s = 0.0;
+    long long c = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = fi[i];
+        if (!isnan(v)) {
+            s += v;
+            ++c;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, off);
+        c += __shfl_down_sync(0xffffffffu, c, off);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { ssum[w] = s; scnt[w] = c; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        s = l < nw ? ssum[l] : 0.0;
+        c = l < nw ? scnt[l] : 0;
+        for (int off = 16; off > 0; off >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, off);
+            c += __shfl_down_sync(0xffffffffu, c, off);
+        }
+        if (l == 0) {
+            atomicAdd(out, s);
+            atomicAdd((unsigned long long *)count, (unsigned long long)c);
+        }
+    }
+}
+
+unsigned blocks_for(int64_t n, int tb) { return (unsigned)((n + tb - 1) / tb); }
+
+}  // namespace
+
+extern "C" {
+
+int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **out)
+{
+    if (!d || !out) return FFA_ERR_INVALID;
+    *out = nullptr;
+    if (d->nsectors <= 0 || d->n_spoly < 0 || d->n_spoly > FFA_MAX_POLY || d->n_spolyp < 0 ||
+        d->n_spolyp > FFA_MAX_POLY || d->n_convex < 0 || d->n_convex > FFA_MAX_SEG || d->max_order < 0)
+        return FFA_ERR_INVALID;
+    if (d->max_order > FFA_MAX_ORDER) return FFA_ERR_UNSUPPORTED;
+    if (d->max_order > 0 && (d->r_size < 2 || d->fi_size < 2 || !d->bz_stack || !d->bfi_stack || !d->br_stack ||
+                             !(d->r_step > 0) || !(d->fi_step > 0)))
+        return FFA_ERR_INVALID;
+    for (int j = 0; j < d->n_convex; ++j)
+        if (!(d->convex[5 * j + 2] != 0.0)) return FFA_ERR_INVALID;
+
+    ffa_fieldmap *fm = (ffa_fieldmap *)calloc(1, sizeof(ffa_fieldmap));
+    if (!fm) return FFA_ERR_NOMEM;
+    FieldK &k = fm->k;
+    k.nsectors = d->nsectors;
+    k.n_spoly = d->n_spoly;
+    k.n_spolyp = d->n_spolyp;
+    k.n_seg = d->n_convex;
+    k.max_order = d->max_order;
+    const int nv = 3 * d->max_order;
+    k.npad = nv <= 4 ? 4 : (nv <= 8 ? 8 : 12);
+    k.B0 = d->B0;
+    k.k = d->k;
+    k.km1 = d->k - 1.0;
+    k.B0k = d->B0 * d->k;
+    k.period = 2.0 * PI / (double)d->nsectors;
+    memcpy(k.spoly, d->spoly, sizeof(k.spoly));
+    memcpy(k.spolyp, d->spolyp, sizeof(k.spolyp));
+    for (int j = 0; j < d->n_convex; ++j) {
+        const double *cp = d->convex + 5 * j;
+        k.seg_x0[j] = cp[0];
+        k.seg_x1[j] = cp[1];
+        k.seg_k[j] = 16.0 / cp[2];
+        k.seg_y[j] = cp[4] * fabs(cp[3]);
+    }
+    k.r_min = d->r_min;
+    k.r_step = d->r_step;
+    k.fi_min = d->fi_min;
+    k.fi_step = d->fi_step;
+    k.r_size = d->r_size;
+    k.fi_size = d->fi_size;
+    if (d->max_order > 0) {
+        const int64_t plane = d->r_size * d->fi_size;
+        if (cudaMalloc(&fm->nodes64, sizeof(double) * plane * k.npad) != cudaSuccess) {
+            free(fm);
+            return FFA_ERR_NOMEM;
+        }
+        if (cudaMalloc(&fm->nodes32, sizeof(float) * plane * k.npad) != cudaSuccess) {
+            cudaFree(fm->nodes64);
+            free(fm);
+            return FFA_ERR_NOMEM;
+        }
+        if (launch_pack_nodes(*d, k.npad, fm->nodes64, fm->nodes32, as_stream(stream)) != cudaSuccess) {
+            cudaFree(fm->nodes64);
+            cudaFree(fm->nodes32);
+            free(fm);
+            return FFA_ERR_CUDA;
+        }
+    }
+    k.nodes64 = fm->nodes64;
+    k.nodes32 = fm->nodes32;
+    *out = fm;
+    return FFA_OK;
+}
+
+int ffa_fieldmap_destroy(ffa_fieldmap *fm)
+{
+    if (!fm) return FFA_OK;
+    if (fm->nodes64) cudaFree(fm->nodes64);
+    if (fm->nodes32) cudaFree(fm->nodes32);
+    free(fm);
+    return FFA_OK;
+}
+
+int ffa_inject(ffa_state_soa *st, int64_t n, int64_t step, void *stream)
+{
+    if (!state_ok(st) || !st->inj_step || n < 0) return FFA_ERR_INVALID;
+    if (n == 0) return FFA_OK;
+    inject_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(*st, n, step);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    return FFA_OK;
+}
+
+int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
+             const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps, double dt,
+             int32_t sc_step, int32_t flags, void *stream, int64_t *status)
+{
+    if (!fm || !rf || !ap || !cs || !tab || !state_ok(st) || n < 0 || nsteps < 0 || step0 < 0) return FFA_ERR_INVALID;
+    if (!tab->drf || !tab->acc || step0 + nsteps > tab->nsteps) return FFA_ERR_INVALID;
+    if (rf->ngaps < 1 || rf->ngaps > FFA_MAX_GAPS) return FFA_ERR_INVALID;
+    if (sc_step < 0) return FFA_ERR_INVALID;
+    if (sc_step > 0 && st->sc_pre &&
+        (!st->sc_pp || !st->e_pre_r || !st->e_pre_z || !st->e_pre_fi || !st->e_pp_r || !st->e_pp_z || !st->e_pp_fi))
+        return FFA_ERR_INVALID;
+    if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_RF_PHYSICAL_SUM)) return FFA_ERR_INVALID;
+    if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
+    if ((flags & FFA_FP32C) && (!st->r_lo || !st->fi_lo)) return FFA_ERR_INVALID;
+    if (n == 0 || nsteps == 0) return FFA_OK;
+
+    PushK p;
+    memset(&p, 0, sizeof(p));
+    p.f = fm->k;
+    p.rf.enable = rf->enable;
+    p.rf.ngaps = rf->ngaps;
+    p.rf.physical_sum = (flags & FFA_RF_PHYSICAL_SUM) ? 1 : 0;
+    memcpy(p.rf.poly_x, rf->poly_x, sizeof(p.rf.poly_x));
+    memcpy(p.rf.poly_y, rf->poly_y, sizeof(p.rf.poly_y));
+    memcpy(p.rf.box, rf->box, sizeof(p.rf.box));
+    memcpy(p.rf.theta_n, rf->theta_n, sizeof(p.rf.theta_n));
+    memcpy(p.rf.rf_shift, rf->rf_shift, sizeof(p.rf.rf_shift));
+    p.ap = *ap;
+    p.cs = *cs;
+    p.st = *st;
+    if (sc_step == 0) p.st.sc_pre = nullptr;
+    p.drf = tab->drf;
+    p.acc = tab->acc;
+    p.n = n;
+    p.step0 = step0;
+    p.nsteps = nsteps;
+    p.sc_step = sc_step;
+    p.dt = dt;
+    p.status = status;
+    cudaError_t e;
+    if (flags & FFA_RK4) e = launch_rk4_f64(p, as_stream(stream));
+    else if (flags & FFA_FP32C) e = launch_boris_f32c(p, as_stream(stream));
+    else e = launch_boris_f64(p, as_stream(stream));
+    return e == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
+}
+
+int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream)
+{
+    if (!aos || !state_ok(st) || n < 0) return FFA_ERR_INVALID;
+    if (n == 0) return FFA_OK;
+    aos_to_soa_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(aos, n, *st);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    return FFA_OK;
+}
+
+int ffa_soa_to_aos(const ffa_state_soa *st, int64_t n, double *aos, void *stream)
+{
+    if (!aos || !state_ok(st) || n < 0) return FFA_ERR_INVALID;
+    if (n == 0) return FFA_OK;
+    soa_to_aos_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(*st, n, aos);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    return FFA_OK;
+}
+
+int ffa_mean_fi(const ffa_state_soa *st, int64_t n, double *out, int64_t *count, void *stream)
+{
+    if (!st || !st->fi || !out || !count || n < 0) return FFA_ERR_INVALID;
+    cudaStream_t s = as_stream(stream);
+    FFA_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+    FFA_CHECK_CUDA(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
+    if (n == 0) return FFA_OK;
+    unsigned nb = blocks_for(n, 256);
+    if (nb > 1184) nb = 1184;
+    mean_fi_kernel<<<nb, 256, 0, s>>>(st->fi, n, out, count);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    return FFA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// ffa_internal.cuh -- shared device-side definitions of libffa_cuda.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/ffa_cuda.h"
+
+#define FFA_CHECK_CUDA(call)                         \
+    do {                                             \
+        cudaError_t e_ = (call);                     \
+        if (e_ != cudaSuccess) return FFA_ERR_CUDA;  \
+    } while (0)
+
+namespace ffa {
+
+constexpr double PI = 3.141592653589793;
+
+// Kernel-side view of the field (analytic parameters precomputed once and the
+// packed z-Taylor node table).  Node (i, j) of the r x fi grid holds, for
+// n = 1..max_order, (bz_n, bfi_n, br_n), padded to `npad` values so a node is
+// 32 B (float32) or 64 B (float64) aligned for max_order <= 2.
+struct FieldK {
+    int32_t nsectors, n_spoly, n_spolyp, n_seg, max_order, npad;
+    double B0, k, km1, B0k;       // B0, k, k - 1, B0 * k
+    double period;                // 2 pi / nsectors
+    double spoly[FFA_MAX_POLY];
+    double spolyp[FFA_MAX_POLY];
+    double seg_x0[FFA_MAX_SEG], seg_x1[FFA_MAX_SEG];
+    double seg_k[FFA_MAX_SEG];    // 16 / W0
+    double seg_y[FFA_MAX_SEG];    // y02 * |y01|
+    double r_min, r_step, fi_min, fi_step;
+    int64_t r_size, fi_size;
+    const double *nodes64;
+    const float *nodes32;
+};
+
+struct RFK {
+    int32_t enable, ngaps, physical_sum, pad0;
+    double poly_x[FFA_MAX_GAPS][4];
+    double poly_y[FFA_MAX_GAPS][4];
+    double box[FFA_MAX_GAPS][4];
+    double theta_n[FFA_MAX_GAPS];
+    double rf_shift[FFA_MAX_GAPS];
+};
+
+struct PushK {
+    FieldK f;
+    RFK rf;
+    ffa_aperture ap;
+    ffa_consts cs;
+    ffa_state_soa st;
+    const double *drf;
+    const double *acc;
+    int64_t n, step0;
+    int32_t nsteps, sc_step;
+    double dt;
+    int64_t *status;
+};
+
+}  // namespace ffa
+
+struct ffa_fieldmap {
+    ffa::FieldK k;
+    double *nodes64;
+    float *nodes32;
+};
+
+// Launchers implemented in ffa_push.cu
+namespace ffa {
+cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s);
+cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s);
+cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s);
+cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, float *n32, cudaStream_t s);
+}  // namespace ffa

@@ -1,0 +1,335 @@
+"""The tracking loop on the GPU.
+
+FFAG_RungeKutta mirrors the reference's integrator object
+(src/FFAG_track.py:31-1049): the two bunch-tracking loops
+rk4_solve_dt_bunch3_withSC_boris / rk4_solve_dt_bunch3_withSC keep their
+signatures and per-step semantics (injection, space-charge cadence and
+extrapolation, push, dumps, the stop test every 1000 steps), and Boris_solve /
+rk4_step_malloc are kept as drop-in single-step calls on an N x 16 matrix.
+
+Design: everything that depends only on the step index (the time sequence
+t_{s+1} = t_s + dt, the RF frequency/voltage per step, each particle's
+injection step, the dump steps) is computed on the host once per chunk of
+steps, so one fused kernel launch can advance the bunch through every step
+up to the next event (space-charge update, dump, stop test).
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .bunch import FFAG_Bunch
+from .constants import FFAG_ConversionTools, FFAG_GlobalParameters
+
+TABLE_CHUNK = 1 << 16
+
+
+class StepClock:
+    """Times and per-step RF scalars for absolute steps [0, n), extended in
+    chunks.  t[s] is the start time of step s, built by the same repeated
+    float64 addition as the reference loop (t_PreStep = t_PreStep + step_t)."""
+
+    def __init__(self, t_start: float, dt: float, emap, solver: str, device):
+        self.t0 = float(t_start)
+        self.dt = float(dt)
+        self.emap = emap
+        self.solver = solver
+        self.device = device
+        self.t = np.array([self.t0], dtype=np.float64)  # t[0..n]
+        self.n = 0
+        self.drf = None
+        self.acc = None
+
+    def ensure(self, nsteps: int) -> bool:
+        """Makes tables cover steps [0, nsteps).  Returns True if extended."""
+        if nsteps <= self.n:
+            return False
+        new_n = max(nsteps, self.n + TABLE_CHUNK)
+        add = new_n - self.n
+        ext = np.empty(add + 1, dtype=np.float64)
+        ext[0] = self.t[-1]
+        ext[1:] = self.dt
+        ts = np.add.accumulate(ext)  # sequential sums: t_{s+1} = t_s + dt
+        self.t = np.concatenate([self.t, ts[1:]])
+        self.n = new_n
+        self._build_tables()
+        return True
+
+    def _build_tables(self):
+        import torch
+        em = self.emap
+        tp = self.t[: self.n]
+        if self.solver == "Boris":
+            f, v = em.Interpolation1D_freq_curve(tp)
+            drf = f * np.pi * 2 * self.dt
+            acc = em.acc_Etot_uniform * v
+        else:
+            h = self.dt
+            ts = np.stack([tp, tp + 0.5 * h, tp + 0.5 * h, tp + h], axis=1).reshape(-1)
+            f, v = em.Interpolation1D_freq_curve(ts)
+            drf = f * np.pi * 2
+            acc = em.acc_Etot_uniform * v
+        self.drf = torch.from_numpy(np.ascontiguousarray(drf)).to(self.device)
+        self.acc = torch.from_numpy(np.ascontiguousarray(acc)).to(self.device)
+        self.table = _lib.StepTable()
+        self.table.drf = self.drf.data_ptr()
+        self.table.acc = self.acc.data_ptr()
+        self.table.nsteps = self.n
+
+    def windows(self, s0: int, s1: int):
+        """Injection windows [(t - dt) * 1e9, t * 1e9] of steps s0..s1-1."""
+        t = self.t[s0:s1]
+        return (t - self.dt) * 1e9, t * 1e9
+
+
+def _aperture(gp) -> "_lib.Aperture":
+    ap = _lib.Aperture()
+    if getattr(gp, "Aperture_enable", False) and gp.Aperture_m is not None:
+        ap.enable = 1
+        ap.rmin, ap.rmax, ap.zmin, ap.zmax = (float(x) for x in gp.Aperture_m)
+    return ap
+
+
+def _consts(gp) -> "_lib.Consts":
+    cs = _lib.Consts()
+    cs.q, cs.c, cs.m0, cs.E0 = float(gp.q), float(gp.c), float(gp.m0), float(gp.E0)
+    return cs
+
+
+class Pusher:
+    """Binds a bunch to the field / RF / aperture descriptors and launches
+    fused push kernels."""
+
+    def __init__(self, bunch: FFAG_Bunch, gp, solver: str, precision: str = "fp64"):
+        import torch
+        self.bunch = bunch
+        self.gp = gp
+        self.solver = solver
+        self.fm = gp.Bmap.device_map(bunch.device)
+        self.rf = gp.Emap.rf_desc()
+        self.ap = _aperture(gp)
+        self.cs = _consts(gp)
+        bh = getattr(gp, "BHarmonics", None)
+        if bh is not None and getattr(bh, "enable_flag", False) and getattr(bh, "Nharm", 0) > 0:
+            raise NotImplementedError("field-error harmonics are not supported by the GPU pushers")
+        self.flags = _lib.FFA_RK4 if solver == "RK4" else _lib.FFA_BORIS
+        if precision == "fp32c":
+            if solver == "RK4":
+                raise NotImplementedError("the compensated float32 pusher is Boris-only")
+            self.flags |= _lib.FFA_FP32C
+        if getattr(gp.Emap, "physical_sum", False):
+            self.flags |= _lib.FFA_RF_PHYSICAL_SUM
+        self.stream = torch.cuda.current_stream(bunch.device)
+
+    def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0) -> None:
+        L = _lib.lib()
+        b = self.bunch
+        rc = L.ffa_push(self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
+                        ctypes.byref(clock.table), ctypes.byref(b.soa()), b.n, step0, nsteps, clock.dt,
+                        sc_step, self.flags, self.stream.cuda_stream, b.status.data_ptr())
+        _lib.check(rc, "ffa_push")
+
+
+class StepDumpSchedule:
+    """Steps at which a StepDumpBunch fires: start < t_post < end and the
+    interval index floor((t - start) / interval) changes between t_pre and
+    t_post (StepDumpBunch.check_and_dump, src/FFAG_dump.py:330-356)."""
+
+    def __init__(self, dump):
+        self.dump = dump
+
+    def steps_in(self, t_pre: np.ndarray, t_post: np.ndarray) -> np.ndarray:
+        d = self.dump
+        inside = (d.start_time < t_post) & (t_post < d.end_time)
+        a = np.floor_divide(t_pre - d.start_time, d.time_interval)
+        b = np.floor_divide(t_post - d.start_time, d.time_interval)
+        return np.nonzero(inside & (a != b))[0]
+
+
+class FFAG_RungeKutta:
+    """Bunch trackers (src/FFAG_track.py:31-1049)."""
+
+    def __init__(self, precision: str = "fp64", verbose: bool = True):
+        self.running = True
+        self.precision = precision
+        self.verbose = verbose
+        self.last_run = {}
+
+    # ------------------------------------------------ drop-in single steps
+    def Boris_solve(self, t, mat_in, dt, *scratch, GlobalParameters=None):
+        """One Boris step of the N x 16 Boris v-format matrix `mat_in`, in
+        place (src/FFAG_track.py:948-1049).  The reference's 25 scratch
+        arrays are accepted and ignored; GlobalParameters may be passed
+        positionally last, as the reference does."""
+        if GlobalParameters is None:
+            GlobalParameters = scratch[-1]
+        out = single_step(mat_in, float(t), float(dt), GlobalParameters, "Boris", self.precision)
+        mat_in[...] = out
+        return mat_in
+
+    def rk4_step_malloc(self, func, t, r, h, GlobalParameters, *scratch):
+        """One RK4 step of the N x 16 RK4 v-format matrix; returns the
+        increment like the reference (src/FFAG_track.py:51-61), plus the
+        three field arrays it returned (not computed here: None)."""
+        new = single_step(r, float(t), float(h), GlobalParameters, "RK4", "fp64")
+        return new - np.asarray(r), None, None, None
+
+    # ---------------------------------------------------------- the loops
+    def rk4_solve_dt_bunch3_withSC_boris(self, func, t_start, BunchObj, GlobalParameters, LocalParameters):
+        return self._solve("Boris", t_start, BunchObj, GlobalParameters, LocalParameters)
+
+    def rk4_solve_dt_bunch3_withSC(self, func, t_start, BunchObj, GlobalParameters, LocalParameters):
+        return self._solve("RK4", t_start, BunchObj, GlobalParameters, LocalParameters)
+
+    def _solve(self, solver, t_start, b: FFAG_Bunch, gp, lp):
+        import torch
+        stop = lp["stop_condition"]
+        dt = float(lp["time_step"])
+        enable_sc = bool(lp.get("enable_SC", False))
+        sc_type = lp.get("SC_type", 1)
+        SC_step = int(lp.get("SC_step", 1))
+        dumps = lp.get("step_dumps")
+        comm = lp.get("comm")
+        max_stepsN = int(stop["max_stepsN"])
+        max_fi = stop["max_turn"] * np.pi * 2
+        max_time = stop["max_time"]
+        if b.BunchType != solver:
+            raise ValueError(f"bunch type {b.BunchType} does not match the {solver} solver")
+        if enable_sc and sc_type != 1:
+            raise NotImplementedError("only the 2.5D slice-by-slice space charge (SC_type 1) is built")
+
+        pusher = Pusher(b, gp, solver, self.precision)
+        clock = StepClock(t_start, dt, gp.Emap, solver, b.device)
+        sc = None
+        if enable_sc:
+            from .space_charge import SpaceCharge
+            sc = SpaceCharge(b, hockney=bool(lp.get("SC_hockney", False)))
+        dump_sched = [StepDumpSchedule(d) for d in (dumps.step_dumps() if dumps is not None else [])]
+        if self.precision == "fp32c":
+            _lib.check(_lib.lib().ffa_fp32c_split(ctypes.byref(b.soa()), b.n, pusher.stream.cuda_stream),
+                       "ffa_fp32c_split")
+
+        steps_i = 0
+        sched_end = 0
+        fi_sum = torch.zeros(1, dtype=torch.float64, device=b.device)
+        fi_cnt = torch.zeros(1, dtype=torch.int64, device=b.device)
+        t_wall = time.time()
+        n_launch = 0
+        b.reset_schedule_count()
+        while steps_i < max_stepsN:
+            if clock.ensure(steps_i + 1) or steps_i >= sched_end:
+                clock.ensure(steps_i + 1)
+                lo, hi = clock.windows(steps_i, clock.n)
+                b.set_injection_schedule(lo, hi, steps_i)
+                b.reset_schedule_count()
+                sched_end = clock.n
+            # the next event bounds the fused chunk
+            end = min(max_stepsN, (steps_i // 1000 + 1) * 1000, sched_end)
+            if enable_sc:
+                if steps_i % SC_step == 0:
+                    _lib.check(_lib.lib().ffa_inject(ctypes.byref(b.soa()), b.n, steps_i, pusher.stream.cuda_stream),
+                               "ffa_inject")
+                    sc.update(first=(steps_i == 0))
+                end = min(end, (steps_i // SC_step + 1) * SC_step)
+            dump_at = None
+            for ds in dump_sched:
+                hit = ds.steps_in(clock.t[steps_i:end], clock.t[steps_i + 1:end + 1])
+                if hit.size:
+                    cand = steps_i + int(hit[0])
+                    dump_at = cand if dump_at is None else min(dump_at, cand)
+            if dump_at is not None:
+                end = dump_at + 1
+            pusher.push(clock, steps_i, end - steps_i, SC_step if enable_sc else 0)
+            n_launch += 1
+            steps_i = end
+            if dump_at is not None:
+                t_post = clock.t[steps_i]
+                t_pre = clock.t[steps_i - 1]
+                for ds in dump_sched:
+                    if ds.steps_in(np.array([t_pre]), np.array([t_post])).size:
+                        ds.dump.dump_bunch(b, t_post, data_type=solver)
+            if steps_i % 1000 == 0:
+                b.UpdateParticleNumGlobal(comm)
+                _lib.check(_lib.lib().ffa_mean_fi(ctypes.byref(b.soa()), b.n, fi_sum.data_ptr(), fi_cnt.data_ptr(),
+                                                  pusher.stream.cuda_stream), "ffa_mean_fi")
+                s, c = float(fi_sum.item()), int(fi_cnt.item())
+                if comm is not None:
+                    v = torch.tensor([s, float(c)], dtype=torch.float64)
+                    comm.all_reduce(v)
+                    s, c = float(v[0]), int(v[1])
+                mean_fi = s / c if c > 0 else float("nan")
+                t_now = clock.t[steps_i]
+                if self.verbose and (comm is None or comm.get_rank() == 0):
+                    print(f"current step={steps_i:.0f}, turn ~= {mean_fi / np.pi / 2:.2f}, "
+                          f"remain particles: {b.SurvivedNum}. tracking time: {t_now * 1e6:.2f} us, "
+                          f"clock: {time.strftime('%m-%d %H:%M:%S', time.localtime())}", flush=True)
+                if abs(mean_fi) > max_fi:
+                    break
+                if t_now > max_time:
+                    break
+        if self.precision == "fp32c":
+            _lib.check(_lib.lib().ffa_fp32c_merge(ctypes.byref(b.soa()), b.n, pusher.stream.cuda_stream),
+                       "ffa_fp32c_merge")
+        torch.cuda.synchronize(b.device)
+        self.last_run = {"steps": steps_i, "t_end": float(clock.t[steps_i]), "launches": n_launch,
+                         "wall_s": time.time() - t_wall, "status": b.status_counts()}
+        return 0
+
+
+def single_step(mat, t, dt, gp, solver, precision="fp64"):
+    """Advances an N x 16 v-format matrix by one step on the GPU and returns
+    the new matrix (cols 6, 13-15 copied through)."""
+    import torch
+    a = np.ascontiguousarray(np.asarray(mat, dtype=np.float64))
+    n = a.shape[0]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    b = _EphemeralBunch(a, solver, dev)
+    clock = StepClock(t, dt, gp.Emap, solver, dev)
+    clock.ensure(1)
+    pusher = Pusher(b, gp, solver, precision)
+    if precision == "fp32c":
+        _lib.check(_lib.lib().ffa_fp32c_split(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_split")
+    pusher.push(clock, 0, 1, 0)
+    if precision == "fp32c":
+        _lib.check(_lib.lib().ffa_fp32c_merge(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_merge")
+    out = b.matrix()
+    return out
+
+
+class _EphemeralBunch:
+    """Device SoA for one N x 16 matrix without the injection bookkeeping
+    (the reference's Boris_solve takes the flags as they are)."""
+
+    def __init__(self, a, solver, dev):
+        import torch
+        self.BunchType = solver
+        self.device = dev
+        self.n = a.shape[0]
+        self._a = a
+        self.aos = torch.from_numpy(a).to(dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.cols = {k: torch.empty(self.n, **f64) for k in ("r", "vr", "z", "vz", "fi", "f5", "rf",
+                                                             "esc_r", "esc_z", "esc_fi")}
+        self.cols["inj"] = torch.empty(self.n, dtype=torch.uint8, device=dev)
+        self.cols["surv"] = torch.empty(self.n, dtype=torch.uint8, device=dev)
+        self.cols["r_lo"] = torch.zeros(self.n, dtype=torch.float32, device=dev)
+        self.cols["fi_lo"] = torch.zeros(self.n, dtype=torch.float32, device=dev)
+        self.status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int64, device=dev)
+        s = _lib.StateSoA()
+        for name, _ in _lib.StateSoA._fields_:
+            t = self.cols.get(name)
+            setattr(s, name, t.data_ptr() if t is not None else None)
+        self._soa = s
+        _lib.check(_lib.lib().ffa_aos_to_soa(self.aos.data_ptr(), self.n, ctypes.byref(s), _lib.stream_ptr(None)),
+                   "ffa_aos_to_soa")
+
+    def soa(self):
+        return self._soa
+
+    def matrix(self):
+        _lib.check(_lib.lib().ffa_soa_to_aos(ctypes.byref(self._soa), self.n, self.aos.data_ptr(), _lib.stream_ptr(None)),
+                   "ffa_soa_to_aos")
+        return self.aos.cpu().numpy()

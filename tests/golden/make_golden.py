@@ -1,0 +1,221 @@
+"""Generates the golden vectors in tests/golden/ by running the reference
+tracker (PyFFA, pure Python + Numba) on seeded synthetic inputs.
+
+Run in the development container, where the reference source is available:
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+The reference imports mpi4py, pyfftw and matplotlib, which are not
+installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
+stand-ins (so the space-charge transforms here are numpy's complex64 FFT,
+not FFTW).  The fixtures store every input (lattice JSON, z-Taylor stacks,
+RF file text, closed-orbit tables, particle matrices) next to the
+reference's outputs, so the tests need neither the reference nor this
+script.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from pyffa_b200 import synthetic  # noqa: E402
+
+# Coarse map band around the 300 MeV closed orbit so the fixture stays small:
+# r 8.0..8.5 m in 5 mm steps, theta step 0.1 deg
+GOLD_R = (8.0, 8.5, 0.005)
+GOLD_THETA_DEG = 0.1
+MAX_ORDER = 2
+
+
+def build_inputs(tmp):
+    bmap_dir = os.path.join(tmp, "bmap")
+    cfg_path = synthetic.write_bmap_folder(bmap_dir, MAX_ORDER, r_range=GOLD_R, theta_step_deg=GOLD_THETA_DEG)
+    emap_path = synthetic.emap_file(os.path.join(tmp, "emap.txt"), gap_azimuth_deg=(1.0, 4.0),
+                                    rf_shift_deg=(0.0, 10.0), voltage=100e3, gap_width=0.2,
+                                    E_range=(7.9, 8.6), acc_phi_deg=30.0, ramp_turns=20, npts=201)
+    return cfg_path, emap_path
+
+
+def ref_objects(cfg_path, emap_path, aperture, enable_rf=True):
+    from FFAG_ParasAndConversion import FFAG_GlobalParameters
+    from FFAG_Field import FFAG_Bfield_analytical, FFAG_EField_new, FFAG_BField_Error
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(FFAG_Bfield_analytical(cfg_path, MAX_ORDER))
+    gp.AddEMap(FFAG_EField_new(emap_path, enable_rf))
+    gp.AddBHarmonics(FFAG_BField_Error([], False))
+    if aperture is not None:
+        gp.AddAperture(*aperture)
+    return gp
+
+
+def p_bunch(n, seed, inj_spread_ns=0.0, dt=None):
+    a = synthetic.centred_bunch(n, seed=seed, sig_x=4e-3, sig_xp=2e-3, sig_z=3e-3, sig_zp=2e-3, sig_delta=2e-3)
+    rng = np.random.Generator(np.random.PCG64(seed + 1000))
+    if inj_spread_ns > 0:
+        a[:, 6] = np.sort(rng.uniform(0.0, inj_spread_ns, n))
+    return a
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(args.ref, "src"))
+    import FFAG_track
+    from FFAG_Bunch import FFAG_Bunch
+    from FFAG_dump import Dumps
+    from FFAG_MathTools import RK4_Post_Step_njit
+    from FFAG_ParasAndConversion import FFAG_ConversionTools
+
+    conv = FFAG_ConversionTools()
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg_path, emap_path = build_inputs(tmp)
+        with open(cfg_path) as f:
+            cfg_text = f.read()
+        with open(emap_path) as f:
+            emap_text = f.read()
+        stacks = {}
+        for comp in ("Bz", "Bfi", "Br"):
+            stacks[comp] = np.stack([np.load(os.path.join(os.path.dirname(cfg_path), f"{comp}_order_{n}.npz"))
+                                     [f"{comp}_Taylor_coeff"] for n in range(MAX_ORDER + 1)])
+        aperture = (8.02, 8.48, -0.006, 0.006)
+        dt = synthetic.design_dt(300.0, 720)
+        t0 = 1.0e-9
+
+        # ---- A: single Boris_solve step (all injected; a few outside the aperture; a few not injected)
+        gp = ref_objects(cfg_path, emap_path, aperture)
+        pa = p_bunch(64, seed=11)
+        pa[:4, 0] = [7.99, 8.015, 8.485, 8.51]             # outside the aperture / map edge
+        pa[4:8, 4] = np.deg2rad([0.95, 1.0, 1.05, 4.0])    # inside the RF gaps
+        va = conv.ConvertPrzek2Vrzek_boris(pa)
+        va[:, 9] = 0.3
+        va[:, 7] = 1.0
+        va[:, 8] = 1.0
+        va[60:, 7] = 0.0
+        va[60:, 8] = 0.0
+        va[8:12, 10:13] = [[1e4, -2e4, 3e3]] * 4            # space-charge field columns
+        bunch = FFAG_Bunch(va.copy(), BunchType="Boris")
+        rk = FFAG_track.FFAG_RungeKutta()
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        rk.Boris_solve(t0, m, dt,
+                       bunch.Malloc_x_cart, bunch.Malloc_y_cart, bunch.Malloc_z_cart,
+                       bunch.Malloc_vx_cart, bunch.Malloc_vy_cart, bunch.Malloc_vz_cart,
+                       bunch.Malloc_Ex_cart, bunch.Malloc_Ey_cart, bunch.Malloc_Ez_cart,
+                       bunch.Malloc_Bx_cart, bunch.Malloc_By_cart, bunch.Malloc_Bz_cart,
+                       bunch.Malloc_RF_phase, bunch.Malloc_mod_fi,
+                       bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+                       bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+                       bunch.Step_SurviveFlag, bunch.Malloc_RF_shift,
+                       bunch.SurvivedNum_Local, bunch.LostNum_Local, gp)
+        out["boris1_in"] = m_in
+        out["boris1_out"] = m.copy()
+        out["boris1_t"] = np.array([t0, dt])
+
+        # ---- B: single RK4 step
+        vr = conv.ConvertPrzek2Vrzek(pa)
+        vr[:, 9] = 0.3
+        vr[:, 7] = 1.0
+        vr[:, 8] = 1.0
+        vr[60:, 7] = 0.0
+        vr[60:, 8] = 0.0
+        vr[8:12, 10:13] = [[1e4, -2e4, 3e3]] * 4
+        bunch = FFAG_Bunch(vr.copy(), BunchType="RK4")
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        dr, _, _, _ = rk.rk4_step_malloc(FFAG_track.FunctionForAccelerationBunch_dt, t0, m, dt, gp,
+                                         bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+                                         bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+                                         bunch.Malloc_mod_fi, bunch.Malloc_RF_shift, bunch.Malloc_RK_dxdt,
+                                         bunch.SurvivedNum_Local, bunch.LostNum_Local)
+        RK4_Post_Step_njit(m, dr)
+        out["rk41_in"] = m_in
+        out["rk41_out"] = m.copy()
+
+        # ---- C: tracking loops with injection spread over the first steps (no SC)
+        def loop(solver, nsteps, p, sc=None):
+            gp_l = ref_objects(cfg_path, emap_path, aperture)
+            v = conv.ConvertPrzek2Vrzek_boris(p) if solver == "Boris" else conv.ConvertPrzek2Vrzek(p)
+            v[:, 9] = 0.3
+            v[:, 15] = np.arange(v.shape[0])
+            grid = (8, 32, 32, 6.0) if sc else (64, 128, 128, 12.0)
+            b = FFAG_Bunch(v.copy(), marcosize=sc["marcosize"] if sc else 1, sc_grid_size=grid, BunchType=solver)
+            if sc:
+                b.SEO_fi_axis, b.SEO_Ek_axis = sc["seo"]["fi_axis"], sc["seo"]["Ek_axis"]
+                b.SEO_r_matrix, b.SEO_pr_matrix = sc["seo"]["r"], sc["seo"]["pr"]
+                b.SEO_perimeter = sc["seo"]["perimeter"]
+            lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9},
+                  "time_step": dt, "enable_SC": bool(sc), "SC_type": 1, "SC_step": sc["step"] if sc else 20,
+                  "step_dumps": Dumps()}
+            v_in = b.LocalBunch.copy()
+            t_start = -0.5 * dt
+            if solver == "Boris":
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC_boris(None, t_start, b, gp_l, lp)
+            else:
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC(FFAG_track.FunctionForAccelerationBunch_dt,
+                                                                       t_start, b, gp_l, lp)
+            return v_in, b.LocalBunch.copy(), t_start
+
+        pl = p_bunch(64, seed=23, inj_spread_ns=4 * dt * 1e9)
+        vin, vout, ts = loop("Boris", 240, pl)
+        out["borisloop_in"], out["borisloop_out"], out["borisloop_t"] = vin, vout, np.array([ts, dt, 240])
+        vin, vout, ts = loop("RK4", 120, pl)
+        out["rk4loop_in"], out["rk4loop_out"], out["rk4loop_t"] = vin, vout, np.array([ts, dt, 120])
+
+        # ---- D: space charge: one update through Build_2_5D_SliceGrid_sbs, and a short loop with SC
+        from pyffa_b200 import orbit
+        seo = orbit.seo_tables(synthetic.lattice_bmap(), np.linspace(290.0, 310.0, 5), nfi=181)
+        seo = {k: seo[k] for k in ("Ek_axis", "fi_axis", "r", "pr", "perimeter")}
+        ps = synthetic.centred_bunch(3000, seed=5, kind="kv", a_x=3e-3, a_z=2e-3, sig_t=3e-9, fi0=0.3)
+        vs = conv.ConvertPrzek2Vrzek_boris(ps)
+        vs[:, 7] = 1.0
+        vs[:, 8] = 1.0
+        vs[:7, 8] = 0.0  # a few lost particles stay out of the deposit
+        b = FFAG_Bunch(vs.copy(), marcosize=1e13 / 3000, sc_grid_size=(8, 32, 32, 6.0), BunchType="Boris")
+        b.SEO_fi_axis, b.SEO_Ek_axis, b.SEO_r_matrix = seo["fi_axis"], seo["Ek_axis"], seo["r"]
+        b.SEO_pr_matrix, b.SEO_perimeter = seo["pr"] + 0.01, seo["perimeter"]
+        b.Step_SurviveFlag[:] = b.LocalBunch[:, 8] != 0
+        sc_in = b.LocalBunch.copy()
+        import pyfftw
+        a_buf = pyfftw.empty_aligned((32, 32), dtype="complex64")
+        b_buf = pyfftw.empty_aligned((32, 32), dtype="complex64")
+        fwd = pyfftw.FFTW(a_buf, b_buf, axes=(0, 1), direction="FFTW_FORWARD")
+        inv = pyfftw.FFTW(b_buf, a_buf, axes=(0, 1), direction="FFTW_BACKWARD")
+        res = b.Build_2_5D_SliceGrid_sbs(fwd, inv)
+        (rho, phi, ex, ez, xmin, xmax, zmin, zmax, BL, _, _, _, _, _, cx, cr0, _, fi_grid) = res
+        out["sc_in"] = sc_in
+        out["sc_out"] = b.LocalBunch.copy()
+        out["sc_rho"], out["sc_phi"], out["sc_ex"], out["sc_ez"] = rho, phi, ex, ez
+        out["sc_box"] = np.array([xmin, xmax, zmin, zmax, BL, fi_grid[0], fi_grid[-1]])
+        out["sc_params"] = np.array([8, 32, 32, 6.0, 1e13 / 3000 * 1.60217662e-19])
+        out["sc_slice_indices"] = b.Malloc_SC_slice_indices[: int((sc_in[:, 8] != 0).sum())].copy()
+        out["seo_pr_offset"] = np.array([0.01])
+        for k, v in seo.items():
+            out["seo_" + k] = v
+
+        psl = synthetic.centred_bunch(1500, seed=9, kind="kv", a_x=3e-3, a_z=2e-3, sig_t=3e-9, fi0=0.0)
+        vin, vout, ts = loop("Boris", 12, psl, sc={"seo": seo, "step": 5, "marcosize": 1e13 / 1500})
+        out["scloop_in"], out["scloop_out"], out["scloop_t"] = vin, vout, np.array([ts, dt, 12, 5, 1e13 / 1500])
+
+        out["cfg_json"] = np.frombuffer(cfg_text.encode(), dtype=np.uint8)
+        out["emap_text"] = np.frombuffer(emap_text.encode(), dtype=np.uint8)
+        for comp in ("Bz", "Bfi", "Br"):
+            out[f"stack_{comp}"] = stacks[comp][1:]  # order 0 is never read
+        out["aperture"] = np.array(aperture)
+    path = os.path.join(HERE, "golden_tracking.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()
