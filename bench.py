@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark of the tracking hot path: particle-turns/s on one B200.
+
+Workload (the multiparticle configuration the metric is quoted on):
+12-sector scaling FFAG, proton 300 MeV, full 1301 x 6000 mid-plane map with
+z-Taylor order 2 (z^4 in Bz, z^5 in Br/Bfi), two RF gaps at 100 kV
+(reference semantics: the last gap's field wins), 1e5-particle seeded 6D
+Gaussian on the closed orbit, 720 steps per turn, relativistic Boris in
+float64.  One benchmark step = one turn = 720 fused push steps over the
+whole bunch, inputs resident in HBM; L2 is flushed between timed steps.
+
+`--impl reference` times the reference's algorithm on the host cores (the
+C restatement in oracle/, all threads) on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+N_PARTICLES = 100_000
+STEPS_PER_TURN = 720
+MAX_ORDER = 2
+# float64 operations per particle-step of the Boris kernel (2 per DFMA,
+# 1 per DADD / DMUL), counted from the kernel's executed instruction mix by
+# ncu on this workload (profiles/boris_f64_c1_1e5.md)
+FP64_FLOP_PER_PARTICLE_STEP = None
+# algorithmic HBM bytes per particle per launch: SoA state read
+# (10 float64 + 2 flag bytes + int32 injection step) and written (10 float64 + 2 bytes)
+STATE_BYTES_PER_PARTICLE = (10 * 8 + 2 + 4) + (10 * 8 + 2)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--n", type=int, default=N_PARTICLES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(seed=7, n=N_PARTICLES):
+    import warnings
+    warnings.simplefilter("ignore")
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools, FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical, FFAG_EField_new
+    cfg = synthetic.lattice_bmap()
+    bm = FFAG_Bfield_analytical(config=cfg, max_order=MAX_ORDER, stacks=synthetic.taylor_stacks(cfg, MAX_ORDER))
+    em = FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=True)
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(bm)
+    gp.AddEMap(em)
+    gp.AddAperture(7.5, 9.5, -0.1, 0.1)
+    p = synthetic.centred_bunch(n, seed=seed)
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(p)
+    v[:, 7] = 1.0
+    v[:, 8] = 1.0
+    dt = synthetic.design_dt(300.0, STEPS_PER_TURN)
+    return gp, v, dt
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(dev_index):
+    """FP64 FMA pipe peak measured live with the probe kernel."""
+    import ctypes
+    import torch
+    from pyffa_b200 import build
+    L = ctypes.CDLL(build.build_probe())
+    L.ffa_probe_fp64_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_float)]
+    sms = torch.cuda.get_device_properties(dev_index).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    out = torch.zeros(blocks, dtype=torch.float64, device="cuda")
+    ms = ctypes.c_float()
+    best = 0.0
+    for _ in range(3):
+        L.ffa_probe_fp64_fma(blocks, iters, ctypes.c_void_p(out.data_ptr()),
+                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), ctypes.byref(ms))
+        flops = 2.0 * 8 * iters * blocks * 256
+        best = max(best, flops / (ms.value * 1e-3) / 1e12)
+    return best
+
+
+def cpu_baseline(gp, v, dt, sample_n=20_000, steps=STEPS_PER_TURN):
+    """The reference algorithm on the host cores (oracle port, all threads):
+    particle-turns/s on a bounded sample of the workload."""
+    from oracle import oracle as O
+    O.build()
+    S = O.Setup(gp.Bmap, gp.Emap, gp)
+    m = np.ascontiguousarray(v[:sample_n].copy())
+    O.boris_step(S, m[:64].copy(), 0.0, dt)  # warm the library
+    t0 = time.perf_counter()
+    O.track(S, "Boris", m, 0.0, dt, steps)
+    el = time.perf_counter() - t0
+    return {"value": sample_n * steps / STEPS_PER_TURN / el, "unit": "particle-turns/s", "cores": O.num_threads(),
+            "kind": "port", "sample": f"{sample_n} particles x {steps} Boris steps (one turn) of the same workload",
+            "seconds": el}
+
+
+def run_reference(args):
+    """--impl reference: the oracle port on the host cores, each step one turn
+    of a bounded sample."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    gp, v, dt = workload(n=args.n)
+    from oracle import oracle as O
+    O.build()
+    S = O.Setup(gp.Bmap, gp.Emap, gp)
+    sample_n = 10_000
+    times = []
+    for k in range(args.warmup + args.steps):
+        m = np.ascontiguousarray(v[:sample_n].copy())
+        t0 = time.perf_counter()
+        O.track(S, "Boris", m, 0.0, dt, STEPS_PER_TURN)
+        el = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(el)
+    tot = sum(times)
+    val = sample_n * len(times) / tot
+    line = {"metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
+            "value": val, "unit": "particle-turns/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": "c1: 12-sector FFAG, 300 MeV, 1301x6000 map, "
+                                                                 "2 RF gaps, Boris fp64, 720 steps/turn",
+                                                     "sample_particles": sample_n},
+            "cpu_baseline": {"value": val, "unit": "particle-turns/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{sample_n} particles x one turn per step"},
+            "e2e": {"value": val, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from pyffa_b200 import _lib
+    from pyffa_b200.track import MatrixTracker, Pusher, StepClock, _EphemeralBunch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    gp, v, dt = workload(seed=7 + rank, n=args.n)
+    n = v.shape[0]
+    total_steps = STEPS_PER_TURN * (args.warmup + args.steps + 1)
+    b = _EphemeralBunch(v, "Boris", dev)
+    pusher = Pusher(b, gp, "Boris", args.precision)
+    clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
+    clock.ensure(total_steps)
+    L = _lib.lib()
+    import ctypes
+    if args.precision == "fp32c":
+        _lib.check(L.ffa_fp32c_split(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_split")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = pusher.stream
+
+    def one_turn(k):
+        pusher.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+
+    for k in range(args.warmup):
+        one_turn(k)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as cs:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (not timed)
+            ev[k][0].record(stream)
+            one_turn(args.warmup + k)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    launch_ms = [a.elapsed_time(bb) for a, bb in ev]
+    t_ms = sum(launch_ms)
+    t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    status = b.status.cpu().numpy()
+    value = n * world * args.steps / (t_ms * 1e-3)
+    clocks = cs.summary()
+
+    # end to end through the host-buffer API: host matrix in, one turn, host matrix out
+    e2e = None
+    if not args.no_e2e:
+        mt = MatrixTracker(n, gp, "Boris", args.precision, device=dev)
+        mt.bind_clock(0.0, dt, total_steps)
+        h_in = torch.from_numpy(v.copy()).pin_memory()
+        h_out = torch.empty_like(h_in).pin_memory()
+        for k in range(args.warmup):
+            mt.run(h_in, h_out, k * STEPS_PER_TURN, STEPS_PER_TURN)
+            mt.pusher.stream.synchronize()
+            h_in.copy_(h_out)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(mt.pusher.stream)
+        for k in range(args.steps):
+            mt.run(h_in, h_out, (args.warmup + k) * STEPS_PER_TURN, STEPS_PER_TURN)
+            mt.pusher.stream.synchronize()
+            h_in.copy_(h_out)
+        e1.record(mt.pusher.stream)
+        torch.cuda.synchronize()
+        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": n * world * args.steps / (float(te.item()) * 1e-3), "unit": "particle-turns/s",
+               "h2d_bytes_per_step": int(n * 16 * 8), "d2h_bytes_per_step": int(n * 16 * 8)}
+
+    if rank == 0:
+        peak64 = fp64_peak_tflops(local)
+        avg_launch_s = (t_ms / args.steps) * 1e-3
+        pstep = n * STEPS_PER_TURN
+        roof = {"bound": "fp64", "unit": "TFLOP/s", "peak": peak64,
+                "peak_source": "measured live: float64 FMA probe kernel (libffa_probe.so)"}
+        if FP64_FLOP_PER_PARTICLE_STEP:
+            ach = FP64_FLOP_PER_PARTICLE_STEP * pstep / avg_launch_s / 1e12
+            roof.update({"achieved": ach, "frac": ach / peak64,
+                         "flop_per_particle_step": FP64_FLOP_PER_PARTICLE_STEP})
+        else:
+            roof.update({"achieved": None, "frac": None})
+        hbm_peak = None
+        try:
+            hbm_peak = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        except Exception:
+            hbm_peak = 6650.0
+        hbm_ach = STATE_BYTES_PER_PARTICLE * n / avg_launch_s / 1e9
+        roof["hbm"] = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+                       "frac": hbm_ach / hbm_peak, "algorithmic_bytes_per_launch": STATE_BYTES_PER_PARTICLE * n,
+                       "traffic": None}
+        roof["traffic"] = None
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(gp, v, dt)
+        line = {
+            "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
+            "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32c",
+            "data": "synthetic (seeded 6D Gaussian bunch, analytic lattice)",
+            "config": {"workload": "c1: 12-sector FFAG, 300 MeV, 1301x6000 map z-Taylor order 2, 2 RF gaps "
+                                   "(last-gap semantics), Boris, 720 steps/turn, 1 turn per step",
+                       "particles_per_gpu": n, "steps_per_turn": STEPS_PER_TURN, "precision": args.precision,
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "status": {"lost": int(status[0]), "nan": int(status[1]), "out_of_map": int(status[2])},
+            "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -59,5 +59,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB_PATH
 
 
+PROBE_PATH = os.path.join(PKG_DIR, "libffa_probe.so")
+
+
+def build_probe(force: bool = False) -> str:
+    """The benchmark's FP64 peak probe (csrc/probe/ffa_probe.cu)."""
+    src = os.path.join(CSRC, "probe", "ffa_probe.cu")
+    if not force and os.path.exists(PROBE_PATH) and os.path.getmtime(PROBE_PATH) >= os.path.getmtime(src):
+        return PROBE_PATH
+    cmd = [nvcc_path(), *ARCH_FLAGS, "-O3", "-Xcompiler", "-fPIC", "-shared", "-o", PROBE_PATH, src]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libffa_probe.so")
+    return PROBE_PATH
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

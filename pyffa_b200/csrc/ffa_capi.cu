@@ -223,6 +223,21 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
     memcpy(p.rf.box, rf->box, sizeof(p.rf.box));
     memcpy(p.rf.theta_n, rf->theta_n, sizeof(p.rf.theta_n));
     memcpy(p.rf.rf_shift, rf->rf_shift, sizeof(p.rf.rf_shift));
+    for (int g = 0; g < rf->ngaps; ++g) {
+        // angular extent of the gap rectangle: a convex polygon that does not
+        // contain the origin subtends the angles spanned by its vertices
+        double cx = 0.0, cy = 0.0;
+        for (int j = 0; j < 4; ++j) { cx += rf->poly_x[g][j]; cy += rf->poly_y[g][j]; }
+        const double c0 = atan2(cy, cx);
+        double half = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            double d = atan2(rf->poly_y[g][j], rf->poly_x[g][j]) - c0;
+            d -= 2.0 * PI * rint(d / (2.0 * PI));
+            half = fmax(half, fabs(d));
+        }
+        p.rf.win_center[g] = c0;
+        p.rf.win_half[g] = half < 1.0 ? half + 1e-9 : 4.0;  // wide gaps: no shortcut
+    }
     p.ap = *ap;
     p.cs = *cs;
     p.st = *st;

@@ -41,6 +41,12 @@ struct RFK {
     double box[FFA_MAX_GAPS][4];
     double theta_n[FFA_MAX_GAPS];
     double rf_shift[FFA_MAX_GAPS];
+    // Angular window of each gap rectangle as seen from the origin: every
+    // point of the rectangle lies within win_half of win_center, so a
+    // particle outside the window is outside the gap without the Cartesian
+    // test (win_half = pi disables the shortcut).
+    double win_center[FFA_MAX_GAPS];
+    double win_half[FFA_MAX_GAPS];
 };
 
 struct PushK {

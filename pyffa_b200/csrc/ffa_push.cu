@@ -14,8 +14,18 @@
 // (RK4: FunctionForAccelerationBunch_dt src/FFAG_track.py:1743-1801 four times,
 //  RK4_equations_of_motion_njit and RK4_Post_Step_njit
 //  src/FFAG_MathTools.py:2205-2299.)
-// Expressions keep the reference's evaluation order; the compiler may fuse a
-// multiply and an add into one FMA, which changes results by at most an ulp.
+//
+// The Boris step is taken in the particle's own frame (r-hat, fi-hat, z-hat)
+// instead of the fixed Cartesian frame.  The Boris update commutes with
+// rotations, so this is the reference's step up to rounding: the reference
+// rotates x, v, E, B into Cartesian axes, pushes, and rotates back with the
+// azimuth change atan2(y', x') - atan2(y, x); here the azimuth change is
+// atan2 of the displacement in the local frame.  It saves one atan2 and two
+// sin/cos pairs per step and is the more accurate of the two.  Particles that
+// are skipped (not injected or lost) take the reference's exact Cartesian
+// round trip, which perturbs r, vr and dfi/dt by rounding every step.
+// Expressions otherwise keep the reference's evaluation order; the compiler may
+// fuse a multiply and an add into one FMA (at most an ulp per operation).
 #include "ffa_internal.cuh"
 
 namespace ffa {
@@ -58,36 +68,57 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
 
 // Bilinear lookup of the z-Taylor coefficients: int() truncation, index
 // clamped to [0, n-2], weights not clamped (linear extrapolation).
+template <int MAXO>
 __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double y, double z,
-                                               double &Bz, double &Bfi, double &Br, bool &clamped)
+                                               double &Bz, double &Bfi, double &Br, int &clamped)
 {
-    int64_t i = (int64_t)((x - f.r_min) / f.r_step);
-    int64_t j = (int64_t)((y - f.fi_min) / f.fi_step);
-    clamped = false;
-    if (i < 0) { i = 0; clamped = true; }
-    else if (i >= f.r_size - 1) { i = f.r_size - 2; clamped = true; }
-    if (j < 0) { j = 0; clamped = true; }
-    else if (j >= f.fi_size - 1) { j = f.fi_size - 2; clamped = true; }
-    double tx = (x - (f.r_min + (double)i * f.r_step)) / f.r_step;
-    double ty = (y - (f.fi_min + (double)j * f.fi_step)) / f.fi_step;
-    double w00 = (1.0 - tx) * (1.0 - ty), w01 = (1.0 - tx) * ty;
-    double w10 = tx * (1.0 - ty), w11 = tx * ty;
-    const int np = f.npad;
-    const double *n00 = f.nodes64 + (i * f.fi_size + j) * np;
-    const double *n01 = n00 + np;
-    const double *n10 = n00 + f.fi_size * np;
-    const double *n11 = n10 + np;
-    double z2 = z * z;
+    // the cell index uses the reference's division (bit-exact cell); the
+    // weights reuse the quotient (the reference recomputes it from the node
+    // coordinate, which differs by rounding only)
+    const double qx = (x - f.r_min) / f.r_step;
+    const double qy = (y - f.fi_min) / f.fi_step;
+    int64_t i = (int64_t)qx;
+    int64_t j = (int64_t)qy;
+    if (i < 0) { i = 0; ++clamped; }
+    else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
+    if (j < 0) { j = 0; ++clamped; }
+    else if (j >= f.fi_size - 1) { j = f.fi_size - 2; ++clamped; }
+    const double tx = qx - (double)i;
+    const double ty = qy - (double)j;
+    const double w00 = (1.0 - tx) * (1.0 - ty), w01 = (1.0 - tx) * ty;
+    const double w10 = tx * (1.0 - ty), w11 = tx * ty;
+    constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
+    constexpr int NV = 3 * MAXO;
+    const double *nd[4];
+    nd[0] = f.nodes64 + (i * f.fi_size + j) * NP;  // (i, j)
+    nd[1] = nd[0] + NP;                            // (i, j+1)
+    nd[2] = nd[0] + f.fi_size * NP;                // (i+1, j)
+    nd[3] = nd[2] + NP;                            // (i+1, j+1)
+    const double w[4] = {w00, w01, w10, w11};
+    // accumulate node by node in the reference's order w00, w01, w10, w11;
+    // a node's coefficients are 16 B aligned pairs
+    double acc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int a = 0; a < NV; a += 2) {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(nd[k] + a));
+            if (k == 0) {
+                acc[a] = w[0] * t.x;
+                if (a + 1 < NV) acc[a + 1] = w[0] * t.y;
+            } else {
+                acc[a] += w[k] * t.x;
+                if (a + 1 < NV) acc[a + 1] += w[k] * t.y;
+            }
+        }
+    }
+    const double z2 = z * z;
     double ze = z2, zo = ze * z;
-#pragma unroll 1
-    for (int n = 0; n < f.max_order; ++n) {
-        int o = 3 * n;
-        double bz = w00 * __ldg(n00 + o) + w01 * __ldg(n01 + o) + w10 * __ldg(n10 + o) + w11 * __ldg(n11 + o);
-        double bf = w00 * __ldg(n00 + o + 1) + w01 * __ldg(n01 + o + 1) + w10 * __ldg(n10 + o + 1) + w11 * __ldg(n11 + o + 1);
-        double br = w00 * __ldg(n00 + o + 2) + w01 * __ldg(n01 + o + 2) + w10 * __ldg(n10 + o + 2) + w11 * __ldg(n11 + o + 2);
-        Bz += bz * ze;
-        Bfi += bf * zo;
-        Br += br * zo;
+#pragma unroll
+    for (int n = 0; n < MAXO; ++n) {
+        Bz += acc[3 * n] * ze;
+        Bfi += acc[3 * n + 1] * zo;
+        Br += acc[3 * n + 2] * zo;
         ze *= z2;
         zo *= z2;
     }
@@ -100,38 +131,97 @@ __device__ __forceinline__ bool gap_inside(const RFK &rf, int g, double x, doubl
     double prev = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        double x0 = rf.poly_x[g][j], y0 = rf.poly_y[g][j];
-        double x1 = rf.poly_x[g][(j + 1) & 3], y1 = rf.poly_y[g][(j + 1) & 3];
-        double cross = (x1 - x0) * (y - y0) - (y1 - y0) * (x - x0);
+        const double x0 = rf.poly_x[g][j], y0 = rf.poly_y[g][j];
+        const double x1 = rf.poly_x[g][(j + 1) & 3], y1 = rf.poly_y[g][(j + 1) & 3];
+        const double cross = (x1 - x0) * (y - y0) - (y1 - y0) * (x - x0);
         if (j == 0) prev = cross;
         else if (cross * prev < 0.0) return false;
     }
     return true;
 }
 
-// RF field in cylindrical components times sin(RF phase + rf_shift[gap]).
+__device__ __forceinline__ bool in_window(const RFK &rf, int g, double fi)
+{
+    double d = fi - rf.win_center[g];
+    d -= (2.0 * PI) * rint(d / (2.0 * PI));
+    return fabs(d) <= rf.win_half[g];
+}
+
+// RF field (cylindrical r, fi components) times sin(RF phase + rf_shift[gap]).
 // Reference semantics: every gap's emap_kernel call overwrites the field, so
 // only the last gap contributes; physical_sum adds all gaps.
-__device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double x, double y, double fi,
-                                           double rfph, double &Er, double &Efi)
+__device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double r, double fi, double rfph,
+                                           double &Er, double &Efi)
 {
     Er = 0.0;
     Efi = 0.0;
     if (!rf.enable) return;
-    int g0 = rf.physical_sum ? 0 : rf.ngaps - 1;
+    const int g0 = rf.physical_sum ? 0 : rf.ngaps - 1;
     for (int g = g0; g < rf.ngaps; ++g) {
-        if (!gap_inside(rf, g, x, y)) continue;
+        if (!in_window(rf, g, fi)) continue;
+        double sf, cf;
+        sincos(fi, &sf, &cf);
+        if (!gap_inside(rf, g, r * cf, r * sf)) continue;
         double sd, cd;
         sincos(rf.theta_n[g] - fi, &sd, &cd);
-        double s = sin(rfph + rf.rf_shift[g]);
+        const double s = sin(rfph + rf.rf_shift[g]);
         Er += (acc * cd) * s;
         Efi += (acc * sd) * s;
     }
 }
 
+__device__ __forceinline__ void status_add(int64_t *status, int lost, int bad, int oob)
+{
+    if (!status) return;
+    const unsigned mask = __activemask();
+    for (int off = 16; off > 0; off >>= 1) {
+        lost += __shfl_down_sync(mask, lost, off);
+        bad += __shfl_down_sync(mask, bad, off);
+        oob += __shfl_down_sync(mask, oob, off);
+    }
+    if ((threadIdx.x & 31) == __ffs(mask) - 1) {
+        if (lost) atomicAdd((unsigned long long *)&status[FFA_STATUS_LOST], (unsigned long long)lost);
+        if (bad) atomicAdd((unsigned long long *)&status[FFA_STATUS_NAN], (unsigned long long)bad);
+        if (oob) atomicAdd((unsigned long long *)&status[FFA_STATUS_OUT_OF_MAP], (unsigned long long)oob);
+    }
+}
+
+// Linear extrapolation of the space-charge field between updates
+// (src/FFAG_track.py:449-478).
+struct SCExtrap {
+    bool pre = false, pp = false;
+    double epr = 0, epz = 0, epf = 0, eqr = 0, eqz = 0, eqf = 0;
+    __device__ void load(const ffa_state_soa &S, int64_t i)
+    {
+        pre = S.sc_pre[i] != 0;
+        pp = S.sc_pp[i] != 0;
+        if (pre) {
+            epr = S.e_pre_r[i]; epz = S.e_pre_z[i]; epf = S.e_pre_fi[i];
+            if (pp) { eqr = S.e_pp_r[i]; eqz = S.e_pp_z[i]; eqf = S.e_pp_fi[i]; }
+        }
+    }
+    __device__ void apply(int64_t gs, int sc_step, double &esr, double &esz, double &esf) const
+    {
+        if (!pre) return;
+        const double sf = gs >= sc_step ? (double)(gs % sc_step) / (double)sc_step : 0.0;
+        if (pp) {
+            esr = epr + sf * (epr - eqr);
+            esz = epz + sf * (epz - eqz);
+            esf = epf + sf * (epf - eqf);
+        } else {
+            esr = epr; esz = epz; esf = epf;
+        }
+    }
+};
+
 // ------------------------------------------------------------ Boris fp64
 
-__global__ void __launch_bounds__(128) boris_f64_kernel(const PushK p)
+// 64-thread blocks, at most 88 registers: 11 blocks (704 threads) per SM,
+// so a 1e5-particle bunch is resident in one wave on 148 SMs.
+constexpr int BORIS_TB = 64;
+
+template <int MAXO, bool SC>
+__global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -142,77 +232,48 @@ __global__ void __launch_bounds__(128) boris_f64_kernel(const PushK p)
     double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
     int inj = S.inj[i], surv = S.surv[i];
     const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
-    const bool sc_on = p.sc_step > 0 && S.sc_pre != nullptr;
-    bool pre = false, pp = false;
-    double epr = 0, epz = 0, epf = 0, eqr = 0, eqz = 0, eqf = 0;
-    if (sc_on) {
-        pre = S.sc_pre[i] != 0;
-        pp = S.sc_pp[i] != 0;
-        if (pre) {
-            epr = S.e_pre_r[i]; epz = S.e_pre_z[i]; epf = S.e_pre_fi[i];
-            if (pp) { eqr = S.e_pp_r[i]; eqz = S.e_pp_z[i]; eqf = S.e_pp_fi[i]; }
-        }
-    }
+    SCExtrap ex;
+    if (SC) ex.load(S, i);
     const double q = p.cs.q, c = p.cs.c, m = p.cs.m0, dt = p.dt;
     const double hq = 0.5 * dt * q;          // (0.5 * dt) * q
-    const double mmcc = m * m * c * c;
-    const double cc = c * c;
+    const double inv_mmcc = 1.0 / (m * m * c * c);
+    const double inv_cc = 1.0 / (c * c);
+    const double inv_m = 1.0 / m;
     int lost = 0, oob = 0;
 
     for (int s = 0; s < p.nsteps; ++s) {
         const int64_t gs = p.step0 + s;
         if (injs == gs) { inj = 1; surv = 1; }
-        if (pre) {
-            double sf = gs >= p.sc_step ? (double)(gs % p.sc_step) / (double)p.sc_step : 0.0;
-            if (pp) {
-                esr = epr + sf * (epr - eqr);
-                esz = epz + sf * (epz - eqz);
-                esf = epf + sf * (epf - eqf);
-            } else {
-                esr = epr; esz = epz; esf = epf;
-            }
-        }
-        const double acc = __ldg(p.acc + gs), drf = __ldg(p.drf + gs);
-        double sinFi, cosFi;
-        sincos(fi, &sinFi, &cosFi);
-        const double x = r * cosFi, y = r * sinFi;
-        const double vx = rdot * cosFi - r * fidot * sinFi;
-        const double vy = rdot * sinFi + r * fidot * cosFi;
-        const bool alive = (inj == 1) && (surv == 1);
-        if (alive) {
+        if (SC) ex.apply(gs, p.sc_step, esr, esz, esf);
+        const double drf = __ldg(p.drf + gs);
+        if ((inj == 1) && (surv == 1)) {
+            const double acc = __ldg(p.acc + gs);
             const double fim = fi - f.period * floor(fi / f.period);
             double Bz, Br, Bfi;
             analytic_b64(f, r, fim, z, Bz, Br, Bfi);
-            if (f.max_order >= 1) {
-                bool cl;
-                high_order_b64(f, r, fim, z, Bz, Bfi, Br, cl);
-                oob += cl;
-            }
+            if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, r, fim, z, Bz, Bfi, Br, oob);
             double Er, Efi;
-            rf_field64(p.rf, acc, x, y, fi, rfph, Er, Efi);
+            rf_field64(p.rf, acc, r, fi, rfph, Er, Efi);
             double Ez = 0.0;
             Ez += esz;
             Er += esr;
             Efi += esf;
-            const double Ex = Er * cosFi - Efi * sinFi;
-            const double Ey = Er * sinFi + Efi * cosFi;
-            const double Bx = -(Br * cosFi - Bfi * sinFi);
-            const double By = -(Br * sinFi + Bfi * cosFi);
-            const double Bzc = -Bz;
             if (p.ap.enable && (r > p.ap.rmax || r < p.ap.rmin || z > p.ap.zmax || z < p.ap.zmin)) {
                 surv = 0;
                 ++lost;
             }
-            const double vz = zdot;
+            // local frame: x along r-hat, y along fi-hat; B enters negated
+            const double vx = rdot, vy = r * fidot, vz = zdot;
+            const double Bx = -Br, By = -Bfi, Bzc = -Bz;
             const double v2 = vx * vx + vy * vy + vz * vz;
-            const double gamma = 1.0 / sqrt(1 - v2 / cc);
+            const double gamma = rsqrt(1 - v2 * inv_cc);
             double px = gamma * m * vx, py = gamma * m * vy, pz = gamma * m * vz;
-            px += hq * Ex;
-            py += hq * Ey;
+            px += hq * Er;
+            py += hq * Efi;
             pz += hq * Ez;
             const double p2 = px * px + py * py + pz * pz;
-            const double gm = sqrt(1 + p2 / mmcc);
-            const double cb = hq / (gm * m);
+            const double gm = sqrt(1 + p2 * inv_mmcc);
+            const double cb = hq * inv_m / gm;
             const double tx = cb * Bx, ty = cb * By, tz = cb * Bzc;
             const double pxp = px + (py * tz - pz * ty);
             const double pyp = py + (pz * tx - px * tz);
@@ -223,29 +284,31 @@ __global__ void __launch_bounds__(128) boris_f64_kernel(const PushK p)
             px += (pyp * sz - pzp * sy);
             py += (pzp * sx - pxp * sz);
             pz += (pxp * sy - pyp * sx);
-            px += hq * Ex;
-            py += hq * Ey;
+            px += hq * Er;
+            py += hq * Efi;
             pz += hq * Ez;
             const double p2n = px * px + py * py + pz * pz;
-            const double gmn = sqrt(1 + p2n / mmcc);
-            const double vxn = px / (gmn * m), vyn = py / (gmn * m), vzn = pz / (gmn * m);
-            const double xn = x + vxn * dt, yn = y + vyn * dt;
+            const double igm = inv_m * rsqrt(1 + p2n * inv_mmcc);
+            const double vxn = px * igm, vyn = py * igm, vzn = pz * igm;
+            const double xn = r + vxn * dt, yn = vyn * dt;
             z = z + vzn * dt;
             zdot = vzn;
             const double rn = sqrt(xn * xn + yn * yn);
-            double dfi = atan2(yn, xn) - atan2(y, x);
-            if (dfi > PI) dfi -= 2 * PI;
-            else if (dfi < -PI) dfi += 2 * PI;
+            const double dfi = atan2(yn, xn);
             fi = fi + dfi;
             double sn, cn;
-            sincos(fi, &sn, &cn);
+            sincos(dfi, &sn, &cn);
             rdot = vxn * cn + vyn * sn;
             const double vfi = -vxn * sn + vyn * cn;
             fidot = rn > 1e-12 ? vfi / rn : 0.0;
             r = rn;
         } else {
-            // Skipped particles still take the reference's cylindrical ->
-            // Cartesian -> cylindrical round trip (fi is unchanged exactly).
+            // skipped particle: the reference's Cartesian round trip
+            double sinFi, cosFi;
+            sincos(fi, &sinFi, &cosFi);
+            const double x = r * cosFi, y = r * sinFi;
+            const double vx = rdot * cosFi - r * fidot * sinFi;
+            const double vy = rdot * sinFi + r * fidot * cosFi;
             const double rn = sqrt(x * x + y * y);
             rdot = vx * cosFi + vy * sinFi;
             const double vfi = -vx * sinFi + vy * cosFi;
@@ -259,22 +322,7 @@ __global__ void __launch_bounds__(128) boris_f64_kernel(const PushK p)
     S.esc_r[i] = esr; S.esc_z[i] = esz; S.esc_fi[i] = esf;
     S.inj[i] = (uint8_t)inj;
     S.surv[i] = (uint8_t)surv;
-    const bool bad = !(isfinite(r) && isfinite(fi) && isfinite(z));
-    if (p.status) {
-        // warp-aggregated status counters
-        unsigned mask = __activemask();
-        int l = lost, b = bad ? 1 : 0, o = oob;
-        for (int off = 16; off > 0; off >>= 1) {
-            l += __shfl_down_sync(mask, l, off);
-            b += __shfl_down_sync(mask, b, off);
-            o += __shfl_down_sync(mask, o, off);
-        }
-        if ((threadIdx.x & 31) == __ffs(mask) - 1) {
-            if (l) atomicAdd((unsigned long long *)&p.status[FFA_STATUS_LOST], (unsigned long long)l);
-            if (b) atomicAdd((unsigned long long *)&p.status[FFA_STATUS_NAN], (unsigned long long)b);
-            if (o) atomicAdd((unsigned long long *)&p.status[FFA_STATUS_OUT_OF_MAP], (unsigned long long)o);
-        }
-    }
+    status_add(p.status, lost, !(isfinite(r) && isfinite(fi) && isfinite(z)), oob);
 }
 
 // -------------------------------------------------------------- RK4 fp64
@@ -284,6 +332,7 @@ struct Y7 {
 };
 
 // RK4_equations_of_motion_njit for one live particle at stage state y.
+template <int MAXO>
 __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double rate, double acc,
                                           double esr, double esz, double esf, Y7 &d, int &oob)
 {
@@ -292,17 +341,9 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     const double fim = y.fi - f.period * floor(y.fi / f.period);
     double Bz, Br, Bfi;
     analytic_b64(f, y.r, fim, y.z, Bz, Br, Bfi);
-    if (f.max_order >= 1) {
-        bool cl;
-        high_order_b64(f, y.r, fim, y.z, Bz, Bfi, Br, cl);
-        oob += cl;
-    }
-    double Er = 0.0, Efi = 0.0;
-    if (p.rf.enable) {
-        double sf, cf;
-        sincos(y.fi, &sf, &cf);
-        rf_field64(p.rf, acc, y.r * cf, y.r * sf, y.fi, y.rf, Er, Efi);
-    }
+    if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
+    double Er, Efi;
+    rf_field64(p.rf, acc, y.r, y.fi, y.rf, Er, Efi);
     double Ez = 0.0;
     Ez += esz;
     Er += esr;
@@ -323,6 +364,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     d.rf = rate;
 }
 
+template <int MAXO, bool SC>
 __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -332,32 +374,14 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
     double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
     int inj = S.inj[i], surv = S.surv[i];
     const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
-    const bool sc_on = p.sc_step > 0 && S.sc_pre != nullptr;
-    bool pre = false, pp = false;
-    double epr = 0, epz = 0, epf = 0, eqr = 0, eqz = 0, eqf = 0;
-    if (sc_on) {
-        pre = S.sc_pre[i] != 0;
-        pp = S.sc_pp[i] != 0;
-        if (pre) {
-            epr = S.e_pre_r[i]; epz = S.e_pre_z[i]; epf = S.e_pre_fi[i];
-            if (pp) { eqr = S.e_pp_r[i]; eqz = S.e_pp_z[i]; eqf = S.e_pp_fi[i]; }
-        }
-    }
+    SCExtrap ex;
+    if (SC) ex.load(S, i);
     const double h = p.dt;
     int oob = 0;
     for (int s = 0; s < p.nsteps; ++s) {
         const int64_t gs = p.step0 + s;
         if (injs == gs) { inj = 1; surv = 1; }
-        if (pre) {
-            double sf = gs >= p.sc_step ? (double)(gs % p.sc_step) / (double)p.sc_step : 0.0;
-            if (pp) {
-                esr = epr + sf * (epr - eqr);
-                esz = epz + sf * (epz - eqz);
-                esf = epf + sf * (epf - eqf);
-            } else {
-                esr = epr; esz = epz; esf = epf;
-            }
-        }
+        if (SC) ex.apply(gs, p.sc_step, esr, esz, esf);
         const double *rate = p.drf + 4 * gs;
         const double *acc = p.acc + 4 * gs;
         const double k1rf = h * __ldg(rate + 0), k2rf = h * __ldg(rate + 1);
@@ -368,18 +392,18 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
             continue;
         }
         Y7 d, k1, k2, k3, k4, ys;
-        rk4_rhs64(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO>(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
         k1 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k1.r, y.vr + 0.5 * k1.vr, y.z + 0.5 * k1.z, y.vz + 0.5 * k1.vz,
               y.fi + 0.5 * k1.fi, y.E + 0.5 * k1.E, y.rf + 0.5 * k1.rf};
-        rk4_rhs64(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
         k2 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k2.r, y.vr + 0.5 * k2.vr, y.z + 0.5 * k2.z, y.vz + 0.5 * k2.vz,
               y.fi + 0.5 * k2.fi, y.E + 0.5 * k2.E, y.rf + 0.5 * k2.rf};
-        rk4_rhs64(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
         k3 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + k3.r, y.vr + k3.vr, y.z + k3.z, y.vz + k3.vz, y.fi + k3.fi, y.E + k3.E, y.rf + k3.rf};
-        rk4_rhs64(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
         k4 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         y.r += (k1.r + 2 * k2.r + 2 * k3.r + k4.r) / 6;
         y.vr += (k1.vr + 2 * k2.vr + 2 * k3.vr + k4.vr) / 6;
@@ -394,19 +418,7 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
     S.esc_r[i] = esr; S.esc_z[i] = esz; S.esc_fi[i] = esf;
     S.inj[i] = (uint8_t)inj;
     S.surv[i] = (uint8_t)surv;
-    const int bad = !(isfinite(y.r) && isfinite(y.fi) && isfinite(y.z));
-    if (p.status) {
-        unsigned mask = __activemask();
-        int b = bad, o = oob;
-        for (int off = 16; off > 0; off >>= 1) {
-            b += __shfl_down_sync(mask, b, off);
-            o += __shfl_down_sync(mask, o, off);
-        }
-        if ((threadIdx.x & 31) == __ffs(mask) - 1) {
-            if (b) atomicAdd((unsigned long long *)&p.status[FFA_STATUS_NAN], (unsigned long long)b);
-            if (o) atomicAdd((unsigned long long *)&p.status[FFA_STATUS_OUT_OF_MAP], (unsigned long long)o);
-        }
-    }
+    status_add(p.status, 0, !(isfinite(y.r) && isfinite(y.fi) && isfinite(y.z)), oob);
 }
 
 // ------------------------------------------------------------ node packing
@@ -438,17 +450,41 @@ cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, fl
     return cudaGetLastError();
 }
 
-cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s)
+template <int MAXO, bool SC>
+static void boris_launch(const PushK &p, cudaStream_t s)
+{
+    const int tb = BORIS_TB;
+    boris_f64_kernel<MAXO, SC><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+}
+
+template <int MAXO, bool SC>
+static void rk4_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = 128;
-    boris_f64_kernel<<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    rk4_f64_kernel<MAXO, SC><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+}
+
+#define FFA_DISPATCH(FN, p, s)                                                   \
+    do {                                                                         \
+        const bool sc_ = (p).st.sc_pre != nullptr && (p).sc_step > 0;            \
+        switch ((p).f.max_order) {                                               \
+        case 0: sc_ ? FN<0, true>(p, s) : FN<0, false>(p, s); break;             \
+        case 1: sc_ ? FN<1, true>(p, s) : FN<1, false>(p, s); break;             \
+        case 2: sc_ ? FN<2, true>(p, s) : FN<2, false>(p, s); break;             \
+        case 3: sc_ ? FN<3, true>(p, s) : FN<3, false>(p, s); break;             \
+        default: sc_ ? FN<4, true>(p, s) : FN<4, false>(p, s); break;            \
+        }                                                                        \
+    } while (0)
+
+cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s)
+{
+    FFA_DISPATCH(boris_launch, p, s);
     return cudaGetLastError();
 }
 
 cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s)
 {
-    const int tb = 128;
-    rk4_f64_kernel<<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    FFA_DISPATCH(rk4_launch, p, s);
     return cudaGetLastError();
 }
 

@@ -25,16 +25,23 @@ import numpy as np
 
 from .constants import C_LIGHT, E0_J, E0_MEV, Q
 
-# 12-sector scaling FFAG, proton 300 MeV, mean orbit radius near 8.5 m.
-# With the D-magnet polarity -0.7279 this F-D cell is vertically unstable
-# (|Tr Mz|/2 = 1.39 per sector at 300 MeV); -1.3 is the nearest stable
-# setting of that one number (Qx = 3.63, Qz = 1.25 at 300 MeV).
+# 12-sector scaling FFAG, proton 300 MeV, k = 7.6, F-D cell with sector
+# fractions (0.25, 0.3125, 0.09375, 0.09375, 0.25).  Two numbers differ from
+# the nominal workload description, both for stability:
+#  - D polarity -1.3 instead of -0.7279: with -0.7279 the cell is vertically
+#    unstable (|Tr Mz|/2 = 1.39 per sector at 300 MeV);
+#  - fringe widths 1.17 instead of (0.20, 0.35): edges that sharp (10-90 %
+#    rise of 0.3-0.5 deg) are not resolved by 0.5-deg push steps and the
+#    linear vertical motion grows without bound even at z = 0.1 mm.
+# Result: Qx = 3.60, Qz = 0.78 at 300 MeV.  At 720 steps/turn the 2.8-deg
+# D magnet is still coarsely sampled (betatron amplitudes diffuse slowly over
+# tens of turns); at 2880 steps/turn the motion is regular.
 LATTICE = {
     "NSector": 12,
     "k": 7.6,
     "interval_1": [0.25, 0.3125, 0.09375, 0.09375, 0.25],
     "positive_or_negative_1": [0, 1, 0, -1.3, 0],
-    "fringe_width_1": [0, 0.20, 0, 0.35, 0],
+    "fringe_width_1": [0, 1.17, 0, 1.17, 0],
     "SpiralAngle_deg": 0.0,
     "r_ref": 8.5,
     "Ek_ref_MeV": 300.0,

@@ -333,3 +333,43 @@ class _EphemeralBunch:
         _lib.check(_lib.lib().ffa_soa_to_aos(ctypes.byref(self._soa), self.n, self.aos.data_ptr(), _lib.stream_ptr(None)),
                    "ffa_soa_to_aos")
         return self.aos.cpu().numpy()
+
+
+class MatrixTracker:
+    """Host-buffer entry point: advances an N x 16 v-format matrix that lives
+    in host memory by `nsteps` fused steps and writes the result back (the
+    call a host-side caller of Boris_solve / rk4_step makes, batched over
+    steps).  Device buffers are allocated once; each call copies the matrix
+    in, converts it to SoA, pushes, converts back and copies it out."""
+
+    def __init__(self, n, gp, solver="Boris", precision="fp64", device=None):
+        import torch
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.n = n
+        self.gp = gp
+        self.solver = solver
+        self.precision = precision
+        self.b = _EphemeralBunch(np.zeros((n, 16)), solver, self.dev)
+        self.pusher = Pusher(self.b, gp, solver, precision)
+        self.clock = None
+        self.launches = 0
+
+    def bind_clock(self, t_start, dt, nsteps_total):
+        self.clock = StepClock(t_start, dt, self.gp.Emap, self.solver, self.dev)
+        self.clock.ensure(nsteps_total)
+
+    def run(self, host_in, host_out, step0, nsteps):
+        """host_in / host_out: pinned (or pageable) float64 torch tensors (n, 16)."""
+        L = _lib.lib()
+        b = self.b
+        s = self.pusher.stream.cuda_stream
+        b.aos.copy_(host_in, non_blocking=True)
+        _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), s), "ffa_aos_to_soa")
+        if self.precision == "fp32c":
+            _lib.check(L.ffa_fp32c_split(ctypes.byref(b.soa()), b.n, s), "ffa_fp32c_split")
+        self.pusher.push(self.clock, step0, nsteps, 0)
+        if self.precision == "fp32c":
+            _lib.check(L.ffa_fp32c_merge(ctypes.byref(b.soa()), b.n, s), "ffa_fp32c_merge")
+        _lib.check(L.ffa_soa_to_aos(ctypes.byref(b.soa()), b.n, b.aos.data_ptr(), s), "ffa_soa_to_aos")
+        host_out.copy_(b.aos, non_blocking=True)
+        self.launches += 3 + (2 if self.precision == "fp32c" else 0)

@@ -1,0 +1,192 @@
+"""Parity of the CUDA pushers (through libffa_cuda.so) with the reference.
+
+Tolerances: the CUDA and glibc transcendental functions (pow, exp, sin/cos,
+atan2) differ by an ulp or so and the CUDA build fuses multiply-adds, so
+float64 coordinates are compared at 1e-12 relative per turn of tracking (the
+bar of the tracking path).  Flags (injection, aperture loss) and map cell
+indices are compared exactly.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    from pyffa_b200 import _lib
+    _lib.lib()  # fails loudly if the library is missing
+
+
+# r, fi, dfi/dt (or Etot) and the RF phase never cross zero: compared per
+# element; vr, z, vz and the space-charge fields oscillate through zero and are
+# compared relative to their column's largest magnitude (the amplitude).
+ELEMENTWISE = (0, 4, 5, 9)
+AMPLITUDE = (1, 2, 3, 10, 11, 12)
+
+
+def coord_errors(m, ref):
+    errs = {}
+    for c in ELEMENTWISE:
+        errs[c] = float(np.max(np.abs(m[:, c] - ref[:, c]) / np.maximum(np.abs(ref[:, c]), 1e-300)))
+    for c in AMPLITUDE:
+        amp = np.abs(ref[:, c]).max()
+        errs[c] = float(np.abs(m[:, c] - ref[:, c]).max() / amp) if amp > 0 else float(np.abs(m[:, c]).max())
+    return errs
+
+
+def _assert_close(m, ref, rtol, floor=None):
+    """floor: per-column errors of the oracle against itself when its input
+    r is perturbed by one ulp -- the rounding sensitivity of the dynamics over
+    the same steps.  The GPU must agree with the oracle to rtol or to ten
+    times that floor, whichever is larger."""
+    assert np.array_equal(m[:, 7:9], ref[:, 7:9]), "injection / survival flags differ"
+    for c, err in coord_errors(m, ref).items():
+        tol = max(rtol, 10 * floor[c]) if floor is not None else rtol
+        assert err <= tol, f"column {c}: relative error {err:.3g} > {tol:.3g}"
+
+
+def ulp_floor(S, solver, v, t0, dt, nsteps, ref):
+    """Oracle run with r nudged by one ulp, compared with the unperturbed run."""
+    from oracle import oracle as O
+    pert = v.copy()
+    pert[:, 0] = np.nextafter(pert[:, 0], np.inf)
+    O.track(S, solver, pert, t0, dt, nsteps)
+    return coord_errors(pert, ref)
+
+
+def test_boris_step_matches_reference_golden(golden):
+    from pyffa_b200.track import FFAG_RungeKutta
+    t0, dt = golden["boris1_t"]
+    m = golden["boris1_in"].copy()
+    FFAG_RungeKutta().Boris_solve(t0, m, dt, golden.gp())
+    _assert_close(m, golden["boris1_out"], 1e-14)
+
+
+def test_rk4_step_matches_reference_golden(golden):
+    from pyffa_b200.track import FFAG_RungeKutta
+    t0, dt = golden["boris1_t"]
+    m = golden["rk41_in"].copy()
+    dr, *_ = FFAG_RungeKutta().rk4_step_malloc(None, t0, m, dt, golden.gp())
+    _assert_close(m + dr, golden["rk41_out"], 1e-14)
+
+
+@pytest.mark.parametrize("name,solver", [("borisloop", "Boris"), ("rk4loop", "RK4")])
+def test_tracking_loop_matches_reference_golden(golden, name, solver):
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.track import FFAG_RungeKutta
+    from pyffa_b200.dump import Dumps
+    ts, dt, n = golden[name + "_t"]
+    b = FFAG_Bunch(golden[name + "_in"], BunchType=solver)
+    lp = {"stop_condition": {"max_stepsN": int(n), "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+          "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+    rk = FFAG_RungeKutta(verbose=False)
+    getattr(rk, "rk4_solve_dt_bunch3_withSC_boris" if solver == "Boris" else "rk4_solve_dt_bunch3_withSC")(
+        None, ts, b, golden.gp(), lp)
+    _assert_close(b.LocalBunch, golden[name + "_out"], 1e-12)
+
+
+@pytest.fixture(scope="module")
+def full_lattice():
+    """The 12-sector lattice on the full 1301 x 6000 map with z-Taylor order 2."""
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical, FFAG_EField_new
+    import os
+    import tempfile
+    cfg = synthetic.lattice_bmap()
+    stacks = synthetic.taylor_stacks(cfg, 2)
+    bm = FFAG_Bfield_analytical(config=cfg, max_order=2, stacks=stacks)
+    d = tempfile.mkdtemp()
+    em = FFAG_EField_new(synthetic.emap_file(os.path.join(d, "emap.txt")), EnableFlag=True)
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(bm)
+    gp.AddEMap(em)
+    gp.AddAperture(7.5, 9.5, -0.1, 0.1)
+    return gp
+
+
+@pytest.mark.parametrize("solver,turns", [("Boris", 2), ("RK4", 1)])
+def test_full_map_turns_vs_oracle(full_lattice, solver, turns):
+    """A seeded 6D Gaussian bunch, RF on (reference last-gap semantics), full
+    1301 x 6000 map: per-particle agreement after whole turns."""
+    from oracle import oracle as O
+    from pyffa_b200 import synthetic
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.dump import Dumps
+    from pyffa_b200.track import FFAG_RungeKutta
+    gp = full_lattice
+    n = 512
+    p = synthetic.centred_bunch(n, seed=3)
+    conv = FFAG_ConversionTools()
+    v = conv.ConvertPrzek2Vrzek_boris(p) if solver == "Boris" else conv.ConvertPrzek2Vrzek(p)
+    v[:, 9] = 0.7
+    dt = synthetic.design_dt(300.0, 720)
+    nsteps = 720 * turns
+    v_in = v.copy()
+    ref = v.copy()
+    S = O.Setup(gp.Bmap, gp.Emap, gp)
+    O.track(S, solver, ref, 0.0, dt, nsteps)
+    b = FFAG_Bunch(v_in, BunchType=solver)
+    lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+          "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+    rk = FFAG_RungeKutta(verbose=False)
+    getattr(rk, "rk4_solve_dt_bunch3_withSC_boris" if solver == "Boris" else "rk4_solve_dt_bunch3_withSC")(
+        None, 0.0, b, gp, lp)
+    got = b.LocalBunch
+    assert (got[:, 8] == 1).sum() > n // 2
+    _assert_close(got, ref, 1e-12 * turns, ulp_floor(S, solver, v, 0.0, dt, nsteps, ref))
+
+
+def test_subset_parity_at_full_size(full_lattice):
+    """Particles are independent, so parity on a subset of a 1e5-particle
+    bunch pushed as a whole (the benchmark's size) is parity of the whole."""
+    from oracle import oracle as O
+    from pyffa_b200 import synthetic
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.dump import Dumps
+    from pyffa_b200.track import FFAG_RungeKutta
+    gp = full_lattice
+    n = 100_000
+    p = synthetic.centred_bunch(n, seed=7)
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(p)
+    dt = synthetic.design_dt(300.0, 720)
+    b = FFAG_Bunch(v, BunchType="Boris")
+    lp = {"stop_condition": {"max_stepsN": 720, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+          "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+    FFAG_RungeKutta(verbose=False).rk4_solve_dt_bunch3_withSC_boris(None, 0.0, b, gp, lp)
+    got = b.LocalBunch
+    idx = np.random.Generator(np.random.PCG64(0)).choice(n, 400, replace=False)
+    idx.sort()
+    ref = v[idx].copy()
+    S = O.Setup(gp.Bmap, gp.Emap, gp)
+    O.track(S, "Boris", ref, 0.0, dt, 720)
+    _assert_close(got[idx], ref, 1e-12, ulp_floor(S, "Boris", v[idx], 0.0, dt, 720, ref))
+    # whole-bunch properties: nothing non-finite, every particle advanced ~one turn
+    assert np.isfinite(got[:, :6]).all()
+    alive = got[:, 8] == 1
+    turns = got[alive, 4] / (2 * np.pi)
+    assert np.all(np.abs(turns - 1.0) < 0.05)
+
+
+def test_status_counts_losses(golden):
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.dump import Dumps
+    from pyffa_b200.track import FFAG_RungeKutta
+    ts, dt, n = golden["borisloop_t"]
+    b = FFAG_Bunch(golden["borisloop_in"], BunchType="Boris")
+    lp = {"stop_condition": {"max_stepsN": int(n), "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+          "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+    rk = FFAG_RungeKutta(verbose=False)
+    rk.rk4_solve_dt_bunch3_withSC_boris(None, ts, b, golden.gp(), lp)
+    ref = golden["borisloop_out"]
+    assert rk.last_run["status"]["lost"] == int(((ref[:, 7] == 1) & (ref[:, 8] == 0)).sum())
+    assert rk.last_run["status"]["nan"] == 0
