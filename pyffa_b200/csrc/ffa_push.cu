@@ -44,7 +44,9 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0r_p = 0.0;
     } else {
         // r^k = r^(k-1) * r: one pow instead of two.
-        double pk1 = pow(ri, f.km1);
+        // exp((k-1) ln r): a few ulp of (k-1) ln r ~ 14, i.e. ~1e-15
+        // relative, a static field error far below the tracking tolerance
+        double pk1 = exp(f.km1 * log(ri));
         B0r_p = f.B0k * pk1;
         B0r = f.B0 * (pk1 * ri);
     }
@@ -170,6 +172,26 @@ __device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double r, 
     }
 }
 
+// Azimuth change atan2(y, x) of one step and its sine / cosine.  A step
+// turns the particle by about 2 pi / (steps per turn); below 0.02 rad the
+// odd / even Taylor series (truncation < 1e-22 relative) replace atan2 and
+// sincos, which is where most of a step's float64 work would go otherwise.
+__device__ __forceinline__ void small_rotation(double y, double x, double &a, double &s, double &c)
+{
+    const double u = y / x;
+    if (x > 0.0 && fabs(u) < 0.02) {
+        const double u2 = u * u;
+        // atan(u) = u (1 - u^2/3 + u^4/5 - u^6/7 + u^8/9 - u^10/11)
+        a = u * (1.0 + u2 * (-1.0 / 3 + u2 * (1.0 / 5 + u2 * (-1.0 / 7 + u2 * (1.0 / 9 + u2 * (-1.0 / 11))))));
+        const double a2 = a * a;
+        s = a * (1.0 + a2 * (-1.0 / 6 + a2 * (1.0 / 120 + a2 * (-1.0 / 5040 + a2 * (1.0 / 362880)))));
+        c = 1.0 + a2 * (-0.5 + a2 * (1.0 / 24 + a2 * (-1.0 / 720 + a2 * (1.0 / 40320))));
+    } else {
+        a = atan2(y, x);
+        sincos(a, &s, &c);
+    }
+}
+
 __device__ __forceinline__ void status_add(int64_t *status, int lost, int bad, int oob)
 {
     if (!status) return;
@@ -216,9 +238,9 @@ struct SCExtrap {
 
 // ------------------------------------------------------------ Boris fp64
 
-// 64-thread blocks, at most 88 registers: 11 blocks (704 threads) per SM,
+// One-warp blocks, at most 88 registers: 23 warps (736 threads) per SM,
 // so a 1e5-particle bunch is resident in one wave on 148 SMs.
-constexpr int BORIS_TB = 64;
+constexpr int BORIS_TB = 32;
 
 template <int MAXO, bool SC>
 __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
@@ -293,14 +315,15 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             const double xn = r + vxn * dt, yn = vyn * dt;
             z = z + vzn * dt;
             zdot = vzn;
-            const double rn = sqrt(xn * xn + yn * yn);
-            const double dfi = atan2(yn, xn);
+            const double rr2 = xn * xn + yn * yn;
+            const double irn = rsqrt(rr2);
+            const double rn = rr2 * irn;
+            double dfi, sn, cn;
+            small_rotation(yn, xn, dfi, sn, cn);
             fi = fi + dfi;
-            double sn, cn;
-            sincos(dfi, &sn, &cn);
             rdot = vxn * cn + vyn * sn;
             const double vfi = -vxn * sn + vyn * cn;
-            fidot = rn > 1e-12 ? vfi / rn : 0.0;
+            fidot = rn > 1e-12 ? vfi * irn : 0.0;
             r = rn;
         } else {
             // skipped particle: the reference's Cartesian round trip

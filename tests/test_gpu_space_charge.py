@@ -93,8 +93,10 @@ def test_update_vs_oracle_at_size(kv_bunch_1e5, hockney):
     m = v.copy()
     ref = O.sc_step(m, m[:, 8] != 0, seo, 64, 128, 128, 12.0, marco * 1.60217662e-19, hockney=hockney)
     rd = ref["diag"]
+    # sums over 1e5 particles in a different order than the serial loop; the
+    # mean gamma - 1 loses a factor gamma / (gamma - 1) to cancellation
     for k in ("xmin", "xmax", "zmin", "zmax", "bunch_length", "fi_s", "fi_e", "mean_gamma_m1"):
-        assert abs(d[k] - rd[k]) <= 1e-12 * max(abs(rd[k]), 1e-3), k
+        assert abs(d[k] - rd[k]) <= 1e-11 * max(abs(rd[k]), 1e-3), k
     assert d["count"] == rd["count"] == 99_000
     assert np.array_equal(buf["slice_idx"], ref["slice_idx"])
     # cell indices: exact except particles within 1e-9 of a cell edge, where
