@@ -34,8 +34,12 @@ STEPS_PER_TURN = 720
 MAX_ORDER = 2
 # float64 operations per particle-step of the Boris kernel (2 per DFMA,
 # 1 per DADD / DMUL), counted from the kernel's executed instruction mix by
-# ncu on this workload (profiles/boris_f64_c1_1e5.md)
-FP64_FLOP_PER_PARTICLE_STEP = None
+# ncu on this workload (profiles/boris_f64_c1_1e5.md): 274.2 DFMA + 45.1 DADD
+# + 101.1 DMUL per particle-step
+FP64_FLOP_PER_PARTICLE_STEP = 694.6
+# DRAM bytes (read + write) of one launch (one turn, 1e5 particles) from the
+# same ncu capture, L2 flushed before the launch
+BORIS_TRAFFIC_PER_LAUNCH = 22.709e6
 # algorithmic HBM bytes per particle per launch: SoA state read
 # (10 float64 + 2 flag bytes + int32 injection step) and written (10 float64 + 2 bytes)
 STATE_BYTES_PER_PARTICLE = (10 * 8 + 2 + 4) + (10 * 8 + 2)
@@ -44,13 +48,14 @@ STATE_BYTES_PER_PARTICLE = (10 * 8 + 2 + 4) + (10 * 8 + 2)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
     ap.add_argument("--n", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sc", action="store_true")
     return ap.parse_args()
 
 
@@ -91,7 +96,7 @@ class ClockSampler:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -150,7 +155,7 @@ def fp64_peak_tflops(dev_index):
     return best
 
 
-def cpu_baseline(gp, v, dt, sample_n=20_000, steps=STEPS_PER_TURN):
+def cpu_baseline(gp, v, dt, sample_n=100_000, steps=STEPS_PER_TURN):
     """The reference algorithm on the host cores (oracle port, all threads):
     particle-turns/s on a bounded sample of the workload."""
     from oracle import oracle as O
@@ -164,6 +169,69 @@ def cpu_baseline(gp, v, dt, sample_n=20_000, steps=STEPS_PER_TURN):
     return {"value": sample_n * steps / STEPS_PER_TURN / el, "unit": "particle-turns/s", "cores": O.num_threads(),
             "kind": "port", "sample": f"{sample_n} particles x {steps} Boris steps (one turn) of the same workload",
             "seconds": el}
+
+
+def sc_workload(n=1_000_000, seed=11):
+    """c2: 1e6 macroparticles for 1e13 protons at 300 MeV, KV transverse with
+    4 mm radii, Gaussian sigma_t = 20 ns, 64 slices on a 128 x 128 grid."""
+    import warnings
+    warnings.simplefilter("ignore")
+    from pyffa_b200 import orbit, synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools
+    t = orbit.seo_tables(synthetic.lattice_bmap(), np.linspace(280.0, 320.0, 9), nfi=721)
+    seo = {k: t[k] for k in ("Ek_axis", "fi_axis", "r", "pr", "perimeter")}
+    p = synthetic.centred_bunch(n, seed=seed, kind="kv", a_x=4e-3, a_z=4e-3, sig_t=20e-9, fi0=np.pi)
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(p)
+    v[:, 7] = 1.0
+    v[:, 8] = 1.0
+    return v, seo
+
+
+def sc_bench(gp, dt, dev, updates=20, warmup=3, turns=2):
+    """Space-charge update time (ms) for the periodic and the open-boundary
+    solve, and particle-turns/s of the c2 cycle: per turn 12 x (update + 60
+    Boris steps with the field extrapolated between updates)."""
+    import torch
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.space_charge import SpaceCharge
+    from pyffa_b200.track import Pusher, StepClock
+    v, seo = sc_workload()
+    n = v.shape[0]
+    out = {"particles": n, "grid": [64, 128, 128], "sigma_ratio": 12.0}
+    for mode in ("periodic", "hockney"):
+        b = FFAG_Bunch(v, marcosize=1e13 / n, sc_grid_size=(64, 128, 128, 12.0), BunchType="Boris", device=dev)
+        b.SEO_fi_axis, b.SEO_Ek_axis, b.SEO_r_matrix = seo["fi_axis"], seo["Ek_axis"], seo["r"]
+        b.SEO_pr_matrix, b.SEO_perimeter = seo["pr"], seo["perimeter"]
+        sc = SpaceCharge(b, hockney=(mode == "hockney"))
+        for k in range(warmup):
+            sc.update(first=(k == 0))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sc.stream)
+        for k in range(updates):
+            sc.update(first=False)
+        e1.record(sc.stream)
+        torch.cuda.synchronize()
+        out[f"{mode}_ms_per_update"] = e0.elapsed_time(e1) / updates
+        if mode == "hockney":
+            sc_steps = STEPS_PER_TURN // 12
+            pusher = Pusher(b, gp, "Boris", "fp64")
+            clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
+            clock.ensure(STEPS_PER_TURN * (turns + 1))
+            step = 0
+            torch.cuda.synchronize()
+            e0.record(sc.stream)
+            for _ in range(turns * 12):
+                sc.update(first=False)
+                pusher.push(clock, step, sc_steps, sc_steps)
+                step += sc_steps
+            e1.record(sc.stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            out["cycle_particle_turns_per_s"] = n * turns / (ms * 1e-3)
+            out["cycle"] = "12 x (open-boundary update + 60 Boris fp64 steps) per turn"
+            out["alive_fraction"] = float((b.cols["surv"] == 1).float().mean().item())
+    return out
 
 
 def run_reference(args):
@@ -312,10 +380,14 @@ def main():
         roof["hbm"] = {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
                        "frac": hbm_ach / hbm_peak, "algorithmic_bytes_per_launch": STATE_BYTES_PER_PARTICLE * n,
                        "traffic": None}
-        roof["traffic"] = None
+        roof["traffic"] = BORIS_TRAFFIC_PER_LAUNCH if args.n == N_PARTICLES and args.precision == "fp64" else None
+        roof["hbm"]["traffic"] = roof["traffic"]
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(gp, v, dt)
+        sc = None
+        if not args.no_sc:
+            sc = sc_bench(gp, dt, dev)
         line = {
             "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
             "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
@@ -332,6 +404,7 @@ def main():
             "e2e": e2e,
             "clocks": clocks,
             "status": {"lost": int(status[0]), "nan": int(status[1]), "out_of_map": int(status[2])},
+            "space_charge": sc,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)
