@@ -222,6 +222,26 @@ int ffa_sc_plan_destroy(ffa_sc_plan *plan);
 int ffa_sc_step(ffa_sc_plan *plan, ffa_state_soa *st, int64_t n, int32_t roll, int32_t first,
                 void *stream, int64_t *status, ffa_sc_diag *diag);
 
+/* Space-charge update that allocates nothing.  No counterpart in the
+ * reference (its space charge runs on host memory); it exists for callers
+ * that cannot allocate device memory while running -- host codes that
+ * reserve their whole device budget at start-up, or tracking loops embedded
+ * in a control system where an allocation could fail or stall the device.
+ * Same inputs, outputs and results as ffa_sc_plan_create + ffa_sc_step, but
+ * all scratch lives in one fixed device array compiled into the library
+ * (about 31 MB, held by every device that loads the library until exit).
+ * Limits: n <= FFA_SC_STATIC_MAX_PARTICLES (else FFA_ERR_INVALID);
+ * ns * nz * nx <= FFA_SC_STATIC_MAX_CELLS, nx, nz <= 128, periodic boundary
+ * (else FFA_ERR_UNSUPPORTED).  Every call on a device shares the array and
+ * finds the previous call's contents there (the charge accumulator is
+ * cleared each call); calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address and fills its FFT tables: make it before any stream capture. */
+#define FFA_SC_STATIC_MAX_PARTICLES 524288
+#define FFA_SC_STATIC_MAX_CELLS 524288
+int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *st, int64_t n, int32_t roll, int32_t first,
+                       void *stream, int64_t *status, ffa_sc_diag *diag);
+
 /* Device views of the plan's last charge, potential and field cubes
  * (float32, (ns, nz, nx)), and of the per-particle slice / cell indices
  * (int32 slice, int64 cell = (s*nz + iz)*nx + ix, -1 when not deposited). */

@@ -116,7 +116,11 @@ EXPORTS = {
     "ffa_sc_step": [d_p, C.POINTER(StateSoA), C.c_int64, C.c_int32, C.c_int32, d_p, d_p, d_p],
     "ffa_sc_buffers": [d_p, C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p),
                        C.POINTER(d_p), C.POINTER(d_p)],
+    "ffa_sc_step_static": [C.POINTER(SCDesc), C.POINTER(StateSoA), C.c_int64, C.c_int32, C.c_int32, d_p, d_p, d_p],
 }
+
+SC_STATIC_MAX_PARTICLES = 524288
+SC_STATIC_MAX_CELLS = 524288
 
 _lib = None
 

@@ -773,3 +773,153 @@ int ffa_sc_buffers(const ffa_sc_plan *p, const float **rho, const float **phi, c
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------
+// Space-charge update without any allocation.
+//
+// Some callers of this library cannot allocate device memory once they are
+// running: a host code that reserves its whole device budget at start-up
+// and hands it out from its own pool, or a tracking loop embedded in a
+// control or online-model system where a cudaMalloc in the middle of a run
+// could fail or stall every stream on the device.  ffa_sc_step_static runs
+// the same update as ffa_sc_plan_create + ffa_sc_step, but takes its scratch
+// from one fixed array compiled into the library, so it calls no cudaMalloc,
+// cudaFree or other allocating routine.
+//
+// Limits (the array holds ~31 MB on every device that loads the library,
+// until the process exits): at most FFA_SC_STATIC_MAX_PARTICLES particles,
+// ns * nz * nx <= FFA_SC_STATIC_MAX_CELLS, nx and nz <= 128, periodic
+// boundary only.  Larger sizes are rejected with FFA_ERR_INVALID (particle
+// count) or FFA_ERR_UNSUPPORTED (grid, open boundary) before anything runs.
+//
+// The array is shared by every call on a device and keeps the previous
+// call's contents; the charge accumulator is cleared at the start of each
+// call, every other region is fully rewritten before it is read.  Calls
+// whose work overlaps on the GPU (different streams, or host threads)
+// race on the array and must be serialised by the caller.
+// The first call on a device looks up the array's device address (with that
+// device current) and fills the FFT twiddle tables; make that first call
+// before capturing any stream.
+// ------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t ST_MAX_N = FFA_SC_STATIC_MAX_PARTICLES;
+constexpr int64_t ST_MAX_CELLS = FFA_SC_STATIC_MAX_CELLS;
+constexpr int ST_MAX_GRID = 128;
+
+constexpr size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t ST_OFF_X = 0;
+constexpr size_t ST_OFF_PR0 = ST_OFF_X + a256(sizeof(double) * ST_MAX_N);
+constexpr size_t ST_OFF_SLICE = ST_OFF_PR0 + a256(sizeof(double) * ST_MAX_N);
+constexpr size_t ST_OFF_CELL = ST_OFF_SLICE + a256(sizeof(int32_t) * ST_MAX_N);
+constexpr size_t ST_OFF_P1 = ST_OFF_CELL + a256(sizeof(int64_t) * ST_MAX_N);
+constexpr size_t ST_OFF_P2 = ST_OFF_P1 + a256(sizeof(Partial1) * SC_BLOCKS);
+constexpr size_t ST_OFF_STATE = ST_OFF_P2 + a256(sizeof(Partial2) * SC_BLOCKS);
+constexpr size_t ST_OFF_ACC = ST_OFF_STATE + a256(sizeof(SCState));
+constexpr size_t ST_OFF_RHO = ST_OFF_ACC + a256(sizeof(unsigned long long) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_PHI = ST_OFF_RHO + a256(sizeof(float) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_EX = ST_OFF_PHI + a256(sizeof(float) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_EZ = ST_OFF_EX + a256(sizeof(float) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_WORK = ST_OFF_EZ + a256(sizeof(float) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_TWX = ST_OFF_WORK + a256(sizeof(float2) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_TWZ = ST_OFF_TWX + a256(sizeof(float2) * ST_MAX_GRID / 2);
+constexpr size_t ST_BYTES = ST_OFF_TWZ + a256(sizeof(float2) * ST_MAX_GRID / 2);
+
+// Twiddles exp(-2 pi i k / n) of both axes, one set per device; the table of
+// an axis is rebuilt when a call uses a different length.
+struct StaticDev {
+    unsigned char *base;  // device address of the array (from cudaGetSymbolAddress)
+    int twx_n, twz_n;
+};
+
+constexpr int ST_MAX_DEVICES = 64;
+StaticDev g_static_dev[ST_MAX_DEVICES];
+
+__global__ void st_twiddles(float2 *tw, int n)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n / 2) return;
+    const double a = -2.0 * PI * (double)k / (double)n;
+    tw[k] = make_float2((float)cos(a), (float)sin(a));
+}
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char ffa_sc_static_scratch[ST_BYTES];
+
+extern "C" int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *S, int64_t n, int32_t roll,
+                                  int32_t first, void *stream, int64_t *status, ffa_sc_diag *diag)
+{
+    if (!desc || !S || !S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r ||
+        !S->esc_z || !S->esc_fi || n < 0)
+        return FFA_ERR_INVALID;
+    const ffa_sc_desc &d = *desc;
+    if (d.ns < 2 || d.nx < 16 || d.nz < 16 || d.nE < 2 || d.nfi < 2 || !d.seo_Ek || !d.seo_r || !d.seo_pr ||
+        !d.seo_perimeter || !(d.dEk > 0) || !(d.dfi > 0))
+        return FFA_ERR_INVALID;
+    if (n > ST_MAX_N) return FFA_ERR_INVALID;  // more particles than the static scratch holds
+    const int lx = ilog2(d.nx), lz = ilog2(d.nz);
+    if (d.hockney || lx < 0 || lz < 0 || d.nx > ST_MAX_GRID || d.nz > ST_MAX_GRID ||
+        (int64_t)d.ns * d.nz * d.nx > ST_MAX_CELLS)
+        return FFA_ERR_UNSUPPORTED;
+    if (roll && (!S->sc_pre || !S->sc_pp || !S->e_pre_r || !S->e_pre_z || !S->e_pre_fi || !S->e_pp_r ||
+                 !S->e_pp_z || !S->e_pp_fi))
+        return FFA_ERR_INVALID;
+    int dev = 0;
+    FFA_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= ST_MAX_DEVICES) return FFA_ERR_UNSUPPORTED;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    StaticDev &sd = g_static_dev[dev];
+    if (!sd.base) {
+        // host code must not use the array's name as a device address: ask
+        // the runtime for the address on this (current) device once
+        void *ptr = nullptr;
+        FFA_CHECK_CUDA(cudaGetSymbolAddress(&ptr, ffa_sc_static_scratch));
+        sd.base = static_cast<unsigned char *>(ptr);
+        sd.twx_n = sd.twz_n = 0;
+    }
+    unsigned char *b = sd.base;
+    double *x = reinterpret_cast<double *>(b + ST_OFF_X);
+    double *pr0 = reinterpret_cast<double *>(b + ST_OFF_PR0);
+    int32_t *slice = reinterpret_cast<int32_t *>(b + ST_OFF_SLICE);
+    int64_t *cell = reinterpret_cast<int64_t *>(b + ST_OFF_CELL);
+    Partial1 *p1 = reinterpret_cast<Partial1 *>(b + ST_OFF_P1);
+    Partial2 *p2 = reinterpret_cast<Partial2 *>(b + ST_OFF_P2);
+    SCState *st = reinterpret_cast<SCState *>(b + ST_OFF_STATE);
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(b + ST_OFF_ACC);
+    float *rho = reinterpret_cast<float *>(b + ST_OFF_RHO);
+    float *phi = reinterpret_cast<float *>(b + ST_OFF_PHI);
+    float *ex = reinterpret_cast<float *>(b + ST_OFF_EX);
+    float *ez = reinterpret_cast<float *>(b + ST_OFF_EZ);
+    float2 *work = reinterpret_cast<float2 *>(b + ST_OFF_WORK);
+    float2 *twx = reinterpret_cast<float2 *>(b + ST_OFF_TWX);
+    float2 *twz = reinterpret_cast<float2 *>(b + ST_OFF_TWZ);
+    if (sd.twx_n != d.nx) {
+        st_twiddles<<<1, 64, 0, s>>>(twx, d.nx);
+        sd.twx_n = d.nx;
+    }
+    if (sd.twz_n != d.nz) {
+        st_twiddles<<<1, 64, 0, s>>>(twz, d.nz);
+        sd.twz_n = d.nz;
+    }
+    const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
+    const unsigned ew = 148 * 8;
+    FFA_CHECK_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * cube, s));
+    sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, pr0, slice, cell, p1);
+    sc_reduce1<<<1, 32, 0, s>>>(p1, SC_BLOCKS, d, st);
+    sc_pass2<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, st, p2);
+    sc_reduce2<<<1, 32, 0, s>>>(p2, SC_BLOCKS, d, st, status);
+    sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, cell, st, acc);
+    sc_convert<<<ew, 256, 0, s>>>(acc, d, st, rho, work, d.nz, d.nx);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    FFA_CHECK_CUDA((fft2d<float, 16>(work, d.ns, d.nz, d.nx, lz, lx, twz, twx, 0, s)));
+    sc_mul_periodic<<<ew, 256, 0, s>>>(work, d, st);
+    FFA_CHECK_CUDA((fft2d<float, 16>(work, d.ns, d.nz, d.nx, lz, lx, twz, twx, 1, s)));
+    sc_potential<<<ew, 256, 0, s>>>(work, d, d.nz, d.nx, st, phi);
+    sc_field<<<ew, 256, 0, s>>>(phi, d, st, ex, ez);
+    sc_gather<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, pr0, slice, st, ex, ez);
+    if (roll) sc_roll<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, first);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    if (diag) FFA_CHECK_CUDA(cudaMemcpyAsync(diag, &st->diag, sizeof(ffa_sc_diag), cudaMemcpyDeviceToDevice, s));
+    return FFA_OK;
+}
