@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-sc", action="store_true")
+    ap.add_argument("--no-fp32c", action="store_true")
     return ap.parse_args()
 
 
@@ -290,38 +291,45 @@ def main():
     n = v.shape[0]
     total_steps = STEPS_PER_TURN * (args.warmup + args.steps + 1)
     b = _EphemeralBunch(v, "Boris", dev)
+    pristine = {k: t.clone() for k, t in b.cols.items()}
     pusher = Pusher(b, gp, "Boris", args.precision)
     clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
     clock.ensure(total_steps)
-    L = _lib.lib()
-    import ctypes
-    if args.precision == "fp32c":
-        _lib.check(L.ffa_fp32c_split(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_split")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = pusher.stream
 
-    def one_turn(k):
-        pusher.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+    def restore():
+        # every timed step starts from the same bunch (not timed)
+        for k, t in b.cols.items():
+            t.copy_(pristine[k])
+
+    def timed_turns(pu, steps):
+        """CUDA-event time of each one-turn launch, L2 flushed and the bunch
+        restored before each (outside the events)."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            restore()
+            flush.zero_()
+            ev[k][0].record(stream)
+            pu.push(clock, (args.warmup + k) * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(bb) for a, bb in ev]
 
     for k in range(args.warmup):
-        one_turn(k)
+        restore()
+        pusher.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    b.status.zero_()
     with ClockSampler(local) as cs:
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        for k in range(args.steps):
-            flush.zero_()  # L2 flush between timed steps (not timed)
-            ev[k][0].record(stream)
-            one_turn(args.warmup + k)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
+        launch_ms = timed_turns(pusher, args.steps)
         if world > 1:
             dist.barrier()
-    launch_ms = [a.elapsed_time(bb) for a, bb in ev]
     t_ms = sum(launch_ms)
     t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
     if world > 1:
@@ -329,6 +337,24 @@ def main():
     t_ms = float(t.item())
     status = b.status.cpu().numpy()
     value = n * world * args.steps / (t_ms * 1e-3)
+
+    # the compensated float32 pusher on the same workload
+    fp32c = None
+    if args.precision == "fp64" and not args.no_fp32c:
+        pu32 = Pusher(b, gp, "Boris", "fp32c")
+        for k in range(args.warmup):
+            restore()
+            pu32.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms32 = timed_turns(pu32, args.steps)
+        t32 = torch.tensor([sum(ms32)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t32, op=dist.ReduceOp.MAX)
+        v32 = n * world * args.steps / (float(t32.item()) * 1e-3)
+        fp32c = {"value": v32, "unit": "particle-turns/s", "ms_per_step": float(t32.item()) / args.steps,
+                 "speedup_vs_fp64": v32 / value, "dtype": "f32 fields/increments, f64 accumulation"}
     clocks = cs.summary()
 
     # end to end through the host-buffer API: host matrix in, one turn, host matrix out
@@ -405,6 +431,7 @@ def main():
             "clocks": clocks,
             "status": {"lost": int(status[0]), "nan": int(status[1]), "out_of_map": int(status[2])},
             "space_charge": sc,
+            "fp32c": fp32c,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)

@@ -48,7 +48,7 @@ enum ffa_push_flags {
     FFA_BORIS = 0,                /* relativistic Boris (solver_type 1) */
     FFA_RK4 = 1,                  /* 4th-order Runge-Kutta (solver_type 0) */
     FFA_FP64 = 0,                 /* all arithmetic in float64 */
-    FFA_FP32C = 2,                /* float32 fields/push, compensated r, fi, phase */
+    FFA_FP32C = 2,                /* float32 fields and push increments, float64 accumulation */
     FFA_RF_PHYSICAL_SUM = 4       /* sum every RF gap (reference: last gap wins) */
 };
 
@@ -122,9 +122,6 @@ typedef struct ffa_state_soa {
     double *e_pre_r, *e_pre_z, *e_pre_fi;
     double *e_pp_r, *e_pp_z, *e_pp_fi;
     uint8_t *sc_pre, *sc_pp;
-    /* FP32C mode: low words of the double-float r and fi (device, float32);
-     * the RF phase stays float64 in `rf`. */
-    float *r_lo, *fi_lo;
 } ffa_state_soa;
 
 /* Per-step host-precomputed scalars (device arrays indexed by absolute step).
@@ -136,6 +133,36 @@ typedef struct ffa_step_table {
     const double *acc;
     int64_t nsteps;               /* entries (Boris) or stage quadruples (RK4) */
 } ffa_step_table;
+
+/* Azimuth-crossing capture (PositionDumpBunch, src/FFAG_dump.py:789-1130;
+ * detect_azimuth_crossing, src/FFAG_MathTools.py:1633-1695).  During a push,
+ * every particle whose survival flag is 1 at the start of a step (after that
+ * step's injection) and whose azimuth mod 2 pi passes one of the targets
+ * within the step appends one record of FFA_CROSSING_RECORD doubles:
+ *   [0] target index, [1] particle index, [2] absolute step,
+ *   [3] interpolation ratio of the target within the step,
+ *   [4..10]  pre-step  r, vr, z, vz, fi, f5, RF phase,
+ *   [11..17] post-step r, vr, z, vz, fi, f5, RF phase,
+ *   [18] post-step survival flag, [19] injection flag,
+ *   [20..22] the space-charge field the step used (Esc r, z, fi).
+ * Records come in no particular order.  `count` (device int64) is advanced
+ * atomically; records past `capacity` are counted but not written. */
+#define FFA_CROSSING_RECORD 23
+#define FFA_MAX_CROSSING_TARGETS 8
+typedef struct ffa_crossing {
+    int32_t ntargets;             /* 1 .. FFA_MAX_CROSSING_TARGETS */
+    int32_t pad;
+    double target[FFA_MAX_CROSSING_TARGETS];  /* rad, each in [0, 2 pi) */
+    double *buf;                  /* device, capacity * FFA_CROSSING_RECORD */
+    int64_t capacity;
+    int64_t *count;               /* device */
+} ffa_crossing;
+
+/* ffa_push with azimuth-crossing capture (all three pushers). */
+int ffa_push_crossing(const struct ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap,
+                      const ffa_consts *cs, const ffa_step_table *tab, ffa_state_soa *st,
+                      int64_t n, int64_t step0, int32_t nsteps, double dt, int32_t sc_step,
+                      int32_t flags, void *stream, int64_t *status, const ffa_crossing *xing);
 
 typedef struct ffa_fieldmap ffa_fieldmap;
 
@@ -167,11 +194,6 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
  * Replaces the LocalBunch column views used throughout src/FFAG_track.py. */
 int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream);
 int ffa_soa_to_aos(const ffa_state_soa *st, int64_t n, double *aos, void *stream);
-
-/* Loads (lo words = 0) or stores the FP32C double-float words from / to the
- * float64 state arrays. */
-int ffa_fp32c_split(ffa_state_soa *st, int64_t n, void *stream);
-int ffa_fp32c_merge(ffa_state_soa *st, int64_t n, void *stream);
 
 /* Sum of fi over the particles whose fi is not NaN, written to *out (device
  * double), and their count to *count (device int64); the host divides.

@@ -177,6 +177,67 @@ def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0):
     return t, h.value
 
 
+def detect_azimuth_crossing(pre_fi, post_fi, survive, target):
+    """Restatement of detect_azimuth_crossing (src/FFAG_MathTools.py:1633-1695)
+    with the mod-2-pi reduction of fast_mod_parallel (src/FFAG_MathTools.py:
+    1554-1557).  Returns (crossed mask, interpolation ratio; 0 where the span
+    is below 1e-12 or nothing crossed)."""
+    tw = 2 * np.pi
+    target = target % tw
+    pre_fi = np.asarray(pre_fi, dtype=np.float64)
+    post_fi = np.asarray(post_fi, dtype=np.float64)
+    a = pre_fi - tw * np.floor(pre_fi / tw)
+    b = post_fi - tw * np.floor(post_fi / tw)
+    alive = np.asarray(survive) == 1
+    fwd = b >= a
+    hit_a = alive & fwd & (a <= target) & (target <= b)
+    hit_b = alive & ~fwd & (((target >= a) & (target < tw)) | ((target >= 0) & (target <= b)))
+    ratio = np.zeros(a.shape)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        span_a = b - a
+        ok = hit_a & (span_a > 1e-12)
+        ratio[ok] = (target - a[ok]) / span_a[ok]
+        span_b = (b + tw) - a
+        tu = np.where(target <= b, target + tw, target)
+        ok = hit_b & (span_b > 1e-12)
+        ratio[ok] = (tu[ok] - a[ok]) / span_b[ok]
+    return hit_a | hit_b, ratio
+
+
+def track_crossings(setup: Setup, solver, mat, t_start, dt, nsteps, targets, head=0):
+    """Injection + push loop that also records, step by step, the azimuth
+    crossings of the reference's PositionDumpBunch (src/FFAG_dump.py:
+    1098-1130, with the pre-step survival flag of UpdataPreStepNjit,
+    src/FFAG_MathTools.py:2179-2201) as records of 23 values: target index,
+    particle, step, ratio, pre-step r vr z vz fi f5 RF phase, the same
+    post-step, post-step survival and injection flags, post-step Esc r z fi.
+    Returns (records, t_end, head)."""
+    _mat(mat)
+    h = C.c_int64(head)
+    t = t_start
+    recs = []
+    cols = [0, 1, 2, 3, 4, 5, 9]
+    for s in range(nsteps):
+        lib().orc_inject(mat.ctypes.data, mat.shape[0], t, dt, C.byref(h))
+        pre = mat[:, cols].copy()
+        surv = mat[:, 8].copy()
+        (boris_step if solver == "Boris" else rk4_step)(setup, mat, t, dt)
+        t = t + dt
+        for k, tg in enumerate(targets):
+            hit, ratio = detect_azimuth_crossing(pre[:, 4], mat[:, 4], surv, tg)
+            idx = np.nonzero(hit)[0]
+            if idx.size:
+                r = np.empty((idx.size, 23))
+                r[:, 0], r[:, 1], r[:, 2], r[:, 3] = k, idx, s, ratio[idx]
+                r[:, 4:11] = pre[idx]
+                r[:, 11:18] = mat[idx][:, cols]
+                r[:, 18], r[:, 19] = mat[idx, 8], mat[idx, 7]
+                r[:, 20:23] = mat[idx, 10:13]
+                recs.append(r)
+    out = np.vstack(recs) if recs else np.zeros((0, 23))
+    return out, t, h.value
+
+
 def sc_step(mat, alive, seo, ns, nx, nz, sigma_ratio, q_macro, boris=True, hockney=False,
             speed_c=2.99792458e8, E0_rest_MeV=938.2723):
     """One space-charge update in place; returns a dict of cubes, indices and

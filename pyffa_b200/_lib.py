@@ -72,12 +72,20 @@ class StateSoA(C.Structure):
         ("e_pre_r", d_p), ("e_pre_z", d_p), ("e_pre_fi", d_p),
         ("e_pp_r", d_p), ("e_pp_z", d_p), ("e_pp_fi", d_p),
         ("sc_pre", d_p), ("sc_pp", d_p),
-        ("r_lo", d_p), ("fi_lo", d_p),
     ]
 
 
 class StepTable(C.Structure):
     _fields_ = [("drf", d_p), ("acc", d_p), ("nsteps", C.c_int64)]
+
+
+CROSSING_RECORD = 23
+MAX_CROSSING_TARGETS = 8
+
+
+class Crossing(C.Structure):
+    _fields_ = [("ntargets", C.c_int32), ("pad", C.c_int32), ("target", C.c_double * MAX_CROSSING_TARGETS),
+                ("buf", d_p), ("capacity", C.c_int64), ("count", d_p)]
 
 
 class SCDesc(C.Structure):
@@ -106,10 +114,11 @@ EXPORTS = {
     "ffa_push": [d_p, C.POINTER(RFDesc), C.POINTER(Aperture), C.POINTER(Consts), C.POINTER(StepTable),
                  C.POINTER(StateSoA), C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                  d_p, d_p],
+    "ffa_push_crossing": [d_p, C.POINTER(RFDesc), C.POINTER(Aperture), C.POINTER(Consts), C.POINTER(StepTable),
+                          C.POINTER(StateSoA), C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32,
+                          d_p, d_p, C.POINTER(Crossing)],
     "ffa_aos_to_soa": [d_p, C.c_int64, C.POINTER(StateSoA), d_p],
     "ffa_soa_to_aos": [C.POINTER(StateSoA), C.c_int64, d_p, d_p],
-    "ffa_fp32c_split": [C.POINTER(StateSoA), C.c_int64, d_p],
-    "ffa_fp32c_merge": [C.POINTER(StateSoA), C.c_int64, d_p],
     "ffa_mean_fi": [C.POINTER(StateSoA), C.c_int64, d_p, d_p, d_p],
     "ffa_sc_plan_create": [C.POINTER(SCDesc), d_p, C.POINTER(d_p)],
     "ffa_sc_plan_destroy": [d_p],

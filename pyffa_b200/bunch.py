@@ -172,23 +172,12 @@ class FFAG_Bunch:
     def restore_from_restart_matrix(self, *, assert_monotonic=True) -> None:
         """Recovers the injection head and counters from the flags of a
         restarted bunch (src/FFAG_Bunch.py:305-366)."""
-        a = self._host_static
-        N = a.shape[0]
-        inj = a[:, COLUMNS["Inj_flag"]] > 0.5
-        sur = a[:, COLUMNS["Survive"]] > 0.5
-        zeros = np.flatnonzero(~inj)
-        head = int(zeros[0]) if zeros.size else N
-        if assert_monotonic:
-            ok = (inj[:head].all() and (~inj[head:]).all()) if head < N else inj.all()
-            if not ok:
-                raise RuntimeError(
-                    "Restart bunch violates the designed structure: Inj_flag is not a step function "
-                    "along inj_t-sorted LocalBunch.")
-        self._uninject_head = head
-        self.InjectedNum_Local = int(inj.sum())
-        self.uninject_num = int(N - self.InjectedNum_Local)
-        self.SurvivedNum_Local = int(sur.sum())
-        self.LostNum_Local = int((inj & ~sur).sum())
+        c = restart_counters(self._host_static, assert_monotonic=assert_monotonic)
+        self._uninject_head = c["head"]
+        self.InjectedNum_Local = c["injected"]
+        self.uninject_num = c["uninjected"]
+        self.SurvivedNum_Local = c["survived"]
+        self.LostNum_Local = c["lost"]
 
     def status_counts(self) -> dict:
         s = self.status.cpu().numpy()
@@ -210,6 +199,26 @@ class FFAG_Bunch:
         if comm is not None:
             comm.all_reduce(vals)
         self.InjectedNum, self.SurvivedNum, self.LostNum = (int(v) for v in vals.tolist())
+
+
+def restart_counters(a: np.ndarray, assert_monotonic: bool = True) -> dict:
+    """Injection head and counters of an inj_t-sorted restart matrix: the
+    head is the first particle not injected; the flags must form a step
+    function [1 ... 1, 0 ... 0] along the matrix (src/FFAG_Bunch.py:305-366)."""
+    N = a.shape[0]
+    inj = a[:, COLUMNS["Inj_flag"]] > 0.5
+    sur = a[:, COLUMNS["Survive"]] > 0.5
+    zeros = np.flatnonzero(~inj)
+    head = int(zeros[0]) if zeros.size else N
+    if assert_monotonic:
+        ok = (inj[:head].all() and (~inj[head:]).all()) if head < N else inj.all()
+        if not ok:
+            raise RuntimeError(
+                "Restart bunch violates the designed structure: Inj_flag is not a step function "
+                "along inj_t-sorted LocalBunch.")
+    injected = int(inj.sum())
+    return {"head": head, "injected": injected, "uninjected": int(N - injected), "survived": int(sur.sum()),
+            "lost": int((inj & ~sur).sum())}
 
 
 def divide_variables(total: int, rank: int, size: int) -> np.ndarray:

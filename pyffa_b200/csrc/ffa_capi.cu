@@ -154,6 +154,21 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     k.fi_step = d->fi_step;
     k.r_size = d->r_size;
     k.fi_size = d->fi_size;
+    k.spiral_zero = 1;
+    for (int a = 0; a < d->n_spoly; ++a) if (d->spoly[a] != 0.0) k.spiral_zero = 0;
+    for (int a = 0; a < d->n_spolyp; ++a) if (d->spolyp[a] != 0.0) k.spiral_zero = 0;
+    k.r_ref = (d->r_size > 1 && d->r_step > 0) ? d->r_min + 0.5 * d->r_step * (double)(d->r_size - 1) : 1.0;
+    k.inv_r_ref = 1.0 / k.r_ref;
+    k.inv_r_step = d->r_step > 0 ? 1.0 / d->r_step : 0.0;
+    k.inv_fi_step = d->fi_step > 0 ? 1.0 / d->fi_step : 0.0;
+    const double c1 = d->k == 0.0 ? d->B0 : d->B0 * pow(k.r_ref, d->k - 1.0);
+    k.c1f = (float)c1;
+    k.kc1f = (float)(d->k * c1);
+    k.km1f = (float)(d->k - 1.0);
+    for (int j = 0; j < d->n_convex; ++j) {
+        k.seg_kf[j] = (float)k.seg_k[j];
+        k.seg_yf[j] = (float)k.seg_y[j];
+    }
     if (d->max_order > 0) {
         const int64_t plane = d->r_size * d->fi_size;
         if (cudaMalloc(&fm->nodes64, sizeof(double) * plane * k.npad) != cudaSuccess) {
@@ -196,9 +211,10 @@ int ffa_inject(ffa_state_soa *st, int64_t n, int64_t step, void *stream)
     return FFA_OK;
 }
 
-int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
-             const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps, double dt,
-             int32_t sc_step, int32_t flags, void *stream, int64_t *status)
+static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
+                     const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps,
+                     double dt, int32_t sc_step, int32_t flags, void *stream, int64_t *status,
+                     const ffa_crossing *xing)
 {
     if (!fm || !rf || !ap || !cs || !tab || !state_ok(st) || n < 0 || nsteps < 0 || step0 < 0) return FFA_ERR_INVALID;
     if (!tab->drf || !tab->acc || step0 + nsteps > tab->nsteps) return FFA_ERR_INVALID;
@@ -209,7 +225,6 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
         return FFA_ERR_INVALID;
     if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_RF_PHYSICAL_SUM)) return FFA_ERR_INVALID;
     if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
-    if ((flags & FFA_FP32C) && (!st->r_lo || !st->fi_lo)) return FFA_ERR_INVALID;
     if (n == 0 || nsteps == 0) return FFA_OK;
 
     PushK p;
@@ -250,11 +265,35 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
     p.sc_step = sc_step;
     p.dt = dt;
     p.status = status;
+    if (xing) {
+        if (!xing->buf || !xing->count || xing->capacity < 0 || xing->ntargets < 1 ||
+            xing->ntargets > FFA_MAX_CROSSING_TARGETS)
+            return FFA_ERR_INVALID;
+        for (int t = 0; t < xing->ntargets; ++t)
+            if (!(xing->target[t] >= 0.0) || !(xing->target[t] < 2.0 * ffa::PI)) return FFA_ERR_INVALID;
+        p.xing = *xing;
+    }
     cudaError_t e;
     if (flags & FFA_RK4) e = launch_rk4_f64(p, as_stream(stream));
     else if (flags & FFA_FP32C) e = launch_boris_f32c(p, as_stream(stream));
     else e = launch_boris_f64(p, as_stream(stream));
     return e == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
+}
+
+int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
+             const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps, double dt,
+             int32_t sc_step, int32_t flags, void *stream, int64_t *status)
+{
+    return push_impl(fm, rf, ap, cs, tab, st, n, step0, nsteps, dt, sc_step, flags, stream, status, nullptr);
+}
+
+int ffa_push_crossing(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
+                      const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps,
+                      double dt, int32_t sc_step, int32_t flags, void *stream, int64_t *status,
+                      const ffa_crossing *xing)
+{
+    if (!xing) return FFA_ERR_INVALID;
+    return push_impl(fm, rf, ap, cs, tab, st, n, step0, nsteps, dt, sc_step, flags, stream, status, xing);
 }
 
 int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream)

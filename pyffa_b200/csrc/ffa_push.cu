@@ -208,6 +208,52 @@ __device__ __forceinline__ void status_add(int64_t *status, int lost, int bad, i
     }
 }
 
+// Azimuth-crossing test of detect_azimuth_crossing (src/FFAG_MathTools.py:
+// 1633-1695) on the step's pre / post azimuth, and the record append.  The
+// reductions mod 2 pi are a - 2 pi floor(a / 2 pi) with no fused multiply-add,
+// as in fast_mod_parallel (src/FFAG_MathTools.py:1554-1557); the target comes
+// targets come in already reduced to [0, 2 pi).
+__device__ __forceinline__ double mod_2pi(double a)
+{
+    const double tw = 2.0 * PI;
+    return __dsub_rn(a, __dmul_rn(tw, floor(a / tw)));
+}
+
+__device__ __forceinline__ void xing_check(const ffa_crossing &xc, int64_t i, int64_t gs, const double pre[7],
+                                           const double post[7], int surv_after, int inj, double esr, double esz,
+                                           double esf)
+{
+    const double tw = 2.0 * PI;
+    const double a = mod_2pi(pre[4]), b = mod_2pi(post[4]);
+    for (int t = 0; t < xc.ntargets; ++t) {
+        const double target = xc.target[t];
+        bool hit;
+        double ratio = 0.0;
+        if (b >= a) {
+            hit = a <= target && target <= b;
+            if (hit && b - a > 1e-12) ratio = (target - a) / (b - a);
+        } else {
+            hit = (target >= a && target < tw) || (target >= 0 && target <= b);
+            if (hit) {
+                const double span = (b + tw) - a;
+                if (span > 1e-12) ratio = ((target <= b ? target + tw : target) - a) / span;
+            }
+        }
+        if (!hit) continue;
+        const unsigned long long k = atomicAdd((unsigned long long *)xc.count, 1ull);
+        if ((int64_t)k >= xc.capacity) continue;
+        double *rec = xc.buf + (int64_t)k * FFA_CROSSING_RECORD;
+        rec[0] = (double)t;
+        rec[1] = (double)i;
+        rec[2] = (double)gs;
+        rec[3] = ratio;
+        for (int c = 0; c < 7; ++c) { rec[4 + c] = pre[c]; rec[11 + c] = post[c]; }
+        rec[18] = (double)surv_after;
+        rec[19] = (double)inj;
+        rec[20] = esr; rec[21] = esz; rec[22] = esf;
+    }
+}
+
 // Linear extrapolation of the space-charge field between updates
 // (src/FFAG_track.py:449-478).
 struct SCExtrap {
@@ -242,7 +288,7 @@ struct SCExtrap {
 // so a 1e5-particle bunch is resident in one wave on 148 SMs.
 constexpr int BORIS_TB = 32;
 
-template <int MAXO, bool SC>
+template <int MAXO, bool SC, bool XING>
 __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -268,6 +314,11 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
         if (injs == gs) { inj = 1; surv = 1; }
         if (SC) ex.apply(gs, p.sc_step, esr, esz, esf);
         const double drf = __ldg(p.drf + gs);
+        double pre[7];
+        const int surv0 = surv;
+        if constexpr (XING) {
+            pre[0] = r; pre[1] = rdot; pre[2] = z; pre[3] = zdot; pre[4] = fi; pre[5] = fidot; pre[6] = rfph;
+        }
         if ((inj == 1) && (surv == 1)) {
             const double acc = __ldg(p.acc + gs);
             const double fim = fi - f.period * floor(fi / f.period);
@@ -339,6 +390,12 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             r = rn;
         }
         rfph += drf;
+        if constexpr (XING) {
+            if (surv0 == 1) {
+                const double post[7] = {r, rdot, z, zdot, fi, fidot, rfph};
+                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+            }
+        }
     }
     S.r[i] = r; S.vr[i] = rdot; S.z[i] = z; S.vz[i] = zdot; S.fi[i] = fi; S.f5[i] = fidot;
     S.rf[i] = rfph;
@@ -387,7 +444,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     d.rf = rate;
 }
 
-template <int MAXO, bool SC>
+template <int MAXO, bool SC, bool XING>
 __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -410,8 +467,17 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
         const double k1rf = h * __ldg(rate + 0), k2rf = h * __ldg(rate + 1);
         const double k3rf = h * __ldg(rate + 2), k4rf = h * __ldg(rate + 3);
         const double drf = (k1rf + 2 * k2rf + 2 * k3rf + k4rf) / 6;
+        Y7 y0;
+        if constexpr (XING) y0 = y;
         if (!((inj == 1) && (surv == 1))) {
             y.rf += drf;
+            if constexpr (XING) {
+                if (surv == 1) {
+                    const double pre[7] = {y0.r, y0.vr, y0.z, y0.vz, y0.fi, y0.E, y0.rf};
+                    const double post[7] = {y.r, y.vr, y.z, y.vz, y.fi, y.E, y.rf};
+                    xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+                }
+            }
             continue;
         }
         Y7 d, k1, k2, k3, k4, ys;
@@ -435,6 +501,11 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
         y.fi += (k1.fi + 2 * k2.fi + 2 * k3.fi + k4.fi) / 6;
         y.E += (k1.E + 2 * k2.E + 2 * k3.E + k4.E) / 6;
         y.rf += (k1.rf + 2 * k2.rf + 2 * k3.rf + k4.rf) / 6;
+        if constexpr (XING) {
+            const double pre[7] = {y0.r, y0.vr, y0.z, y0.vz, y0.fi, y0.E, y0.rf};
+            const double post[7] = {y.r, y.vr, y.z, y.vz, y.fi, y.E, y.rf};
+            xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+        }
     }
     S.r[i] = y.r; S.vr[i] = y.vr; S.z[i] = y.z; S.vz[i] = y.vz; S.fi[i] = y.fi; S.f5[i] = y.E;
     S.rf[i] = y.rf;
@@ -442,6 +513,246 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
     S.inj[i] = (uint8_t)inj;
     S.surv[i] = (uint8_t)surv;
     status_add(p.status, 0, !(isfinite(y.r) && isfinite(y.fi) && isfinite(y.z)), oob);
+}
+
+// ---------------------------------------------------- Boris, compensated fp32
+//
+// The float64 kernel spends most of its time in float64 transcendentals.  This
+// variant evaluates the field and forms the Boris increments in float32, and
+// keeps in float64 only what accumulates over many steps: the position
+// (r, fi, z), the momentum per unit mass u = gamma v in the local frame, the
+// RF phase, and the frame rotation of u after each step.  Float32 errors then
+// enter as small pseudo-random relative errors of per-step increments rather
+// than of the state:
+//  - field: accurately rounded expf / log1pf (no fast intrinsics); each
+//    sigmoid argument k (fi - x0) is formed in float64 before rounding, and
+//    r^(k-1) = r_ref^(k-1) (1 + eps)^(k-1) with eps formed in float64;
+//  - Boris: the electric half kicks and the magnetic rotation increment are
+//    float32; |u| is renormalised in float64 after the rotation, so the
+//    magnetic push conserves energy to float64 rounding;
+//  - 1/gamma for the drift, the azimuth change and the frame rotation are
+//    float64 (series in the small per-step angle).
+// Particles that are skipped take the same float64 Cartesian round trip as the
+// float64 kernel.
+
+template <int MAXO>
+__device__ __forceinline__ void field_b32(const FieldK &f, double r, double fim, float zf, float &Bz, float &Br,
+                                          float &Bfi, int &clamped)
+{
+    double spiral = 0.0, spiral_p = 0.0;
+    if (!f.spiral_zero) {
+        for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * r + f.spoly[a];
+        for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * r + f.spolyp[a];
+    }
+    float B0r, B0r_p;
+    const float rf = (float)r;
+    if (f.k == 0.0) {
+        B0r = (float)f.B0;
+        B0r_p = 0.0f;
+    } else {
+        const float eps = (float)((r - f.r_ref) * f.inv_r_ref);
+        const float g = expf(f.km1f * log1pf(eps));   // ((r / r_ref))^(k-1)
+        B0r_p = f.kc1f * g;
+        B0r = f.c1f * g * rf;
+    }
+    double fs = fim - spiral;
+    fs -= f.period * floor(fs / f.period);
+    float F = 0.0f, Fp = 0.0f;
+    for (int j = 0; j < f.n_seg; ++j) {
+        const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
+        const float a2 = (float)(f.seg_k[j] * (fs - f.seg_x1[j]));
+        const float e1 = expf(-a1), e2 = expf(a2);
+        const float s1 = __frcp_rn(1.0f + e1);
+        const float s2 = __frcp_rn(1.0f + e2);
+        // 1 - s = e s exactly: no cancellation when the sigmoid saturates
+        const float c1 = e1 * s1, c2 = e2 * s2;
+        const float ks = f.seg_kf[j], y = f.seg_yf[j];
+        F += y * s1 * s2;
+        Fp += y * (ks * s1 * c1 * s2 - s1 * ks * s2 * c2);
+    }
+    Bz = B0r * F;
+    Bfi = B0r * Fp * __frcp_rn(rf) * zf;
+    Br = (B0r_p * F - B0r * Fp * (float)spiral_p) * zf;
+    if constexpr (MAXO >= 1) {
+        const double qx = (r - f.r_min) * f.inv_r_step;
+        const double qy = (fim - f.fi_min) * f.inv_fi_step;
+        int64_t i = (int64_t)qx, jj = (int64_t)qy;
+        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
+        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
+        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
+        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
+        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
+        constexpr int NV = 3 * MAXO;
+        const float *nd[4];
+        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
+        nd[1] = nd[0] + NP;
+        nd[2] = nd[0] + f.fi_size * NP;
+        nd[3] = nd[2] + NP;
+        float acc[NV];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int a = 0; a < NV; a += 4) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+            }
+        }
+        const float z2 = zf * zf;
+        float ze = z2, zo = z2 * zf;
+#pragma unroll
+        for (int n = 0; n < MAXO; ++n) {
+            Bz += acc[3 * n] * ze;
+            Bfi += acc[3 * n + 1] * zo;
+            Br += acc[3 * n + 2] * zo;
+            ze *= z2;
+            zo *= z2;
+        }
+    }
+}
+
+template <int MAXO, bool SC, bool XING>
+__global__ void __launch_bounds__(128) boris_f32c_kernel(const PushK p)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const FieldK &f = p.f;
+    const ffa_state_soa &S = p.st;
+    double r = S.r[i], rdot = S.vr[i], z = S.z[i], zdot = S.vz[i], fi = S.fi[i], fidot = S.f5[i];
+    double rfph = S.rf[i];
+    double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
+    int inj = S.inj[i], surv = S.surv[i];
+    const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
+    SCExtrap ex;
+    if (SC) ex.load(S, i);
+    const double q = p.cs.q, c = p.cs.c, m = p.cs.m0, dt = p.dt;
+    const double inv_cc = 1.0 / (c * c);
+    const double hkd = 0.5 * dt * q / m;         // u kick per unit field: (q / m) dt / 2
+    const float hk = (float)hkd;
+    double ur = 0, uf = 0, uz = 0;                 // u = gamma v, local frame
+    bool umode = false;                            // u holds the velocity state
+    int lost = 0, oob = 0;
+
+    for (int s = 0; s < p.nsteps; ++s) {
+        const int64_t gs = p.step0 + s;
+        if (injs == gs) { inj = 1; surv = 1; }
+        if (SC) ex.apply(gs, p.sc_step, esr, esz, esf);
+        const double drf = __ldg(p.drf + gs);
+        const bool alive = (inj == 1) && (surv == 1);
+        if (alive && !umode) {
+            const double vf = r * fidot;
+            const double g = rsqrt(1.0 - (rdot * rdot + vf * vf + zdot * zdot) * inv_cc);
+            ur = g * rdot; uf = g * vf; uz = g * zdot;
+            umode = true;
+        } else if (!alive && umode) {
+            const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
+            rdot = ur * ig; zdot = uz * ig; fidot = uf * ig / r;
+            umode = false;
+        }
+        double pre[7];
+        const int surv0 = surv;
+        if constexpr (XING) {
+            if (surv0 == 1) {
+                pre[0] = r; pre[2] = z; pre[4] = fi; pre[6] = rfph;
+                if (alive) {
+                    const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
+                    pre[1] = ur * ig; pre[3] = uz * ig; pre[5] = uf * ig / r;
+                } else {
+                    pre[1] = rdot; pre[3] = zdot; pre[5] = fidot;
+                }
+            }
+        }
+        if (alive) {
+            const double acc = __ldg(p.acc + gs);
+            const double fim = fi - f.period * floor(fi / f.period);
+            float Bz, Br, Bfi;
+            field_b32<MAXO>(f, r, fim, (float)z, Bz, Br, Bfi, oob);
+            double Er64, Efi64;
+            rf_field64(p.rf, acc, r, fi, rfph, Er64, Efi64);
+            const float Er = (float)(Er64 + esr), Efi = (float)(Efi64 + esf), Ez = (float)esz;
+            if (p.ap.enable && (r > p.ap.rmax || r < p.ap.rmin || z > p.ap.zmax || z < p.ap.zmin)) {
+                surv = 0;
+                ++lost;
+            }
+            // half electric kick (float32 increment, float64 state)
+            const float d1x = hk * Er, d1y = hk * Efi, d1z = hk * Ez;
+            const double mx = ur + d1x, my = uf + d1y, mz = uz + d1z;
+            const float fx = (float)mx, fy = (float)my, fz = (float)mz;
+            // magnetic rotation: increment in float32, |u| restored in float64
+            // q dt / (2 m gamma) from the float64 |u|: a float32 gamma would
+            // bias every step's bend by its rounding
+            const double nm = mx * mx + my * my + mz * mz;
+            const float cb = (float)(hkd * rsqrt(1.0 + nm * inv_cc));
+            const float tx = -cb * Br, ty = -cb * Bfi, tz = -cb * Bz;
+            const float pxp = fx + (fy * tz - fz * ty);
+            const float pyp = fy + (fz * tx - fx * tz);
+            const float pzp = fz + (fx * ty - fy * tx);
+            const float sb = 2.0f * __frcp_rn(1.0f + (tx * tx + ty * ty + tz * tz));
+            const float sx = sb * tx, sy = sb * ty, sz = sb * tz;
+            double px = mx + (double)(pyp * sz - pzp * sy);
+            double py = my + (double)(pzp * sx - pxp * sz);
+            double pz = mz + (double)(pxp * sy - pyp * sx);
+            const double np = px * px + py * py + pz * pz;
+            const double sc = 1.0 + 0.5 * (double)((float)(nm - np) * __frcp_rn((float)np));
+            px = px * sc + d1x;
+            py = py * sc + d1y;
+            pz = pz * sc + d1z;
+            // drift with 1/gamma in float64
+            const double ig = rsqrt(1.0 + (px * px + py * py + pz * pz) * inv_cc);
+            const double dxr = px * ig * dt, yn = py * ig * dt;
+            z = z + pz * ig * dt;
+            const double xr = r + dxr;
+            double ix = (double)__frcp_rn((float)xr);
+            ix = ix * (2.0 - xr * ix);
+            ix = ix * (2.0 - xr * ix);
+            const double tn = yn * ix;                // tan of the azimuth change
+            const float tf = (float)tn, t2f = tf * tf;
+            const double dfi = tn + (double)(tf * t2f * (-1.0f / 3 + t2f * (0.2f - t2f * (1.0f / 7))));
+            r = xr + (double)((float)xr * (t2f * (0.5f - t2f * (0.125f - t2f * 0.0625f))));
+            fi = fi + dfi;
+            // rotate u into the new local frame
+            const double d2 = dfi * dfi;
+            const double sn = dfi * (1.0 - d2 * (1.0 / 6 - d2 * (1.0 / 120)));
+            const double cm1 = -d2 * (0.5 - d2 * (1.0 / 24 - d2 * (1.0 / 720)));
+            ur = px + (px * cm1 + py * sn);
+            uf = py + (py * cm1 - px * sn);
+            uz = pz;
+        } else {
+            double sinFi, cosFi;
+            sincos(fi, &sinFi, &cosFi);
+            const double x = r * cosFi, y = r * sinFi;
+            const double vx = rdot * cosFi - r * fidot * sinFi;
+            const double vy = rdot * sinFi + r * fidot * cosFi;
+            const double rn = sqrt(x * x + y * y);
+            rdot = vx * cosFi + vy * sinFi;
+            const double vfi = -vx * sinFi + vy * cosFi;
+            fidot = rn > 1e-12 ? vfi / rn : 0.0;
+            r = rn;
+        }
+        rfph += drf;
+        if constexpr (XING) {
+            if (surv0 == 1) {
+                double post[7] = {r, rdot, z, zdot, fi, fidot, rfph};
+                if (alive) {
+                    const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
+                    post[1] = ur * ig; post[3] = uz * ig; post[5] = uf * ig / r;
+                }
+                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+            }
+        }
+    }
+    if (umode) {
+        const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
+        rdot = ur * ig; zdot = uz * ig; fidot = uf * ig / r;
+    }
+    S.r[i] = r; S.vr[i] = rdot; S.z[i] = z; S.vz[i] = zdot; S.fi[i] = fi; S.f5[i] = fidot;
+    S.rf[i] = rfph;
+    S.esc_r[i] = esr; S.esc_z[i] = esz; S.esc_fi[i] = esf;
+    S.inj[i] = (uint8_t)inj;
+    S.surv[i] = (uint8_t)surv;
+    status_add(p.status, lost, !(isfinite(r) && isfinite(fi) && isfinite(z)), oob);
 }
 
 // ------------------------------------------------------------ node packing
@@ -477,14 +788,16 @@ template <int MAXO, bool SC>
 static void boris_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = BORIS_TB;
-    boris_f64_kernel<MAXO, SC><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    else boris_f64_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
 template <int MAXO, bool SC>
 static void rk4_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = 128;
-    rk4_f64_kernel<MAXO, SC><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    if (p.xing.buf) rk4_f64_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    else rk4_f64_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
 #define FFA_DISPATCH(FN, p, s)                                                   \
@@ -508,6 +821,20 @@ cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s)
 cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s)
 {
     FFA_DISPATCH(rk4_launch, p, s);
+    return cudaGetLastError();
+}
+
+template <int MAXO, bool SC>
+static void boris32_launch(const PushK &p, cudaStream_t s)
+{
+    const int tb = 128;
+    if (p.xing.buf) boris_f32c_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    else boris_f32c_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+}
+
+cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s)
+{
+    FFA_DISPATCH(boris32_launch, p, s);
     return cudaGetLastError();
 }
 

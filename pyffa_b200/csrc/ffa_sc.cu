@@ -183,13 +183,16 @@ __global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ff
     }
 }
 
-__global__ void sc_reduce1(const Partial1 *part, int nblk, ffa_sc_desc d, SCState *st)
+// One block of SC_TB threads: each thread folds a fixed strided subset of the
+// block partials, then a fixed-shape tree -- the same order on every run.
+__global__ void __launch_bounds__(SC_TB) sc_reduce1(const Partial1 *part, int nblk, ffa_sc_desc d, SCState *st)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double shd[32];
+    __shared__ long long shl[32];
     double sg = 0.0;
     long long cnt = 0;
     double mn[4] = {1e30, 1e30, 1e30, 1e30}, mx[4] = {-1e30, -1e30, -1e30, -1e30};
-    for (int b = 0; b < nblk; ++b) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         sg += part[b].sum_gamma;
         cnt += part[b].count;
         for (int k = 0; k < 4; ++k) {
@@ -197,6 +200,13 @@ __global__ void sc_reduce1(const Partial1 *part, int nblk, ffa_sc_desc d, SCStat
             mx[k] = fmax(mx[k], part[b].amax[k]);
         }
     }
+    sg = block_sum(sg, shd);
+    cnt = block_sum(cnt, shl);
+    for (int k = 0; k < 4; ++k) {
+        mn[k] = block_min(mn[k], shd);
+        mx[k] = block_max(mx[k], shd);
+    }
+    if (threadIdx.x != 0) return;
     const double shifts[4] = {0.0, PI, PI * 0.5, PI * 1.5};
     int best = 0;
     double best_span = mx[0] - mn[0];
@@ -239,13 +249,19 @@ __global__ void __launch_bounds__(SC_TB) sc_pass2(ffa_state_soa S, int64_t n, ff
     if (threadIdx.x == 0) part[blockIdx.x] = Partial2{a, b, c, e};
 }
 
-__global__ void sc_reduce2(const Partial2 *part, int nblk, ffa_sc_desc d, SCState *st, int64_t *status)
+__global__ void __launch_bounds__(SC_TB) sc_reduce2(const Partial2 *part, int nblk, ffa_sc_desc d, SCState *st,
+                                                    int64_t *status)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double shd[32];
     double sx = 0, sz = 0, sx2 = 0, sz2 = 0;
-    for (int b = 0; b < nblk; ++b) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         sx += part[b].sx; sz += part[b].sz; sx2 += part[b].sx2; sz2 += part[b].sz2;
     }
+    sx = block_sum(sx, shd);
+    sz = block_sum(sz, shd);
+    sx2 = block_sum(sx2, shd);
+    sz2 = block_sum(sz2, shd);
+    if (threadIdx.x != 0) return;
     ffa_sc_diag &D = st->diag;
     const long long cnt = D.count;
     double mx = 0, mz = 0, sgx = 0, sgz = 0;
@@ -734,9 +750,9 @@ int ffa_sc_step(ffa_sc_plan *p, ffa_state_soa *S, int64_t n, int32_t roll, int32
     const unsigned ew = 148 * 8;  // elementwise grids
     FFA_CHECK_CUDA(cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * cube, s));
     sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->pr0, p->slice, p->cell, p->p1);
-    sc_reduce1<<<1, 32, 0, s>>>(p->p1, SC_BLOCKS, d, p->st);
+    sc_reduce1<<<1, SC_TB, 0, s>>>(p->p1, SC_BLOCKS, d, p->st);
     sc_pass2<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->slice, p->st, p->p2);
-    sc_reduce2<<<1, 32, 0, s>>>(p->p2, SC_BLOCKS, d, p->st, status);
+    sc_reduce2<<<1, SC_TB, 0, s>>>(p->p2, SC_BLOCKS, d, p->st, status);
     sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->slice, p->cell, p->st, p->acc);
     sc_convert<<<ew, 256, 0, s>>>(p->acc, d, p->st, p->rho, p->work, p->NZ, p->NX);
     FFA_CHECK_CUDA(cudaGetLastError());
@@ -906,9 +922,9 @@ extern "C" int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *S, int
     const unsigned ew = 148 * 8;
     FFA_CHECK_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * cube, s));
     sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, pr0, slice, cell, p1);
-    sc_reduce1<<<1, 32, 0, s>>>(p1, SC_BLOCKS, d, st);
+    sc_reduce1<<<1, SC_TB, 0, s>>>(p1, SC_BLOCKS, d, st);
     sc_pass2<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, st, p2);
-    sc_reduce2<<<1, 32, 0, s>>>(p2, SC_BLOCKS, d, st, status);
+    sc_reduce2<<<1, SC_TB, 0, s>>>(p2, SC_BLOCKS, d, st, status);
     sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, cell, st, acc);
     sc_convert<<<ew, 256, 0, s>>>(acc, d, st, rho, work, d.nz, d.nx);
     FFA_CHECK_CUDA(cudaGetLastError());

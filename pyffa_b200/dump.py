@@ -6,6 +6,15 @@ per dump time with key ``particles`` = p-format N x 16 matrix of the
 (optionally surviving) particles plus the dump time as column 17, appended
 to an existing file (append_to_npz, src/FFAG_dump.py:1428-1448).  The file
 is what main_track reads back with ``-r`` (examples/main_track.py:92-111).
+
+PositionDumpBunch writes the azimuth-crossing file of the reference
+(src/FFAG_dump.py:789-1130): every post-step row of a particle that crossed
+the target azimuth in a step ending inside (start_time, end_time), saved once
+the tracking time passes end_time as
+``crossing_angle_{deg:.1f}_start_{t0_ns:.3f}_end_{t1_ns:.3f}_rank_{r}.npz``
+(key ``particles``: p-format N x 16 rows with the RF phase reduced mod 2 pi,
+plus the step's end time as column 17).  The crossing test itself runs in the
+push kernels (ffa_push_crossing); this class holds the rows and writes them.
 """
 from __future__ import annotations
 
@@ -67,6 +76,65 @@ class StepDumpBunch:
         append_to_npz(fn, np.hstack((p, np.full((p.shape[0], 1), time_Post))))
 
 
+class PositionDumpBunch:
+    def __init__(self, target_azimuth_angle_deg, start_time, end_time, save_folder="dump_data", rank=0,
+                 allow_existing=False):
+        self.target_azimuth_angle = np.deg2rad(target_azimuth_angle_deg) % (2 * np.pi)
+        self.save_folder = save_folder
+        self.start_time = start_time
+        self.end_time = end_time
+        self.save_flag = False
+        self.rank = rank
+        self._rows = []
+        self.write_cursor = 0
+        if rank == 0:
+            if not os.path.exists(save_folder):
+                os.makedirs(save_folder)
+            elif os.listdir(save_folder) and not allow_existing:
+                # the reference aborts every rank here (src/FFAG_dump.py:812-822)
+                sys.stderr.write(f"Error: dump folder {save_folder} exists and is not empty\n")
+                raise SystemExit(1)
+
+    def in_window(self, t_post: np.ndarray) -> np.ndarray:
+        """Steps whose crossings are recorded (src/FFAG_dump.py:1107)."""
+        return (t_post < self.end_time) & (t_post > self.start_time)
+
+    def add_particles(self, particle_data, time_i):
+        """Appends v-format rows with the time column (src/FFAG_dump.py:965-993);
+        time_i may be one value or one per row."""
+        particle_data = np.asarray(particle_data, dtype=np.float64)
+        t = np.broadcast_to(np.asarray(time_i, dtype=np.float64), (particle_data.shape[0],))
+        self._rows.append(np.hstack((particle_data, t[:, None])))
+        self.write_cursor += particle_data.shape[0]
+
+    @property
+    def saved_data(self) -> np.ndarray:
+        if len(self._rows) > 1:
+            self._rows = [np.vstack(self._rows)]
+        return self._rows[0] if self._rows else np.zeros((0, 17))
+
+    def file_name(self) -> str:
+        return (f"crossing_angle_{np.rad2deg(self.target_azimuth_angle):.1f}_start_{self.start_time * 1e9:.3f}"
+                f"_end_{self.end_time * 1e9:.3f}_rank_{self.rank}.npz")
+
+    def save_all_particles(self, data_type):
+        """src/FFAG_dump.py:996-1026 (writes even when no particle crossed)."""
+        data = self.saved_data
+        conv = FFAG_ConversionTools()
+        if data_type == "RK4":
+            p = conv.ConvertVrzek2Przek(data[:, :-1])
+        elif data_type == "Boris":
+            p = conv.ConvertVrzek2Przek_boris(data[:, :-1])
+        else:
+            raise ValueError("data_type must be RK4 or Boris")
+        p[:, 9] = np.mod(p[:, 9], 2 * np.pi)
+        np.savez(os.path.join(self.save_folder, self.file_name()), particles=np.hstack((p, data[:, [-1]])))
+
+    def check_and_dump(self, time_Pre, time_Post, bunch_obj, data_type):
+        raise NotImplementedError("the azimuth-crossing test runs inside the push kernels; track with "
+                                  "FFAG_RungeKutta's loops, which feed this dump")
+
+
 class Dumps:
     """Registry of dump instances (src/FFAG_dump.py:1255-1284)."""
 
@@ -78,6 +146,9 @@ class Dumps:
 
     def step_dumps(self):
         return [d for d in self.dumps if isinstance(d, StepDumpBunch)]
+
+    def position_dumps(self):
+        return [d for d in self.dumps if isinstance(d, PositionDumpBunch)]
 
     def check_and_dump(self, time_Pre, time_Post, bunch_obj, data_type="RK4"):
         for d in self.dumps:

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from .bunch import FFAG_Bunch
-from .constants import FFAG_ConversionTools, FFAG_GlobalParameters
+from .constants import C_LIGHT, COLUMNS, FFAG_ConversionTools, FFAG_GlobalParameters
 
 TABLE_CHUNK = 1 << 16
 
@@ -124,13 +124,85 @@ class Pusher:
             self.flags |= _lib.FFA_RF_PHYSICAL_SUM
         self.stream = torch.cuda.current_stream(bunch.device)
 
-    def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0) -> None:
+    def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0, xing=None) -> None:
         L = _lib.lib()
         b = self.bunch
-        rc = L.ffa_push(self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
-                        ctypes.byref(clock.table), ctypes.byref(b.soa()), b.n, step0, nsteps, clock.dt,
-                        sc_step, self.flags, self.stream.cuda_stream, b.status.data_ptr())
-        _lib.check(rc, "ffa_push")
+        args = (self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
+                ctypes.byref(clock.table), ctypes.byref(b.soa()), b.n, step0, nsteps, clock.dt,
+                sc_step, self.flags, self.stream.cuda_stream, b.status.data_ptr())
+        if xing is None:
+            _lib.check(L.ffa_push(*args), "ffa_push")
+        else:
+            _lib.check(L.ffa_push_crossing(*args, ctypes.byref(xing)), "ffa_push_crossing")
+
+
+class CrossingCapture:
+    """Device buffers of the azimuth-crossing records for a set of target
+    azimuths, and their conversion to the post-step rows the reference's
+    PositionDumpBunch appends (src/FFAG_dump.py:1098-1130).
+
+    A launch of `nsteps` steps can see a particle cross one target at most
+    1 + nsteps * dt * f_max / (2 pi) times, with f_max = c / r_low the
+    fastest angular velocity inside the aperture (or the field map); the
+    capacity is sized from that bound and an overflow raises."""
+
+    def __init__(self, bunch: FFAG_Bunch, targets, gp, dt: float):
+        import torch
+        if not 1 <= len(targets) <= _lib.MAX_CROSSING_TARGETS:
+            raise ValueError(f"1 to {_lib.MAX_CROSSING_TARGETS} crossing targets per bunch")
+        self.bunch = bunch
+        self.dt = dt
+        self.x = _lib.Crossing()
+        self.x.ntargets = len(targets)
+        for k, t in enumerate(targets):
+            self.x.target[k] = float(t) % (2 * np.pi)
+        r_low = gp.Aperture_m[0] if getattr(gp, "Aperture_enable", False) else gp.Bmap.r_min
+        self.f_max = C_LIGHT / max(float(r_low), 1e-3)
+        self.count = torch.zeros(1, dtype=torch.int64, device=bunch.device)
+        self.buf = torch.empty(0, dtype=torch.float64, device=bunch.device)
+
+    def max_steps(self) -> int:
+        """Longest launch whose bound stays at 5 records per particle and target."""
+        return max(1, int(3 * 2 * np.pi / (self.dt * self.f_max)))
+
+    def prepare(self, nsteps: int):
+        import torch
+        per = 2 + int(np.ceil(nsteps * self.dt * self.f_max / (2 * np.pi)))
+        cap = self.bunch.n * self.x.ntargets * per
+        if self.buf.numel() < cap * _lib.CROSSING_RECORD:
+            self.buf = torch.empty(cap * _lib.CROSSING_RECORD, dtype=torch.float64, device=self.bunch.device)
+        self.count.zero_()
+        self.x.buf = self.buf.data_ptr()
+        self.x.capacity = cap
+        self.x.count = self.count.data_ptr()
+        return self.x
+
+    def records(self) -> np.ndarray:
+        """The launch's records, sorted by (target, step, particle)."""
+        k = int(self.count.item())
+        if k > self.x.capacity:
+            raise RuntimeError(f"crossing records overflowed: {k} > {self.x.capacity}")
+        rec = self.buf[:k * _lib.CROSSING_RECORD].view(k, _lib.CROSSING_RECORD).cpu().numpy()
+        return rec[np.lexsort((rec[:, 1], rec[:, 2], rec[:, 0]))]
+
+    def rows(self, rec: np.ndarray) -> np.ndarray:
+        return crossing_rows(rec, self.bunch._host_static)
+
+
+def crossing_rows(rec: np.ndarray, host_static: np.ndarray) -> np.ndarray:
+    """Post-step v-format rows (N x 16) of crossing records: the LocalBunch
+    rows PositionDumpBunch.check_and_dump selects (src/FFAG_dump.py:1120);
+    injection time and the ID columns come from the bunch's host matrix."""
+    idx = rec[:, 1].astype(np.int64)
+    out = np.zeros((rec.shape[0], 16))
+    out[:, 0:6] = rec[:, 11:17]
+    out[:, 6] = host_static[idx, COLUMNS["inj_t"]]
+    out[:, 7] = rec[:, 19]
+    out[:, 8] = rec[:, 18]
+    out[:, 9] = rec[:, 17]
+    out[:, 10:13] = rec[:, 20:23]
+    out[:, 13:16] = host_static[idx, 13:16]
+    return out
 
 
 class StepDumpSchedule:
@@ -208,9 +280,8 @@ class FFAG_RungeKutta:
             from .space_charge import SpaceCharge
             sc = SpaceCharge(b, hockney=bool(lp.get("SC_hockney", False)))
         dump_sched = [StepDumpSchedule(d) for d in (dumps.step_dumps() if dumps is not None else [])]
-        if self.precision == "fp32c":
-            _lib.check(_lib.lib().ffa_fp32c_split(ctypes.byref(b.soa()), b.n, pusher.stream.cuda_stream),
-                       "ffa_fp32c_split")
+        pos_dumps = dumps.position_dumps() if dumps is not None else []
+        xcap = CrossingCapture(b, [d.target_azimuth_angle for d in pos_dumps], gp, dt) if pos_dumps else None
 
         steps_i = 0
         sched_end = 0
@@ -242,8 +313,26 @@ class FFAG_RungeKutta:
                     dump_at = cand if dump_at is None else min(dump_at, cand)
             if dump_at is not None:
                 end = dump_at + 1
-            pusher.push(clock, steps_i, end - steps_i, SC_step if enable_sc else 0)
+            t_chunk = clock.t[steps_i + 1:end + 1]
+            capture = xcap is not None and any(not d.save_flag and d.in_window(t_chunk).any() for d in pos_dumps)
+            if capture and end - steps_i > xcap.max_steps():
+                end = steps_i + xcap.max_steps()
+                t_chunk = clock.t[steps_i + 1:end + 1]
+            pusher.push(clock, steps_i, end - steps_i, SC_step if enable_sc else 0,
+                        xcap.prepare(end - steps_i) if capture else None)
             n_launch += 1
+            if capture:
+                rec = xcap.records()
+                for k, d in enumerate(pos_dumps):
+                    r = rec[rec[:, 0] == k]
+                    tp = clock.t[r[:, 2].astype(np.int64) + 1]
+                    keep = d.in_window(tp) if not d.save_flag else np.zeros(len(r), bool)
+                    if keep.any():
+                        d.add_particles(xcap.rows(r[keep]), tp[keep])
+            for d in pos_dumps:
+                if not d.save_flag and (t_chunk > d.end_time).any():
+                    d.save_all_particles(solver)
+                    d.save_flag = True
             steps_i = end
             if dump_at is not None:
                 t_post = clock.t[steps_i]
@@ -270,9 +359,6 @@ class FFAG_RungeKutta:
                     break
                 if t_now > max_time:
                     break
-        if self.precision == "fp32c":
-            _lib.check(_lib.lib().ffa_fp32c_merge(ctypes.byref(b.soa()), b.n, pusher.stream.cuda_stream),
-                       "ffa_fp32c_merge")
         torch.cuda.synchronize(b.device)
         self.last_run = {"steps": steps_i, "t_end": float(clock.t[steps_i]), "launches": n_launch,
                          "wall_s": time.time() - t_wall, "status": b.status_counts()}
@@ -290,11 +376,7 @@ def single_step(mat, t, dt, gp, solver, precision="fp64"):
     clock = StepClock(t, dt, gp.Emap, solver, dev)
     clock.ensure(1)
     pusher = Pusher(b, gp, solver, precision)
-    if precision == "fp32c":
-        _lib.check(_lib.lib().ffa_fp32c_split(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_split")
     pusher.push(clock, 0, 1, 0)
-    if precision == "fp32c":
-        _lib.check(_lib.lib().ffa_fp32c_merge(ctypes.byref(b.soa()), n, pusher.stream.cuda_stream), "ffa_fp32c_merge")
     out = b.matrix()
     return out
 
@@ -315,8 +397,6 @@ class _EphemeralBunch:
                                                              "esc_r", "esc_z", "esc_fi")}
         self.cols["inj"] = torch.empty(self.n, dtype=torch.uint8, device=dev)
         self.cols["surv"] = torch.empty(self.n, dtype=torch.uint8, device=dev)
-        self.cols["r_lo"] = torch.zeros(self.n, dtype=torch.float32, device=dev)
-        self.cols["fi_lo"] = torch.zeros(self.n, dtype=torch.float32, device=dev)
         self.status = torch.zeros(_lib.STATUS_WORDS, dtype=torch.int64, device=dev)
         s = _lib.StateSoA()
         for name, _ in _lib.StateSoA._fields_:
@@ -365,11 +445,7 @@ class MatrixTracker:
         s = self.pusher.stream.cuda_stream
         b.aos.copy_(host_in, non_blocking=True)
         _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), s), "ffa_aos_to_soa")
-        if self.precision == "fp32c":
-            _lib.check(L.ffa_fp32c_split(ctypes.byref(b.soa()), b.n, s), "ffa_fp32c_split")
         self.pusher.push(self.clock, step0, nsteps, 0)
-        if self.precision == "fp32c":
-            _lib.check(L.ffa_fp32c_merge(ctypes.byref(b.soa()), b.n, s), "ffa_fp32c_merge")
         _lib.check(L.ffa_soa_to_aos(ctypes.byref(b.soa()), b.n, b.aos.data_ptr(), s), "ffa_soa_to_aos")
         host_out.copy_(b.aos, non_blocking=True)
-        self.launches += 3 + (2 if self.precision == "fp32c" else 0)
+        self.launches += 3

@@ -217,5 +217,69 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def crossing_main(ref):
+    """Azimuth-crossing dumps: the reference's Boris and RK4 loops with
+    PositionDumpBunch instances registered, and the files they write
+    (golden_crossing.npz)."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    import FFAG_track
+    from FFAG_Bunch import FFAG_Bunch
+    from FFAG_dump import Dumps, PositionDumpBunch
+    from FFAG_ParasAndConversion import FFAG_ConversionTools
+
+    conv = FFAG_ConversionTools()
+    out = {}
+    aperture = (8.02, 8.48, -0.006, 0.006)
+    dt = synthetic.design_dt(300.0, 720)
+    t_start = -0.5 * dt
+    # (solver, steps, [(target deg, start, end)]); the last Boris window ends
+    # after the run, so the reference never writes that file
+    cases = {
+        "xb": ("Boris", 300, [(40.0, t_start, t_start + 280 * dt), (100.3, t_start + 50 * dt, t_start + 290 * dt),
+                              (7.0, t_start, t_start + 400 * dt)]),
+        "xr": ("RK4", 150, [(20.0, t_start, t_start + 140 * dt)]),
+    }
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg_path, emap_path = build_inputs(tmp)
+        for key, (solver, nsteps, windows) in cases.items():
+            gp = ref_objects(cfg_path, emap_path, aperture)
+            p = p_bunch(64, seed=29, inj_spread_ns=4 * dt * 1e9)
+            v = conv.ConvertPrzek2Vrzek_boris(p) if solver == "Boris" else conv.ConvertPrzek2Vrzek(p)
+            v[:, 9] = 0.3
+            v[:, 15] = np.arange(v.shape[0])
+            b = FFAG_Bunch(v.copy(), BunchType=solver)
+            dumps = Dumps()
+            folders = []
+            for k, (deg, t0, t1) in enumerate(windows):
+                folders.append(os.path.join(tmp, f"{key}_{k}"))
+                dumps.add_dump(PositionDumpBunch(deg, t0, t1, save_folder=folders[-1]))
+            lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9},
+                  "time_step": dt, "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": dumps}
+            out[f"{key}_in"] = b.LocalBunch.copy()
+            if solver == "Boris":
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC_boris(None, t_start, b, gp, lp)
+            else:
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC(FFAG_track.FunctionForAccelerationBunch_dt,
+                                                                       t_start, b, gp, lp)
+            out[f"{key}_out"] = b.LocalBunch.copy()
+            out[f"{key}_t"] = np.array([t_start, dt, nsteps])
+            out[f"{key}_windows"] = np.array(windows, dtype=np.float64)
+            for k, folder in enumerate(folders):
+                files = sorted(os.listdir(folder))
+                assert len(files) <= 1, files
+                if files:
+                    out[f"{key}_file{k}"] = np.frombuffer(files[0].encode(), dtype=np.uint8)
+                    out[f"{key}_dump{k}"] = np.load(os.path.join(folder, files[0]))["particles"]
+    path = os.path.join(HERE, "golden_crossing.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if "--crossing" in sys.argv:
+        sys.argv.remove("--crossing")
+        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
+        crossing_main(ref)
+    else:
+        main()
