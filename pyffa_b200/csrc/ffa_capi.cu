@@ -161,14 +161,9 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     k.inv_r_ref = 1.0 / k.r_ref;
     k.inv_r_step = d->r_step > 0 ? 1.0 / d->r_step : 0.0;
     k.inv_fi_step = d->fi_step > 0 ? 1.0 / d->fi_step : 0.0;
-    const double c1 = d->k == 0.0 ? d->B0 : d->B0 * pow(k.r_ref, d->k - 1.0);
-    k.c1f = (float)c1;
-    k.kc1f = (float)(d->k * c1);
-    k.km1f = (float)(d->k - 1.0);
-    for (int j = 0; j < d->n_convex; ++j) {
-        k.seg_kf[j] = (float)k.seg_k[j];
-        k.seg_yf[j] = (float)k.seg_y[j];
-    }
+    k.c1 = d->k == 0.0 ? d->B0 : d->B0 * pow(k.r_ref, d->k - 1.0);
+    k.kc1 = d->k * k.c1;
+    for (int j = 0; j < d->n_convex; ++j) k.seg_yk[j] = k.seg_y[j] * k.seg_k[j];
     if (d->max_order > 0) {
         const int64_t plane = d->r_size * d->fi_size;
         if (cudaMalloc(&fm->nodes64, sizeof(double) * plane * k.npad) != cudaSuccess) {

@@ -32,12 +32,12 @@ struct FieldK {
     int64_t r_size, fi_size;
     const double *nodes64;
     const float *nodes32;
-    // float32 path: B0 r^(k-1) = c1 * (1 + eps)^(k-1), eps = (r - r_ref) / r_ref
+    // float32 field: B0 r^(k-1) = c1 * (1 + eps)^(k-1), eps = (r - r_ref) / r_ref
     int32_t spiral_zero;          // s(r) == 0: skip the spiral polynomials
     int32_t pad1;
     double r_ref, inv_r_ref, inv_r_step, inv_fi_step;
-    float c1f, kc1f, km1f, pad2;  // B0 r_ref^(k-1), k * c1, k - 1
-    float seg_kf[FFA_MAX_SEG], seg_yf[FFA_MAX_SEG];
+    double c1, kc1;               // B0 r_ref^(k-1), k * c1
+    double seg_yk[FFA_MAX_SEG];   // seg_y * seg_k
 };
 
 struct RFK {

@@ -32,7 +32,7 @@ namespace ffa {
 
 // ----------------------------------------------------------- field (fp64)
 
-__device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double fim, double zi,
+__device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double ir, double fim, double zi,
                                              double &Bz, double &Br, double &Bfi)
 {
     double spiral = 0.0, spiral_p = 0.0;
@@ -64,7 +64,7 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0Fp += y * (s1p * s2 + s1 * s2p);
     }
     Bz = B0r * B0F;
-    Bfi = B0r * B0Fp / ri * zi;
+    Bfi = B0r * B0Fp * ir * zi;    // ir = 1 / ri to an ulp
     Br = (B0r_p * B0F - B0r * B0Fp * spiral_p) * zi;
 }
 
@@ -74,11 +74,12 @@ template <int MAXO>
 __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double y, double z,
                                                double &Bz, double &Bfi, double &Br, int &clamped)
 {
-    // the cell index uses the reference's division (bit-exact cell); the
-    // weights reuse the quotient (the reference recomputes it from the node
-    // coordinate, which differs by rounding only)
-    const double qx = (x - f.r_min) / f.r_step;
-    const double qy = (y - f.fi_min) / f.fi_step;
+    // cell index and weights from (x - x_min) times 1 / step: within an ulp
+    // of the reference's quotient; where that moves the index across a node
+    // line, the bilinear interpolant is continuous there, so the field
+    // changes by rounding only
+    const double qx = (x - f.r_min) * f.inv_r_step;
+    const double qy = (y - f.fi_min) * f.inv_fi_step;
     int64_t i = (int64_t)qx;
     int64_t j = (int64_t)qy;
     if (i < 0) { i = 0; ++clamped; }
@@ -282,14 +283,110 @@ struct SCExtrap {
     }
 };
 
+// ------------------------------------------------- field, float32 kernels
+//
+// The FP32C Boris pusher spends float32 arithmetic only where float64 is
+// expensive: the exponentials of the fringe sigmoids and of the power law
+// (expf / log1pf, accurately rounded library functions) and the bilinear
+// lookup of the z-Taylor nodes (float32 table).  The constants these values
+// are combined with, the products with r and z, and the whole Boris push stay
+// float64, so float32 rounding enters the field as an error of relative size
+// ~1e-7 that changes from step to step, never as a fixed scale error of the
+// bending (a fixed bias of the bending shifts the revolution time and, with
+// the RF on, the synchronous phase).
+template <int MAXO>
+__device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir, double fim, double z,
+                                            double &Bz, double &Br, double &Bfi, int &clamped)
+{
+    double spiral = 0.0, spiral_p = 0.0;
+    if (!f.spiral_zero) {
+        for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * r + f.spoly[a];
+        for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * r + f.spolyp[a];
+    }
+    double B0r, B0r_p;
+    if (f.k == 0.0) {
+        B0r = f.B0;
+        B0r_p = 0.0;
+    } else {
+        // (r / r_ref)^(k-1) with r / r_ref = 1 + eps, eps formed in float64
+        const float eps = (float)((r - f.r_ref) * f.inv_r_ref);
+        const double g = (double)expf((float)(f.km1 * (double)log1pf(eps)));
+        B0r_p = f.kc1 * g;
+        B0r = f.c1 * g * r;
+    }
+    double fs = fim - spiral;
+    fs -= f.period * floor(fs / f.period);
+    double F = 0.0, Fp = 0.0;
+    for (int j = 0; j < f.n_seg; ++j) {
+        const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
+        const float a2 = (float)(f.seg_k[j] * (fs - f.seg_x1[j]));
+        // exponents capped at 80 so e stays finite: past it s < 2e-35, which
+        // is 0 in every sum below, and e * s would otherwise be inf * 0
+        const float e1 = expf(fminf(-a1, 80.0f)), e2 = expf(fminf(a2, 80.0f));
+        const float s1 = __frcp_rn(1.0f + e1), s2 = __frcp_rn(1.0f + e2);
+        const float ss = s1 * s2;
+        // s1' s2 + s1 s2' = k s1 s2 ((1 - s1) - (1 - s2)) with 1 - s = e s:
+        // no cancellation where a sigmoid saturates
+        const float dd = e1 * s1 - e2 * s2;
+        F += f.seg_y[j] * (double)ss;
+        Fp += f.seg_yk[j] * (double)(ss * dd);
+    }
+    Bz = B0r * F;
+    Bfi = B0r * Fp * ir * z;
+    Br = (B0r_p * F - B0r * Fp * spiral_p) * z;
+    if constexpr (MAXO >= 1) {
+        const double qx = (r - f.r_min) * f.inv_r_step;
+        const double qy = (fim - f.fi_min) * f.inv_fi_step;
+        int64_t i = (int64_t)qx, jj = (int64_t)qy;
+        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
+        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
+        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
+        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
+        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
+        constexpr int NV = 3 * MAXO;
+        const float *nd[4];
+        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
+        nd[1] = nd[0] + NP;
+        nd[2] = nd[0] + f.fi_size * NP;
+        nd[3] = nd[2] + NP;
+        float acc[NV];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int a = 0; a < NV; a += 4) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+            }
+        }
+        const double z2 = z * z;
+        double ze = z2, zo = z2 * z;
+#pragma unroll
+        for (int n = 0; n < MAXO; ++n) {
+            Bz += (double)acc[3 * n] * ze;
+            Bfi += (double)acc[3 * n + 1] * zo;
+            Br += (double)acc[3 * n + 2] * zo;
+            ze *= z2;
+            zo *= z2;
+        }
+    }
+}
+
 // ------------------------------------------------------------ Boris fp64
 
-// One-warp blocks, at most 88 registers: 23 warps (736 threads) per SM,
-// so a 1e5-particle bunch is resident in one wave on 148 SMs.
+// One-warp blocks, at most 80 registers.  The register file is split over
+// the SM's four schedulers (16384 registers each): 80 x 32 = 2560 registers
+// per warp gives 6 warps per scheduler, 24 per SM, 3552 on 148 SMs, so the
+// 3125 warps of a 1e5-particle bunch are resident in one wave.  At 88
+// registers it is 5 per scheduler (2960 warps): the last 165 warps then run
+// all their steps as a second, nearly empty wave (measured: 5.09 ms per
+// 720-step turn at 88 registers, 3.81 ms at 80).
 constexpr int BORIS_TB = 32;
 
-template <int MAXO, bool SC, bool XING>
-__global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
+template <int MAXO, bool SC, bool XING, bool F32>
+__global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -307,6 +404,8 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
     const double inv_mmcc = 1.0 / (m * m * c * c);
     const double inv_cc = 1.0 / (c * c);
     const double inv_m = 1.0 / m;
+    const double hqm = hq * inv_m;
+    double ir = 1.0 / r;                     // 1 / r, carried from the previous step
     int lost = 0, oob = 0;
 
     for (int s = 0; s < p.nsteps; ++s) {
@@ -323,8 +422,12 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             const double acc = __ldg(p.acc + gs);
             const double fim = fi - f.period * floor(fi / f.period);
             double Bz, Br, Bfi;
-            analytic_b64(f, r, fim, z, Bz, Br, Bfi);
-            if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, r, fim, z, Bz, Bfi, Br, oob);
+            if constexpr (F32) {
+                field_mixed<MAXO>(f, r, ir, fim, z, Bz, Br, Bfi, oob);
+            } else {
+                analytic_b64(f, r, ir, fim, z, Bz, Br, Bfi);
+                if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, r, fim, z, Bz, Bfi, Br, oob);
+            }
             double Er, Efi;
             rf_field64(p.rf, acc, r, fi, rfph, Er, Efi);
             double Ez = 0.0;
@@ -345,8 +448,7 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             py += hq * Efi;
             pz += hq * Ez;
             const double p2 = px * px + py * py + pz * pz;
-            const double gm = sqrt(1 + p2 * inv_mmcc);
-            const double cb = hq * inv_m / gm;
+            const double cb = hqm * rsqrt(1 + p2 * inv_mmcc);
             const double tx = cb * Bx, ty = cb * By, tz = cb * Bzc;
             const double pxp = px + (py * tz - pz * ty);
             const double pyp = py + (pz * tx - px * tz);
@@ -376,6 +478,7 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             const double vfi = -vxn * sn + vyn * cn;
             fidot = rn > 1e-12 ? vfi * irn : 0.0;
             r = rn;
+            ir = irn;
         } else {
             // skipped particle: the reference's Cartesian round trip
             double sinFi, cosFi;
@@ -388,6 +491,7 @@ __global__ void __maxnreg__(88) boris_f64_kernel(const PushK p)
             const double vfi = -vx * sinFi + vy * cosFi;
             fidot = rn > 1e-12 ? vfi / rn : 0.0;
             r = rn;
+            ir = 1.0 / rn;
         }
         rfph += drf;
         if constexpr (XING) {
@@ -420,7 +524,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     const double q = p.cs.q, c = p.cs.c, E0 = p.cs.E0;
     const double fim = y.fi - f.period * floor(y.fi / f.period);
     double Bz, Br, Bfi;
-    analytic_b64(f, y.r, fim, y.z, Bz, Br, Bfi);
+    analytic_b64(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi);
     if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
     double Er, Efi;
     rf_field64(p.rf, acc, y.r, y.fi, y.rf, Er, Efi);
@@ -515,246 +619,6 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
     status_add(p.status, 0, !(isfinite(y.r) && isfinite(y.fi) && isfinite(y.z)), oob);
 }
 
-// ---------------------------------------------------- Boris, compensated fp32
-//
-// The float64 kernel spends most of its time in float64 transcendentals.  This
-// variant evaluates the field and forms the Boris increments in float32, and
-// keeps in float64 only what accumulates over many steps: the position
-// (r, fi, z), the momentum per unit mass u = gamma v in the local frame, the
-// RF phase, and the frame rotation of u after each step.  Float32 errors then
-// enter as small pseudo-random relative errors of per-step increments rather
-// than of the state:
-//  - field: accurately rounded expf / log1pf (no fast intrinsics); each
-//    sigmoid argument k (fi - x0) is formed in float64 before rounding, and
-//    r^(k-1) = r_ref^(k-1) (1 + eps)^(k-1) with eps formed in float64;
-//  - Boris: the electric half kicks and the magnetic rotation increment are
-//    float32; |u| is renormalised in float64 after the rotation, so the
-//    magnetic push conserves energy to float64 rounding;
-//  - 1/gamma for the drift, the azimuth change and the frame rotation are
-//    float64 (series in the small per-step angle).
-// Particles that are skipped take the same float64 Cartesian round trip as the
-// float64 kernel.
-
-template <int MAXO>
-__device__ __forceinline__ void field_b32(const FieldK &f, double r, double fim, float zf, float &Bz, float &Br,
-                                          float &Bfi, int &clamped)
-{
-    double spiral = 0.0, spiral_p = 0.0;
-    if (!f.spiral_zero) {
-        for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * r + f.spoly[a];
-        for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * r + f.spolyp[a];
-    }
-    float B0r, B0r_p;
-    const float rf = (float)r;
-    if (f.k == 0.0) {
-        B0r = (float)f.B0;
-        B0r_p = 0.0f;
-    } else {
-        const float eps = (float)((r - f.r_ref) * f.inv_r_ref);
-        const float g = expf(f.km1f * log1pf(eps));   // ((r / r_ref))^(k-1)
-        B0r_p = f.kc1f * g;
-        B0r = f.c1f * g * rf;
-    }
-    double fs = fim - spiral;
-    fs -= f.period * floor(fs / f.period);
-    float F = 0.0f, Fp = 0.0f;
-    for (int j = 0; j < f.n_seg; ++j) {
-        const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
-        const float a2 = (float)(f.seg_k[j] * (fs - f.seg_x1[j]));
-        const float e1 = expf(-a1), e2 = expf(a2);
-        const float s1 = __frcp_rn(1.0f + e1);
-        const float s2 = __frcp_rn(1.0f + e2);
-        // 1 - s = e s exactly: no cancellation when the sigmoid saturates
-        const float c1 = e1 * s1, c2 = e2 * s2;
-        const float ks = f.seg_kf[j], y = f.seg_yf[j];
-        F += y * s1 * s2;
-        Fp += y * (ks * s1 * c1 * s2 - s1 * ks * s2 * c2);
-    }
-    Bz = B0r * F;
-    Bfi = B0r * Fp * __frcp_rn(rf) * zf;
-    Br = (B0r_p * F - B0r * Fp * (float)spiral_p) * zf;
-    if constexpr (MAXO >= 1) {
-        const double qx = (r - f.r_min) * f.inv_r_step;
-        const double qy = (fim - f.fi_min) * f.inv_fi_step;
-        int64_t i = (int64_t)qx, jj = (int64_t)qy;
-        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
-        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
-        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
-        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
-        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
-        constexpr int NV = 3 * MAXO;
-        const float *nd[4];
-        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
-        nd[1] = nd[0] + NP;
-        nd[2] = nd[0] + f.fi_size * NP;
-        nd[3] = nd[2] + NP;
-        float acc[NV];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-#pragma unroll
-            for (int a = 0; a < NV; a += 4) {
-                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
-                const float tv[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
-            }
-        }
-        const float z2 = zf * zf;
-        float ze = z2, zo = z2 * zf;
-#pragma unroll
-        for (int n = 0; n < MAXO; ++n) {
-            Bz += acc[3 * n] * ze;
-            Bfi += acc[3 * n + 1] * zo;
-            Br += acc[3 * n + 2] * zo;
-            ze *= z2;
-            zo *= z2;
-        }
-    }
-}
-
-template <int MAXO, bool SC, bool XING>
-__global__ void __launch_bounds__(128) boris_f32c_kernel(const PushK p)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
-    const FieldK &f = p.f;
-    const ffa_state_soa &S = p.st;
-    double r = S.r[i], rdot = S.vr[i], z = S.z[i], zdot = S.vz[i], fi = S.fi[i], fidot = S.f5[i];
-    double rfph = S.rf[i];
-    double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
-    int inj = S.inj[i], surv = S.surv[i];
-    const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
-    SCExtrap ex;
-    if (SC) ex.load(S, i);
-    const double q = p.cs.q, c = p.cs.c, m = p.cs.m0, dt = p.dt;
-    const double inv_cc = 1.0 / (c * c);
-    const double hkd = 0.5 * dt * q / m;         // u kick per unit field: (q / m) dt / 2
-    const float hk = (float)hkd;
-    double ur = 0, uf = 0, uz = 0;                 // u = gamma v, local frame
-    bool umode = false;                            // u holds the velocity state
-    int lost = 0, oob = 0;
-
-    for (int s = 0; s < p.nsteps; ++s) {
-        const int64_t gs = p.step0 + s;
-        if (injs == gs) { inj = 1; surv = 1; }
-        if (SC) ex.apply(gs, p.sc_step, esr, esz, esf);
-        const double drf = __ldg(p.drf + gs);
-        const bool alive = (inj == 1) && (surv == 1);
-        if (alive && !umode) {
-            const double vf = r * fidot;
-            const double g = rsqrt(1.0 - (rdot * rdot + vf * vf + zdot * zdot) * inv_cc);
-            ur = g * rdot; uf = g * vf; uz = g * zdot;
-            umode = true;
-        } else if (!alive && umode) {
-            const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
-            rdot = ur * ig; zdot = uz * ig; fidot = uf * ig / r;
-            umode = false;
-        }
-        double pre[7];
-        const int surv0 = surv;
-        if constexpr (XING) {
-            if (surv0 == 1) {
-                pre[0] = r; pre[2] = z; pre[4] = fi; pre[6] = rfph;
-                if (alive) {
-                    const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
-                    pre[1] = ur * ig; pre[3] = uz * ig; pre[5] = uf * ig / r;
-                } else {
-                    pre[1] = rdot; pre[3] = zdot; pre[5] = fidot;
-                }
-            }
-        }
-        if (alive) {
-            const double acc = __ldg(p.acc + gs);
-            const double fim = fi - f.period * floor(fi / f.period);
-            float Bz, Br, Bfi;
-            field_b32<MAXO>(f, r, fim, (float)z, Bz, Br, Bfi, oob);
-            double Er64, Efi64;
-            rf_field64(p.rf, acc, r, fi, rfph, Er64, Efi64);
-            const float Er = (float)(Er64 + esr), Efi = (float)(Efi64 + esf), Ez = (float)esz;
-            if (p.ap.enable && (r > p.ap.rmax || r < p.ap.rmin || z > p.ap.zmax || z < p.ap.zmin)) {
-                surv = 0;
-                ++lost;
-            }
-            // half electric kick (float32 increment, float64 state)
-            const float d1x = hk * Er, d1y = hk * Efi, d1z = hk * Ez;
-            const double mx = ur + d1x, my = uf + d1y, mz = uz + d1z;
-            const float fx = (float)mx, fy = (float)my, fz = (float)mz;
-            // magnetic rotation: increment in float32, |u| restored in float64
-            // q dt / (2 m gamma) from the float64 |u|: a float32 gamma would
-            // bias every step's bend by its rounding
-            const double nm = mx * mx + my * my + mz * mz;
-            const float cb = (float)(hkd * rsqrt(1.0 + nm * inv_cc));
-            const float tx = -cb * Br, ty = -cb * Bfi, tz = -cb * Bz;
-            const float pxp = fx + (fy * tz - fz * ty);
-            const float pyp = fy + (fz * tx - fx * tz);
-            const float pzp = fz + (fx * ty - fy * tx);
-            const float sb = 2.0f * __frcp_rn(1.0f + (tx * tx + ty * ty + tz * tz));
-            const float sx = sb * tx, sy = sb * ty, sz = sb * tz;
-            double px = mx + (double)(pyp * sz - pzp * sy);
-            double py = my + (double)(pzp * sx - pxp * sz);
-            double pz = mz + (double)(pxp * sy - pyp * sx);
-            const double np = px * px + py * py + pz * pz;
-            const double sc = 1.0 + 0.5 * (double)((float)(nm - np) * __frcp_rn((float)np));
-            px = px * sc + d1x;
-            py = py * sc + d1y;
-            pz = pz * sc + d1z;
-            // drift with 1/gamma in float64
-            const double ig = rsqrt(1.0 + (px * px + py * py + pz * pz) * inv_cc);
-            const double dxr = px * ig * dt, yn = py * ig * dt;
-            z = z + pz * ig * dt;
-            const double xr = r + dxr;
-            double ix = (double)__frcp_rn((float)xr);
-            ix = ix * (2.0 - xr * ix);
-            ix = ix * (2.0 - xr * ix);
-            const double tn = yn * ix;                // tan of the azimuth change
-            const float tf = (float)tn, t2f = tf * tf;
-            const double dfi = tn + (double)(tf * t2f * (-1.0f / 3 + t2f * (0.2f - t2f * (1.0f / 7))));
-            r = xr + (double)((float)xr * (t2f * (0.5f - t2f * (0.125f - t2f * 0.0625f))));
-            fi = fi + dfi;
-            // rotate u into the new local frame
-            const double d2 = dfi * dfi;
-            const double sn = dfi * (1.0 - d2 * (1.0 / 6 - d2 * (1.0 / 120)));
-            const double cm1 = -d2 * (0.5 - d2 * (1.0 / 24 - d2 * (1.0 / 720)));
-            ur = px + (px * cm1 + py * sn);
-            uf = py + (py * cm1 - px * sn);
-            uz = pz;
-        } else {
-            double sinFi, cosFi;
-            sincos(fi, &sinFi, &cosFi);
-            const double x = r * cosFi, y = r * sinFi;
-            const double vx = rdot * cosFi - r * fidot * sinFi;
-            const double vy = rdot * sinFi + r * fidot * cosFi;
-            const double rn = sqrt(x * x + y * y);
-            rdot = vx * cosFi + vy * sinFi;
-            const double vfi = -vx * sinFi + vy * cosFi;
-            fidot = rn > 1e-12 ? vfi / rn : 0.0;
-            r = rn;
-        }
-        rfph += drf;
-        if constexpr (XING) {
-            if (surv0 == 1) {
-                double post[7] = {r, rdot, z, zdot, fi, fidot, rfph};
-                if (alive) {
-                    const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
-                    post[1] = ur * ig; post[3] = uz * ig; post[5] = uf * ig / r;
-                }
-                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
-            }
-        }
-    }
-    if (umode) {
-        const double ig = rsqrt(1.0 + (ur * ur + uf * uf + uz * uz) * inv_cc);
-        rdot = ur * ig; zdot = uz * ig; fidot = uf * ig / r;
-    }
-    S.r[i] = r; S.vr[i] = rdot; S.z[i] = z; S.vz[i] = zdot; S.fi[i] = fi; S.f5[i] = fidot;
-    S.rf[i] = rfph;
-    S.esc_r[i] = esr; S.esc_z[i] = esz; S.esc_fi[i] = esf;
-    S.inj[i] = (uint8_t)inj;
-    S.surv[i] = (uint8_t)surv;
-    status_add(p.status, lost, !(isfinite(r) && isfinite(fi) && isfinite(z)), oob);
-}
-
 // ------------------------------------------------------------ node packing
 
 __global__ void pack_nodes_kernel(const double *__restrict__ bz, const double *__restrict__ bfi,
@@ -788,8 +652,8 @@ template <int MAXO, bool SC>
 static void boris_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = BORIS_TB;
-    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
-    else boris_f64_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    else boris_f64_kernel<MAXO, SC, false, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
 template <int MAXO, bool SC>
@@ -827,9 +691,9 @@ cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s)
 template <int MAXO, bool SC>
 static void boris32_launch(const PushK &p, cudaStream_t s)
 {
-    const int tb = 128;
-    if (p.xing.buf) boris_f32c_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
-    else boris_f32c_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    const int tb = BORIS_TB;
+    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    else boris_f64_kernel<MAXO, SC, false, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s)

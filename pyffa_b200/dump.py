@@ -86,6 +86,7 @@ class PositionDumpBunch:
         self.save_flag = False
         self.rank = rank
         self._rows = []
+        self._records = []
         self.write_cursor = 0
         if rank == 0:
             if not os.path.exists(save_folder):
@@ -106,6 +107,21 @@ class PositionDumpBunch:
         t = np.broadcast_to(np.asarray(time_i, dtype=np.float64), (particle_data.shape[0],))
         self._rows.append(np.hstack((particle_data, t[:, None])))
         self.write_cursor += particle_data.shape[0]
+
+    def add_records(self, records, t_post):
+        """Keeps the raw crossing records behind the rows (layout of
+        ffa_push_crossing, plus the step's end time as a last column): the
+        pre-step state and the ratio let an analysis interpolate to the exact
+        azimuth, which the saved post-step rows do not."""
+        records = np.asarray(records, dtype=np.float64)
+        t = np.broadcast_to(np.asarray(t_post, dtype=np.float64), (records.shape[0],))
+        self._records.append(np.hstack((records, t[:, None])))
+
+    @property
+    def crossing_records(self) -> np.ndarray:
+        if len(self._records) > 1:
+            self._records = [np.vstack(self._records)]
+        return self._records[0] if self._records else np.zeros((0, 24))
 
     @property
     def saved_data(self) -> np.ndarray:

@@ -329,6 +329,7 @@ class FFAG_RungeKutta:
                     keep = d.in_window(tp) if not d.save_flag else np.zeros(len(r), bool)
                     if keep.any():
                         d.add_particles(xcap.rows(r[keep]), tp[keep])
+                        d.add_records(r[keep], tp[keep])
             for d in pos_dumps:
                 if not d.save_flag and (t_chunk > d.end_time).any():
                     d.save_all_particles(solver)
