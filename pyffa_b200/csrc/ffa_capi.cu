@@ -259,6 +259,14 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     p.nsteps = nsteps;
     p.sc_step = sc_step;
     p.dt = dt;
+    {
+        const double q = cs->q, c = cs->c, m = cs->m0;
+        p.hq = 0.5 * dt * q;
+        p.inv_mmcc = 1.0 / (m * m * c * c);
+        p.inv_cc = 1.0 / (c * c);
+        p.inv_m = 1.0 / m;
+        p.hqm = p.hq * p.inv_m;
+    }
     p.status = status;
     if (xing) {
         if (!xing->buf || !xing->count || xing->capacity < 0 || xing->ntargets < 1 ||

@@ -68,6 +68,13 @@ struct PushK {
     double dt;
     int64_t *status;
     ffa_crossing xing;  // records.buf == NULL: no crossing capture
+    // Boris constants, formed on the host so the kernel reads them from the
+    // parameter bank instead of holding them in registers
+    double hq;          // (0.5 dt) q
+    double hqm;         // hq / m
+    double inv_m;       // 1 / m
+    double inv_cc;      // 1 / c^2
+    double inv_mmcc;    // 1 / (m^2 c^2)
 };
 
 }  // namespace ffa

@@ -399,12 +399,8 @@ __global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
     const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
     SCExtrap ex;
     if (SC) ex.load(S, i);
-    const double q = p.cs.q, c = p.cs.c, m = p.cs.m0, dt = p.dt;
-    const double hq = 0.5 * dt * q;          // (0.5 * dt) * q
-    const double inv_mmcc = 1.0 / (m * m * c * c);
-    const double inv_cc = 1.0 / (c * c);
-    const double inv_m = 1.0 / m;
-    const double hqm = hq * inv_m;
+    const double m = p.cs.m0, dt = p.dt;
+    const double hq = p.hq, hqm = p.hqm, inv_m = p.inv_m, inv_cc = p.inv_cc, inv_mmcc = p.inv_mmcc;
     double ir = 1.0 / r;                     // 1 / r, carried from the previous step
     int lost = 0, oob = 0;
 
