@@ -34,12 +34,12 @@ STEPS_PER_TURN = 720
 MAX_ORDER = 2
 # float64 operations per particle-step of the Boris kernel (2 per DFMA,
 # 1 per DADD / DMUL), counted from the kernel's executed instruction mix by
-# ncu on this workload (profiles/boris_f64_c1_1e5.md): 274.2 DFMA + 45.1 DADD
-# + 101.1 DMUL per particle-step
-FP64_FLOP_PER_PARTICLE_STEP = 694.6
+# ncu on this workload (profiles/boris_f64_c1_1e5.md): 630.5 FP64 flop per
+# particle-step
+FP64_FLOP_PER_PARTICLE_STEP = 630.5
 # DRAM bytes (read + write) of one launch (one turn, 1e5 particles) from the
 # same ncu capture, L2 flushed before the launch
-BORIS_TRAFFIC_PER_LAUNCH = 22.709e6
+BORIS_TRAFFIC_PER_LAUNCH = 19.164e6
 # algorithmic HBM bytes per particle per launch: SoA state read
 # (10 float64 + 2 flag bytes + int32 injection step) and written (10 float64 + 2 bytes)
 STATE_BYTES_PER_PARTICLE = (10 * 8 + 2 + 4) + (10 * 8 + 2)
@@ -156,7 +156,7 @@ def fp64_peak_tflops(dev_index):
     return best
 
 
-def cpu_baseline(gp, v, dt, sample_n=100_000, steps=STEPS_PER_TURN):
+def cpu_baseline(gp, v, dt, sample_n=100_000, steps=8 * STEPS_PER_TURN):
     """The reference algorithm on the host cores (oracle port, all threads):
     particle-turns/s on a bounded sample of the workload."""
     from oracle import oracle as O
@@ -168,7 +168,8 @@ def cpu_baseline(gp, v, dt, sample_n=100_000, steps=STEPS_PER_TURN):
     O.track(S, "Boris", m, 0.0, dt, steps)
     el = time.perf_counter() - t0
     return {"value": sample_n * steps / STEPS_PER_TURN / el, "unit": "particle-turns/s", "cores": O.num_threads(),
-            "kind": "port", "sample": f"{sample_n} particles x {steps} Boris steps (one turn) of the same workload",
+            "kind": "port", "sample": f"{sample_n} particles x {steps} Boris steps ({steps // STEPS_PER_TURN} turns) of the "
+                                "same workload",
             "seconds": el}
 
 
@@ -354,7 +355,8 @@ def main():
             dist.all_reduce(t32, op=dist.ReduceOp.MAX)
         v32 = n * world * args.steps / (float(t32.item()) * 1e-3)
         fp32c = {"value": v32, "unit": "particle-turns/s", "ms_per_step": float(t32.item()) / args.steps,
-                 "speedup_vs_fp64": v32 / value, "dtype": "f32 fields/increments, f64 accumulation"}
+                 "speedup_vs_fp64": v32 / value,
+                 "dtype": "f32 field exponentials and map lookup, f64 push and state"}
     clocks = cs.summary()
 
     # end to end through the host-buffer API: host matrix in, one turn, host matrix out

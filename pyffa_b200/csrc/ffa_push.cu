@@ -54,13 +54,24 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
     fs -= f.period * floor(fs / f.period);
     double B0F = 0.0, B0Fp = 0.0;
     for (int j = 0; j < f.n_seg; ++j) {
-        double ks = f.seg_k[j];
-        double s1 = 1.0 / (1.0 + exp(-ks * (fs - f.seg_x0[j])));
-        double s2 = 1.0 / (1.0 + exp(ks * (fs - f.seg_x1[j])));
-        double y = f.seg_y[j];
+        const double ks = f.seg_k[j];
+        // Past 37.5 the exponential is below 2^-54, so 1 + e rounds to 1 and
+        // the sigmoid is exactly 1 (its derivative exactly 0): the branch
+        // skips only exponentials that cannot change the result.  Inside a
+        // magnet both of its sigmoids saturate; outside it, one of them.
+        const double a1 = ks * (fs - f.seg_x0[j]);
+        const double a2 = ks * (fs - f.seg_x1[j]);
+        double s1 = 1.0, s2 = 1.0, s1p = 0.0, s2p = 0.0;
+        if (a1 < 37.5) {
+            s1 = 1.0 / (1.0 + exp(-a1));
+            s1p = ks * s1 * (1.0 - s1);
+        }
+        if (a2 > -37.5) {
+            s2 = 1.0 / (1.0 + exp(a2));
+            s2p = -ks * s2 * (1.0 - s2);
+        }
+        const double y = f.seg_y[j];
         B0F += y * s1 * s2;
-        double s1p = ks * s1 * (1.0 - s1);
-        double s2p = -ks * s2 * (1.0 - s2);
         B0Fp += y * (s1p * s2 + s1 * s2p);
     }
     Bz = B0r * B0F;
@@ -321,8 +332,12 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
         const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
         const float a2 = (float)(f.seg_k[j] * (fs - f.seg_x1[j]));
         // exponents capped at 80 so e stays finite: past it s < 2e-35, which
-        // is 0 in every sum below, and e * s would otherwise be inf * 0
-        const float e1 = expf(fminf(-a1, 80.0f)), e2 = expf(fminf(a2, 80.0f));
+        // is 0 in every sum below, and e * s would otherwise be inf * 0.
+        // Where a sigmoid is saturated at 1 (e < 4e-11) its exponential is
+        // skipped and e taken as 0.
+        float e1 = 0.0f, e2 = 0.0f;
+        if (a1 < 24.0f) e1 = expf(fminf(-a1, 80.0f));
+        if (a2 > -24.0f) e2 = expf(fminf(a2, 80.0f));
         const float s1 = __frcp_rn(1.0f + e1), s2 = __frcp_rn(1.0f + e2);
         const float ss = s1 * s2;
         // s1' s2 + s1 s2' = k s1 s2 ((1 - s1) - (1 - s2)) with 1 - s = e s:
