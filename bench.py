@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-sc", action="store_true")
     ap.add_argument("--no-fp32c", action="store_true")
+    ap.add_argument("--no-mapgen", action="store_true")
     return ap.parse_args()
 
 
@@ -234,6 +235,53 @@ def sc_bench(gp, dt, dev, updates=20, warmup=3, turns=2):
             out["cycle"] = "12 x (open-boundary update + 60 Boris fp64 steps) per turn"
             out["alive_fraction"] = float((b.cols["surv"] == 1).float().mean().item())
     return out
+
+
+def mapgen_bench(dev, hbm_peak, reps=5):
+    """z-Taylor map generation on the workloads' 1301 x 6000 grid, order 2
+    (the reference's offline Generate_Bmaps_MultiProcess): device time of the
+    build (CUDA events, tables resident in HBM), end-to-end time of the
+    reference-facing call (numpy tables on the host), and the oracle port on
+    a sample of rows, scaled to the whole map."""
+    import torch
+    from numpy.polynomial import Polynomial
+    from oracle import mapgen as M
+    from pyffa_b200 import mapgen as G
+    from pyffa_b200 import synthetic
+    B = synthetic.lattice_bmap()["Bmap"]
+    B["SpiralAngle_deg"] = 20.0
+    r, fi = G.map_axes(B)
+    sfit = Polynomial.fit(r, G.calculate_s(r, 0.0, B["SpiralAngle_deg"]), 5)
+    conv = G.BmapParams_to_ConvexParams(B)
+    ak = B["coefficients_tupel"]
+    plan = G.MapgenPlan(2, r, fi, conv, sfit, ak, device=dev)
+    for _ in range(3):
+        plan.run()
+    torch.cuda.synchronize(dev)
+    ms = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        plan.run()
+        b.record()
+        torch.cuda.synchronize(dev)
+        ms.append(a.elapsed_time(b))
+    del plan
+    t0 = time.perf_counter()
+    G.Generate_Bmaps(2, r, fi, conv, sfit, ak)
+    e2e_s = time.perf_counter() - t0
+    rows = [0, 650]
+    t0 = time.perf_counter()
+    M.generate_bmaps(2, r[rows], fi, M.convex_params(B), sfit, ak)
+    cpu_row_s = (time.perf_counter() - t0) / len(rows)
+    written = 9 * len(r) * len(fi) * 8
+    gpu_s = statistics.median(ms) / 1e3
+    return {"grid": [len(r), len(fi)], "max_order": 2, "spiral_deg": 20.0,
+            "gpu_ms": statistics.median(ms), "e2e_s": e2e_s,
+            "hbm": {"bytes_written": written, "achieved_gbs": written / gpu_s / 1e9, "peak_gbs": hbm_peak,
+                    "frac": written / gpu_s / 1e9 / hbm_peak},
+            "cpu_port_s_per_map": cpu_row_s * len(r), "cpu_port_sample": f"{len(rows)} rows x {len(fi)} azimuths, "
+                                                                        "1 thread, scaled to the map"}
 
 
 def run_reference(args):
@@ -416,6 +464,9 @@ def main():
         sc = None
         if not args.no_sc:
             sc = sc_bench(gp, dt, dev)
+        mg = None
+        if not args.no_mapgen:
+            mg = mapgen_bench(dev, hbm_peak)
         line = {
             "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
             "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
@@ -434,6 +485,7 @@ def main():
             "status": {"lost": int(status[0]), "nan": int(status[1]), "out_of_map": int(status[2])},
             "space_charge": sc,
             "fp32c": fp32c,
+            "mapgen": mg,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)

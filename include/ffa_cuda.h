@@ -271,6 +271,41 @@ int ffa_sc_buffers(const ffa_sc_plan *plan, const float **rho, const float **phi
                    const float **ex, const float **ez, const int32_t **slice_idx,
                    const int64_t **cell_idx);
 
+/* ---------------------------------------------------------- map generation
+ * z-Taylor coefficient tables of a scaling map, B0(r, th) = a r^k G(th - s(r))
+ * (Generate_Bmaps / Generate_Bmaps_MultiProcess, src/FFAG_HighOrder.py:828-998;
+ * main_Bmap, examples/main_Bmap.py:17-75).  Every table entry is a linear
+ * combination of the flutter derivatives G^(p) on the theta grid, rolled by
+ * the row's integer spiral shift (shift_function, src/FFAG_HighOrder.py:393-398):
+ *   T[c][n][i][j] = sum_p weights[c][n][i][p] * G^(p)[(j - shift[i]) mod n_theta] / mean(G)
+ * with c = 0 Bz, 1 Br, 2 Bfi.  The host forms the weights from the Laplacian
+ * term algebra (r-only factors); the library computes the flutter derivatives
+ * (sigmoid-derivative polynomials, src/FFAG_HighOrder.py:212-350), their
+ * sector mean, and the tables. */
+#define FFA_MAPGEN_MAX_DERIV 16
+typedef struct ffa_mapgen_desc {
+    int32_t n_seg;                /* flutter magnets, <= FFA_MAX_SEG */
+    int32_t n_deriv;              /* G derivatives 0 .. n_deriv-1, <= FFA_MAPGEN_MAX_DERIV */
+    int32_t n_orders;             /* Taylor orders 0 .. n_orders-1 */
+    int32_t pad;
+    int64_t n_r, n_theta;
+    double seg_x0[FFA_MAX_SEG], seg_x1[FFA_MAX_SEG];   /* rad */
+    double seg_k[FFA_MAX_SEG];    /* 16 / W0 */
+    double seg_y[FFA_MAX_SEG];    /* signed amplitude */
+    /* device [n_seg][2][n_deriv][n_deriv + 1]: coefficients, highest power
+     * first, of the i-th sigmoid derivative as a polynomial in the sigmoid,
+     * for steepness +k (entry / 0) and -k (exit / 1); row i uses i + 2 of them */
+    const double *sig_poly;
+    const double *theta;          /* device [n_theta] */
+    const double *weights;        /* device [3][n_orders][n_r][n_deriv] */
+    const int32_t *shift;         /* device [n_r] */
+    double *gder;                 /* device scratch [n_deriv][n_theta] */
+    double *gmean;                /* device scratch [1]: sector mean of G */
+    double *bz, *br, *bfi;        /* device [n_orders][n_r][n_theta] */
+} ffa_mapgen_desc;
+
+int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

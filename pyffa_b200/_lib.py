@@ -88,6 +88,18 @@ class Crossing(C.Structure):
                 ("buf", d_p), ("capacity", C.c_int64), ("count", d_p)]
 
 
+MAPGEN_MAX_DERIV = 16
+
+
+class MapgenDesc(C.Structure):
+    _fields_ = [("n_seg", C.c_int32), ("n_deriv", C.c_int32), ("n_orders", C.c_int32), ("pad", C.c_int32),
+                ("n_r", C.c_int64), ("n_theta", C.c_int64),
+                ("seg_x0", C.c_double * MAX_SEG), ("seg_x1", C.c_double * MAX_SEG),
+                ("seg_k", C.c_double * MAX_SEG), ("seg_y", C.c_double * MAX_SEG),
+                ("sig_poly", d_p), ("theta", d_p), ("weights", d_p), ("shift", d_p),
+                ("gder", d_p), ("gmean", d_p), ("bz", d_p), ("br", d_p), ("bfi", d_p)]
+
+
 class SCDesc(C.Structure):
     _fields_ = [
         ("ns", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32), ("hockney", C.c_int32),
@@ -118,6 +130,7 @@ EXPORTS = {
                           C.POINTER(StateSoA), C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32,
                           d_p, d_p, C.POINTER(Crossing)],
     "ffa_aos_to_soa": [d_p, C.c_int64, C.POINTER(StateSoA), d_p],
+    "ffa_mapgen": [C.POINTER(MapgenDesc), d_p],
     "ffa_soa_to_aos": [C.POINTER(StateSoA), C.c_int64, d_p, d_p],
     "ffa_mean_fi": [C.POINTER(StateSoA), C.c_int64, d_p, d_p, d_p],
     "ffa_sc_plan_create": [C.POINTER(SCDesc), d_p, C.POINTER(d_p)],

@@ -2,7 +2,9 @@
 tracker (PyFFA, pure Python + Numba) on seeded synthetic inputs.
 
 Run in the development container, where the reference source is available:
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref /root/reference]              # tracking
+    python tests/golden/make_golden.py --crossing [--ref /root/reference]   # crossing dumps
+    python tests/golden/make_golden.py --mapgen [--ref /root/reference]     # z-Taylor maps
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -276,8 +278,42 @@ def crossing_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def mapgen_main(ref):
+    """The reference's z-Taylor map generator (Generate_Bmaps,
+    src/FFAG_HighOrder.py:828-911, driven as examples/main_Bmap.py:17-75
+    does) on two small lattices: the synthetic one (no spiral) and the same
+    with a 35-degree spiral (golden_mapgen.npz)."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    from numpy.polynomial import Polynomial
+    from FFAG_HighOrder import BmapParams_to_ConvexParams, Generate_Bmaps, calculate_s
+
+    out = {}
+    for key, spiral in (("flat", 0.0), ("spiral", 35.0)):
+        cfg = synthetic.lattice_bmap(r_range=(8.0, 8.5, 0.05), theta_step_deg=0.1)
+        B = cfg["Bmap"]
+        B["SpiralAngle_deg"] = spiral
+        rmin, rmax, rstep = B["rmin_max_step_m"]
+        n_r = int((rmax - rmin) / rstep) + 1
+        n_fi = int((np.pi * 2 / B["NSector"] - 0.0) / B["theta_step_rad"]) + 1
+        fi = np.linspace(0, np.pi * 2 / B["NSector"], n_fi)
+        r = np.linspace(rmin, rmax, n_r)
+        s = calculate_s(r, 0.0, spiral)
+        sfit = Polynomial.fit(r, s, 5)
+        Br, Bz, Bfi = Generate_Bmaps(2, r, fi, BmapParams_to_ConvexParams(B), sfit, B["coefficients_tupel"])
+        out[f"{key}_cfg"] = np.frombuffer(json.dumps(cfg).encode(), dtype=np.uint8)
+        out[f"{key}_Br"], out[f"{key}_Bz"], out[f"{key}_Bfi"] = np.stack(Br), np.stack(Bz), np.stack(Bfi)
+    path = os.path.join(HERE, "golden_mapgen.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    if "--crossing" in sys.argv:
+    if "--mapgen" in sys.argv:
+        sys.argv.remove("--mapgen")
+        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
+        mapgen_main(ref)
+    elif "--crossing" in sys.argv:
         sys.argv.remove("--crossing")
         ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
         crossing_main(ref)
