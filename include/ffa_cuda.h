@@ -271,6 +271,27 @@ int ffa_sc_buffers(const ffa_sc_plan *plan, const float **rho, const float **phi
                    const float **ex, const float **ez, const int32_t **slice_idx,
                    const int64_t **cell_idx);
 
+/* ------------------------------------------------------ closed-orbit tracks
+ * Tracks of the closed-orbit search (FunctionForSEO through rk4_solve /
+ * rk4_solve_vect, src/FFAG_track.py:582-640 and 1698-1740): m trajectories
+ * (r, pr, z, pz) at fixed momentum P with the azimuth as independent variable,
+ * from 0 over n_points - 1 RK4 steps of h = t_end / (n_points - 1) through
+ * the analytic field of `fm` (the mid-plane field and its z-linear terms; the
+ * z-Taylor tables are not used).  Stage azimuths of step i: i h (time_mode 0,
+ * rk4_solve) or the running sum of h (time_mode 1, rk4_solve_vect). */
+typedef struct ffa_theta_track_desc {
+    int64_t m;                    /* trajectories */
+    int32_t n_points;             /* azimuth points, >= 2 */
+    int32_t time_mode;            /* 0: i h, 1: running sum */
+    double t_end;                 /* rad */
+    double q;                     /* charge [C] */
+    const double *x0;             /* device [m][5]: r, pr, z, pz, P */
+    double *x1;                   /* device [m][4]: r, pr, z, pz at t_end */
+    double *traj;                 /* device [m][n_points][2]: r, pr at every point, or NULL */
+} ffa_theta_track_desc;
+
+int ffa_theta_track(const struct ffa_fieldmap *fm, const ffa_theta_track_desc *desc, void *stream);
+
 /* ---------------------------------------------------------- map generation
  * z-Taylor coefficient tables of a scaling map, B0(r, th) = a r^k G(th - s(r))
  * (Generate_Bmaps / Generate_Bmaps_MultiProcess, src/FFAG_HighOrder.py:828-998;

@@ -488,6 +488,59 @@ double orc_track(int solver /*1 Boris, 0 RK4*/, double *mat, int64_t N, double t
     return t;
 }
 
+/* FunctionForSEO (src/FFAG_track.py:1698-1740): d/dtheta of (r, pr, z, pz)
+ * at fixed momentum P, mid-plane field and its z-linear terms. */
+static void seo_rhs(const orc_field *f, double t, const double *x, double P, double q, double *d)
+{
+    double fi = fmod(t, 2.0 * M_PI);
+    double fim = fmod(fi, 2.0 * M_PI / (double)f->nsectors);
+    double r = x[0], pr = x[1], z = x[2], pz = x[3];
+    double Bz, Br, Bfi;
+    analytic_B(f, r, fim, z, &Bz, &Br, &Bfi);
+    double pfi = sqrt(1 - pr * pr - pz * pz);
+    d[0] = r * pr / pfi;
+    d[1] = pfi - q / P * (r * Bz - r * pz / pfi * Bfi);
+    d[2] = r * pz / pfi;
+    d[3] = q / P * (r * Br - r * pr / pfi * Bfi);
+}
+
+/* rk4_solve / rk4_solve_vect (src/FFAG_track.py:582-640) in the azimuth:
+ * m trajectories x0[m][5] = r, pr, z, pz, P over n_points - 1 steps of
+ * h = t_end / (n_points - 1); stage azimuths i*h (time_mode 0) or a running
+ * sum (time_mode 1).  x1[m][4] the end state, traj[m][n_points][2] (r, pr)
+ * when not NULL. */
+void orc_theta_track(const orc_field *f, const double *x0, int64_t m, int n_points, int time_mode,
+                     double t_end, double q, double *x1, double *traj)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < m; ++i) {
+        double x[4] = {x0[5 * i], x0[5 * i + 1], x0[5 * i + 2], x0[5 * i + 3]};
+        double P = x0[5 * i + 4];
+        double h = t_end / (double)(n_points - 1);
+        double *tr = traj ? traj + i * (int64_t)n_points * 2 : NULL;
+        if (tr) { tr[0] = x[0]; tr[1] = x[1]; }
+        double t = 0.0;
+        for (int s = 0; s < n_points - 1; ++s) {
+            if (time_mode == 0) t = (double)s * h;
+            double k1[4], k2[4], k3[4], k4[4], y[4], d[4];
+            seo_rhs(f, t, x, P, q, d);
+            for (int c = 0; c < 4; ++c) { k1[c] = h * d[c]; y[c] = x[c] + 0.5 * k1[c]; }
+            seo_rhs(f, t + 0.5 * h, y, P, q, d);
+            for (int c = 0; c < 4; ++c) { k2[c] = h * d[c]; y[c] = x[c] + 0.5 * k2[c]; }
+            seo_rhs(f, t + 0.5 * h, y, P, q, d);
+            for (int c = 0; c < 4; ++c) { k3[c] = h * d[c]; y[c] = x[c] + k3[c]; }
+            seo_rhs(f, t + h, y, P, q, d);
+            for (int c = 0; c < 4; ++c) {
+                k4[c] = h * d[c];
+                x[c] = x[c] + (k1[c] + 2 * k2[c] + 2 * k3[c] + k4[c]) / 6;
+            }
+            if (time_mode != 0) t = t + h;
+            if (tr) { tr[2 * (s + 1)] = x[0]; tr[2 * (s + 1) + 1] = x[1]; }
+        }
+        for (int c = 0; c < 4; ++c) x1[4 * i + c] = x[c];
+    }
+}
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP

@@ -83,6 +83,8 @@ def lib():
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_track.restype = C.c_double
         L.orc_inject.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
+        L.orc_theta_track.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
+                                      C.c_double, C.c_void_p, C.c_void_p]
         L.orc_sc_step.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_sc_step.restype = C.c_int
@@ -92,32 +94,59 @@ def lib():
     return _lib
 
 
+def _orc_field(bmap, keep):
+    """OrcField of the product's FFAG_Bfield_analytical; arrays it points to
+    are appended to `keep`."""
+    f = OrcField()
+    f.nsectors = int(bmap.Nsectors)
+    sp = np.asarray(bmap.s_rad_polynomial, np.float64)
+    spp = np.asarray(bmap.s_rad_polynomial_prime, np.float64)
+    f.n_spoly, f.n_spolyp = len(sp), len(spp)
+    f.spoly[:len(sp)] = sp.tolist()
+    f.spolyp[:len(spp)] = spp.tolist()
+    cp = np.asarray(bmap.convex_params, np.float64)
+    f.n_convex = len(cp)
+    f.convex[:cp.size] = cp.reshape(-1).tolist()
+    f.max_order = int(bmap.max_order)
+    f.B0, f.k = float(bmap.B0), float(bmap.k_value)
+    f.r_min, f.r_step, f.r_size = float(bmap.r_min), float(bmap.r_step), int(bmap.r_size)
+    f.fi_min, f.fi_step, f.fi_size = float(bmap.fi_min), float(bmap.fi_step), int(bmap.fi_size)
+    if f.max_order >= 1:
+        for name, arr in (("bz_stack", bmap.Bz_stack), ("bfi_stack", bmap.Bfi_stack), ("br_stack", bmap.Br_stack)):
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            keep.append(a)
+            setattr(f, name, a.ctypes.data)
+    return f
+
+
+class ThetaTracker:
+    """Azimuth-domain closed-orbit tracks (orc_theta_track), same interface
+    as pyffa_b200.seo.ThetaTracker."""
+
+    def __init__(self, bmap, q):
+        self._keep = []
+        self.field = _orc_field(bmap, self._keep)
+        self.q = float(q)
+
+    def run(self, x0, t_end, h, time_mode=0, traj=False):
+        x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, 5)
+        m = x0.shape[0]
+        n = int((t_end - 0) / h)
+        t_points = np.linspace(0, t_end, n)
+        x1 = np.zeros((m, 4))
+        tr = np.zeros((m, n, 2)) if traj else None
+        lib().orc_theta_track(C.byref(self.field), x0.ctypes.data, m, n, int(time_mode), float(t_end), self.q,
+                              x1.ctypes.data, tr.ctypes.data if traj else None)
+        return x1, tr, t_points
+
+
 class Setup:
     """Oracle parameter blocks built from the product's host-side objects
     (FFAG_Bfield_analytical, FFAG_EField_new, FFAG_GlobalParameters)."""
 
     def __init__(self, bmap, emap, gp):
         self._keep = []
-        f = OrcField()
-        f.nsectors = int(bmap.Nsectors)
-        sp = np.asarray(bmap.s_rad_polynomial, np.float64)
-        spp = np.asarray(bmap.s_rad_polynomial_prime, np.float64)
-        f.n_spoly, f.n_spolyp = len(sp), len(spp)
-        f.spoly[:len(sp)] = sp.tolist()
-        f.spolyp[:len(spp)] = spp.tolist()
-        cp = np.asarray(bmap.convex_params, np.float64)
-        f.n_convex = len(cp)
-        f.convex[:cp.size] = cp.reshape(-1).tolist()
-        f.max_order = int(bmap.max_order)
-        f.B0, f.k = float(bmap.B0), float(bmap.k_value)
-        f.r_min, f.r_step, f.r_size = float(bmap.r_min), float(bmap.r_step), int(bmap.r_size)
-        f.fi_min, f.fi_step, f.fi_size = float(bmap.fi_min), float(bmap.fi_step), int(bmap.fi_size)
-        if f.max_order >= 1:
-            for name, arr in (("bz_stack", bmap.Bz_stack), ("bfi_stack", bmap.Bfi_stack), ("br_stack", bmap.Br_stack)):
-                a = np.ascontiguousarray(arr, dtype=np.float64)
-                self._keep.append(a)
-                setattr(f, name, a.ctypes.data)
-        self.field = f
+        self.field = _orc_field(bmap, self._keep)
         e = OrcEmap()
         e.enable = 1 if emap.EnableFlag else 0
         e.ngaps = len(emap.gap_azimuths)

@@ -88,6 +88,11 @@ class Crossing(C.Structure):
                 ("buf", d_p), ("capacity", C.c_int64), ("count", d_p)]
 
 
+class ThetaTrackDesc(C.Structure):
+    _fields_ = [("m", C.c_int64), ("n_points", C.c_int32), ("time_mode", C.c_int32), ("t_end", C.c_double),
+                ("q", C.c_double), ("x0", d_p), ("x1", d_p), ("traj", d_p)]
+
+
 MAPGEN_MAX_DERIV = 16
 
 
@@ -131,6 +136,7 @@ EXPORTS = {
                           d_p, d_p, C.POINTER(Crossing)],
     "ffa_aos_to_soa": [d_p, C.c_int64, C.POINTER(StateSoA), d_p],
     "ffa_mapgen": [C.POINTER(MapgenDesc), d_p],
+    "ffa_theta_track": [d_p, C.POINTER(ThetaTrackDesc), d_p],
     "ffa_soa_to_aos": [C.POINTER(StateSoA), C.c_int64, d_p, d_p],
     "ffa_mean_fi": [C.POINTER(StateSoA), C.c_int64, d_p, d_p, d_p],
     "ffa_sc_plan_create": [C.POINTER(SCDesc), d_p, C.POINTER(d_p)],

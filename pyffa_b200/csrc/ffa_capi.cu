@@ -283,6 +283,15 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     return e == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }
 
+int ffa_theta_track(const ffa_fieldmap *fm, const ffa_theta_track_desc *d, void *stream)
+{
+    if (!fm || !d || d->m < 0 || d->n_points < 2 || !(d->t_end > 0.0) || !d->x0 || !d->x1)
+        return FFA_ERR_INVALID;
+    if (d->time_mode != 0 && d->time_mode != 1) return FFA_ERR_INVALID;
+    if (d->m == 0) return FFA_OK;
+    return launch_theta_track(fm->k, *d, as_stream(stream)) == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
+}
+
 int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap, const ffa_consts *cs,
              const ffa_step_table *tab, ffa_state_soa *st, int64_t n, int64_t step0, int32_t nsteps, double dt,
              int32_t sc_step, int32_t flags, void *stream, int64_t *status)

@@ -90,5 +90,6 @@ namespace ffa {
 cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s);
 cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s);
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s);
+cudaError_t launch_theta_track(const FieldK &f, const ffa_theta_track_desc &d, cudaStream_t s);
 cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, float *n32, cudaStream_t s);
 }  // namespace ffa

@@ -630,6 +630,63 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
     status_add(p.status, 0, !(isfinite(y.r) && isfinite(y.fi) && isfinite(y.z)), oob);
 }
 
+// ------------------------------------------------- closed-orbit tracks
+
+// d/dtheta of (r, pr, z, pz) at fixed momentum P (FunctionForSEO,
+// src/FFAG_track.py:1698-1740), same operation order.
+__device__ __forceinline__ void seo_rhs(const FieldK &f, double t, const double x[4], double P, double q,
+                                        double d[4])
+{
+    const double tw = 2.0 * PI;
+    const double fi = fmod(t, tw);
+    const double fim = fmod(fi, f.period);
+    const double r = x[0], pr = x[1], z = x[2], pz = x[3];
+    double Bz, Br, Bfi;
+    analytic_b64(f, r, 1.0 / r, fim, z, Bz, Br, Bfi);
+    const double pfi = sqrt(1.0 - pr * pr - pz * pz);
+    const double qP = q / P;
+    d[0] = r * pr / pfi;
+    d[1] = pfi - qP * (r * Bz - r * pz / pfi * Bfi);
+    d[2] = r * pz / pfi;
+    d[3] = qP * (r * Br - r * pr / pfi * Bfi);
+}
+
+__global__ void __launch_bounds__(64) theta_track_kernel(const FieldK f, const ffa_theta_track_desc d)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.m) return;
+    double x[4] = {d.x0[5 * i], d.x0[5 * i + 1], d.x0[5 * i + 2], d.x0[5 * i + 3]};
+    const double P = d.x0[5 * i + 4], q = d.q;
+    const double h = d.t_end / (double)(d.n_points - 1);
+    double *tr = d.traj ? d.traj + (int64_t)i * d.n_points * 2 : nullptr;
+    if (tr) { tr[0] = x[0]; tr[1] = x[1]; }
+    double t = 0.0;
+    for (int s = 0; s < d.n_points - 1; ++s) {
+        if (d.time_mode == 0) t = (double)s * h;
+        double k1[4], k2[4], k3[4], k4[4], y[4], dd[4];
+        seo_rhs(f, t, x, P, q, dd);
+        for (int c = 0; c < 4; ++c) { k1[c] = h * dd[c]; y[c] = x[c] + 0.5 * k1[c]; }
+        seo_rhs(f, t + 0.5 * h, y, P, q, dd);
+        for (int c = 0; c < 4; ++c) { k2[c] = h * dd[c]; y[c] = x[c] + 0.5 * k2[c]; }
+        seo_rhs(f, t + 0.5 * h, y, P, q, dd);
+        for (int c = 0; c < 4; ++c) { k3[c] = h * dd[c]; y[c] = x[c] + k3[c]; }
+        seo_rhs(f, t + h, y, P, q, dd);
+        for (int c = 0; c < 4; ++c) {
+            k4[c] = h * dd[c];
+            x[c] = x[c] + (k1[c] + 2 * k2[c] + 2 * k3[c] + k4[c]) / 6;
+        }
+        if (d.time_mode != 0) t = t + h;
+        if (tr) { tr[2 * (s + 1)] = x[0]; tr[2 * (s + 1) + 1] = x[1]; }
+    }
+    for (int c = 0; c < 4; ++c) d.x1[4 * i + c] = x[c];
+}
+
+cudaError_t launch_theta_track(const FieldK &f, const ffa_theta_track_desc &d, cudaStream_t s)
+{
+    theta_track_kernel<<<(unsigned)((d.m + 63) / 64), 64, 0, s>>>(f, d);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ node packing
 
 __global__ void pack_nodes_kernel(const double *__restrict__ bz, const double *__restrict__ bfi,

@@ -93,6 +93,11 @@ class FFAG_Bfield_analytical:
         self.fi_step = fi_axis[1] - fi_axis[0]
         self.r_size, self.fi_size = len(r_axis), len(fi_axis)
         self.convex_params = convex_params(bm)
+        self.r_axis_Bmean = bm.get("r_axis")
+        self.f1 = None
+        if self.Bmean is not None:
+            from scipy.interpolate import interp1d
+            self.f1 = interp1d(self.r_axis_Bmean, self.Bmean, kind="linear", fill_value="extrapolate")
         self.max_order = int(max_order)
         self.flag3D = flag3D
         self.config_path = config_Bmap_path
@@ -116,6 +121,42 @@ class FFAG_Bfield_analytical:
                     raise ValueError(
                         f"z-Taylor stack must have shape (>= {self.max_order + 1}, {self.r_size}, {self.fi_size})")
         self._device = {}
+
+    # -- host evaluation of the mid-plane field (table setup only)
+    def GetBz(self, r, fi):
+        """Mid-plane Bz = B0 r^k F(fi - s(r)) on the host (GetBz,
+        src/FFAG_Field.py:794-815, without the search-mode clamp)."""
+        r = np.asarray(r, dtype=np.float64)
+        fi = np.asarray(fi, dtype=np.float64)
+        s = np.zeros_like(r)
+        for c in self.s_rad_polynomial:
+            s = s * r + c
+        amp = self.B0 * np.power(r, self.k_value)
+        period = 2 * np.pi / self.Nsectors
+        x = fi - s
+        x = x - period * np.floor(x / period)
+        F = x * 0.0
+        for x0, x1, W0, y01, y02 in self.convex_params:
+            k = 16 / W0
+            F += y02 * np.abs(y01) * (1 / (1 + np.exp(-k * (x - x0)))) * (1 / (1 + np.exp(k * (x - x1))))
+        return amp * F
+
+    def UpdataConfig(self, save_folder=None):
+        """Sector-mean field per radius, written back into the lattice JSON
+        as Bmap.Bmean / Bmap.r_axis (UpdataConfig, src/FFAG_Field.py:904-943);
+        the closed-orbit search starts from it (func_get_R_B0)."""
+        from scipy.interpolate import interp1d
+        self.Bmean = [float(np.mean(self.GetBz(np.full_like(self.fi_axis, r), self.fi_axis))) for r in self.r_axis]
+        self.r_axis_Bmean = self.r_axis.tolist()
+        self.f1 = interp1d(self.r_axis_Bmean, self.Bmean, kind="linear", fill_value="extrapolate")
+        if self.config_path:
+            with open(self.config_path) as f:
+                cfg = json.load(f)
+            cfg["Bmap"]["Bmean"] = self.Bmean
+            cfg["Bmap"]["r_axis"] = self.r_axis_Bmean
+            folder = save_folder or self.BmapFoldName
+            with open(os.path.join(folder, "config_Bmap.json"), "w") as f:
+                json.dump(cfg, f, indent=4)
 
     # -- kernel descriptor
     def field_desc(self) -> "_lib.FieldDesc":

@@ -5,6 +5,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py [--ref /root/reference]              # tracking
     python tests/golden/make_golden.py --crossing [--ref /root/reference]   # crossing dumps
     python tests/golden/make_golden.py --mapgen [--ref /root/reference]     # z-Taylor maps
+    python tests/golden/make_golden.py --seo [--ref /root/reference]        # closed orbits
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -308,8 +309,52 @@ def mapgen_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def seo_main(ref):
+    """The reference's closed-orbit search (FFAG_SearchSEO.SearchSEOsControllerVect,
+    src/FFAG_track.py:1380-1512, driven as examples/main_SEO.py:13-31) on the
+    synthetic lattice (two energies) and on the same lattice with a
+    25-degree spiral (one energy); the SEO files it writes (golden_seo.npz)."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    from FFAG_Field import FFAG_Bfield_analytical, FFAG_BField_Error
+    from FFAG_ParasAndConversion import FFAG_GlobalParameters
+    from FFAG_track import FFAG_SearchSEO
+
+    out = {}
+    for key, spiral, energies in (("flat", 0.0, [300.0, 330.0]), ("spiral", 25.0, [310.0])):
+        with tempfile.TemporaryDirectory() as tmp:
+            cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
+            cfg["Bmap"]["SpiralAngle_deg"] = spiral
+            cfg["config"]["folder"] = tmp
+            path = os.path.join(tmp, "config_Bmap.json")
+            with open(path, "w") as f:
+                json.dump(cfg, f)
+            FFAG_Bfield_analytical(path, 0, AddNumricalMap=False).UpdataConfig()
+            gp = FFAG_GlobalParameters()
+            gp.AddBMap(FFAG_Bfield_analytical(path, 0, AddNumricalMap=False))
+            gp.AddBHarmonics(FFAG_BField_Error([], False))
+            gp.SEO_SaveFold = "seo"
+            fold = FFAG_SearchSEO(gp).SearchSEOsControllerVect(np.array(energies))
+            with open(path) as f:
+                out[f"{key}_cfg"] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+            with open(os.path.join(fold, "SEO_ini.txt")) as f:
+                text = f.read()
+            # the first line names the temporary map folder: keep the rest
+            out[f"{key}_ini"] = np.frombuffer(text.split("\n", 1)[1].encode(), dtype=np.uint8)
+            out[f"{key}_r"] = np.loadtxt(os.path.join(fold, "SEO_r.txt"), skiprows=1)
+            out[f"{key}_pr"] = np.loadtxt(os.path.join(fold, "SEO_pr.txt"), skiprows=1)
+            out[f"{key}_Ek"] = np.array(energies)
+    path = os.path.join(HERE, "golden_seo.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    if "--mapgen" in sys.argv:
+    if "--seo" in sys.argv:
+        sys.argv.remove("--seo")
+        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
+        seo_main(ref)
+    elif "--mapgen" in sys.argv:
         sys.argv.remove("--mapgen")
         ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
         mapgen_main(ref)

@@ -22,7 +22,7 @@ def test_library_builds_and_exports_header_symbols():
     assert os.path.exists(path)
     L = ctypes.CDLL(path)
     names = declared_entry_points()
-    assert len(names) >= 14
+    assert len(names) >= 15
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 
@@ -38,9 +38,9 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "ffa_cuda.h"
-int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d\n", sizeof(ffa_field_desc), sizeof(ffa_rf_desc),
+int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d\n", sizeof(ffa_field_desc), sizeof(ffa_rf_desc),
  sizeof(ffa_aperture), sizeof(ffa_consts), sizeof(ffa_state_soa), sizeof(ffa_step_table), sizeof(ffa_sc_desc),
- sizeof(ffa_sc_diag), sizeof(ffa_crossing), sizeof(ffa_mapgen_desc), sizeof(void*), FFA_CROSSING_RECORD); return 0;}
+ sizeof(ffa_sc_diag), sizeof(ffa_crossing), sizeof(ffa_mapgen_desc), sizeof(ffa_theta_track_desc), sizeof(void*), FFA_CROSSING_RECORD); return 0;}
 '''
     d = tempfile.mkdtemp()
     with open(os.path.join(d, "s.c"), "w") as f:
@@ -51,7 +51,7 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d\n", sizeof
     sizes = [int(x) for x in out]
     py = [ctypes.sizeof(t) for t in (_lib.FieldDesc, _lib.RFDesc, _lib.Aperture, _lib.Consts, _lib.StateSoA,
                                      _lib.StepTable, _lib.SCDesc, _lib.SCDiag, _lib.Crossing,
-                                     _lib.MapgenDesc)] + \
+                                     _lib.MapgenDesc, _lib.ThetaTrackDesc)] + \
         [ctypes.sizeof(ctypes.c_void_p), _lib.CROSSING_RECORD]
     assert sizes == py
 
