@@ -283,11 +283,13 @@ typedef struct ffa_theta_track_desc {
     int64_t m;                    /* trajectories */
     int32_t n_points;             /* azimuth points, >= 2 */
     int32_t time_mode;            /* 0: i h, 1: running sum */
+    int32_t traj_cols;            /* 2: r, pr; 7: r, pr, z, pz, Bz, Br, Bfi (field at that point) */
+    int32_t pad;
     double t_end;                 /* rad */
     double q;                     /* charge [C] */
     const double *x0;             /* device [m][5]: r, pr, z, pz, P */
     double *x1;                   /* device [m][4]: r, pr, z, pz at t_end */
-    double *traj;                 /* device [m][n_points][2]: r, pr at every point, or NULL */
+    double *traj;                 /* device [m][n_points][traj_cols] at every point, or NULL */
 } ffa_theta_track_desc;
 
 int ffa_theta_track(const struct ffa_fieldmap *fm, const ffa_theta_track_desc *desc, void *stream);

@@ -507,18 +507,30 @@ static void seo_rhs(const orc_field *f, double t, const double *x, double P, dou
 /* rk4_solve / rk4_solve_vect (src/FFAG_track.py:582-640) in the azimuth:
  * m trajectories x0[m][5] = r, pr, z, pz, P over n_points - 1 steps of
  * h = t_end / (n_points - 1); stage azimuths i*h (time_mode 0) or a running
- * sum (time_mode 1).  x1[m][4] the end state, traj[m][n_points][2] (r, pr)
- * when not NULL. */
+ * sum (time_mode 1).  x1[m][4] the end state, traj[m][n_points][nc] when
+ * not NULL: r, pr (nc = 2) or r, pr, z, pz, Bz, Br, Bfi at each point (nc = 7). */
+static void theta_record(const orc_field *f, const double *x, double ts, double *row, int nc)
+{
+    row[0] = x[0];
+    row[1] = x[1];
+    if (nc == 7) {
+        row[2] = x[2];
+        row[3] = x[3];
+        double fim = fmod(fmod(ts, 2.0 * M_PI), 2.0 * M_PI / (double)f->nsectors);
+        analytic_B(f, x[0], fim, x[2], &row[4], &row[5], &row[6]);
+    }
+}
+
 void orc_theta_track(const orc_field *f, const double *x0, int64_t m, int n_points, int time_mode,
-                     double t_end, double q, double *x1, double *traj)
+                     double t_end, double q, double *x1, double *traj, int nc)
 {
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < m; ++i) {
         double x[4] = {x0[5 * i], x0[5 * i + 1], x0[5 * i + 2], x0[5 * i + 3]};
         double P = x0[5 * i + 4];
         double h = t_end / (double)(n_points - 1);
-        double *tr = traj ? traj + i * (int64_t)n_points * 2 : NULL;
-        if (tr) { tr[0] = x[0]; tr[1] = x[1]; }
+        double *tr = traj ? traj + i * (int64_t)n_points * nc : NULL;
+        if (tr) theta_record(f, x, 0.0, tr, nc);
         double t = 0.0;
         for (int s = 0; s < n_points - 1; ++s) {
             if (time_mode == 0) t = (double)s * h;
@@ -535,7 +547,7 @@ void orc_theta_track(const orc_field *f, const double *x0, int64_t m, int n_poin
                 x[c] = x[c] + (k1[c] + 2 * k2[c] + 2 * k3[c] + k4[c]) / 6;
             }
             if (time_mode != 0) t = t + h;
-            if (tr) { tr[2 * (s + 1)] = x[0]; tr[2 * (s + 1) + 1] = x[1]; }
+            if (tr) theta_record(f, x, time_mode != 0 ? t : (double)(s + 1) * h, tr + (int64_t)(s + 1) * nc, nc);
         }
         for (int c = 0; c < 4; ++c) x1[4 * i + c] = x[c];
     }

@@ -84,7 +84,7 @@ def lib():
         L.orc_track.restype = C.c_double
         L.orc_inject.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
         L.orc_theta_track.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
-                                      C.c_double, C.c_void_p, C.c_void_p]
+                                      C.c_double, C.c_void_p, C.c_void_p, C.c_int]
         L.orc_sc_step.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_sc_step.restype = C.c_int
@@ -128,15 +128,15 @@ class ThetaTracker:
         self.field = _orc_field(bmap, self._keep)
         self.q = float(q)
 
-    def run(self, x0, t_end, h, time_mode=0, traj=False):
+    def run(self, x0, t_end, h, time_mode=0, traj=False, traj_cols=2):
         x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, 5)
         m = x0.shape[0]
         n = int((t_end - 0) / h)
         t_points = np.linspace(0, t_end, n)
         x1 = np.zeros((m, 4))
-        tr = np.zeros((m, n, 2)) if traj else None
+        tr = np.zeros((m, n, traj_cols)) if traj else None
         lib().orc_theta_track(C.byref(self.field), x0.ctypes.data, m, n, int(time_mode), float(t_end), self.q,
-                              x1.ctypes.data, tr.ctypes.data if traj else None)
+                              x1.ctypes.data, tr.ctypes.data if traj else None, traj_cols)
         return x1, tr, t_points
 
 

@@ -89,7 +89,8 @@ class Crossing(C.Structure):
 
 
 class ThetaTrackDesc(C.Structure):
-    _fields_ = [("m", C.c_int64), ("n_points", C.c_int32), ("time_mode", C.c_int32), ("t_end", C.c_double),
+    _fields_ = [("m", C.c_int64), ("n_points", C.c_int32), ("time_mode", C.c_int32), ("traj_cols", C.c_int32),
+                ("pad", C.c_int32), ("t_end", C.c_double),
                 ("q", C.c_double), ("x0", d_p), ("x1", d_p), ("traj", d_p)]
 
 

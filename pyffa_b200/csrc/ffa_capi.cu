@@ -288,6 +288,7 @@ int ffa_theta_track(const ffa_fieldmap *fm, const ffa_theta_track_desc *d, void 
     if (!fm || !d || d->m < 0 || d->n_points < 2 || !(d->t_end > 0.0) || !d->x0 || !d->x1)
         return FFA_ERR_INVALID;
     if (d->time_mode != 0 && d->time_mode != 1) return FFA_ERR_INVALID;
+    if (d->traj && d->traj_cols != 2 && d->traj_cols != 7) return FFA_ERR_INVALID;
     if (d->m == 0) return FFA_OK;
     return launch_theta_track(fm->k, *d, as_stream(stream)) == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }

@@ -658,9 +658,22 @@ __global__ void __launch_bounds__(64) theta_track_kernel(const FieldK f, const f
     double x[4] = {d.x0[5 * i], d.x0[5 * i + 1], d.x0[5 * i + 2], d.x0[5 * i + 3]};
     const double P = d.x0[5 * i + 4], q = d.q;
     const double h = d.t_end / (double)(d.n_points - 1);
-    double *tr = d.traj ? d.traj + (int64_t)i * d.n_points * 2 : nullptr;
-    if (tr) { tr[0] = x[0]; tr[1] = x[1]; }
+    const int nc = d.traj_cols;
+    double *tr = d.traj ? d.traj + (int64_t)i * d.n_points * nc : nullptr;
     double t = 0.0;
+    // row of point s: the state and, for 7 columns, the field there
+    auto record = [&](int s, double ts) {
+        double *row = tr + (int64_t)s * nc;
+        row[0] = x[0];
+        row[1] = x[1];
+        if (nc == 7) {
+            row[2] = x[2];
+            row[3] = x[3];
+            const double fim = fmod(fmod(ts, 2.0 * PI), f.period);
+            analytic_b64(f, x[0], 1.0 / x[0], fim, x[2], row[4], row[5], row[6]);
+        }
+    };
+    if (tr) record(0, 0.0);
     for (int s = 0; s < d.n_points - 1; ++s) {
         if (d.time_mode == 0) t = (double)s * h;
         double k1[4], k2[4], k3[4], k4[4], y[4], dd[4];
@@ -676,7 +689,7 @@ __global__ void __launch_bounds__(64) theta_track_kernel(const FieldK f, const f
             x[c] = x[c] + (k1[c] + 2 * k2[c] + 2 * k3[c] + k4[c]) / 6;
         }
         if (d.time_mode != 0) t = t + h;
-        if (tr) { tr[2 * (s + 1)] = x[0]; tr[2 * (s + 1) + 1] = x[1]; }
+        if (tr) record(s + 1, d.time_mode != 0 ? t : (double)(s + 1) * h);
     }
     for (int c = 0; c < 4; ++c) d.x1[4 * i + c] = x[c];
 }

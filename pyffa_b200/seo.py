@@ -53,9 +53,10 @@ class ThetaTracker:
         self.fm = bmap.device_map(self.dev)
         self.q = float(q)
 
-    def run(self, x0, t_end, h, time_mode=0, traj=False):
-        """x0: (m, 5) r, pr, z, pz, P.  Returns (x1 (m, 4), traj (m, n, 2) or
-        None, t_points) for the reference's n = int(t_end / h) azimuth points."""
+    def run(self, x0, t_end, h, time_mode=0, traj=False, traj_cols=2):
+        """x0: (m, 5) r, pr, z, pz, P.  Returns (x1 (m, 4), traj (m, n,
+        traj_cols) or None, t_points) for the reference's n = int(t_end / h)
+        azimuth points; 7 columns add z, pz and the field Bz, Br, Bfi."""
         import torch
         x0 = np.ascontiguousarray(x0, dtype=np.float64).reshape(-1, 5)
         m = x0.shape[0]
@@ -64,9 +65,10 @@ class ThetaTracker:
         f64 = dict(dtype=torch.float64, device=self.dev)
         tx0 = torch.from_numpy(x0).to(self.dev)
         tx1 = torch.empty((m, 4), **f64)
-        ttr = torch.empty((m, n, 2), **f64) if traj else None
+        ttr = torch.empty((m, n, traj_cols), **f64) if traj else None
         d = _lib.ThetaTrackDesc()
         d.m, d.n_points, d.time_mode, d.t_end, d.q = m, n, int(time_mode), float(t_end), self.q
+        d.traj_cols = traj_cols
         d.x0, d.x1 = tx0.data_ptr(), tx1.data_ptr()
         d.traj = ttr.data_ptr() if traj else None
         stream = torch.cuda.current_stream(self.dev)
@@ -329,9 +331,8 @@ def LoadSEOParams(SEOFileName, Ek_c):
 def main_SEO(json_path: str, device=None) -> str:
     """examples/main_SEO.py: energies start_Ek..end_Ek by delta_Ek plus
     extra_Ek, the map folder's config_Bmap.json (with Bmap.Bmean), the SEO
-    files into <map folder>/<SEO_folder>, and the configuration copied there
-    as config_SEO.json.  Returns the SEO folder.  (The reference also writes
-    Twiss tables with FFAG_BetaFuncCalc; those are not produced here.)"""
+    files and the Twiss tables into <map folder>/<SEO_folder>, and the
+    configuration copied there as config_SEO.json.  Returns the SEO folder."""
     import json
 
     from .fields import FFAG_Bfield_analytical
@@ -347,7 +348,143 @@ def main_SEO(json_path: str, device=None) -> str:
     gp = FFAG_GlobalParameters()
     gp.AddBMap(FFAG_Bfield_analytical(os.path.join(c["Bmap_path"], "config_Bmap.json"), 0, AddNumricalMap=False))
     gp.SEO_SaveFold = c["SEO_folder"]
-    fold = FFAG_SearchSEO(gp, device).SearchSEOsControllerVect(Ek)
+    finder = FFAG_SearchSEO(gp, device)
+    fold = finder.SearchSEOsControllerVect(Ek)
+    CalcBetaFunc(fold, Ek, gp, tracker=finder.tracker)
     with open(os.path.join(fold, "config_SEO.json"), "w") as f:
         json.dump(cfg, f, indent=2, sort_keys=True)
     return fold
+
+
+# ------------------------------------------------------------------ Twiss
+
+
+def _two_points(X, xi):
+    """find_two_points_non_uniform_vect (src/FFAG_MathTools.py:59-82): bracketing
+    indices, end intervals extended."""
+    xi = np.atleast_1d(xi)
+    right = np.searchsorted(X, xi, side="right")
+    left = right - 1
+    i0, i1 = left.copy(), right.copy()
+    lo = left < 0
+    i0[lo], i1[lo] = 0, 1
+    hi = right > len(X) - 1
+    i0[hi], i1[hi] = len(X) - 2, len(X) - 1
+    return i0, i1
+
+
+def _interp_2p5d(M, ax0, ax1, fi0, pid):
+    """My2p5DInterp (src/FFAG_MathTools.py:329-364): bilinear in (azimuth
+    step, particle id) of M[step, id, :], the reference's weight formulas."""
+    a0, a1 = _two_points(ax0, fi0)
+    b0, b1 = _two_points(ax1, pid)
+    x0, x1, y0, y1 = ax0[a0], ax0[a1], ax1[b0], ax1[b1]
+    L00 = (fi0 - x1) * (pid - y1) / (x0 - x1) / (y0 - y1)
+    L01 = (fi0 - x1) * (pid - y0) / (x0 - x1) / (y1 - y0)
+    L10 = (fi0 - x0) * (pid - y1) / (x1 - x0) / (y0 - y1)
+    L11 = (fi0 - x0) * (pid - y0) / (x1 - x0) / (y1 - y0)
+    return (L00[:, None] * M[a0, b0, :] + L01[:, None] * M[a0, b1, :] + L10[:, None] * M[a1, b0, :]
+            + L11[:, None] * M[a1, b1, :])
+
+
+def _find_coef(r1_s, pr1_s, r1_e, pr1_e, r2_s, pr2_s, r2_e, pr2_e):
+    """Transfer-matrix elements from two trajectories by Cramer's rule
+    (FFAG_BetaFuncCalc.find_coef, src/FFAG_BetaFunc.py:26-43)."""
+    m00 = np.array([[r1_s, pr1_s, 0, 0], [0, 0, r1_s, pr1_s], [r2_s, pr2_s, 0, 0], [0, 0, r2_s, pr2_s]])
+    rhs = np.array([r1_e, pr1_e, r2_e, pr2_e])
+    d0 = np.linalg.det(m00)
+    out = []
+    for col in range(4):
+        m = m00.copy()
+        m[:, col] = rhs
+        out.append(np.linalg.det(m) / d0)
+    return tuple(out)
+
+
+def load_seo_params_vect(SEOFileName, Ek_arr):
+    """FFAG_BetaFuncCalc.LoadSEOParams (src/FFAG_BetaFunc.py:17-24)."""
+    path = os.path.dirname(os.path.dirname(SEOFileName))
+    data = np.atleast_2d(np.loadtxt(SEOFileName, skiprows=2))
+    Ek0, r0, pr0 = data[:, 1], data[:, 6], data[:, 7]
+    Ek_arr = np.atleast_1d(np.asarray(Ek_arr, dtype=np.float64))
+    i0, i1 = _two_points(Ek0, Ek_arr)
+    lin = lambda Y: Y[i0] + (Ek_arr - Ek0[i0]) / (Ek0[i1] - Ek0[i0]) * (Y[i1] - Y[i0])
+    return np.column_stack([Ek_arr, lin(r0), lin(pr0)]), path, data
+
+
+def CalcBetaFunc(SEOPATHName, Ek_arr, GlobalParas=None, tracker=None, device=None, write=True):
+    """Twiss functions along one sector for every energy
+    (FFAG_BetaFuncCalc.CalcBetaFunc, src/FFAG_BetaFunc.py:45-240): five
+    trajectories per energy (the closed orbit and r, pr, z, pz nudged by
+    1e-7) tracked over two sectors in one batched launch; at 1000 azimuths
+    the one-sector transfer matrices from the interpolated trajectories give
+    beta = m12 / sin(mu), alpha = (m11 - m22) / (2 sin(mu)).  Writes
+    BetaFuncR/Z.txt, AlphaFuncR/Z.txt and the field along the orbit Bz/Br/Bf.txt
+    into SEOPATHName; returns (beta_r, beta_z, alpha_r, alpha_z, fi_deg)."""
+    from .constants import FFAG_GlobalParameters
+    from .fields import FFAG_Bfield_analytical
+    h = 0.001
+    Ek_arr = np.asarray(Ek_arr, dtype=np.float64)
+    nE = len(Ek_arr)
+    ini, bmap_path, _ = load_seo_params_vect(os.path.join(SEOPATHName, "SEO_ini.txt"), Ek_arr)
+    conv = FFAG_ConversionTools()
+    if GlobalParas is None:
+        GlobalParas = FFAG_GlobalParameters()
+        GlobalParas.AddBMap(FFAG_Bfield_analytical(os.path.join(bmap_path, "config_Bmap.json"), 0,
+                                                   AddNumricalMap=False))
+    bm = GlobalParas.Bmap
+    if tracker is None:
+        tracker = ThetaTracker(bm, GlobalParas.q, device)
+    P0 = conv.Ek2P(ini[:, 0])
+    base = np.column_stack((ini[:, 1], ini[:, 2], np.zeros(nE), np.zeros(nE), P0))
+    delta = np.array([[0, 0, 0, 0, 0], [1e-7, 0, 0, 0, 0], [0, 1e-7, 0, 0, 0], [0, 0, 1e-7, 0, 0],
+                      [0, 0, 0, 1e-7, 0]], dtype=np.float64)
+    x0 = np.repeat(base, 5, axis=0) + np.tile(delta, (nE, 1))
+    sector = np.pi * 2 / bm.Nsectors
+    t_end = np.pi * 2 * 2 / bm.Nsectors + 0
+    _, tr, tp = tracker.run(x0, t_end, h, time_mode=1, traj=True, traj_cols=7)
+    hs = tp[1] - tp[0]
+    times = np.zeros(tr.shape[1])
+    for i in range(1, len(times)):
+        times[i] = times[i - 1] + hs
+    M = np.concatenate((times[None, :, None].repeat(x0.shape[0], axis=0).transpose(1, 0, 2),
+                        tr[:, :, 0:4].transpose(1, 0, 2)), axis=2)       # [step, id, (t, r, pr, z, pz)]
+    ids = np.arange(x0.shape[0], dtype=np.float64)
+    fi0 = np.linspace(0, sector, 1000)
+    br, bz, ar, az = (np.zeros((nE, 1000)) for _ in range(4))
+    for n in range(1000):
+        ts = fi0[n]
+        te = ts + sector
+        s = _interp_2p5d(M, times, ids, np.full(len(ids), ts), ids)
+        e = _interp_2p5d(M, times, ids, np.full(len(ids), te), ids)
+        for k in range(nE):
+            xs = s[k * 5 + 1:(k + 1) * 5, 1:5] - s[k * 5, 1:5]
+            xe = e[k * 5 + 1:(k + 1) * 5, 1:5] - e[k * 5, 1:5]
+            a11, a12, a21, a22 = _find_coef(xs[0, 0], xs[0, 1], xe[0, 0], xe[0, 1],
+                                            xs[1, 0], xs[1, 1], xe[1, 0], xe[1, 1])
+            b11, b12, b21, b22 = _find_coef(xs[2, 2], xs[2, 3], xe[2, 2], xe[2, 3],
+                                            xs[3, 2], xs[3, 3], xe[3, 2], xe[3, 3])
+            cr, cz = (a11 + a22) / 2, (b11 + b22) / 2
+            sr, sz = np.sqrt(1 - cr ** 2), np.sqrt(1 - cz ** 2)
+            if a12 * sr < 0:
+                sr = sr * (-1)
+            if b12 * sz < 0:
+                sz = sz * (-1)
+            br[k, n], bz[k, n] = a12 / sr, b12 / sz
+            ar[k, n], az[k, n] = (a11 - a22) / sr / 2, (b11 - b22) / sz / 2
+    fi_deg = np.rad2deg(fi0)
+    if write:
+        a = np.insert(Ek_arr, 0, 0)
+        files = [("BetaFuncR.txt", "unitBeta=m", np.vstack((fi_deg, br))),
+                 ("BetaFuncZ.txt", "unitBeta=m", np.vstack((fi_deg, bz))),
+                 ("AlphaFuncR.txt", "unitAlpha=1", np.vstack((fi_deg, ar))),
+                 ("AlphaFuncZ.txt", "unitAlpha=m", np.vstack((fi_deg, az))),
+                 ("Bz.txt", "unitB=T", np.vstack((times[None, :], tr[::5, :, 4]))),
+                 ("Br.txt", "unitB=T", np.vstack((times[None, :], tr[3::5, :, 5]))),
+                 ("Bf.txt", "unitB=T", np.vstack((times[None, :], tr[3::5, :, 6])))]
+        for name, unit, mat in files:
+            with open(os.path.join(SEOPATHName, name), "w") as f:
+                f.write(f"unitEk=MeV, unitFi=deg, {unit}\n")
+            with open(os.path.join(SEOPATHName, name), "a") as f:
+                np.savetxt(f, np.column_stack((a, mat)))
+    return br, bz, ar, az, fi_deg

@@ -313,15 +313,17 @@ def seo_main(ref):
     """The reference's closed-orbit search (FFAG_SearchSEO.SearchSEOsControllerVect,
     src/FFAG_track.py:1380-1512, driven as examples/main_SEO.py:13-31) on the
     synthetic lattice (two energies) and on the same lattice with a
-    25-degree spiral (one energy); the SEO files it writes (golden_seo.npz)."""
+    25-degree spiral (two energies), then FFAG_BetaFuncCalc.CalcBetaFunc as
+    main_SEO does; the files they write (golden_seo.npz)."""
     sys.path.insert(0, os.path.join(HERE, "shims"))
     sys.path.insert(0, os.path.join(ref, "src"))
     from FFAG_Field import FFAG_Bfield_analytical, FFAG_BField_Error
     from FFAG_ParasAndConversion import FFAG_GlobalParameters
     from FFAG_track import FFAG_SearchSEO
+    from FFAG_BetaFunc import FFAG_BetaFuncCalc
 
     out = {}
-    for key, spiral, energies in (("flat", 0.0, [300.0, 330.0]), ("spiral", 25.0, [310.0])):
+    for key, spiral, energies in (("flat", 0.0, [300.0, 330.0]), ("spiral", 25.0, [310.0, 320.0])):
         with tempfile.TemporaryDirectory() as tmp:
             cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
             cfg["Bmap"]["SpiralAngle_deg"] = spiral
@@ -330,6 +332,11 @@ def seo_main(ref):
             with open(path, "w") as f:
                 json.dump(cfg, f)
             FFAG_Bfield_analytical(path, 0, AddNumricalMap=False).UpdataConfig()
+            # CalcBetaFunc opens the map folder's order-0 tables (it evaluates
+            # the analytic field, so their values are not used)
+            shape = (len(np.linspace(7.5, 9.5, 201)), int((np.pi * 2 / 12) / np.deg2rad(0.05)) + 1)
+            for comp in ("Br", "Bz", "Bfi"):
+                np.savez(os.path.join(tmp, f"{comp}_order_0.npz"), **{f"{comp}_Taylor_coeff": np.zeros(shape)})
             gp = FFAG_GlobalParameters()
             gp.AddBMap(FFAG_Bfield_analytical(path, 0, AddNumricalMap=False))
             gp.AddBHarmonics(FFAG_BField_Error([], False))
@@ -344,6 +351,10 @@ def seo_main(ref):
             out[f"{key}_r"] = np.loadtxt(os.path.join(fold, "SEO_r.txt"), skiprows=1)
             out[f"{key}_pr"] = np.loadtxt(os.path.join(fold, "SEO_pr.txt"), skiprows=1)
             out[f"{key}_Ek"] = np.array(energies)
+            # Twiss tables (FFAG_BetaFuncCalc.CalcBetaFunc, src/FFAG_BetaFunc.py:45-240)
+            FFAG_BetaFuncCalc().CalcBetaFunc(fold, np.array(energies))
+            for name in ("BetaFuncR", "BetaFuncZ", "AlphaFuncR", "AlphaFuncZ", "Bz", "Br", "Bf"):
+                out[f"{key}_{name}"] = np.loadtxt(os.path.join(fold, name + ".txt"), skiprows=1)
     path = os.path.join(HERE, "golden_seo.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -2,10 +2,10 @@
 
 tests/golden/golden_seo.npz holds what the reference's
 SearchSEOsControllerVect wrote for the synthetic lattice (300 and 330 MeV)
-and for the same lattice with a 25-degree spiral (310 MeV)
-(tests/golden/make_golden.py --seo).  The search runs on the host rules of
-pyffa_b200.seo with either the oracle's azimuth tracker (CPU) or the
-library's (GPU)."""
+and for the same lattice with a 25-degree spiral (310 and 320 MeV), and
+the Twiss tables of FFAG_BetaFuncCalc (tests/golden/make_golden.py --seo).
+The search runs on the host rules of pyffa_b200.seo with either the
+oracle's azimuth tracker (CPU) or the library's (GPU)."""
 import json
 import os
 import tempfile
@@ -88,6 +88,41 @@ def test_load_seo_params_roundtrip(gs):
     np.testing.assert_array_equal(r, gs["flat_r"])
 
 
+def _check_twiss(gs, key, tracker_factory):
+    gp = _gp(gs, key)
+    d = tempfile.mkdtemp()
+    fold = os.path.join(d, "seo")
+    os.makedirs(fold)
+    lines, ref = _golden_table(gs, key)
+    Ek = gs[key + "_Ek"]
+    S.write_seo_files(fold, d, 0.001, ref, gs[key + "_r"][0, 1:], Ek, gs[key + "_r"][1:, 1:],
+                      gs[key + "_pr"][1:, 1:])
+    S.CalcBetaFunc(fold, Ek, gp, tracker=tracker_factory(gp))
+    for name, tol in (("BetaFuncR", 1e-6), ("BetaFuncZ", 1e-6), ("AlphaFuncR", 1e-6), ("AlphaFuncZ", 1e-6),
+                      ("Bz", 1e-12), ("Br", 1e-12), ("Bf", 1e-12)):
+        got = np.loadtxt(os.path.join(fold, name + ".txt"), skiprows=1)
+        want = gs[f"{key}_{name}"]
+        assert got.shape == want.shape, name
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[:, 0], want[:, 0])
+        scale = np.abs(want[1:, 1:]).max()
+        assert np.abs(got[1:, 1:] - want[1:, 1:]).max() <= tol * scale, (name, np.abs(got - want).max())
+
+
+@pytest.mark.parametrize("key", ["flat", "spiral"])
+def test_twiss_with_oracle_tracker_matches_reference(gs, key):
+    _check_twiss(gs, key, lambda gp: O.ThetaTracker(gp.Bmap, gp.q))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", ["flat", "spiral"])
+def test_gpu_twiss_matches_reference(gs, key):
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA device required")
+    _check_twiss(gs, key, lambda gp: S.ThetaTracker(gp.Bmap, gp.q))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("key", ["flat", "spiral"])
 def test_gpu_search_matches_reference(gs, key):
@@ -104,15 +139,16 @@ def test_gpu_theta_tracks_match_oracle(gs):
     if not torch.cuda.is_available():
         pytest.skip("CUDA device required")
     gp = _gp(gs, "spiral")
+    from pyffa_b200.constants import FFAG_ConversionTools
     rng = np.random.Generator(np.random.PCG64(5))
     m = 64
-    P = 1.0e-18 * (1 + 0.05 * rng.random(m))
+    P = FFAG_ConversionTools().Ek2P(300.0 + 20.0 * rng.random(m))
     x0 = np.stack([8.2 + 0.05 * rng.standard_normal(m), 0.1 + 0.01 * rng.standard_normal(m),
-                   1e-3 * rng.standard_normal(m), 1e-3 * rng.standard_normal(m),
-                   np.full(m, 8.0e-19) + P * 0], axis=1)
-    x0[:, 4] = S.FFAG_SearchSEO(gp, tracker=O.ThetaTracker(gp.Bmap, gp.q)).conv.Ek2P(300.0)
+                   1e-3 * rng.standard_normal(m), 1e-3 * rng.standard_normal(m), P], axis=1)
     for mode in (0, 1):
-        g1, gt, _ = S.ThetaTracker(gp.Bmap, gp.q).run(x0, np.pi / 6, 0.001, time_mode=mode, traj=True)
-        o1, ot, _ = O.ThetaTracker(gp.Bmap, gp.q).run(x0, np.pi / 6, 0.001, time_mode=mode, traj=True)
-        assert np.abs(g1 - o1).max() <= 1e-12 * np.abs(o1).max()
-        assert np.abs(gt - ot).max() <= 1e-12 * np.abs(ot).max()
+        for cols in (2, 7):
+            g1, gt, _ = S.ThetaTracker(gp.Bmap, gp.q).run(x0, np.pi / 6, 0.001, mode, True, cols)
+            o1, ot, _ = O.ThetaTracker(gp.Bmap, gp.q).run(x0, np.pi / 6, 0.001, mode, True, cols)
+            assert np.abs(g1 - o1).max() <= 1e-12 * np.abs(o1).max()
+            for c in range(cols):
+                assert np.abs(gt[..., c] - ot[..., c]).max() <= 1e-12 * np.abs(ot[..., c]).max(), (mode, c)
