@@ -1,0 +1,415 @@
+"""Injected-bunch generation (GenerateBunches and its helpers,
+src/FFAG_Distribution.py:16-1640), seeded.
+
+The reference draws every particle from Python's and NumPy's global random
+streams one particle at a time (unseeded), so its bunches are reproducible
+only by pre-generating them.  Here each generator draws all particles of a
+sub-bunch at once from a numpy Generator (seeded through ``BunchPara["Seed"]``
+or the ``rng`` argument); the transformations — normalised coordinates to
+(u, u') through the Twiss parameters, the KV / water-bag / Gauss / hollow
+shapes and their emittance factors, the injection point on the closed orbit
+from the SEO tables, the painting offsets — are the reference's, so the
+bunches agree with the reference's in distribution (moments, emittances,
+Twiss), not particle by particle.
+
+The output is the reference's p-format matrix (N x 16: r, pr, z, pz, fi,
+Ek [MeV], inj_t [ns], flags 0, RF phase 0, space-charge fields 0, Bunch_ID,
+Local_ID, Global_ID), one block per painted sub-bunch.
+"""
+from __future__ import annotations
+
+import math
+import os
+import re
+
+import numpy as np
+
+from .constants import COLUMNS
+
+# ---------------------------------------------------------------- Twiss
+
+
+class TwissContainer:
+    """alpha, beta, emittance; (u_norm, u'_norm) -> (u, u')
+    (src/FFAG_Distribution.py:16-73)."""
+
+    def __init__(self, alpha, beta, emittance):
+        self.alpha = alpha
+        self.beta = beta
+        self.emittance = emittance
+        self._init()
+
+    def _init(self):
+        self.gamma = (1.0 + self.alpha ** 2) / self.beta
+        self.u_max = math.sqrt(self.beta * self.emittance)
+        self.up_coeff = math.sqrt(self.emittance / self.beta)
+        self.up_max = math.sqrt(self.gamma * self.emittance)
+
+    def setEmittance(self, emittance):
+        self.emittance = emittance
+        self._init()
+
+    def getNormalizedH(self, u, up):
+        return (u ** 2 + (self.alpha * u + self.beta * up) ** 2) / (self.beta * self.emittance)
+
+    def getU_Max(self):
+        return self.u_max
+
+    def getUP_Max(self):
+        return self.up_max
+
+    def getU_UP(self, u_norm, up_norm):
+        return self.u_max * u_norm, self.up_coeff * (up_norm - self.alpha * u_norm)
+
+    def getAlphaBetaGammaEmitt(self):
+        return self.alpha, self.beta, self.gamma, self.emittance
+
+    def getAlphaBetaEmitt(self):
+        return self.alpha, self.beta, self.emittance
+
+
+_default_rng = np.random.default_rng()
+
+
+class _Dist:
+    """sample(n, rng) draws n particles at once; getCoordinates() draws one."""
+
+    def getCoordinates(self):
+        return tuple(float(c[0]) for c in self.sample(1, _default_rng))
+
+
+class KVDist1D(_Dist):
+    """1D KV; 100 % emittance = 2 x rms."""
+
+    def __init__(self, twiss=None):
+        twiss = twiss or TwissContainer(0., 1., 1.)
+        a, b, e = twiss.getAlphaBetaEmitt()
+        self.twiss = TwissContainer(a, b, 2 * e)
+
+    def sample(self, n, rng):
+        x = np.sin(2 * np.pi * (rng.random(n) - 0.5))
+        xp = rng.choice((-1.0, 1.0), n) * np.sqrt(1.0 - x ** 2)
+        return self.twiss.getU_UP(x, xp)
+
+    def getTwissContainers(self):
+        return (self.twiss,)
+
+
+class WaterBagDist1D(_Dist):
+    def __init__(self, twiss=None):
+        twiss = twiss or TwissContainer(0., 1., 1.)
+        a, b, e = twiss.getAlphaBetaEmitt()
+        self.kv = KVDist1D(TwissContainer(a, b, 2 * e))
+
+    def sample(self, n, rng):
+        u, up = self.kv.sample(n, rng)
+        g = np.sqrt(rng.random(n))
+        return g * u, g * up
+
+    def getTwissContainers(self):
+        return self.kv.getTwissContainers()
+
+
+class HollowWaterBagDist1D(_Dist):
+    def __init__(self, twiss=None):
+        twiss = twiss or TwissContainer(0., 1., 1.)
+        a, b, e = twiss.getAlphaBetaEmitt()
+        self.kv = KVDist1D(TwissContainer(a, b, e / 2))
+
+    def sample(self, n, rng):
+        u, up = self.kv.sample(n, rng)
+        g = rng.uniform(0.4, 1.0, n)
+        return g * u, g * up
+
+    def getTwissContainers(self):
+        return self.kv.getTwissContainers()
+
+
+class GaussDist1D(_Dist):
+    def __init__(self, twiss=None, cut_off=-1.0):
+        self.twiss = twiss or TwissContainer(0., 1., 1.)
+        self.cut_off = cut_off
+
+    def sample(self, n, rng):
+        x = rng.standard_normal(n)
+        xp = rng.standard_normal(n)
+        if self.cut_off > 0:
+            bad = x ** 2 + xp ** 2 > self.cut_off ** 2
+            while bad.any():
+                k = int(bad.sum())
+                x[bad], xp[bad] = rng.standard_normal(k), rng.standard_normal(k)
+                bad = x ** 2 + xp ** 2 > self.cut_off ** 2
+        return self.twiss.getU_UP(x, xp)
+
+    def getTwissContainers(self):
+        return (self.twiss,)
+
+
+class KVDist2D(_Dist):
+    """2D KV (uniform on the 4D hyper-ellipsoid surface); 100 % = 4 x rms."""
+
+    def __init__(self, twissX=None, twissY=None):
+        twissX = twissX or TwissContainer(0., 1., 1.)
+        twissY = twissY or TwissContainer(0., 1., 1.)
+        ax, bx, ex = twissX.getAlphaBetaEmitt()
+        ay, by, ey = twissY.getAlphaBetaEmitt()
+        self.twissX = TwissContainer(ax, bx, 4 * ex)
+        self.twissY = TwissContainer(ay, by, 4 * ey)
+
+    def sample(self, n, rng):
+        phi = 2 * np.pi * (rng.random(n) - 0.5)
+        rho = np.sqrt(rng.random(n))
+        x, y = rho * np.cos(phi), rho * np.sin(phi)
+        p0 = np.sqrt(np.abs(1.0 - rho ** 2))
+        phi = 2 * np.pi * (rng.random(n) - 0.5)
+        xp, yp = p0 * np.cos(phi), p0 * np.sin(phi)
+        return (*self.twissX.getU_UP(x, xp), *self.twissY.getU_UP(y, yp))
+
+    def getTwissContainers(self):
+        return self.twissX, self.twissY
+
+
+class WaterBagDist2D(_Dist):
+    def __init__(self, twissX=None, twissY=None):
+        twissX = twissX or TwissContainer(0., 1., 1.)
+        twissY = twissY or TwissContainer(0., 1., 1.)
+        ax, bx, ex = twissX.getAlphaBetaEmitt()
+        ay, by, ey = twissY.getAlphaBetaEmitt()
+        self.kv = KVDist2D(TwissContainer(ax, bx, 6.0 * ex / 4.0), TwissContainer(ay, by, 6.0 * ey / 4.0))
+
+    def sample(self, n, rng):
+        x, xp, y, yp = self.kv.sample(n, rng)
+        g = np.sqrt(np.sqrt(rng.random(n)))
+        return g * x, g * xp, g * y, g * yp
+
+    def getTwissContainers(self):
+        return self.kv.getTwissContainers()
+
+
+class GaussDist2D(_Dist):
+    def __init__(self, twissX=None, twissY=None, cut_off=-1.0):
+        self.gx = GaussDist1D(twissX, cut_off)
+        self.gy = GaussDist1D(twissY, cut_off)
+
+    def sample(self, n, rng):
+        return (*self.gx.sample(n, rng), *self.gy.sample(n, rng))
+
+    def getTwissContainers(self):
+        return self.gx.twiss, self.gy.twiss
+
+
+class IndependentHollowWaterBagDist2D(_Dist):
+    """Hollow water bags in x-x' and y-y', kept where 0.3 <= (x/xm)^2 + (y/ym)^2 <= 1."""
+
+    def __init__(self, twissX=None, twissY=None):
+        self.hx = HollowWaterBagDist1D(twissX)
+        self.hy = HollowWaterBagDist1D(twissY)
+
+    def sample(self, n, rng):
+        out = [np.zeros(n) for _ in range(4)]
+        todo = np.arange(n)
+        xm, ym = self.hx.kv.twiss.getU_Max(), self.hy.kv.twiss.getU_Max()
+        while todo.size:
+            x, xp = self.hx.sample(todo.size, rng)
+            y, yp = self.hy.sample(todo.size, rng)
+            q = x ** 2 / xm ** 2 + y ** 2 / ym ** 2
+            ok = (q >= 0.3) & (q <= 1)
+            for o, v in zip(out, (x, xp, y, yp)):
+                o[todo[ok]] = v[ok]
+            todo = todo[~ok]
+        return tuple(out)
+
+    def getTwissContainers(self):
+        return self.hx.getTwissContainers(), self.hy.getTwissContainers()
+
+
+class CustomDist3D(_Dist):
+    """Transverse 2D distribution times a longitudinal 1D one."""
+
+    def __init__(self, dist_transverse, dist_longitudinal):
+        self.dist_transverse = dist_transverse
+        self.dist_longitudinal = dist_longitudinal
+
+    def sample(self, n, rng):
+        return (*self.dist_transverse.sample(n, rng), *self.dist_longitudinal.sample(n, rng))
+
+    def getTwissContainers(self):
+        return tuple(self.dist_transverse.getTwissContainers()) + (self.dist_longitudinal.getTwissContainers(),)
+
+
+def create_distribution(dist_type, twiss_transverse=None, twiss_longitudinal=None):
+    """src/FFAG_Distribution.py:1107-1149."""
+    if dist_type == "gauss":
+        return GaussDist2D(*twiss_transverse) if twiss_transverse is not None else GaussDist1D(twiss_longitudinal)
+    if dist_type == "kv":
+        return KVDist2D(*twiss_transverse) if twiss_transverse is not None else KVDist1D(twiss_longitudinal)
+    if dist_type == "waterbag":
+        return WaterBagDist2D(*twiss_transverse) if twiss_transverse is not None else \
+            WaterBagDist1D(twiss_longitudinal)
+    if dist_type == "hollow_waterbag":
+        return IndependentHollowWaterBagDist2D(*twiss_transverse) if twiss_transverse is not None else \
+            HollowWaterBagDist1D(twiss_longitudinal)
+    if dist_type in ("match", "UniformGauss"):
+        return GaussDist1D(twiss_longitudinal)
+    raise ValueError(f"Unknown distribution type: {dist_type}")
+
+
+# ------------------------------------------------------ SEO table lookups
+
+
+def _four_points(X, xi):
+    """find_four_points_non_uniform_vector (src/FFAG_MathTools.py:109-145)."""
+    right = np.searchsorted(X, xi, side="right")
+    left = right - 1
+    idx = np.stack([left - 1, left, right, right + 1])
+    lo = (left - 1) < 0
+    idx[:, lo] = np.array([0, 1, 2, 3])[:, None]
+    hi = (right + 1) > len(X) - 1
+    idx[:, hi] = np.array([len(X) - 4, len(X) - 3, len(X) - 2, len(X) - 1])[:, None]
+    return idx
+
+
+def Lagrange_interp_2D_vect(X, Y, Z, Xi, Yi):
+    """Four-by-four-point Lagrange interpolation (src/FFAG_MathTools.py:274-315);
+    returns (values, out-of-range flags)."""
+    X, Y, Z = np.asarray(X), np.asarray(Y), np.asarray(Z)
+    Xi, Yi = np.atleast_1d(Xi).astype(np.float64), np.atleast_1d(Yi).astype(np.float64)
+    ix, iy = _four_points(X, Xi), _four_points(Y, Yi)
+    xs, ys = X[ix], Y[iy]
+
+    def weights(s, v):
+        L = np.zeros((4, len(v)))
+        for a in range(4):
+            o = [b for b in range(4) if b != a]
+            num = (v - s[o[0]]) * (v - s[o[1]]) * (v - s[o[2]])
+            L[a] = num / (s[a] - s[o[0]]) / (s[a] - s[o[1]]) / (s[a] - s[o[2]])
+        return L
+
+    Lx, Ly = weights(xs, Xi), weights(ys, Yi)
+    zs = Z[ix[:, None, :], iy[None, :, :]]
+    val = np.sum(Lx[:, None, :] * Ly[None, :, :] * zs, axis=(0, 1))
+    flag = (np.searchsorted(X, Xi, side="right") - 2 < 0) | (np.searchsorted(X, Xi, side="right") + 1 > len(X) - 1)
+    return val, flag
+
+
+def LoadSEOBetaFunc(SEOPATHName, Ek_c, fi_c):
+    """(beta_z, beta_r, alpha_z, alpha_r) at (Ek_c, fi_c) from the Twiss files
+    (src/FFAG_Distribution.py:1430-1457).  As in the reference, fi_c [rad] is
+    reduced modulo the table's azimuth span converted to rad but looked up on
+    the table's azimuth axis, which is in degrees."""
+    out = []
+    for name in ("BetaFuncZ.txt", "BetaFuncR.txt", "AlphaFuncZ.txt", "AlphaFuncR.txt"):
+        d = np.loadtxt(os.path.join(SEOPATHName, name), skiprows=1)
+        Ek_axis, fi_axis, M = d[1:, 0], d[0, 1:], d[1:, 1:]
+        fi = np.mod(np.array([fi_c]), np.deg2rad(fi_axis[-1] - fi_axis[0]))
+        out.append(Lagrange_interp_2D_vect(Ek_axis, fi_axis, M, np.array([Ek_c]), fi)[0][0])
+    return tuple(out)
+
+
+def GetInitRAndFiForInjection(SEO_R, SEO_Pr, InjectCL, Ek):
+    """Injection point (azimuth, r, pr) on the closed orbit of energy Ek at the
+    azimuth InjectCL [deg] (src/FFAG_Distribution.py:1347-1414; the
+    central-line-file variant is not supported)."""
+    if isinstance(InjectCL, np.ndarray):
+        raise NotImplementedError("injection along a central-line file is not supported; give the azimuth in deg")
+    Ek_axis, fi_axis = SEO_R[1:, 0], SEO_R[0, 1:]
+    theta = np.array([np.deg2rad(InjectCL)])
+    r = Lagrange_interp_2D_vect(Ek_axis, fi_axis, SEO_R[1:, 1:], np.array([Ek]), theta)[0][0]
+    pr = Lagrange_interp_2D_vect(Ek_axis, fi_axis, SEO_Pr[1:, 1:], np.array([Ek]), theta)[0][0]
+    return theta[0], r, pr
+
+
+# ------------------------------------------------------------ generators
+
+
+def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit, num_points, InjTimeNanoSec,
+                                     LongitudeAlpha, LongitudeBeta, LongitudeT, acc_U0=100.0e3, acc_phi0=0.0,
+                                     TwissParams=None, dist_types=("gauss", "gauss"), dx_xp_y_yp=(0.0, 0.0, 0.0, 0.0),
+                                     Bunch_ID=0.0, bucket_obj=None, rng=None):
+    """One sub-bunch (src/FFAG_Distribution.py:1152-1345): returns (p-format
+    matrix, distribution, centre (r, pr, z, pz, Ek, t), bucket_obj)."""
+    from .seo import LoadSEOParams
+    rng = rng if rng is not None else _default_rng
+    eR, eZ, eFi = Emit[0] / 1000.0 / 1000.0, Emit[1] / 1000.0 / 1000.0, Emit[2]
+    ini, _, _ = LoadSEOParams(os.path.join(SEOFileName, "SEO_ini.txt"), Ek_c)
+    SEO_R = np.loadtxt(os.path.join(SEOFileName, "SEO_r.txt"), skiprows=1)
+    SEO_Pr = np.loadtxt(os.path.join(SEOFileName, "SEO_pr.txt"), skiprows=1)
+    Ek_c = ini[0]
+    if isinstance(InjectionPosition, dict):
+        fi_c, r_c, pr_c = InjectionPosition["fi"], InjectionPosition["r"], InjectionPosition["pr"]
+    elif isinstance(InjectionPosition, (float, int)):
+        fi_c, r_c, pr_c = GetInitRAndFiForInjection(SEO_R, SEO_Pr, float(InjectionPosition), Ek_c)
+    else:
+        raise ValueError("Unsupported type for InjectionPosition")
+    if TwissParams is not None:
+        bZ, bR, aZ, aR = TwissParams
+    else:
+        bZ, bR, aZ, aR = LoadSEOBetaFunc(SEOFileName, Ek_c, fi_c)
+    ttype, ltype = dist_types
+    if ltype == "match":
+        raise NotImplementedError("the RF-bucket-matched longitudinal distribution (FFAG_bucket) is not built")
+    if ltype == "kv":
+        eFi *= 2
+    tw_fi = TwissContainer(LongitudeAlpha, LongitudeBeta, eFi)
+    dist = CustomDist3D(create_distribution(ttype, twiss_transverse=(TwissContainer(aR, bR, eR),
+                                                                       TwissContainer(aZ, bZ, eZ))),
+                        create_distribution(ltype, twiss_longitudinal=tw_fi))
+    r, pr, z, pz, t_inj, Ek = dist.sample(num_points, rng)
+    if ltype == "UniformGauss":
+        sigma = math.sqrt(eFi / LongitudeBeta)
+        t_inj = rng.uniform(-0.5 * LongitudeT, 0.5 * LongitudeT, num_points)
+        Ek = rng.normal(0.0, sigma, num_points)
+    rc, prc, zc, pzc = r_c + dx_xp_y_yp[0], pr_c + dx_xp_y_yp[1], dx_xp_y_yp[2], dx_xp_y_yp[3]
+    a = np.zeros((num_points, 16))
+    a[:, COLUMNS["r"]] = r + rc
+    a[:, COLUMNS["vr"]] = pr + prc
+    a[:, COLUMNS["z"]] = z + zc
+    a[:, COLUMNS["vz"]] = pz + pzc
+    a[:, COLUMNS["fi"]] = fi_c
+    a[:, 5] = Ek + Ek_c
+    a[:, COLUMNS["inj_t"]] = t_inj + InjTimeNanoSec
+    a[:, 13] = Bunch_ID
+    a[:, 14] = np.arange(num_points)
+    a[:, 15] = np.arange(num_points)
+    return a, dist, (rc, prc, zc, pzc, Ek_c, InjTimeNanoSec), bucket_obj
+
+
+def _emap_paint_params(path):
+    with open(path) as f:
+        content = f.read()
+    get = lambda key: (float(m.group(1)) if (m := re.search(key + r" = ([\d.eE+-]+)", content)) else None)
+    return get("gap_azimuth"), get("acc_phi_paint"), get("acc_voltage_paint")
+
+
+def GenerateBunches(BunchPara, rng=None):
+    """All painted sub-bunches, stacked (src/FFAG_Distribution.py:1542-1640).
+    BunchPara holds the reference's keys (SEO, InjectEk, InjPosition,
+    ParticleNum, TransverseREmit, TransverseZEmit, LongitudeT, LongitudeDEk,
+    InjTimeNanoSec, TransverseDistType, LongitudeDistType, PaintEnable,
+    PaintMaxNum, PaintTimeInterval, PaintCurve, EmapPATHName) and optionally
+    Seed."""
+    if rng is None:
+        rng = np.random.default_rng(BunchPara.get("Seed"))
+    _, acc_phi0, acc_V0 = _emap_paint_params(BunchPara["EmapPATHName"])
+    if BunchPara["PaintEnable"]:
+        curve = np.loadtxt(BunchPara["PaintCurve"], skiprows=1)
+        nb = int(min(np.floor(np.max(curve[:, 0]) / BunchPara["PaintTimeInterval"]), BunchPara["PaintMaxNum"]))
+    else:
+        curve, nb = None, 1
+    LT, LdE = BunchPara["LongitudeT"], BunchPara["LongitudeDEk"]
+    out = []
+    bucket = None
+    for i in range(nb):
+        t_inj = i * BunchPara["PaintTimeInterval"]
+        if curve is not None:
+            off = tuple(np.interp(t_inj, curve[:, 0], curve[:, c]) for c in (1, 2, 3, 4))
+        else:
+            off = (0, 0, 0, 0)
+        sub, _, _, bucket = GenerateInitDistributionDtInjNew(
+            BunchPara["SEO"], BunchPara["InjPosition"], BunchPara["InjectEk"],
+            [BunchPara["TransverseREmit"], BunchPara["TransverseZEmit"], LT * LdE / 16], BunchPara["ParticleNum"],
+            t_inj, 0.0, LT / LdE, LT, acc_U0=acc_V0, acc_phi0=acc_phi0,
+            dist_types=(BunchPara["TransverseDistType"], BunchPara["LongitudeDistType"]), dx_xp_y_yp=off,
+            Bunch_ID=i, bucket_obj=bucket, rng=rng)
+        out.append(sub)
+    return np.vstack(out)

@@ -6,6 +6,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py --crossing [--ref /root/reference]   # crossing dumps
     python tests/golden/make_golden.py --mapgen [--ref /root/reference]     # z-Taylor maps
     python tests/golden/make_golden.py --seo [--ref /root/reference]        # closed orbits
+    python tests/golden/make_golden.py --bunch [--ref /root/reference]      # injected bunches
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -360,8 +361,82 @@ def seo_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def bunch_main(ref):
+    """The reference's bunch generator (GenerateBunches,
+    src/FFAG_Distribution.py:1542-1741) on SEO and Twiss tables it computed
+    for the synthetic lattice, with Python's and NumPy's global random
+    streams seeded; plus its deterministic helpers (injection point on the
+    closed orbit, Twiss at injection).  golden_bunch.npz."""
+    import random
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    from FFAG_BetaFunc import FFAG_BetaFuncCalc
+    from FFAG_Distribution import GenerateBunches, GetInitRAndFiForInjection, LoadSEOBetaFunc
+    from FFAG_Field import FFAG_Bfield_analytical, FFAG_BField_Error
+    from FFAG_ParasAndConversion import FFAG_GlobalParameters
+    from FFAG_track import FFAG_SearchSEO
+
+    out = {}
+    energies = [290.0, 300.0, 310.0, 320.0]
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
+        cfg["config"]["folder"] = tmp
+        path = os.path.join(tmp, "config_Bmap.json")
+        with open(path, "w") as f:
+            json.dump(cfg, f)
+        FFAG_Bfield_analytical(path, 0, AddNumricalMap=False).UpdataConfig()
+        shape = (201, int((np.pi * 2 / 12) / np.deg2rad(0.05)) + 1)
+        for comp in ("Br", "Bz", "Bfi"):
+            np.savez(os.path.join(tmp, f"{comp}_order_0.npz"), **{f"{comp}_Taylor_coeff": np.zeros(shape)})
+        gp = FFAG_GlobalParameters()
+        gp.AddBMap(FFAG_Bfield_analytical(path, 0, AddNumricalMap=False))
+        gp.AddBHarmonics(FFAG_BField_Error([], False))
+        gp.SEO_SaveFold = "seo"
+        fold = FFAG_SearchSEO(gp).SearchSEOsControllerVect(np.array(energies))
+        FFAG_BetaFuncCalc().CalcBetaFunc(fold, np.array(energies))
+        for name in ("SEO_ini", "SEO_r", "SEO_pr", "BetaFuncR", "BetaFuncZ", "AlphaFuncR", "AlphaFuncZ"):
+            with open(os.path.join(fold, name + ".txt")) as f:
+                out[f"file_{name}"] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+        emap = synthetic.emap_file(os.path.join(tmp, "emap.txt"))
+        with open(emap) as f:
+            out["file_emap"] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+        curve = os.path.join(tmp, "paint.txt")
+        with open(curve, "w") as f:
+            f.write("t_ns x px y py\n")
+            for t, x, px, y, py in ((0.0, 0.0, 0.0, 0.0, 0.0), (2000.0, 0.004, 0.001, 0.003, -0.001)):
+                f.write(f"{t} {x} {px} {y} {py}\n")
+        with open(curve) as f:
+            out["file_paint"] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+        SEO_R = np.loadtxt(os.path.join(fold, "SEO_r.txt"), skiprows=1)
+        SEO_Pr = np.loadtxt(os.path.join(fold, "SEO_pr.txt"), skiprows=1)
+        out["inj_point"] = np.array(GetInitRAndFiForInjection(SEO_R, SEO_Pr, 7.5, 305.0), dtype=np.float64)
+        out["inj_twiss"] = np.array(LoadSEOBetaFunc(fold, 305.0, float(out["inj_point"][0])), dtype=np.float64)
+        cases = {
+            "paint": dict(TransverseDistType="gauss", LongitudeDistType="UniformGauss", PaintEnable=True,
+                          ParticleNum=4000, PaintMaxNum=3, PaintTimeInterval=700.0),
+            "kv": dict(TransverseDistType="kv", LongitudeDistType="gauss", PaintEnable=False,
+                       ParticleNum=8000, PaintMaxNum=1, PaintTimeInterval=700.0),
+        }
+        for key, extra in cases.items():
+            bp = dict(SEO=fold, BmapPATHName=tmp, InjectEk=305.0, InjPosition=7.5, TransverseREmit=0.3,
+                      TransverseZEmit=0.2, LongitudeT=72.0, LongitudeDEk=1.0, InjTimeNanoSec=0,
+                      PlotFlag=False, PlotRMS=False, PaintCurve=curve, EmapPATHName=emap, **extra)
+            random.seed(7)
+            np.random.seed(7)
+            out[f"{key}_bunch"] = GenerateBunches(dict(bp))
+            bp_store = {k: v for k, v in bp.items() if k not in ("SEO", "BmapPATHName", "PaintCurve", "EmapPATHName")}
+            out[f"{key}_para"] = np.frombuffer(json.dumps(bp_store).encode(), dtype=np.uint8)
+    path = os.path.join(HERE, "golden_bunch.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    if "--seo" in sys.argv:
+    if "--bunch" in sys.argv:
+        sys.argv.remove("--bunch")
+        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
+        bunch_main(ref)
+    elif "--seo" in sys.argv:
         sys.argv.remove("--seo")
         ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
         seo_main(ref)
