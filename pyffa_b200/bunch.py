@@ -147,6 +147,13 @@ class FFAG_Bunch:
         self._counted = 0
 
     # ------------------------------------------------------------- views
+    def alive_at_step(self, step: int) -> np.ndarray:
+        """Survival flags at the start of absolute step `step` after that
+        step's injection (the reference's Step_SurviveFlag), read before the
+        step is pushed."""
+        surv = self.cols["surv"].cpu().numpy().astype(bool)
+        return surv | (self.cols["inj_step"].cpu().numpy() == step)
+
     @property
     def LocalBunch(self) -> np.ndarray:
         """The N x 16 v-format matrix (device -> host copy)."""

@@ -151,6 +151,120 @@ class PositionDumpBunch:
                                   "FFAG_RungeKutta's loops, which feed this dump")
 
 
+def _prepare_folder(save_folder, rank, allow_existing):
+    if rank == 0:
+        if not os.path.exists(save_folder):
+            os.makedirs(save_folder)
+        elif os.listdir(save_folder) and not allow_existing:
+            sys.stderr.write(f"Error: dump folder {save_folder} exists and is not empty\n")
+            raise SystemExit(1)
+
+
+class StepDump:
+    """Time snapshots of selected particles, one file per particle
+    (src/FFAG_dump.py:140-290): at every step whose [t_pre, t_post] crosses
+    a new start_time + k * time_interval node (both inside the open window),
+    the post-step rows of the tracked global IDs that were alive at the start
+    of the step, converted to p-format, with t_post as column 17; written
+    (``particle_{gid}_rank_{r}.npz``, key ``particles``) once t_pre passes
+    end_time.  The tracking loop feeds it (record)."""
+
+    def __init__(self, start_time, end_time, time_interval, tracked_particle_id_global, save_folder="dump_data",
+                 rank=0, allow_existing=False):
+        self.start_time, self.end_time = float(start_time), float(end_time)
+        self.time_interval = float(time_interval)
+        if not self.time_interval > 0:
+            raise ValueError("time_interval must be > 0")
+        self.save_folder = save_folder
+        self.rank = rank
+        self.tracked_global_ids = np.asarray(tracked_particle_id_global, dtype=np.int64)
+        self.particle_buffer_dict = {}
+        self.save_flag = False
+        _prepare_folder(save_folder, rank, allow_existing)
+
+    def fires(self, t_pre, t_post) -> np.ndarray:
+        """The step trigger of check_and_dump (src/FFAG_dump.py:250-276)."""
+        t_pre, t_post = np.asarray(t_pre), np.asarray(t_post)
+        inside = (self.start_time < t_pre) & (t_pre < self.end_time) & (self.start_time < t_post) & \
+            (t_post < self.end_time)
+        eps = 1e-12
+        a = np.floor((t_pre - self.start_time) / self.time_interval + eps)
+        b = np.floor((t_post - self.start_time) / self.time_interval + eps)
+        return inside & (a != b)
+
+    def record(self, rows_v, alive_pre, time_stamp, data_type):
+        """rows_v: post-step v-format rows of the tracked particles present in
+        the bunch; alive_pre: their survival at the start of the step."""
+        conv = FFAG_ConversionTools()
+        for row, alive in zip(np.atleast_2d(rows_v), np.atleast_1d(alive_pre)):
+            if not alive:
+                continue
+            st = row[None, :]
+            c = conv.ConvertVrzek2Przek(st) if data_type == "RK4" else conv.ConvertVrzek2Przek_boris(st)
+            gid = int(row[15])
+            self.particle_buffer_dict.setdefault(gid, []).append(np.hstack((c.ravel(), [time_stamp])))
+
+    def dump_all_particles(self):
+        for gid, rows in self.particle_buffer_dict.items():
+            if rows:
+                np.savez_compressed(os.path.join(self.save_folder, f"particle_{gid}_rank_{self.rank}.npz"),
+                                    particles=np.vstack(rows))
+
+    def check_and_dump(self, time_Pre, time_Post, bunch_obj, data_type):
+        raise NotImplementedError("StepDump is fed by FFAG_RungeKutta's loops")
+
+
+class PositionDump:
+    """Crossing records of selected particles, one file per particle
+    (src/FFAG_dump.py:534-788): the post-step row of every tracked particle
+    that crossed the target azimuth in a step ending inside (start_time,
+    end_time), p-format with the RF phase reduced mod 2 pi and the step's end
+    time as column 17, at most max_records per particle; written as
+    ``particle_{gid}_angle_{deg:.1f}_rank_{r}.npz`` once the tracking time
+    passes end_time.  The crossing test runs in the push kernels."""
+
+    def __init__(self, target_azimuth_angle_deg, start_time, end_time, tracked_particle_id_global,
+                 save_folder="dump_data", max_records=10000, rank=0, allow_existing=False):
+        self.target_azimuth_angle = np.deg2rad(target_azimuth_angle_deg) % (2 * np.pi)
+        self.start_time, self.end_time = start_time, end_time
+        self.tracked_global_ids = np.asarray(tracked_particle_id_global, dtype=np.int64)
+        self.save_folder = save_folder
+        self.max_records = max_records
+        self.save_flag = False
+        self.rank = rank
+        self.particle_buffer_dict = {}
+        _prepare_folder(save_folder, rank, allow_existing)
+
+    def in_window(self, t_post):
+        return (t_post < self.end_time) & (t_post > self.start_time)
+
+    def add_particles(self, rows_v, time_i, data_type="Boris"):
+        rows_v = np.atleast_2d(rows_v)
+        keep = np.isin(rows_v[:, 15].astype(np.int64), self.tracked_global_ids)
+        if not keep.any():
+            return
+        rows_v = rows_v[keep]
+        t = np.broadcast_to(np.asarray(time_i, dtype=np.float64), keep.shape)[keep]
+        conv = FFAG_ConversionTools()
+        c = conv.ConvertVrzek2Przek(rows_v) if data_type == "RK4" else conv.ConvertVrzek2Przek_boris(rows_v)
+        c[:, 9] = np.mod(c[:, 9], 2 * np.pi)
+        full = np.hstack((c, t[:, None]))
+        for gid, row in zip(rows_v[:, 15].astype(np.int64), full):
+            buf = self.particle_buffer_dict.setdefault(int(gid), [])
+            if len(buf) < self.max_records:
+                buf.append(row)
+
+    def save_all_particles(self, data_type=None):
+        deg = np.rad2deg(self.target_azimuth_angle)
+        for gid, rows in self.particle_buffer_dict.items():
+            if rows:
+                np.savez(os.path.join(self.save_folder, f"particle_{gid}_angle_{deg:.1f}_rank_{self.rank}.npz"),
+                         particles=np.vstack(rows))
+
+    def check_and_dump(self, time_Pre, time_Post, bunch_obj, data_type):
+        raise NotImplementedError("PositionDump is fed by FFAG_RungeKutta's loops")
+
+
 class Dumps:
     """Registry of dump instances (src/FFAG_dump.py:1255-1284)."""
 
@@ -164,7 +278,10 @@ class Dumps:
         return [d for d in self.dumps if isinstance(d, StepDumpBunch)]
 
     def position_dumps(self):
-        return [d for d in self.dumps if isinstance(d, PositionDumpBunch)]
+        return [d for d in self.dumps if isinstance(d, (PositionDumpBunch, PositionDump))]
+
+    def particle_step_dumps(self):
+        return [d for d in self.dumps if isinstance(d, StepDump)]
 
     def check_and_dump(self, time_Pre, time_Post, bunch_obj, data_type="RK4"):
         for d in self.dumps:

@@ -268,7 +268,10 @@ Generate_Bmaps_MultiProcess = Generate_Bmaps
 
 def main_Bmap(json_path: str) -> str:
     """examples/main_Bmap.py: reads the lattice JSON, writes the order tables
-    into config.folder (relative to the JSON) and returns that folder."""
+    and the JSON with the sector-mean field (Bmap.Bmean, Bmap.r_axis, which the
+    closed-orbit search starts from) into config.folder (relative to the
+    JSON), and returns that folder."""
+    from .fields import FFAG_Bfield_analytical
     json_dir = os.path.dirname(os.path.abspath(json_path))
     with open(json_path) as f:
         cfg = json.load(f)
@@ -276,6 +279,7 @@ def main_Bmap(json_path: str) -> str:
     folder = cfg["config"]["folder"]
     out_dir = folder if os.path.isabs(folder) else os.path.join(json_dir, folder)
     os.makedirs(out_dir, exist_ok=True)
+    FFAG_Bfield_analytical(json_path, 0, AddNumricalMap=False).UpdataConfig(out_dir)
     r, fi = map_axes(bmap)
     s = calculate_s(r, 0.0, bmap["SpiralAngle_deg"])
     sfit = Polynomial.fit(r, s, 5)

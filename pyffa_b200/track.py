@@ -23,6 +23,7 @@ import numpy as np
 from . import _lib
 from .bunch import FFAG_Bunch
 from .constants import C_LIGHT, COLUMNS, FFAG_ConversionTools, FFAG_GlobalParameters
+from .dump import PositionDump
 
 TABLE_CHUNK = 1 << 16
 
@@ -280,6 +281,7 @@ class FFAG_RungeKutta:
             from .space_charge import SpaceCharge
             sc = SpaceCharge(b, hockney=bool(lp.get("SC_hockney", False)))
         dump_sched = [StepDumpSchedule(d) for d in (dumps.step_dumps() if dumps is not None else [])]
+        pdumps = dumps.particle_step_dumps() if dumps is not None else []
         pos_dumps = dumps.position_dumps() if dumps is not None else []
         xcap = CrossingCapture(b, [d.target_azimuth_angle for d in pos_dumps], gp, dt) if pos_dumps else None
 
@@ -311,8 +313,24 @@ class FFAG_RungeKutta:
                 if hit.size:
                     cand = steps_i + int(hit[0])
                     dump_at = cand if dump_at is None else min(dump_at, cand)
+            for pd in pdumps:
+                if pd.save_flag:
+                    continue
+                hit = np.nonzero(pd.fires(clock.t[steps_i:end], clock.t[steps_i + 1:end + 1]))[0]
+                if hit.size:
+                    cand = steps_i + int(hit[0])
+                    dump_at = cand if dump_at is None else min(dump_at, cand)
             if dump_at is not None:
                 end = dump_at + 1
+            pre_alive = None
+            if pdumps and dump_at is not None and any(
+                    not pd.save_flag and pd.fires(clock.t[dump_at], clock.t[dump_at + 1]) for pd in pdumps):
+                # the trigger step alone, so its pre-step survival can be read
+                if dump_at > steps_i:
+                    end = dump_at
+                    dump_at = None
+                else:
+                    pre_alive = b.alive_at_step(steps_i)
             t_chunk = clock.t[steps_i + 1:end + 1]
             capture = xcap is not None and any(not d.save_flag and d.in_window(t_chunk).any() for d in pos_dumps)
             if capture and end - steps_i > xcap.max_steps():
@@ -328,8 +346,11 @@ class FFAG_RungeKutta:
                     tp = clock.t[r[:, 2].astype(np.int64) + 1]
                     keep = d.in_window(tp) if not d.save_flag else np.zeros(len(r), bool)
                     if keep.any():
-                        d.add_particles(xcap.rows(r[keep]), tp[keep])
-                        d.add_records(r[keep], tp[keep])
+                        if isinstance(d, PositionDump):
+                            d.add_particles(xcap.rows(r[keep]), tp[keep], solver)
+                        else:
+                            d.add_particles(xcap.rows(r[keep]), tp[keep])
+                            d.add_records(r[keep], tp[keep])
             for d in pos_dumps:
                 if not d.save_flag and (t_chunk > d.end_time).any():
                     d.save_all_particles(solver)
@@ -341,6 +362,16 @@ class FFAG_RungeKutta:
                 for ds in dump_sched:
                     if ds.steps_in(np.array([t_pre]), np.array([t_post])).size:
                         ds.dump.dump_bunch(b, t_post, data_type=solver)
+                if pre_alive is not None:
+                    local = b.LocalBunch
+                    for pd in pdumps:
+                        if not pd.save_flag and pd.fires(t_pre, t_post):
+                            rows = np.nonzero(np.isin(local[:, 15].astype(np.int64), pd.tracked_global_ids))[0]
+                            pd.record(local[rows], pre_alive[rows], t_post, solver)
+            for pd in pdumps:
+                if not pd.save_flag and clock.t[steps_i - 1] > pd.end_time:
+                    pd.dump_all_particles()
+                    pd.save_flag = True
             if steps_i % 1000 == 0:
                 b.UpdateParticleNumGlobal(comm)
                 _lib.check(_lib.lib().ffa_mean_fi(ctypes.byref(b.soa()), b.n, fi_sum.data_ptr(), fi_cnt.data_ptr(),
