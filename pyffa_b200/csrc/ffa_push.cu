@@ -36,8 +36,10 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
                                              double &Bz, double &Br, double &Bfi)
 {
     double spiral = 0.0, spiral_p = 0.0;
-    for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * ri + f.spoly[a];
-    for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * ri + f.spolyp[a];
+    if (!f.spiral_zero) {   // all-zero coefficients evaluate to exactly 0
+        for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * ri + f.spoly[a];
+        for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * ri + f.spolyp[a];
+    }
     double B0r, B0r_p;
     if (f.k == 0.0) {
         B0r = f.B0;
@@ -309,6 +311,47 @@ template <int MAXO>
 __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir, double fim, double z,
                                             double &Bz, double &Br, double &Bfi, int &clamped)
 {
+    // the table lookup first, so its loads are in flight during the rest
+    double hz = 0.0, hf = 0.0, hr = 0.0;
+    if constexpr (MAXO >= 1) {
+        const double qx = (r - f.r_min) * f.inv_r_step;
+        const double qy = (fim - f.fi_min) * f.inv_fi_step;
+        int64_t i = (int64_t)qx, jj = (int64_t)qy;
+        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
+        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
+        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
+        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
+        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
+        constexpr int NV = 3 * MAXO;
+        const float *nd[4];
+        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
+        nd[1] = nd[0] + NP;
+        nd[2] = nd[0] + f.fi_size * NP;
+        nd[3] = nd[2] + NP;
+        float acc[NV];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int a = 0; a < NV; a += 4) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+            }
+        }
+        const double z2 = z * z;
+        double ze = z2, zo = z2 * z;
+#pragma unroll
+        for (int n = 0; n < MAXO; ++n) {
+            hz += (double)acc[3 * n] * ze;
+            hf += (double)acc[3 * n + 1] * zo;
+            hr += (double)acc[3 * n + 2] * zo;
+            ze *= z2;
+            zo *= z2;
+        }
+    }
+
     double spiral = 0.0, spiral_p = 0.0;
     if (!f.spiral_zero) {
         for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * r + f.spoly[a];
@@ -346,47 +389,9 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
         F += f.seg_y[j] * (double)ss;
         Fp += f.seg_yk[j] * (double)(ss * dd);
     }
-    Bz = B0r * F;
-    Bfi = B0r * Fp * ir * z;
-    Br = (B0r_p * F - B0r * Fp * spiral_p) * z;
-    if constexpr (MAXO >= 1) {
-        const double qx = (r - f.r_min) * f.inv_r_step;
-        const double qy = (fim - f.fi_min) * f.inv_fi_step;
-        int64_t i = (int64_t)qx, jj = (int64_t)qy;
-        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
-        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
-        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
-        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
-        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
-        constexpr int NV = 3 * MAXO;
-        const float *nd[4];
-        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
-        nd[1] = nd[0] + NP;
-        nd[2] = nd[0] + f.fi_size * NP;
-        nd[3] = nd[2] + NP;
-        float acc[NV];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-#pragma unroll
-            for (int a = 0; a < NV; a += 4) {
-                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
-                const float tv[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
-            }
-        }
-        const double z2 = z * z;
-        double ze = z2, zo = z2 * z;
-#pragma unroll
-        for (int n = 0; n < MAXO; ++n) {
-            Bz += (double)acc[3 * n] * ze;
-            Bfi += (double)acc[3 * n + 1] * zo;
-            Br += (double)acc[3 * n + 2] * zo;
-            ze *= z2;
-            zo *= z2;
-        }
-    }
+    Bz = B0r * F + hz;
+    Bfi = B0r * Fp * ir * z + hf;
+    Br = (B0r_p * F - B0r * Fp * spiral_p) * z + hr;
 }
 
 // ------------------------------------------------------------ Boris fp64
@@ -436,8 +441,15 @@ __global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
             if constexpr (F32) {
                 field_mixed<MAXO>(f, r, ir, fim, z, Bz, Br, Bfi, oob);
             } else {
+                // the table lookup first: its loads are in flight while the
+                // analytic part computes (measured 3.53 vs 3.64 ms per
+                // 1e5-particle turn; 3.30 ms with the zero-spiral skip)
+                double hz = 0.0, hf = 0.0, hr = 0.0;
+                if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, r, fim, z, hz, hf, hr, oob);
                 analytic_b64(f, r, ir, fim, z, Bz, Br, Bfi);
-                if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, r, fim, z, Bz, Bfi, Br, oob);
+                Bz += hz;
+                Bfi += hf;
+                Br += hr;
             }
             double Er, Efi;
             rf_field64(p.rf, acc, r, fi, rfph, Er, Efi);
