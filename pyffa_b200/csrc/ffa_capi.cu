@@ -163,7 +163,12 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     k.inv_fi_step = d->fi_step > 0 ? 1.0 / d->fi_step : 0.0;
     k.c1 = d->k == 0.0 ? d->B0 : d->B0 * pow(k.r_ref, d->k - 1.0);
     k.kc1 = d->k * k.c1;
-    for (int j = 0; j < d->n_convex; ++j) k.seg_yk[j] = k.seg_y[j] * k.seg_k[j];
+    for (int j = 0; j < d->n_convex; ++j) {
+        k.seg_yk[j] = k.seg_y[j] * k.seg_k[j];
+        const double hc = 0.5 * k.seg_k[j] * (k.seg_x1[j] - k.seg_x0[j]);
+        k.seg_hc[j] = hc <= 300.0 ? hc : 1e300;
+        k.seg_K[j] = hc <= 300.0 ? exp(-hc) : 0.0;
+    }
     if (d->max_order > 0) {
         const int64_t plane = d->r_size * d->fi_size;
         if (cudaMalloc(&fm->nodes64, sizeof(double) * plane * k.npad) != cudaSuccess) {

@@ -38,6 +38,9 @@ struct FieldK {
     double r_ref, inv_r_ref, inv_r_step, inv_fi_step;
     double c1, kc1;               // B0 r_ref^(k-1), k * c1
     double seg_yk[FFA_MAX_SEG];   // seg_y * seg_k
+    // paired sigmoids: half the edge-to-edge exponent c/2 = k (x1 - x0) / 2
+    // (a huge value disables the pairing) and exp(-c/2)
+    double seg_hc[FFA_MAX_SEG], seg_K[FFA_MAX_SEG];
 };
 
 struct RFK {

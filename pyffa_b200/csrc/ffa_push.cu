@@ -64,13 +64,31 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         const double a1 = ks * (fs - f.seg_x0[j]);
         const double a2 = ks * (fs - f.seg_x1[j]);
         double s1 = 1.0, s2 = 1.0, s1p = 0.0, s2p = 0.0;
-        if (a1 < 37.5) {
-            s1 = 1.0 / (1.0 + exp(-a1));
+        const double v = a1 - f.seg_hc[j];
+        if (a1 < 37.5 && a2 > -37.5 && fabs(v) <= 300.0) {
+            // Both edges active: one exponential and one division for the
+            // pair.  With c = k (x1 - x0), u = exp(a1 - c/2), K = exp(-c/2):
+            // exp(-a1) = K / u and exp(a2) = K u, so
+            //   s1 = u / (u + K),  s2 = 1 / (1 + K u),
+            // both over the common denominator (u + K)(1 + K u), which stays
+            // finite for |a1 - c/2|, c/2 <= 300.  Each sigmoid then carries
+            // a few ulp instead of one.
+            const double u = exp(v), K = f.seg_K[j];
+            const double p1 = u + K, p2 = 1.0 + K * u;
+            const double R = 1.0 / (p1 * p2);
+            s1 = u * p2 * R;
+            s2 = p1 * R;
             s1p = ks * s1 * (1.0 - s1);
-        }
-        if (a2 > -37.5) {
-            s2 = 1.0 / (1.0 + exp(a2));
             s2p = -ks * s2 * (1.0 - s2);
+        } else {
+            if (a1 < 37.5) {
+                s1 = 1.0 / (1.0 + exp(-a1));
+                s1p = ks * s1 * (1.0 - s1);
+            }
+            if (a2 > -37.5) {
+                s2 = 1.0 / (1.0 + exp(a2));
+                s2p = -ks * s2 * (1.0 - s2);
+            }
         }
         const double y = f.seg_y[j];
         B0F += y * s1 * s2;
