@@ -163,6 +163,28 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     k.inv_fi_step = d->fi_step > 0 ? 1.0 / d->fi_step : 0.0;
     k.c1 = d->k == 0.0 ? d->B0 : d->B0 * pow(k.r_ref, d->k - 1.0);
     k.kc1 = d->k * k.c1;
+    // binomial series of (1 + t)^(k-1) around the map centre (see FieldK)
+    k.pw_tlim = -1.0;
+    if (d->k != 0.0 && d->r_size > 1 && d->r_step > 0) {
+        const double m = d->k - 1.0;
+        k.pw_r0 = d->r_min + 0.5 * d->r_step * (double)(d->r_size - 1);
+        k.pw_inv_r0 = 1.0 / k.pw_r0;
+        k.pw_r0m = pow(k.pw_r0, m);
+        double c = 1.0;
+        for (int n = 0; n < 16; ++n) {
+            k.pw_c[n] = c;
+            c = c * (m - n) / (double)(n + 1);
+        }
+        // c is now the first omitted coefficient: largest |t| whose remainder
+        // bound |c| |t|^16 / (1 - |t|) stays below 2^-56 (1 - |t|)^m
+        double lo = 0.0, hi = 0.5;
+        for (int it = 0; it < 60; ++it) {
+            const double t = 0.5 * (lo + hi);
+            const double rem = fabs(c) * pow(t, 16) / (1.0 - t);
+            if (rem < ldexp(1.0, -56) * pow(1.0 - t, fabs(m))) lo = t; else hi = t;
+        }
+        k.pw_tlim = lo;
+    }
     for (int j = 0; j < d->n_convex; ++j) {
         k.seg_yk[j] = k.seg_y[j] * k.seg_k[j];
         const double hc = 0.5 * k.seg_k[j] * (k.seg_x1[j] - k.seg_x0[j]);

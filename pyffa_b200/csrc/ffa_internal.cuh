@@ -41,6 +41,11 @@ struct FieldK {
     // paired sigmoids: half the edge-to-edge exponent c/2 = k (x1 - x0) / 2
     // (a huge value disables the pairing) and exp(-c/2)
     double seg_hc[FFA_MAX_SEG], seg_K[FFA_MAX_SEG];
+    // power law near the map centre: r^(k-1) = r0^(k-1) (1 + t)^(k-1),
+    // t = (r - r0) / r0, as a 16-term binomial series for |t| <= pw_tlim
+    // (truncation below 2^-56 relative); pw_tlim = -1 disables it
+    double pw_r0, pw_inv_r0, pw_tlim, pw_r0m;
+    double pw_c[16];
 };
 
 struct RFK {

@@ -45,10 +45,20 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0r = f.B0;
         B0r_p = 0.0;
     } else {
-        // r^k = r^(k-1) * r: one pow instead of two.
-        // exp((k-1) ln r): a few ulp of (k-1) ln r ~ 14, i.e. ~1e-15
-        // relative, a static field error far below the tracking tolerance
-        double pk1 = exp(f.km1 * log(ri));
+        // r^k = r^(k-1) * r: one power instead of two.  Near the map centre
+        // the binomial series of (1 + t)^(k-1) (16 terms, truncation below
+        // 2^-56, a few ulp of rounding); elsewhere exp((k-1) ln r), whose
+        // error is a few ulp of (k-1) ln r ~ 14, i.e. ~1e-15 relative.
+        double pk1;
+        const double t = (ri - f.pw_r0) * f.pw_inv_r0;
+        if (fabs(t) <= f.pw_tlim) {
+            double P = f.pw_c[15];
+#pragma unroll
+            for (int a = 14; a >= 0; --a) P = P * t + f.pw_c[a];
+            pk1 = f.pw_r0m * P;
+        } else {
+            pk1 = exp(f.km1 * log(ri));
+        }
         B0r_p = f.B0k * pk1;
         B0r = f.B0 * (pk1 * ri);
     }
