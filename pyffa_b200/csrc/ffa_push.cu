@@ -214,20 +214,20 @@ __device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double r, 
     }
 }
 
-// Azimuth change atan2(y, x) of one step and its sine / cosine.  A step
-// turns the particle by about 2 pi / (steps per turn); below 0.02 rad the
-// odd / even Taylor series (truncation < 1e-22 relative) replace atan2 and
-// sincos, which is where most of a step's float64 work would go otherwise.
-__device__ __forceinline__ void small_rotation(double y, double x, double &a, double &s, double &c)
+// Azimuth change of one step and its sine / cosine, from the new position's
+// unit vector in the local frame: sin and cos of the step angle are y / r and
+// x / r (r^-1 is at hand from the drift); a step turns the particle by about
+// 2 pi / (steps per turn), and for |sin| < 0.02 the angle is the arcsine series
+//   asin(s) = s (1 + s^2/6 + 3 s^4/40 + 5 s^6/112 + 35 s^8/1152 + 63 s^10/2816)
+// (truncation < 1e-22 relative): no division and no sin/cos series.
+__device__ __forceinline__ void step_rotation(double y, double x, double ir, double &a, double &s, double &c)
 {
-    const double u = y / x;
-    if (x > 0.0 && fabs(u) < 0.02) {
-        const double u2 = u * u;
-        // atan(u) = u (1 - u^2/3 + u^4/5 - u^6/7 + u^8/9 - u^10/11)
-        a = u * (1.0 + u2 * (-1.0 / 3 + u2 * (1.0 / 5 + u2 * (-1.0 / 7 + u2 * (1.0 / 9 + u2 * (-1.0 / 11))))));
-        const double a2 = a * a;
-        s = a * (1.0 + a2 * (-1.0 / 6 + a2 * (1.0 / 120 + a2 * (-1.0 / 5040 + a2 * (1.0 / 362880)))));
-        c = 1.0 + a2 * (-0.5 + a2 * (1.0 / 24 + a2 * (-1.0 / 720 + a2 * (1.0 / 40320))));
+    const double s0 = y * ir;
+    if (x > 0.0 && fabs(s0) < 0.02) {
+        const double s2 = s0 * s0;
+        a = s0 * (1.0 + s2 * (1.0 / 6 + s2 * (3.0 / 40 + s2 * (5.0 / 112 + s2 * (35.0 / 1152 + s2 * (63.0 / 2816))))));
+        s = s0;
+        c = x * ir;
     } else {
         a = atan2(y, x);
         sincos(a, &s, &c);
@@ -523,7 +523,7 @@ __global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
             const double irn = rsqrt(rr2);
             const double rn = rr2 * irn;
             double dfi, sn, cn;
-            small_rotation(yn, xn, dfi, sn, cn);
+            step_rotation(yn, xn, irn, dfi, sn, cn);
             fi = fi + dfi;
             rdot = vxn * cn + vyn * sn;
             const double vfi = -vxn * sn + vyn * cn;
