@@ -395,18 +395,22 @@ __global__ void __launch_bounds__(256) fft_axis(typename C2<T>::t *data, int nsl
         const unsigned rk = __brev((unsigned)k) >> (32 - logn);
         sm[l * ld + rk] = base[l * lstride + (int64_t)k * estride];
     }
+    // twiddles exp(-2 pi i k / n), k < n / 2, staged once per block
+    V *tws = sm + LINES * ld;
+    for (int k = threadIdx.x; k < (n >> 1); k += blockDim.x) tws[k] = tw[k];
     __syncthreads();
     const T sgn = inverse ? (T)1 : (T)-1;
+    const int hb = logn - 1;                  // log2(n / 2)
     for (int s = 1; s <= logn; ++s) {
         const int half = 1 << (s - 1);
-        const int twstep = n >> s;
+        const int twshift = logn - s;         // twiddle index j * (n >> s)
         for (int b = threadIdx.x; b < LINES * (n >> 1); b += blockDim.x) {
-            const int l = b / (n >> 1);
-            const int bb = b - l * (n >> 1);
+            const int l = b >> hb;
+            const int bb = b & ((n >> 1) - 1);
             const int grp = bb >> (s - 1);
             const int j = bb & (half - 1);
             const int i0 = grp * (half << 1) + j, i1 = i0 + half;
-            const V w = tw[j * twstep];
+            const V w = tws[j << twshift];
             const T wr = w.x, wi = sgn * (-w.y);  // table holds exp(-2 pi i k/n)
             V *p = sm + l * ld;
             const V a = p[i0], c = p[i1];
@@ -659,7 +663,8 @@ cudaError_t fft2d(typename C2<T>::t *data, int nslices, int NZ, int NX, int logn
                   const typename C2<T>::t *twz, const typename C2<T>::t *twx, int inverse, cudaStream_t s)
 {
     using V = typename C2<T>::t;
-    const size_t smx = sizeof(V) * LINES * (NX + 1), smz = sizeof(V) * LINES * (NZ + 1);
+    // lines (padded pitch) + the n / 2 twiddles
+    const size_t smx = sizeof(V) * (LINES * (NX + 1) + NX / 2), smz = sizeof(V) * (LINES * (NZ + 1) + NZ / 2);
     cudaFuncSetAttribute(fft_axis<T, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smx > smz ? smx : smz));
     if (!inverse) {
         fft_axis<T, LINES><<<(unsigned)((int64_t)nslices * NZ / LINES), 256, smx, s>>>(data, nslices, NZ, NX, 1, lognx, twx, 0);
