@@ -34,12 +34,12 @@ STEPS_PER_TURN = 720
 MAX_ORDER = 2
 # float64 operations per particle-step of the Boris kernel (2 per DFMA,
 # 1 per DADD / DMUL), counted from the kernel's executed instruction mix by
-# ncu on this workload (profiles/boris_f64_c1_1e5.md): 630.5 FP64 flop per
+# ncu on this workload (profiles/boris_f64_c1_1e5.md): 464.8 FP64 flop per
 # particle-step
-FP64_FLOP_PER_PARTICLE_STEP = 630.5
+FP64_FLOP_PER_PARTICLE_STEP = 464.8
 # DRAM bytes (read + write) of one launch (one turn, 1e5 particles) from the
 # same ncu capture, L2 flushed before the launch
-BORIS_TRAFFIC_PER_LAUNCH = 19.164e6
+BORIS_TRAFFIC_PER_LAUNCH = 19.167e6
 # algorithmic HBM bytes per particle per launch: SoA state read
 # (10 float64 + 2 flag bytes + int32 injection step) and written (10 float64 + 2 bytes)
 STATE_BYTES_PER_PARTICLE = (10 * 8 + 2 + 4) + (10 * 8 + 2)
