@@ -139,6 +139,7 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     k.km1 = d->k - 1.0;
     k.B0k = d->B0 * d->k;
     k.period = 2.0 * PI / (double)d->nsectors;
+    k.inv_period = 1.0 / k.period;
     memcpy(k.spoly, d->spoly, sizeof(k.spoly));
     memcpy(k.spolyp, d->spolyp, sizeof(k.spolyp));
     for (int j = 0; j < d->n_convex; ++j) {

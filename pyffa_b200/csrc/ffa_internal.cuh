@@ -23,6 +23,7 @@ struct FieldK {
     int32_t nsectors, n_spoly, n_spolyp, n_seg, max_order, npad;
     double B0, k, km1, B0k;       // B0, k, k - 1, B0 * k
     double period;                // 2 pi / nsectors
+    double inv_period;            // nsectors / (2 pi)
     double spoly[FFA_MAX_POLY];
     double spolyp[FFA_MAX_POLY];
     double seg_x0[FFA_MAX_SEG], seg_x1[FFA_MAX_SEG];

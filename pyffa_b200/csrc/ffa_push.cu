@@ -63,7 +63,7 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0r = f.B0 * (pk1 * ri);
     }
     double fs = fim - spiral;
-    fs -= f.period * floor(fs / f.period);
+    fs -= f.period * floor(fs * f.inv_period);
     double B0F = 0.0, B0Fp = 0.0;
     for (int j = 0; j < f.n_seg; ++j) {
         const double ks = f.seg_k[j];
@@ -187,7 +187,7 @@ __device__ __forceinline__ bool gap_inside(const RFK &rf, int g, double x, doubl
 __device__ __forceinline__ bool in_window(const RFK &rf, int g, double fi)
 {
     double d = fi - rf.win_center[g];
-    d -= (2.0 * PI) * rint(d / (2.0 * PI));
+    d -= (2.0 * PI) * rint(d * (0.5 / PI));   // a flip of rint at a half turn leaves |d| ~ pi, outside
     return fabs(d) <= rf.win_half[g];
 }
 
@@ -397,7 +397,7 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
         B0r = f.c1 * g * r;
     }
     double fs = fim - spiral;
-    fs -= f.period * floor(fs / f.period);
+    fs -= f.period * floor(fs * f.inv_period);
     double F = 0.0, Fp = 0.0;
     for (int j = 0; j < f.n_seg; ++j) {
         const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
@@ -464,7 +464,11 @@ __global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
         }
         if ((inj == 1) && (surv == 1)) {
             const double acc = __ldg(p.acc + gs);
-            const double fim = fi - f.period * floor(fi / f.period);
+            // fi mod the sector; a multiply by 1 / period instead of the
+            // division can move floor() only where fi / period is within an
+            // ulp of an integer, i.e. between two equal values of the
+            // periodic field (0 and the period)
+            const double fim = fi - f.period * floor(fi * f.inv_period);
             double Bz, Br, Bfi;
             if constexpr (F32) {
                 field_mixed<MAXO>(f, r, ir, fim, z, Bz, Br, Bfi, oob);
