@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-sc", action="store_true")
     ap.add_argument("--no-fp32c", action="store_true")
     ap.add_argument("--no-mapgen", action="store_true")
+    ap.add_argument("--no-scan", action="store_true")
     return ap.parse_args()
 
 
@@ -284,6 +285,49 @@ def mapgen_bench(dev, hbm_peak, reps=5):
                                                                         "1 thread, scaled to the map"}
 
 
+def seo_scan_bench(dev, n_energies=256):
+    """Batched closed-orbit and tune scan: 256 energies 300-600 MeV through the
+    GPU closed-orbit search (all energies' azimuth tracks of an iteration in
+    one launch), and the same search with the oracle's CPU tracker on a
+    sample of energies, scaled."""
+    import torch
+    from oracle import oracle as O
+    from pyffa_b200 import seo, synthetic
+    from pyffa_b200.constants import FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical
+    cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
+    bm = FFAG_Bfield_analytical(config=cfg, max_order=0, AddNumricalMap=False)
+    bm.UpdataConfig()
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(bm)
+    Ek = np.linspace(300.0, 600.0, n_energies)
+    finder = seo.FFAG_SearchSEO(gp, device=dev)
+    calls = {"n": 0}
+    run = finder.tracker.run
+
+    def counted(*a, **k):
+        calls["n"] += 1
+        return run(*a, **k)
+
+    finder.tracker.run = counted
+    finder.search(Ek[:4])          # warm-up
+    torch.cuda.synchronize(dev)
+    calls["n"] = 0
+    t0 = time.perf_counter()
+    res = finder.search(Ek)
+    gpu_s = time.perf_counter() - t0
+    sample = Ek[::64]
+    cpu = seo.FFAG_SearchSEO(gp, tracker=O.ThetaTracker(gp.Bmap, gp.q))
+    t0 = time.perf_counter()
+    cpu.search(sample)
+    cpu_s = (time.perf_counter() - t0) * len(Ek) / len(sample)
+    return {"energies": n_energies, "Ek_MeV": [300.0, 600.0], "wall_s": gpu_s, "launches": calls["n"],
+            "Qr_range": [float(res["table"][:, 2].min()), float(res["table"][:, 2].max())],
+            "Qz_range": [float(res["table"][:, 3].min()), float(res["table"][:, 3].max())],
+            "cpu_port_s_est": cpu_s, "cpu_port_threads": O.num_threads(),
+            "cpu_port_sample": f"{len(sample)} of the energies with the oracle tracker, scaled"}
+
+
 def run_reference(args):
     """--impl reference: the oracle port on the host cores, each step one turn
     of a bounded sample."""
@@ -467,6 +511,9 @@ def main():
         mg = None
         if not args.no_mapgen:
             mg = mapgen_bench(dev, hbm_peak)
+        scan = None
+        if not args.no_scan:
+            scan = seo_scan_bench(dev)
         line = {
             "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
             "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
@@ -486,6 +533,7 @@ def main():
             "space_charge": sc,
             "fp32c": fp32c,
             "mapgen": mg,
+            "co_scan": scan,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)
