@@ -329,6 +329,75 @@ typedef struct ffa_mapgen_desc {
 
 int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
 
+/* ------------------------------------------------------ learned sector map
+ * A residual network for the one-sector transfer map in normalised
+ * coordinates s = (u, pu, v, pv, e, 0):
+ *   y = s + s Ws + bs + f(s),  f = L4 . SiLU . L3 . SiLU . L2 . SiLU . L1,
+ * widths 6 -> 256 -> 256 -> 256 -> 6, L(h) = h W + b.  The reference has no
+ * counterpart; the map it learns is one sector of the azimuth-domain tracker
+ * (ffa_theta_track), which follows FunctionForSEO (src/FFAG_track.py:1597-1640).
+ *
+ * Parameters: one float32 block of FFA_MLP_PARAMS values, row-major (n_in,
+ * n_out) matrices with padded shapes:
+ *   W1 [16][256] (rows 6..15 zero), b1 [256], W2 [256][256], b2 [256],
+ *   W3 [256][256], b3 [256], W4 [256][8] (columns 6, 7 zero), b4 [8],
+ *   Ws [8][8] (6 x 6 used), bs [8].
+ * Hidden-layer products run on the tensor cores with bfloat16 operands and
+ * float32 accumulation; the skip layer and the state stay float32.
+ * Samples and states: float32 [n][8], columns 6, 7 ignored. */
+#define FFA_MLP_HIDDEN 256
+#define FFA_MLP_PARAMS 138064
+#define FFA_MLP_WPACK_BYTES 274432   /* bfloat16 copies of W1..W4 for inference */
+
+/* One optimiser step: forward, mean-squared error over the first n_fit
+ * outputs, backward into `grads` (every parameter, same layout), then Adam
+ * on the entries whose `mask` byte is non-zero (mask NULL: all) when lr > 0.
+ * `step` is the 1-based Adam step (bias correction).  `work` holds
+ * 8 * batch * 256 + 24 * batch floats; `loss_part` 148 doubles whose sum is
+ * the batch's summed squared error (before the step). */
+typedef struct ffa_mlp_train_desc {
+    int64_t batch;
+    int32_t n_fit;                /* 1..6 */
+    int32_t step;
+    float lr, beta1, beta2, eps;
+    float *params, *grads, *adam_m, *adam_v;
+    const uint8_t *mask;
+    const float *x, *target;      /* device [batch][8] */
+    float *work;
+    double *loss_part;
+} ffa_mlp_train_desc;
+
+int ffa_mlp_train_step(const ffa_mlp_train_desc *desc, void *stream);
+
+/* C[M][N] = op(A) op(B) (+ bias[N]) in bfloat16 x bfloat16 -> float32 on
+ * the tensor cores; op(A)[m][k] = A[m lda + k] (transA 0) or A[k lda + m],
+ * op(B)[k][n] = B[k ldb + n] (transB 0) or B[n ldb + k].  The training step's
+ * building block, exported for tests. */
+int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, int transB, float *C, int ldc,
+                 int M, int N, int K, const float *bias, void *stream);
+
+/* Inference weights: the bfloat16 packing of a parameter block into `wpack`
+ * (FFA_MLP_WPACK_BYTES, 16-byte aligned).  Call again after the parameters
+ * change. */
+int ffa_mlp_pack(const float *params, void *wpack, void *stream);
+
+/* Applies the map n_apply times to each state in place.  A state takes a map
+ * only while it is inside the training domain, u^2 + pu^2 <= radius2,
+ * v^2 + pv^2 <= radius2 and |e| <= 1 (radius2 <= 0: no check); the first
+ * state outside it is kept, and applied[i] (when not NULL) is the number of
+ * maps state i took. */
+typedef struct ffa_mlp_infer_desc {
+    int64_t n;
+    int32_t n_apply;
+    float radius2;
+    const float *params;
+    const void *wpack;
+    float *state;                 /* device [n][8] */
+    int32_t *applied;             /* device [n] or NULL */
+} ffa_mlp_infer_desc;
+
+int ffa_mlp_infer(const ffa_mlp_infer_desc *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,6 +106,23 @@ class MapgenDesc(C.Structure):
                 ("gder", d_p), ("gmean", d_p), ("bz", d_p), ("br", d_p), ("bfi", d_p)]
 
 
+MLP_HIDDEN = 256
+MLP_PARAMS = 138064
+MLP_WPACK_BYTES = 274432
+
+
+class MlpTrainDesc(C.Structure):
+    _fields_ = [("batch", C.c_int64), ("n_fit", C.c_int32), ("step", C.c_int32),
+                ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+                ("params", d_p), ("grads", d_p), ("adam_m", d_p), ("adam_v", d_p), ("mask", d_p),
+                ("x", d_p), ("target", d_p), ("work", d_p), ("loss_part", d_p)]
+
+
+class MlpInferDesc(C.Structure):
+    _fields_ = [("n", C.c_int64), ("n_apply", C.c_int32), ("radius2", C.c_float),
+                ("params", d_p), ("wpack", d_p), ("state", d_p), ("applied", d_p)]
+
+
 class SCDesc(C.Structure):
     _fields_ = [
         ("ns", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32), ("hockney", C.c_int32),
@@ -146,6 +163,11 @@ EXPORTS = {
     "ffa_sc_buffers": [d_p, C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p), C.POINTER(d_p),
                        C.POINTER(d_p), C.POINTER(d_p)],
     "ffa_sc_step_static": [C.POINTER(SCDesc), C.POINTER(StateSoA), C.c_int64, C.c_int32, C.c_int32, d_p, d_p, d_p],
+    "ffa_mlp_train_step": [C.POINTER(MlpTrainDesc), d_p],
+    "ffa_mlp_gemm": [d_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int, d_p,
+                     d_p],
+    "ffa_mlp_pack": [d_p, d_p, d_p],
+    "ffa_mlp_infer": [C.POINTER(MlpInferDesc), d_p],
 }
 
 SC_STATIC_MAX_PARTICLES = 524288

@@ -38,9 +38,11 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "ffa_cuda.h"
-int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d\n", sizeof(ffa_field_desc), sizeof(ffa_rf_desc),
- sizeof(ffa_aperture), sizeof(ffa_consts), sizeof(ffa_state_soa), sizeof(ffa_step_table), sizeof(ffa_sc_desc),
- sizeof(ffa_sc_diag), sizeof(ffa_crossing), sizeof(ffa_mapgen_desc), sizeof(ffa_theta_track_desc), sizeof(void*), FFA_CROSSING_RECORD); return 0;}
+int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d %d %d %d\n", sizeof(ffa_field_desc),
+ sizeof(ffa_rf_desc), sizeof(ffa_aperture), sizeof(ffa_consts), sizeof(ffa_state_soa), sizeof(ffa_step_table),
+ sizeof(ffa_sc_desc), sizeof(ffa_sc_diag), sizeof(ffa_crossing), sizeof(ffa_mapgen_desc), sizeof(ffa_theta_track_desc),
+ sizeof(ffa_mlp_train_desc), sizeof(ffa_mlp_infer_desc), sizeof(void*), FFA_CROSSING_RECORD, FFA_MLP_HIDDEN,
+ FFA_MLP_PARAMS, FFA_MLP_WPACK_BYTES); return 0;}
 '''
     d = tempfile.mkdtemp()
     with open(os.path.join(d, "s.c"), "w") as f:
@@ -51,8 +53,8 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d\n", si
     sizes = [int(x) for x in out]
     py = [ctypes.sizeof(t) for t in (_lib.FieldDesc, _lib.RFDesc, _lib.Aperture, _lib.Consts, _lib.StateSoA,
                                      _lib.StepTable, _lib.SCDesc, _lib.SCDiag, _lib.Crossing,
-                                     _lib.MapgenDesc, _lib.ThetaTrackDesc)] + \
-        [ctypes.sizeof(ctypes.c_void_p), _lib.CROSSING_RECORD]
+                                     _lib.MapgenDesc, _lib.ThetaTrackDesc, _lib.MlpTrainDesc, _lib.MlpInferDesc)] + \
+        [ctypes.sizeof(ctypes.c_void_p), _lib.CROSSING_RECORD, _lib.MLP_HIDDEN, _lib.MLP_PARAMS, _lib.MLP_WPACK_BYTES]
     assert sizes == py
 
 
@@ -69,3 +71,12 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.ffa_fieldmap_create(ctypes.byref(d), None, ctypes.byref(out)) == 4
     assert L.ffa_push(None, None, None, None, None, None, 0, 0, 0, 0.0, 0, 0, None, None) == 1
     assert L.ffa_aos_to_soa(None, 0, None, None) == 1
+    # learned sector map entry points
+    assert L.ffa_mlp_train_step(None, None) == 1
+    assert L.ffa_mlp_gemm(None, 1, 0, None, 1, 0, None, 1, 1, 1, 1, None, None) == 1
+    assert L.ffa_mlp_pack(None, None, None) == 1
+    assert L.ffa_mlp_infer(None, None) == 1
+    t = _lib.MlpTrainDesc()
+    t.batch = 16
+    t.n_fit = 9
+    assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
