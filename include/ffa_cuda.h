@@ -347,7 +347,7 @@ int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
  * Samples and states: float32 [n][8], columns 6, 7 ignored. */
 #define FFA_MLP_HIDDEN 256
 #define FFA_MLP_PARAMS 138064
-#define FFA_MLP_WPACK_BYTES 274432   /* bfloat16 copies of W1..W4 for inference */
+#define FFA_MLP_WPACK_BYTES 278528   /* bfloat16 copies of W1..W4 for inference */
 
 /* One optimiser step: forward, mean-squared error over the first n_fit
  * outputs, backward into `grads` (every parameter, same layout), then Adam
@@ -381,19 +381,23 @@ int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, i
  * change. */
 int ffa_mlp_pack(const float *params, void *wpack, void *stream);
 
-/* Applies the map n_apply times to each state in place.  A state takes a map
- * only while it is inside the training domain, u^2 + pu^2 <= radius2,
- * v^2 + pv^2 <= radius2 and |e| <= 1 (radius2 <= 0: no check); the first
- * state outside it is kept, and applied[i] (when not NULL) is the number of
- * maps state i took. */
+/* Applies the map n_apply times to each state in place (tcgen05 tensor
+ * cores, one CTA per SM).  A state takes a map only while it is inside the
+ * training domain, u^2 + pu^2 <= radius2, v^2 + pv^2 <= radius2 and
+ * |e| <= 1 (radius2 <= 0: no check); the first state outside it is kept, and
+ * applied[i] (when not NULL) is the number of maps state i took.  The
+ * kernel's internal pipeline waits are bounded (2 s): if one runs out, the
+ * kernel stops, leaves the states it had not finished unchanged and sets
+ * *error to 1 (when not NULL). */
 typedef struct ffa_mlp_infer_desc {
     int64_t n;
     int32_t n_apply;
     float radius2;
     const float *params;
     const void *wpack;
-    float *state;                 /* device [n][8] */
+    float *state;                 /* device [n][8], 16-byte aligned */
     int32_t *applied;             /* device [n] or NULL */
+    int32_t *error;               /* device word or NULL */
 } ffa_mlp_infer_desc;
 
 int ffa_mlp_infer(const ffa_mlp_infer_desc *desc, void *stream);

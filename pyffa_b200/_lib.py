@@ -108,7 +108,7 @@ class MapgenDesc(C.Structure):
 
 MLP_HIDDEN = 256
 MLP_PARAMS = 138064
-MLP_WPACK_BYTES = 274432
+MLP_WPACK_BYTES = 278528
 
 
 class MlpTrainDesc(C.Structure):
@@ -120,7 +120,7 @@ class MlpTrainDesc(C.Structure):
 
 class MlpInferDesc(C.Structure):
     _fields_ = [("n", C.c_int64), ("n_apply", C.c_int32), ("radius2", C.c_float),
-                ("params", d_p), ("wpack", d_p), ("state", d_p), ("applied", d_p)]
+                ("params", d_p), ("wpack", d_p), ("state", d_p), ("applied", d_p), ("error", d_p)]
 
 
 class SCDesc(C.Structure):

@@ -50,12 +50,26 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], uint32
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
+__device__ __forceinline__ float tanh_approx(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 
+// SiLU(z) = z sigmoid(z) = h + h tanh(h), h = z / 2 (training and inference
+// evaluate it the same way)
+__device__ __forceinline__ float silu(float z)
+{
+    const float h = 0.5f * z;
+    return fmaf(h, tanh_approx(h), h);
+}
+
+// d SiLU / dz = sigmoid(z) (1 + z (1 - sigmoid(z))) = (1 + t)(1 + h (1 - t)) / 2
 __device__ __forceinline__ float dsilu(float z)
 {
-    const float s = 1.0f / (1.0f + expf(-z));
-    return s * (1.0f + z * (1.0f - s));
+    const float h = 0.5f * z, t = tanh_approx(h);
+    return 0.5f * (1.0f + t) * fmaf(h, 1.0f - t, 1.0f);
 }
 
 // ------------------------------------------------------------ GEMM (training)
@@ -243,162 +257,453 @@ __global__ void adam_kernel(float *P, const float *G, float *m, float *v, int64_
 // bank conflicts), W1^T [n][16], W4^T [8][k + 8], biases, skip layer, the
 // state of the block's 128 particles.  W3^T bf16 [n][k] is read from global
 // (L1 / L2 resident: 128 KB shared by every block).
-constexpr int KP = H + 8;
-constexpr int INF_WARPS = 8;
-constexpr size_t INF_SMEM = sizeof(__nv_bfloat16) * ((size_t)H * KP + (size_t)H * KIN + (size_t)NOUT * KP) +
-                            sizeof(float) * (3 * H + NOUT + NOUT * NOUT + NOUT + INF_WARPS * 16 * NOUT) +
-                            sizeof(int) * 2 * INF_WARPS * 16;
+// ------------------------------------------------------- fused inference
+// tcgen05 tensor cores, one 128-state tile per CTA at a time (persistent grid,
+// one CTA per SM).  Every layer is one 128 x N accumulator in tensor memory:
+// D0 = columns 0..255, D1 = columns 256..511, layers 1..4 alternate D0, D1.
+// Warp roles: warp 0 streams W2 / W3 from global (L2-resident) into a ring
+// of three 32 KB shared-memory slots with cp.async.bulk; warp 1 owns tensor
+// memory and issues the MMAs (one thread); warps 2..5 are the epilogue, one
+// thread per state (its tensor-memory lane): it reads its accumulator row,
+// adds the bias, applies SiLU, rounds to bfloat16 and writes the next
+// layer's A operand one 64-column chunk at a time, so the next layer's MMAs
+// on chunk c start while chunk c + 1 is still being written.  The state,
+// the domain check and the float32 skip layer stay in the epilogue
+// thread's registers for all n_apply maps.
+//
+// Shared-memory operand layouts (K-major):
+//  - A (activations, 128 x 256) and W2 / W3 / W4 (B operand, N x 256): four
+//    64-column chunks, each row 128 B with the 128-byte swizzle (16-byte
+//    unit j of row m stored at unit j ^ (m mod 8)), rows consecutive,
+//    chunk bases 1024-aligned; descriptor SBO = 1024 B; the K = 16 slices of
+//    a chunk start 32 B apart;
+//  - X (layer-1 input, 128 x 16) and W1 (256 x 16): no swizzle, 8 x 8 core
+//    matrices of 128 B, the two K halves 128 B apart (LBO) and 8-row groups
+//    256 B apart (SBO).
+// The inference weight pack in global memory holds W1, W4, W2, W3 in exactly
+// these layouts, so each ring slot is one linear bulk copy.
+constexpr int TC_M = 128;
+constexpr int TC_CHUNK = 64;                                 // K columns per chunk
+constexpr uint32_t A_CHUNK_BYTES = TC_M * 128;               // 16 KB
+constexpr uint32_t W_CHUNK_BYTES = H * 128;                  // 32 KB
+constexpr uint32_t W4_CHUNK_BYTES = 16 * 128;                // 2 KB
+constexpr int RING = 3;
+// weight pack (bytes)
+constexpr uint32_t PK_W1 = 0;                                // 256 x 16 bf16, core matrices
+constexpr uint32_t PK_W4 = PK_W1 + H * KIN * 2;              // 4 chunks x 16 rows
+constexpr uint32_t PK_W2 = PK_W4 + 4 * W4_CHUNK_BYTES;       // 4 chunks x 256 rows
+constexpr uint32_t PK_W3 = PK_W2 + 4 * W_CHUNK_BYTES;
+constexpr uint32_t PK_TOTAL = PK_W3 + 4 * W_CHUNK_BYTES;
+// shared memory (bytes from the 1024-aligned base)
+constexpr uint32_t SM_A = 0;
+constexpr uint32_t SM_RING = SM_A + 4 * A_CHUNK_BYTES;
+constexpr uint32_t SM_W4 = SM_RING + RING * W_CHUNK_BYTES;
+constexpr uint32_t SM_W1 = SM_W4 + 4 * W4_CHUNK_BYTES;
+constexpr uint32_t SM_X = SM_W1 + H * KIN * 2;
+constexpr uint32_t SM_BIAS = SM_X + TC_M * KIN * 2;          // b1 b2 b3 (halved), float
+constexpr uint32_t SM_TAIL = SM_BIAS + 3 * H * 4;            // b4[8] Ws[64] bs[8]
+constexpr uint32_t SM_BAR = SM_TAIL + 80 * 4;                // mbarriers (8 B each)
+constexpr int NBAR = 1 + 4 + 1 + 2 * RING + 1;               // x_ready, a_ready[4], d_full, full[], empty[], drain
+constexpr uint32_t SM_MISC = SM_BAR + NBAR * 8;              // tmem base, abort flag
+constexpr uint32_t SM_TOTAL = SM_MISC + 16;
+constexpr size_t TC_SMEM = SM_TOTAL + 1024;                  // + alignment slack
+constexpr uint64_t WAIT_NS = 2000000000ull;                  // a pipeline wait gives up after 2 s
 
-__global__ void pack_weights_kernel(const float *P, __nv_bfloat16 *w1t, __nv_bfloat16 *w2t, __nv_bfloat16 *w3t,
-                                    __nv_bfloat16 *w4t)
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t global_ns()
 {
-    // transposed bf16 copies: w?t[n][k] = W?[k][n]
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid < H * KIN) { const int n = tid / KIN, k = tid % KIN; w1t[tid] = __float2bfloat16_rn(P[P_W1 + k * H + n]); }
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of `bar` with `parity` for at most WAIT_NS, whatever
+// the abort flag says (teardown: copies and MMAs in flight must land).
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
+{
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, parity))
+        if (global_ns() - t0 > WAIT_NS) return false;
+    return true;
+}
+
+// Waits for the phase of `bar` with `parity`; gives up (and raises the
+// block's abort flag) after WAIT_NS or when another thread has raised it.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag)
+{
+    if (mbar_test(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (true) {
+        if (mbar_test(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (global_ns() - t0 > WAIT_NS) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// smem matrix descriptor: start, leading / stride byte offsets, layout
+// (0: no swizzle, 2: 128-byte swizzle), version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout)
+{
+    return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
+}
+
+// instruction descriptor, kind::f16: bfloat16 A and B (K-major), float32 D
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+#define TMEM_LD32(taddr, v)                                                                                  \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15," \
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"              \
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),      \
+                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),  \
+                   "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),             \
+                   "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),             \
+                   "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])              \
+                 : "r"(taddr))
+
+#define TMEM_LD16(taddr, v)                                                                                  \
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}," \
+                 " [%16];"                                                                                   \
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),      \
+                   "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),  \
+                   "=r"(v[14]), "=r"(v[15])                                                                  \
+                 : "r"(taddr))
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// byte offset of element (row, k) in a 128-byte-swizzled chunked operand
+// with `rows` rows per chunk
+__host__ __device__ __forceinline__ uint32_t swz_off(int row, int k, int rows)
+{
+    return (uint32_t)((k >> 6) * rows * 128 + row * 128 + ((((k & 63) >> 3) ^ (row & 7)) << 4) + ((k & 7) << 1));
+}
+
+// byte offset of element (row, k) of a no-swizzle K = 16 operand
+__host__ __device__ __forceinline__ uint32_t core_off(int row, int k)
+{
+    return (uint32_t)((((row >> 3) * 2 + (k >> 3)) << 7) + ((row & 7) << 4) + ((k & 7) << 1));
+}
+
+// float32 parameters -> the inference weight pack (bfloat16, layouts above)
+__global__ void pack_weights_kernel(const float *__restrict__ P, unsigned char *__restrict__ wp)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid < H * H) {
         const int n = tid / H, k = tid % H;
-        w2t[tid] = __float2bfloat16_rn(P[P_W2 + k * H + n]);
-        w3t[tid] = __float2bfloat16_rn(P[P_W3 + k * H + n]);
+        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W2 + swz_off(n, k, H)) = __float2bfloat16_rn(P[P_W2 + k * H + n]);
+        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W3 + swz_off(n, k, H)) = __float2bfloat16_rn(P[P_W3 + k * H + n]);
     }
-    if (tid < NOUT * H) { const int n = tid / H, k = tid % H; w4t[tid] = __float2bfloat16_rn(P[P_W4 + k * NOUT + n]); }
-}
-
-// one hidden layer: in (16 k tiles of A fragments) -> out, bias + SiLU
-template <bool GLOBAL_B>
-__device__ __forceinline__ void hidden_layer(const uint32_t (&in)[16][4], uint32_t (&out)[16][4],
-                                             const __nv_bfloat16 *W, int ldw, const float *bias, int lane)
-{
-    const int r = lane >> 2, c2 = (lane & 3) * 2;
-#pragma unroll
-    for (int nt = 0; nt < H / 8; ++nt) {
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        const __nv_bfloat16 *wr = W + (int64_t)(nt * 8 + r) * ldw;
-#pragma unroll
-        for (int kt = 0; kt < H / 16; ++kt) {
-            uint32_t b0, b1;
-            if (GLOBAL_B) {
-                b0 = __ldg(reinterpret_cast<const unsigned int *>(wr + kt * 16 + c2));
-                b1 = __ldg(reinterpret_cast<const unsigned int *>(wr + kt * 16 + c2 + 8));
-            } else {
-                b0 = *reinterpret_cast<const uint32_t *>(wr + kt * 16 + c2);
-                b1 = *reinterpret_cast<const uint32_t *>(wr + kt * 16 + c2 + 8);
-            }
-            mma_bf16(acc, in[kt], b0, b1);
-        }
-        const float bb0 = bias[nt * 8 + c2], bb1 = bias[nt * 8 + c2 + 1];
-        const uint32_t lo = pack_bf16(silu(acc[0] + bb0), silu(acc[1] + bb1));   // row r
-        const uint32_t hi = pack_bf16(silu(acc[2] + bb0), silu(acc[3] + bb1));   // row r + 8
-        if ((nt & 1) == 0) { out[nt >> 1][0] = lo; out[nt >> 1][1] = hi; }
-        else { out[nt >> 1][2] = lo; out[nt >> 1][3] = hi; }
+    if (tid < H * KIN) {
+        const int n = tid / KIN, k = tid % KIN;
+        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W1 + core_off(n, k)) = __float2bfloat16_rn(P[P_W1 + k * H + n]);
+    }
+    if (tid < 16 * H) {
+        const int n = tid / H, k = tid % H;
+        const float v = n < NOUT ? P[P_W4 + k * NOUT + n] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W4 + swz_off(n, k, 16)) = __float2bfloat16_rn(v);
     }
 }
 
-__global__ void __launch_bounds__(INF_WARPS * 32, 1)
-    mlp_infer_kernel(const float *P, const __nv_bfloat16 *w1t, const __nv_bfloat16 *w2t, const __nv_bfloat16 *w3t,
-                     const __nv_bfloat16 *w4t, float *state, int32_t *applied, int64_t n, int n_apply, float radius2)
+// SiLU of 8 accumulator values (bias pre-halved), packed to 4 bfloat16 pairs
+__device__ __forceinline__ uint4 silu8(const uint32_t *v, const float *hb)
 {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    __nv_bfloat16 *sW2 = reinterpret_cast<__nv_bfloat16 *>(smraw);
-    __nv_bfloat16 *sW1 = sW2 + (size_t)H * KP;
-    __nv_bfloat16 *sW4 = sW1 + (size_t)H * KIN;
-    float *sB = reinterpret_cast<float *>(sW4 + (size_t)NOUT * KP);   // b1 b2 b3
-    float *sB4 = sB + 3 * H;
-    float *sWs = sB4 + NOUT;
-    float *sBs = sWs + NOUT * NOUT;
-    float *sX = sBs + NOUT;                                             // [128][8]
-    int *sAct = reinterpret_cast<int *>(sX + INF_WARPS * 16 * NOUT);   // [128]
-    int *sCnt = sAct + INF_WARPS * 16;                                  // [128]
-    for (int e = threadIdx.x; e < H * H; e += blockDim.x) {
-        const int nn = e / H, k = e - nn * H;
-        sW2[nn * KP + k] = w2t[e];
-    }
-    for (int e = threadIdx.x; e < H * KIN; e += blockDim.x) sW1[e] = w1t[e];
-    for (int e = threadIdx.x; e < NOUT * H; e += blockDim.x) {
-        const int nn = e / H, k = e - nn * H;
-        sW4[nn * KP + k] = w4t[e];
-    }
-    for (int e = threadIdx.x; e < H; e += blockDim.x) {
-        sB[e] = P[P_B1 + e];
-        sB[H + e] = P[P_B2 + e];
-        sB[2 * H + e] = P[P_B3 + e];
-    }
-    if (threadIdx.x < NOUT) { sB4[threadIdx.x] = P[P_B4 + threadIdx.x]; sBs[threadIdx.x] = P[P_BS + threadIdx.x]; }
-    if (threadIdx.x < NOUT * NOUT) sWs[threadIdx.x] = P[P_WS + threadIdx.x];
+    float h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = fmaf(__uint_as_float(v[i]), 0.5f, hb[i]);
+    uint4 o;
+    o.x = pack_bf16(fmaf(h[0], tanh_approx(h[0]), h[0]), fmaf(h[1], tanh_approx(h[1]), h[1]));
+    o.y = pack_bf16(fmaf(h[2], tanh_approx(h[2]), h[2]), fmaf(h[3], tanh_approx(h[3]), h[3]));
+    o.z = pack_bf16(fmaf(h[4], tanh_approx(h[4]), h[4]), fmaf(h[5], tanh_approx(h[5]), h[5]));
+    o.w = pack_bf16(fmaf(h[6], tanh_approx(h[6]), h[6]), fmaf(h[7], tanh_approx(h[7]), h[7]));
+    return o;
+}
+
+__global__ void __launch_bounds__(192, 1)
+    mlp_infer_tc_kernel(const float *__restrict__ P, const unsigned char *__restrict__ wp, float *__restrict__ state,
+                        int32_t *__restrict__ applied, int32_t *__restrict__ error, int64_t n, int n_apply,
+                        float radius2)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t s0 = smem_u32(sm);
+    float *sbias = reinterpret_cast<float *>(sm + SM_BIAS);
+    float *stail = reinterpret_cast<float *>(sm + SM_TAIL);   // b4[0..7], Ws[8..71], bs[72..79]
+    const uint32_t bar0 = s0 + SM_BAR;
+    const uint32_t BAR_X = bar0, BAR_A = bar0 + 8, BAR_D = bar0 + 40, BAR_FULL = bar0 + 48,
+                   BAR_EMPTY = bar0 + 48 + 8 * RING, BAR_DRAIN = bar0 + 48 + 16 * RING;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(sm + SM_MISC);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + SM_MISC + 4);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = lane >> 2, c2 = (lane & 3) * 2;
-    const int64_t p0 = (int64_t)blockIdx.x * (INF_WARPS * 16) + warp * 16;
-    float *x = sX + warp * 16 * NOUT;
-    int *act = sAct + warp * 16, *cnt = sCnt + warp * 16;
-    for (int e = lane; e < 16 * NOUT; e += 32) {
-        const int64_t p = p0 + e / NOUT;
-        x[e] = p < n ? state[p * NOUT + (e % NOUT)] : 0.0f;
+    const int64_t ntiles = (n + TC_M - 1) / TC_M;
+
+    // resident operands and constants
+    for (int i = threadIdx.x; i < (int)(H * KIN * 2 / 16); i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + SM_W1)[i] = reinterpret_cast<const uint4 *>(wp + PK_W1)[i];
+    for (int i = threadIdx.x; i < (int)(4 * W4_CHUNK_BYTES / 16); i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + SM_W4)[i] = reinterpret_cast<const uint4 *>(wp + PK_W4)[i];
+    for (int i = threadIdx.x; i < 3 * H; i += blockDim.x) sbias[i] = 0.5f * P[(i < H ? P_B1 : i < 2 * H ? P_B2 : P_B3) + (i % H)];
+    for (int i = threadIdx.x; i < 80; i += blockDim.x)
+        stail[i] = i < 8 ? P[P_B4 + i] : i < 72 ? P[P_WS + (i - 8)] : P[P_BS + (i - 72)];
+    if (threadIdx.x == 0) {
+        mbar_init(BAR_X, 4);
+        for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * c, 4);
+        mbar_init(BAR_D, 1);
+        for (int s = 0; s < RING; ++s) {
+            mbar_init(BAR_FULL + 8 * s, 1);
+            mbar_init(BAR_EMPTY + 8 * s, 1);
+        }
+        mbar_init(BAR_DRAIN, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (lane < 16) { act[lane] = (p0 + lane) < n; cnt[lane] = 0; }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    tc_before_sync();
     __syncthreads();
-    uint32_t a[16][4], b[16][4];
-    for (int it = 0; it < n_apply; ++it) {
-        if (lane < 16 && radius2 > 0.0f) {
-            const float *xs = x + lane * NOUT;
-            const bool inside = xs[0] * xs[0] + xs[1] * xs[1] <= radius2 && xs[2] * xs[2] + xs[3] * xs[3] <= radius2 &&
-                                fabsf(xs[4]) <= 1.0f;
-            if (!inside) act[lane] = 0;
+    tc_after_sync();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == 0) {
+        // ---------------------------------------------------- weight stream
+        if (lane == 0) {
+            uint32_t q = 0;
+            for (int64_t tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x)
+                for (int it = 0; it < n_apply && !*abort_flag; ++it)
+                    for (int l = 0; l < 2; ++l)
+                        for (int c = 0; c < 4; ++c, ++q) {
+                            const uint32_t slot = q % RING, use = q / RING;
+                            if (!mbar_wait(BAR_EMPTY + 8 * slot, (use & 1) ^ 1, abort_flag)) break;
+                            mbar_expect_tx(BAR_FULL + 8 * slot, W_CHUNK_BYTES);
+                            bulk_load(s0 + SM_RING + slot * W_CHUNK_BYTES,
+                                      wp + (l == 0 ? PK_W2 : PK_W3) + c * W_CHUNK_BYTES, W_CHUNK_BYTES,
+                                      BAR_FULL + 8 * slot);
+                        }
+            // drain: every issued copy has landed before the block exits
+            const uint32_t issued = q;
+            for (uint32_t r = issued > RING ? issued - RING : 0; r < issued; ++r)
+                if (!mbar_wait_bounded(BAR_FULL + 8 * (r % RING), (r / RING) & 1)) *abort_flag = 1;
         }
-        __syncwarp();
-        // layer 1: one k tile of the (6-wide, zero-padded) input
-        {
-            uint32_t in[4];
-            in[0] = (c2 < 6) ? pack_bf16(x[r * NOUT + c2], x[r * NOUT + c2 + 1]) : 0u;
-            in[1] = (c2 < 6) ? pack_bf16(x[(r + 8) * NOUT + c2], x[(r + 8) * NOUT + c2 + 1]) : 0u;
-            in[2] = 0u;
-            in[3] = 0u;
+    } else if (warp == 1) {
+        // ---------------------------------------------------- MMA issue
+        if (lane == 0) {
+            const uint32_t ID256 = idesc_bf16(TC_M, H), ID16 = idesc_bf16(TC_M, 16);
+            const uint32_t D0 = tmem, D1 = tmem + 256;
+            uint32_t q = 0, nx = 0, na = 0;
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+                for (int it = 0; it < n_apply && ok; ++it) {
+                    // layer 1: X (128 x 16) x W1^T -> D0
+                    ok = mbar_wait(BAR_X, nx++ & 1, abort_flag);
+                    if (!ok) break;
+                    tc_after_sync();
+                    umma(D0, sdesc(s0 + SM_X, 128, 256, 0), sdesc(s0 + SM_W1, 128, 256, 0), ID256, 0);
+                    umma_commit(BAR_D);
+                    // layers 2, 3: A (128 x 256) x W^T (streamed) -> D1, D0
+                    for (int l = 0; l < 2 && ok; ++l) {
+                        const uint32_t D = l == 0 ? D1 : D0;
+                        for (int c = 0; c < 4; ++c, ++q) {
+                            const uint32_t slot = q % RING, use = q / RING;
+                            ok = mbar_wait(BAR_A + 8 * c, na & 1, abort_flag) &&
+                                 mbar_wait(BAR_FULL + 8 * slot, use & 1, abort_flag);
+                            if (!ok) break;
+                            tc_after_sync();
+                            const uint32_t a0 = s0 + SM_A + c * A_CHUNK_BYTES;
+                            const uint32_t b0 = s0 + SM_RING + slot * W_CHUNK_BYTES;
 #pragma unroll
-            for (int nt = 0; nt < H / 8; ++nt) {
-                float acc[4] = {0.f, 0.f, 0.f, 0.f};
-                const __nv_bfloat16 *wr = sW1 + (nt * 8 + r) * KIN;
-                mma_bf16(acc, in, *reinterpret_cast<const uint32_t *>(wr + c2),
-                         *reinterpret_cast<const uint32_t *>(wr + c2 + 8));
-                const float bb0 = sB[nt * 8 + c2], bb1 = sB[nt * 8 + c2 + 1];
-                const uint32_t lo = pack_bf16(silu(acc[0] + bb0), silu(acc[1] + bb1));
-                const uint32_t hi = pack_bf16(silu(acc[2] + bb0), silu(acc[3] + bb1));
-                if ((nt & 1) == 0) { a[nt >> 1][0] = lo; a[nt >> 1][1] = hi; }
-                else { a[nt >> 1][2] = lo; a[nt >> 1][3] = hi; }
+                            for (int kk = 0; kk < 4; ++kk)
+                                umma(D, sdesc(a0 + 32 * kk, 16, 1024, 2), sdesc(b0 + 32 * kk, 16, 1024, 2), ID256,
+                                     (c | kk) != 0);
+                            umma_commit(BAR_EMPTY + 8 * slot);
+                        }
+                        ++na;
+                        if (ok) umma_commit(BAR_D);
+                    }
+                    if (!ok) break;
+                    // layer 4: A (128 x 256) x W4^T (16 x 256, resident) -> D1 columns 0..15
+                    for (int c = 0; c < 4; ++c) {
+                        ok = mbar_wait(BAR_A + 8 * c, na & 1, abort_flag);
+                        if (!ok) break;
+                        tc_after_sync();
+                        const uint32_t a0 = s0 + SM_A + c * A_CHUNK_BYTES;
+                        const uint32_t b0 = s0 + SM_W4 + c * W4_CHUNK_BYTES;
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)
+                            umma(D1, sdesc(a0 + 32 * kk, 16, 1024, 2), sdesc(b0 + 32 * kk, 16, 1024, 2), ID16,
+                                 (c | kk) != 0);
+                    }
+                    ++na;
+                    if (ok) umma_commit(BAR_D);
+                }
+            // drain: every MMA issued has completed before tensor memory is freed
+            umma_commit(BAR_DRAIN);
+            if (!mbar_wait_bounded(BAR_DRAIN, 0)) *abort_flag = 1;
+        }
+    } else {
+        // ---------------------------------------------------- epilogue
+        const int quarter = warp & 3;                 // tensor-memory lanes 32 * quarter ..
+        const int row = quarter * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+        uint32_t nd = 0;
+        bool ok = true;
+        for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const int64_t p = tile * TC_M + row;
+            float x[NOUT];
+            if (p < n) {
+                const float4 u = reinterpret_cast<const float4 *>(state)[2 * p];
+                const float4 w = reinterpret_cast<const float4 *>(state)[2 * p + 1];
+                x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w; x[4] = w.x; x[5] = w.y; x[6] = w.z; x[7] = w.w;
+            } else {
+#pragma unroll
+                for (int i = 0; i < NOUT; ++i) x[i] = 0.0f;
+            }
+            bool act = p < n;
+            int cnt = 0;
+            for (int it = 0; it < n_apply && ok; ++it) {
+                if (radius2 > 0.0f)
+                    act = act && (x[0] * x[0] + x[1] * x[1] <= radius2) && (x[2] * x[2] + x[3] * x[3] <= radius2) &&
+                          (fabsf(x[4]) <= 1.0f);
+                // layer-1 input row: bfloat16 of s0..s5, zero padding to 16
+                {
+                    uint4 lo, hi;
+                    lo.x = pack_bf16(x[0], x[1]);
+                    lo.y = pack_bf16(x[2], x[3]);
+                    lo.z = pack_bf16(x[4], x[5]);
+                    lo.w = 0u;
+                    hi = make_uint4(0u, 0u, 0u, 0u);
+                    *reinterpret_cast<uint4 *>(sm + SM_X + core_off(row, 0)) = lo;
+                    *reinterpret_cast<uint4 *>(sm + SM_X + core_off(row, 8)) = hi;
+                    fence_async_smem();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(BAR_X);
+                }
+                // hidden layers: D0 (layer 1), D1 (layer 2), D0 (layer 3)
+                for (int l = 0; l < 3 && ok; ++l) {
+                    ok = __all_sync(0xffffffffu, mbar_wait(BAR_D, nd++ & 1, abort_flag));
+                    if (!ok) break;
+                    tc_after_sync();
+                    const uint32_t dcol = (l == 1) ? 256u : 0u;
+                    const float *hb = sbias + l * H;
+                    for (int c = 0; c < 4; ++c) {
+                        uint32_t v[64];
+                        TMEM_LD32(lane_base + dcol + c * TC_CHUNK, v);
+                        TMEM_LD32(lane_base + dcol + c * TC_CHUNK + 32, (v + 32));
+                        tmem_wait_ld();
+                        unsigned char *arow = sm + SM_A + c * A_CHUNK_BYTES + row * 128;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const uint4 o = silu8(v + 8 * j, hb + c * TC_CHUNK + 8 * j);
+                            *reinterpret_cast<uint4 *>(arow + ((j ^ (row & 7)) << 4)) = o;
+                        }
+                        fence_async_smem();
+                        tc_before_sync();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(BAR_A + 8 * c);
+                    }
+                }
+                if (!ok) break;
+                // layer 4 and the residual update
+                ok = __all_sync(0xffffffffu, mbar_wait(BAR_D, nd++ & 1, abort_flag));
+                if (!ok) break;
+                tc_after_sync();
+                uint32_t f[16];
+                TMEM_LD16(lane_base + 256, f);
+                tmem_wait_ld();
+                tc_before_sync();
+                if (act) {
+                    float y[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        float lin = stail[72 + c];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) lin = fmaf(x[k], stail[8 + k * NOUT + c], lin);
+                        y[c] = x[c] + (lin + (__uint_as_float(f[c]) + stail[c]));
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) x[c] = y[c];
+                    ++cnt;
+                }
+            }
+            if (p < n && ok) {
+                reinterpret_cast<float4 *>(state)[2 * p] = make_float4(x[0], x[1], x[2], x[3]);
+                reinterpret_cast<float4 *>(state)[2 * p + 1] = make_float4(x[4], x[5], x[6], x[7]);
+                if (applied) applied[p] = cnt;
             }
         }
-        hidden_layer<false>(a, b, sW2, KP, sB + H, lane);
-        hidden_layer<true>(b, a, w3t, H, sB + 2 * H, lane);
-        // layer 4 and the residual: rows r and r + 8, columns c2, c2 + 1
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        const __nv_bfloat16 *wr = sW4 + r * KP;
-#pragma unroll
-        for (int kt = 0; kt < H / 16; ++kt)
-            mma_bf16(acc, a[kt], *reinterpret_cast<const uint32_t *>(wr + kt * 16 + c2),
-                     *reinterpret_cast<const uint32_t *>(wr + kt * 16 + c2 + 8));
-        float y[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int row = r + ((q & 2) ? 8 : 0), col = c2 + (q & 1);
-            float v = x[row * NOUT + col];
-            if (col < 6) {
-                float lin = sBs[col];
-                for (int k = 0; k < 6; ++k) lin += x[row * NOUT + k] * sWs[k * NOUT + col];
-                v += lin + (acc[q] + sB4[col]);
-            }
-            y[q] = v;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int row = r + ((q & 2) ? 8 : 0), col = c2 + (q & 1);
-            if (col < 4 && act[row]) x[row * NOUT + col] = y[q];   // e and the spare column stay
-        }
-        if (lane < 16) cnt[lane] += act[lane];
-        __syncwarp();
     }
-    for (int e = lane; e < 16 * NOUT; e += 32) {
-        const int64_t p = p0 + e / NOUT;
-        if (p < n) state[p * NOUT + (e % NOUT)] = x[e];
+    // teardown: the MMA thread has drained its MMAs, the epilogue its loads
+    tc_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
     }
-    if (applied && lane < 16 && p0 + lane < n) applied[p0 + lane] = cnt[lane];
+    if (threadIdx.x == 0 && *abort_flag && error) atomicExch(error, 1);
 }
 
 int blocks_for(int64_t n, int tb) { return (int)((n + tb - 1) / tb < 4096 ? (n + tb - 1) / tb : 4096); }
@@ -407,7 +712,10 @@ int blocks_for(int64_t n, int tb) { return (int)((n + tb - 1) / tb < 4096 ? (n +
 
 // ------------------------------------------------------------------ C ABI
 
-static_assert(2 * (H * KIN + 2 * H * H + NOUT * H) == FFA_MLP_WPACK_BYTES, "inference weight pack size");
+
+static_assert(PK_TOTAL == FFA_MLP_WPACK_BYTES, "inference weight pack size");
+static_assert(TC_SMEM <= 232448, "inference kernel shared memory");
+
 
 extern "C" int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, int transB, float *C,
                             int ldc, int M, int N, int K, const float *bias, void *stream)
@@ -476,27 +784,32 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }
 
+
 extern "C" int ffa_mlp_pack(const float *params, void *wpack, void *stream)
 {
     if (!params || !wpack || (reinterpret_cast<uintptr_t>(wpack) & 15)) return FFA_ERR_INVALID;
-    __nv_bfloat16 *w1t = reinterpret_cast<__nv_bfloat16 *>(wpack);
-    __nv_bfloat16 *w2t = w1t + H * KIN, *w3t = w2t + H * H, *w4t = w3t + H * H;
-    pack_weights_kernel<<<(H * H + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, w1t, w2t, w3t, w4t);
+    pack_weights_kernel<<<(H * H + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        params, reinterpret_cast<unsigned char *>(wpack));
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }
 
 extern "C" int ffa_mlp_infer(const ffa_mlp_infer_desc *d, void *stream)
 {
     if (!d || !d->params || !d->wpack || !d->state || d->n < 0 || d->n_apply < 0 ||
-        (reinterpret_cast<uintptr_t>(d->wpack) & 15))
+        (reinterpret_cast<uintptr_t>(d->wpack) & 15) || (reinterpret_cast<uintptr_t>(d->state) & 15))
         return FFA_ERR_INVALID;
-    if (d->n == 0) return FFA_OK;
-    const int64_t blocks = (d->n + INF_WARPS * 16 - 1) / (INF_WARPS * 16);
-    if (blocks > INT32_MAX) return FFA_ERR_UNSUPPORTED;
-    const __nv_bfloat16 *w1t = reinterpret_cast<const __nv_bfloat16 *>(d->wpack);
-    const __nv_bfloat16 *w2t = w1t + H * KIN, *w3t = w2t + H * H, *w4t = w3t + H * H;
-    FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)INF_SMEM));
-    mlp_infer_kernel<<<(unsigned)blocks, INF_WARPS * 32, INF_SMEM, (cudaStream_t)stream>>>(
-        d->params, w1t, w2t, w3t, w4t, d->state, d->applied, d->n, d->n_apply, d->radius2);
+    if (d->n == 0 || d->n_apply == 0) {
+        if (d->applied && d->n > 0) FFA_CHECK_CUDA(cudaMemsetAsync(d->applied, 0, sizeof(int32_t) * d->n, (cudaStream_t)stream));
+        return FFA_OK;
+    }
+    int dev = 0, sms = 0;
+    FFA_CHECK_CUDA(cudaGetDevice(&dev));
+    FFA_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int64_t tiles = (d->n + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < sms ? tiles : sms);
+    FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+    mlp_infer_tc_kernel<<<grid, 192, TC_SMEM, (cudaStream_t)stream>>>(
+        d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n, d->n_apply,
+        d->radius2);
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }

@@ -450,6 +450,7 @@ class LearnedSectorMap:
         self.radius2 = float(radius) ** 2
         self.audit_every, self.audit_frac, self.audit_tol = int(audit_every), float(audit_frac), float(audit_tol)
         self.wpack = torch.empty(_lib.MLP_WPACK_BYTES, dtype=torch.uint8, device=self.dev)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.rng = np.random.Generator(np.random.PCG64(seed))
         self.launches = 0
         self.pack()
@@ -469,9 +470,14 @@ class LearnedSectorMap:
         d.radius2 = self.radius2 if radius2 is None else float(radius2)
         d.params, d.wpack, d.state = self.p.data_ptr(), self.wpack.data_ptr(), state.data_ptr()
         d.applied = applied.data_ptr() if applied is not None else None
+        d.error = self.err.data_ptr()
         stream = torch.cuda.current_stream(self.dev).cuda_stream
         _lib.check(_lib.lib().ffa_mlp_infer(ctypes.byref(d), stream), "ffa_mlp_infer")
         self.launches += 1
+
+    def error_flag(self):
+        """Non-zero when an inference launch gave up on a pipeline wait."""
+        return int(self.err.item())
 
     def track(self, phys, turns, record=False):
         """phys (n, 5) r, pr, z, pz, P at a sector entrance (float64).  Returns
@@ -521,6 +527,8 @@ class LearnedSectorMap:
                 audits.append(self._audit(turn, state, plain, plain_phys, e, P))
             if record:
                 rec.append(self._norm4(state, plain, plain_phys, e, P).cpu())
+        if self.error_flag():
+            raise _lib.FFAError("ffa_mlp_infer: a pipeline wait timed out")
         out = self.frame.to_phys(state, e)
         out[plain] = plain_phys[plain]
         res = {"phys": out, "plain": plain, "audits": audits}

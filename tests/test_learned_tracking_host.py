@@ -47,6 +47,9 @@ class RotMap(learned.LearnedSectorMap):
     def pack(self):
         pass
 
+    def error_flag(self):
+        return 0
+
     def apply(self, state, n_apply, applied=None, radius2=None):
         r2 = self.radius2 if radius2 is None else radius2
         cnt = torch.zeros(state.shape[0], dtype=torch.int32)
