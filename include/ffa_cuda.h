@@ -332,8 +332,10 @@ int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
 /* ------------------------------------------------------ learned sector map
  * A residual network for the one-sector transfer map in normalised
  * coordinates s = (u, pu, v, pv, e, 0):
- *   y = s + s Ws + bs + f(s),  f = L4 . SiLU . L3 . SiLU . L2 . SiLU . L1,
- * widths 6 -> 256 -> 256 -> 256 -> 6, L(h) = h W + b.  The reference has no
+ *   y = s + s Ws + bs + q(s) Wq + f(s),  f = L4 . SiLU . L3 . SiLU . L2 . SiLU . L1,
+ * with q(s) the 15 products s_i s_j (i <= j < 5, ordered (0,0), (0,1) .. (0,4),
+ * (1,1) .. (4,4)): a second-order skip connection around a network of widths
+ * 6 -> 256 -> 256 -> 256 -> 6, L(h) = h W + b.  The reference has no
  * counterpart; the map it learns is one sector of the azimuth-domain tracker
  * (ffa_theta_track), which follows FunctionForSEO (src/FFAG_track.py:1597-1640).
  *
@@ -341,19 +343,20 @@ int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
  * n_out) matrices with padded shapes:
  *   W1 [16][256] (rows 6..15 zero), b1 [256], W2 [256][256], b2 [256],
  *   W3 [256][256], b3 [256], W4 [256][8] (columns 6, 7 zero), b4 [8],
- *   Ws [8][8] (6 x 6 used), bs [8].
+ *   Ws [8][8] (6 x 6 used), bs [8], Wq [16][8] (15 x 6 used).
  * Hidden-layer products run on the tensor cores with bfloat16 operands and
- * float32 accumulation; the skip layer and the state stay float32.
+ * float32 accumulation; the skip connection and the state stay float32.
  * Samples and states: float32 [n][8], columns 6, 7 ignored. */
 #define FFA_MLP_HIDDEN 256
-#define FFA_MLP_PARAMS 138064
+#define FFA_MLP_PARAMS 138192
 #define FFA_MLP_WPACK_BYTES 278528   /* bfloat16 copies of W1..W4 for inference */
+#define FFA_MLP_SPLIT_WORK 1048576    /* floats of split-K partial products in the training work area */
 
 /* One optimiser step: forward, mean-squared error over the first n_fit
  * outputs, backward into `grads` (every parameter, same layout), then Adam
  * on the entries whose `mask` byte is non-zero (mask NULL: all) when lr > 0.
  * `step` is the 1-based Adam step (bias correction).  `work` holds
- * 8 * batch * 256 + 24 * batch floats; `loss_part` 148 doubles whose sum is
+ * 8 * batch * 256 + 24 * batch + FFA_MLP_SPLIT_WORK floats; `loss_part` 148 doubles whose sum is
  * the batch's summed squared error (before the step). */
 typedef struct ffa_mlp_train_desc {
     int64_t batch;

@@ -7,14 +7,17 @@ The network has no counterpart in the reference (PyFFA tracks with the
 pushers only); what it learns is the one-sector map of the azimuth-domain
 tracker that follows FunctionForSEO (src/FFAG_track.py:1597-1640).
 
-Residual MLP y = x + x Ws + bs + f(x), f = L4 . SiLU . L3 . SiLU . L2 .
+Residual MLP y = x + x Ws + bs + q(x) Wq + f(x) (q: the 15 products
+x_i x_j, i <= j < 5), f = L4 . SiLU . L3 . SiLU . L2 .
 SiLU . L1, layer widths 6 -> 256 -> 256 -> 256 -> 6 (W_l: (n_in, n_out),
 L(h) = h W_l + b_l), loss = mean over samples and the first `n_fit` outputs
 of (y - target)^2.
 
-`bf16=True` rounds every operand of a tensor-core product to bfloat16
+`bf16=True` rounds the operands of the tensor-core products to bfloat16
 (round to nearest even) the way the GPU kernels stage them: both factors of
-each of the seven training products and the four inference products; the
+every product except layer 1, where only W1 is rounded (the kernels keep the
+float32 input exact: training multiplies it in float32, inference splits it
+into high and low bfloat16 parts against a doubled W1); the
 products themselves, biases, SiLU, the skip layer and the loss stay in
 float64 here (float32 on the GPU).  The GPU evaluates SiLU(z) as
 h + h tanh(h), h = z / 2, with the hardware tanh approximation (relative
@@ -26,7 +29,13 @@ from __future__ import annotations
 import numpy as np
 
 FITTED_SHAPES = {"W1": (6, 256), "b1": (256,), "W2": (256, 256), "b2": (256,), "W3": (256, 256),
-                 "b3": (256,), "W4": (256, 6), "b4": (6,), "Ws": (6, 6), "bs": (6,)}
+                 "b3": (256,), "W4": (256, 6), "b4": (6,), "Ws": (6, 6), "bs": (6,), "Wq": (15, 6)}
+QUAD = [(i, j) for i in range(5) for j in range(i, 5)]
+
+
+def quad(x):
+    """The 15 second-order skip features s_i s_j, i <= j < 5."""
+    return np.stack([x[:, i] * x[:, j] for i, j in QUAD], 1)
 
 
 def bf16(a):
@@ -56,13 +65,18 @@ def forward(params, x, bf16_ops=False):
     h = x
     cache = {"h0": x}
     for l in (1, 2, 3):
-        z = _mm(h, params[f"W{l}"], bf16_ops) + params[f"b{l}"]
+        if l == 1:
+            # the input stays exact (the kernels split it into two bfloat16
+            # parts); only W1 is rounded
+            z = h @ (bf16(params["W1"]) if bf16_ops else params["W1"]) + params["b1"]
+        else:
+            z = _mm(h, params[f"W{l}"], bf16_ops) + params[f"b{l}"]
         cache[f"z{l}"] = z
         h = silu(z)
         cache[f"h{l}"] = h
     f = _mm(h, params["W4"], bf16_ops) + params["b4"]
     cache["f"] = f
-    y = x + x @ params["Ws"] + params["bs"] + f
+    y = x + x @ params["Ws"] + params["bs"] + quad(x) @ params["Wq"] + f
     return y, cache
 
 
@@ -74,7 +88,7 @@ def loss_and_grads(params, x, target, n_fit=4, bf16_ops=False):
     d = np.zeros_like(y)
     d[:, :n_fit] = 2.0 * (y[:, :n_fit] - target[:, :n_fit]) / (B * n_fit)
     sse = float(np.sum((y[:, :n_fit] - target[:, :n_fit]) ** 2))
-    g = {"Ws": np.asarray(x, np.float64).T @ d, "bs": d.sum(0),
+    g = {"Ws": np.asarray(x, np.float64).T @ d, "bs": d.sum(0), "Wq": quad(np.asarray(x, np.float64)).T @ d,
          "W4": _mm(c["h3"].T, d, bf16_ops), "b4": d.sum(0)}
     dh = _mm(d, params["W4"].T, bf16_ops)
     for l in (3, 2, 1):

@@ -107,8 +107,9 @@ class MapgenDesc(C.Structure):
 
 
 MLP_HIDDEN = 256
-MLP_PARAMS = 138064
+MLP_PARAMS = 138192
 MLP_WPACK_BYTES = 278528
+MLP_SPLIT_WORK = 1048576
 
 
 class MlpTrainDesc(C.Structure):

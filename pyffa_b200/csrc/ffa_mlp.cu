@@ -33,7 +33,21 @@ constexpr int64_t P_W4 = P_B3 + H;                // [H][NOUT]
 constexpr int64_t P_B4 = P_W4 + H * NOUT;
 constexpr int64_t P_WS = P_B4 + NOUT;             // [NOUT][NOUT] (6 x 6 used)
 constexpr int64_t P_BS = P_WS + NOUT * NOUT;
-constexpr int64_t P_TOTAL = P_BS + NOUT;
+constexpr int64_t P_WQ = P_BS + NOUT;             // [16][NOUT] (15 x 6 used)
+constexpr int64_t P_TOTAL = P_WQ + 16 * NOUT;
+// quadratic skip features: s_i s_j for i <= j < 5, in this order
+__device__ __constant__ int8_t QI[15] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4};
+__device__ __constant__ int8_t QJ[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
+
+// the 15 quadratic features of a register-resident state, in QI / QJ order
+__device__ __forceinline__ void quad_features(const float *x, float *q)
+{
+    q[0] = x[0] * x[0]; q[1] = x[0] * x[1]; q[2] = x[0] * x[2]; q[3] = x[0] * x[3]; q[4] = x[0] * x[4];
+    q[5] = x[1] * x[1]; q[6] = x[1] * x[2]; q[7] = x[1] * x[3]; q[8] = x[1] * x[4];
+    q[9] = x[2] * x[2]; q[10] = x[2] * x[3]; q[11] = x[2] * x[4];
+    q[12] = x[3] * x[3]; q[13] = x[3] * x[4];
+    q[14] = x[4] * x[4];
+}
 static_assert(P_TOTAL == FFA_MLP_PARAMS, "parameter block layout");
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
@@ -83,11 +97,19 @@ constexpr int GT_M = 64, GT_N = 64, GT_K = 32, GT_PAD = 8;
 __global__ void __launch_bounds__(128) gemm_tc(const float *__restrict__ A, int lda, int transA,
                                                const float *__restrict__ B, int ldb, int transB,
                                                float *__restrict__ C, int ldc, int M, int N, int K,
-                                               const float *__restrict__ bias)
+                                               const float *__restrict__ bias, int k_chunk)
 {
     __shared__ __align__(16) __nv_bfloat16 sA[GT_M][GT_K + GT_PAD];
     __shared__ __align__(16) __nv_bfloat16 sB[GT_N][GT_K + GT_PAD];
     const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
+    // split K: block z covers [kb, ke) and writes its partial product to
+    // C + z * M * N (row stride N) when gridDim.z > 1
+    const int kb = blockIdx.z * k_chunk, ke = min(K, kb + k_chunk);
+    if (gridDim.z > 1) {
+        C += (int64_t)blockIdx.z * M * N;
+        ldc = N;
+        bias = nullptr;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int r = lane >> 2, c2 = (lane & 3) * 2;
@@ -98,20 +120,34 @@ __global__ void __launch_bounds__(128) gemm_tc(const float *__restrict__ A, int 
         for (int j = 0; j < 4; ++j)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += GT_K) {
-        for (int e = threadIdx.x; e < GT_M * GT_K; e += blockDim.x) {
-            const int mm = e / GT_K, kk = e - mm * GT_K;
-            const int gm = m0 + mm, gk = k0 + kk;
-            float v = 0.0f;
-            if (gm < M && gk < K) v = transA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk];
-            sA[mm][kk] = __float2bfloat16_rn(v);
+    for (int k0 = kb; k0 < ke; k0 += GT_K) {
+        // staging: the index that is contiguous in global memory runs fastest
+        // across threads (coalesced loads), converted to bfloat16
+        if (!transA) {
+            for (int e = threadIdx.x; e < GT_M * GT_K; e += blockDim.x) {
+                const int mm = e / GT_K, kk = e - mm * GT_K;
+                const int gm = m0 + mm, gk = k0 + kk;
+                sA[mm][kk] = __float2bfloat16_rn((gm < M && gk < ke) ? A[(int64_t)gm * lda + gk] : 0.0f);
+            }
+        } else {
+            for (int e = threadIdx.x; e < GT_M * GT_K; e += blockDim.x) {
+                const int kk = e / GT_M, mm = e - kk * GT_M;
+                const int gm = m0 + mm, gk = k0 + kk;
+                sA[mm][kk] = __float2bfloat16_rn((gm < M && gk < ke) ? A[(int64_t)gk * lda + gm] : 0.0f);
+            }
         }
-        for (int e = threadIdx.x; e < GT_N * GT_K; e += blockDim.x) {
-            const int nn = e / GT_K, kk = e - nn * GT_K;
-            const int gn = n0 + nn, gk = k0 + kk;
-            float v = 0.0f;
-            if (gn < N && gk < K) v = transB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn];
-            sB[nn][kk] = __float2bfloat16_rn(v);
+        if (transB) {
+            for (int e = threadIdx.x; e < GT_N * GT_K; e += blockDim.x) {
+                const int nn = e / GT_K, kk = e - nn * GT_K;
+                const int gn = n0 + nn, gk = k0 + kk;
+                sB[nn][kk] = __float2bfloat16_rn((gn < N && gk < ke) ? B[(int64_t)gn * ldb + gk] : 0.0f);
+            }
+        } else {
+            for (int e = threadIdx.x; e < GT_N * GT_K; e += blockDim.x) {
+                const int kk = e / GT_N, nn = e - kk * GT_N;
+                const int gn = n0 + nn, gk = k0 + kk;
+                sB[nn][kk] = __float2bfloat16_rn((gn < N && gk < ke) ? B[(int64_t)gk * ldb + gn] : 0.0f);
+            }
         }
         __syncthreads();
 #pragma unroll
@@ -148,7 +184,38 @@ __global__ void __launch_bounds__(128) gemm_tc(const float *__restrict__ A, int 
             }
 }
 
+// C[m][n] = sum over the splits of part[z][m][n], in split order
+__global__ void split_sum_kernel(const float *__restrict__ part, int splits, int M, int N, float *__restrict__ C,
+                                 int ldc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M * N) return;
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[(int64_t)z * M * N + i];
+    C[(int64_t)(i / N) * ldc + (i % N)] = s;
+}
+
+constexpr int SPLITS_MAX = 16;
+constexpr int64_t SPLIT_WORK = (int64_t)SPLITS_MAX * H * H;   // floats
+static_assert(SPLIT_WORK == FFA_MLP_SPLIT_WORK, "training split-K work area");
+
 // ------------------------------------------------------- element-wise (training)
+// layer 1: z1 = x W1 + b1 with the float32 input and bfloat16-rounded W1, the
+// values the inference kernel's split-input product forms
+__global__ void layer1_kernel(const float *__restrict__ x, const float *__restrict__ P, float *__restrict__ z1,
+                              int64_t B)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B * H; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / H;
+        const int n = (int)(i - r * H);
+        float z = P[P_B1 + n];
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            z = fmaf(x[r * NOUT + k], __bfloat162float(__float2bfloat16_rn(P[P_W1 + k * H + n])), z);
+        z1[i] = z;
+    }
+}
+
 __global__ void silu_kernel(const float *z, float *h, int64_t n)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -174,6 +241,7 @@ __global__ void out_grad_kernel(const float *x, const float *t, const float *f, 
             if (c < 6) {
                 v = x[i * NOUT + c] + f[i * NOUT + c] + P[P_BS + c];
                 for (int k = 0; k < 6; ++k) v += x[i * NOUT + k] * P[P_WS + k * NOUT + c];
+                for (int m = 0; m < 15; ++m) v += x[i * NOUT + QI[m]] * x[i * NOUT + QJ[m]] * P[P_WQ + m * NOUT + c];
             }
             y[i * NOUT + c] = v;
             float g = 0.0f;
@@ -213,18 +281,21 @@ __global__ void __launch_bounds__(256) colsum_kernel(const float *d, int64_t B, 
     }
 }
 
-// skip-layer gradient gWs[k][c] = sum_i x[i][k] d[i][c] (k, c < 6): block k,
-// 256 threads over rows, fixed-order reduction.
+// skip-layer gradients: block k < 8 forms gWs[k][c] = sum_i x[i][k] d[i][c],
+// block 8 + m forms gWq[m][c] = sum_i x[i][QI[m]] x[i][QJ[m]] d[i][c]
+// (c < 6), 256 threads over rows, fixed-order reduction
 __global__ void __launch_bounds__(256) skip_grad_kernel(const float *x, const float *d, int64_t B, float *G)
 {
     __shared__ float sh[256][NOUT + 1];
     const int k = blockIdx.x;
+    const bool quad = k >= NOUT;
+    const int m = k - NOUT;
     float s[NOUT];
 #pragma unroll
     for (int c = 0; c < NOUT; ++c) s[c] = 0.0f;
-    if (k < 6)
+    if ((!quad && k < 6) || (quad && m < 15))
         for (int64_t i = threadIdx.x; i < B; i += blockDim.x) {
-            const float xk = x[i * NOUT + k];
+            const float xk = quad ? x[i * NOUT + QI[m]] * x[i * NOUT + QJ[m]] : x[i * NOUT + k];
 #pragma unroll
             for (int c = 0; c < 6; ++c) s[c] += xk * d[i * NOUT + c];
         }
@@ -234,7 +305,7 @@ __global__ void __launch_bounds__(256) skip_grad_kernel(const float *x, const fl
     if (threadIdx.x < NOUT) {
         float t = 0.0f;
         for (int i = 0; i < (int)blockDim.x; ++i) t += sh[i][threadIdx.x];
-        G[P_WS + k * NOUT + threadIdx.x] = t;
+        G[(quad ? P_WQ + m * NOUT : P_WS + k * NOUT) + threadIdx.x] = t;
     }
 }
 
@@ -263,13 +334,14 @@ __global__ void adam_kernel(float *P, const float *G, float *m, float *v, int64_
 // D0 = columns 0..255, D1 = columns 256..511, layers 1..4 alternate D0, D1.
 // Warp roles: warp 0 streams W2 / W3 from global (L2-resident) into a ring
 // of three 32 KB shared-memory slots with cp.async.bulk; warp 1 owns tensor
-// memory and issues the MMAs (one thread); warps 2..5 are the epilogue, one
-// thread per state (its tensor-memory lane): it reads its accumulator row,
-// adds the bias, applies SiLU, rounds to bfloat16 and writes the next
-// layer's A operand one 64-column chunk at a time, so the next layer's MMAs
-// on chunk c start while chunk c + 1 is still being written.  The state,
-// the domain check and the float32 skip layer stay in the epilogue
-// thread's registers for all n_apply maps.
+// memory and issues the MMAs (one thread); warps 2..9 are the epilogue, two
+// threads per state (its tensor-memory lane), one per half of each 64-column
+// chunk.  They read the accumulator row, add the bias, apply SiLU, round to
+// bfloat16 and write the next layer's A operand one chunk at a time (the
+// next chunk's tensor-memory load in flight meanwhile), so the next layer's
+// MMAs on chunk c start while chunk c + 1 is still being written.  The
+// state, the domain check and the float32 skip layer stay in the registers
+// of the half-0 thread for all n_apply maps.
 //
 // Shared-memory operand layouts (K-major):
 //  - A (activations, 128 x 256) and W2 / W3 / W4 (B operand, N x 256): four
@@ -301,8 +373,8 @@ constexpr uint32_t SM_W4 = SM_RING + RING * W_CHUNK_BYTES;
 constexpr uint32_t SM_W1 = SM_W4 + 4 * W4_CHUNK_BYTES;
 constexpr uint32_t SM_X = SM_W1 + H * KIN * 2;
 constexpr uint32_t SM_BIAS = SM_X + TC_M * KIN * 2;          // b1 b2 b3 (halved), float
-constexpr uint32_t SM_TAIL = SM_BIAS + 3 * H * 4;            // b4[8] Ws[64] bs[8]
-constexpr uint32_t SM_BAR = SM_TAIL + 80 * 4;                // mbarriers (8 B each)
+constexpr uint32_t SM_TAIL = SM_BIAS + 3 * H * 4;            // b4[8] Ws[64] bs[8] Wq[128]
+constexpr uint32_t SM_BAR = SM_TAIL + 208 * 4;               // mbarriers (8 B each)
 constexpr int NBAR = 1 + 4 + 1 + 2 * RING + 1;               // x_ready, a_ready[4], d_full, full[], empty[], drain
 constexpr uint32_t SM_MISC = SM_BAR + NBAR * 8;              // tmem base, abort flag
 constexpr uint32_t SM_TOTAL = SM_MISC + 16;
@@ -359,12 +431,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
 
 // Waits for the phase of `bar` with `parity`; gives up (and raises the
 // block's abort flag) after WAIT_NS or when another thread has raised it.
+// try_wait suspends the thread for a while by itself; the clock and the flag
+// are read once every 64 polls.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag)
 {
     if (mbar_test(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     while (true) {
-        if (mbar_test(bar, parity)) return true;
+#pragma unroll 1
+        for (int i = 0; i < 64; ++i)
+            if (mbar_test(bar, parity)) return true;
         if (*abort_flag) return false;
         if (global_ns() - t0 > WAIT_NS) {
             *abort_flag = 1;
@@ -433,6 +509,15 @@ __device__ __forceinline__ void umma_commit(uint32_t bar)
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// keeps the compiler from moving uses of tcgen05.ld results above the wait
+#define REG_FENCE16(v)                                                                                       \
+    asm volatile("" : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]), "+r"(v[6]),   \
+                 "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]), "+r"(v[12]), "+r"(v[13]),      \
+                 "+r"(v[14]), "+r"(v[15]))
+#define REG_FENCE32(v)  \
+    REG_FENCE16(v);     \
+    REG_FENCE16((v + 16))
+
 // byte offset of element (row, k) in a 128-byte-swizzled chunked operand
 // with `rows` rows per chunk
 __host__ __device__ __forceinline__ uint32_t swz_off(int row, int k, int rows)
@@ -456,8 +541,10 @@ __global__ void pack_weights_kernel(const float *__restrict__ P, unsigned char *
         *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W3 + swz_off(n, k, H)) = __float2bfloat16_rn(P[P_W3 + k * H + n]);
     }
     if (tid < H * KIN) {
+        // columns 0..5 and 6..11 both hold W1 rows 0..5 (high / low input parts)
         const int n = tid / KIN, k = tid % KIN;
-        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W1 + core_off(n, k)) = __float2bfloat16_rn(P[P_W1 + k * H + n]);
+        const float v = k < 12 ? P[P_W1 + (k % 6) * H + n] : 0.0f;
+        *reinterpret_cast<__nv_bfloat16 *>(wp + PK_W1 + core_off(n, k)) = __float2bfloat16_rn(v);
     }
     if (tid < 16 * H) {
         const int n = tid / H, k = tid % H;
@@ -480,7 +567,7 @@ __device__ __forceinline__ uint4 silu8(const uint32_t *v, const float *hb)
     return o;
 }
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320, 1)
     mlp_infer_tc_kernel(const float *__restrict__ P, const unsigned char *__restrict__ wp, float *__restrict__ state,
                         int32_t *__restrict__ applied, int32_t *__restrict__ error, int64_t n, int n_apply,
                         float radius2)
@@ -489,7 +576,7 @@ __global__ void __launch_bounds__(192, 1)
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t s0 = smem_u32(sm);
     float *sbias = reinterpret_cast<float *>(sm + SM_BIAS);
-    float *stail = reinterpret_cast<float *>(sm + SM_TAIL);   // b4[0..7], Ws[8..71], bs[72..79]
+    float *stail = reinterpret_cast<float *>(sm + SM_TAIL);   // b4[0..7], Ws[8..71], bs[72..79], Wq[80..207]
     const uint32_t bar0 = s0 + SM_BAR;
     const uint32_t BAR_X = bar0, BAR_A = bar0 + 8, BAR_D = bar0 + 40, BAR_FULL = bar0 + 48,
                    BAR_EMPTY = bar0 + 48 + 8 * RING, BAR_DRAIN = bar0 + 48 + 16 * RING;
@@ -504,11 +591,11 @@ __global__ void __launch_bounds__(192, 1)
     for (int i = threadIdx.x; i < (int)(4 * W4_CHUNK_BYTES / 16); i += blockDim.x)
         reinterpret_cast<uint4 *>(sm + SM_W4)[i] = reinterpret_cast<const uint4 *>(wp + PK_W4)[i];
     for (int i = threadIdx.x; i < 3 * H; i += blockDim.x) sbias[i] = 0.5f * P[(i < H ? P_B1 : i < 2 * H ? P_B2 : P_B3) + (i % H)];
-    for (int i = threadIdx.x; i < 80; i += blockDim.x)
-        stail[i] = i < 8 ? P[P_B4 + i] : i < 72 ? P[P_WS + (i - 8)] : P[P_BS + (i - 72)];
+    for (int i = threadIdx.x; i < 208; i += blockDim.x)
+        stail[i] = i < 8 ? P[P_B4 + i] : i < 72 ? P[P_WS + (i - 8)] : i < 80 ? P[P_BS + (i - 72)] : P[P_WQ + (i - 80)];
     if (threadIdx.x == 0) {
         mbar_init(BAR_X, 4);
-        for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * c, 4);
+        for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * c, 8);
         mbar_init(BAR_D, 1);
         for (int s = 0; s < RING; ++s) {
             mbar_init(BAR_FULL + 8 * s, 1);
@@ -606,9 +693,13 @@ __global__ void __launch_bounds__(192, 1)
         }
     } else {
         // ---------------------------------------------------- epilogue
-        const int quarter = warp & 3;                 // tensor-memory lanes 32 * quarter ..
+        // warps 2..9: tensor-memory lane quarter warp % 4, column half
+        // (warp - 2) / 4 of every 64-column chunk; the half-0 thread of a row
+        // owns that state
+        const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
-        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + 32 * half;
         uint32_t nd = 0;
         bool ok = true;
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -625,17 +716,25 @@ __global__ void __launch_bounds__(192, 1)
             bool act = p < n;
             int cnt = 0;
             for (int it = 0; it < n_apply && ok; ++it) {
-                if (radius2 > 0.0f)
-                    act = act && (x[0] * x[0] + x[1] * x[1] <= radius2) && (x[2] * x[2] + x[3] * x[3] <= radius2) &&
-                          (fabsf(x[4]) <= 1.0f);
-                // layer-1 input row: bfloat16 of s0..s5, zero padding to 16
-                {
+                if (half == 0) {
+                    if (radius2 > 0.0f)
+                        act = act && (x[0] * x[0] + x[1] * x[1] <= radius2) &&
+                              (x[2] * x[2] + x[3] * x[3] <= radius2) && (fabsf(x[4]) <= 1.0f);
+                    // layer-1 input row: s0..s5 split into bfloat16 high and low
+                    // parts (columns 0..5 and 6..11; W1 is stacked twice), so
+                    // the product sees the float32 state, zero padding to 16
+                    float xl[6];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) xl[k] = x[k] - __bfloat162float(__float2bfloat16_rn(x[k]));
                     uint4 lo, hi;
                     lo.x = pack_bf16(x[0], x[1]);
                     lo.y = pack_bf16(x[2], x[3]);
                     lo.z = pack_bf16(x[4], x[5]);
-                    lo.w = 0u;
-                    hi = make_uint4(0u, 0u, 0u, 0u);
+                    lo.w = pack_bf16(xl[0], xl[1]);
+                    hi.x = pack_bf16(xl[2], xl[3]);
+                    hi.y = pack_bf16(xl[4], xl[5]);
+                    hi.z = 0u;
+                    hi.w = 0u;
                     *reinterpret_cast<uint4 *>(sm + SM_X + core_off(row, 0)) = lo;
                     *reinterpret_cast<uint4 *>(sm + SM_X + core_off(row, 8)) = hi;
                     fence_async_smem();
@@ -647,49 +746,67 @@ __global__ void __launch_bounds__(192, 1)
                     ok = __all_sync(0xffffffffu, mbar_wait(BAR_D, nd++ & 1, abort_flag));
                     if (!ok) break;
                     tc_after_sync();
-                    const uint32_t dcol = (l == 1) ? 256u : 0u;
-                    const float *hb = sbias + l * H;
-                    for (int c = 0; c < 4; ++c) {
-                        uint32_t v[64];
-                        TMEM_LD32(lane_base + dcol + c * TC_CHUNK, v);
-                        TMEM_LD32(lane_base + dcol + c * TC_CHUNK + 32, (v + 32));
-                        tmem_wait_ld();
-                        unsigned char *arow = sm + SM_A + c * A_CHUNK_BYTES + row * 128;
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            const uint4 o = silu8(v + 8 * j, hb + c * TC_CHUNK + 8 * j);
-                            *reinterpret_cast<uint4 *>(arow + ((j ^ (row & 7)) << 4)) = o;
-                        }
-                        fence_async_smem();
-                        tc_before_sync();
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(BAR_A + 8 * c);
-                    }
+                    const uint32_t src = lane_base + ((l == 1) ? 256u : 0u);
+                    const float *hb = sbias + l * H + 32 * half;
+                    unsigned char *arow = sm + SM_A + row * 128;
+                    uint32_t va[32], vb[32];
+                    TMEM_LD32(src, va);
+                    tmem_wait_ld();
+                    REG_FENCE32(va);
+                    // chunk c is converted while chunk c + 1 is in flight
+#define EPI_CHUNK(c, cur, nxt)                                                                           \
+    {                                                                                                    \
+        if ((c) < 3) TMEM_LD32(src + ((c) + 1) * TC_CHUNK, nxt);                                         \
+        _Pragma("unroll") for (int j = 0; j < 4; ++j)                                                    \
+        {                                                                                                \
+            const uint4 o = silu8(cur + 8 * j, hb + (c) * TC_CHUNK + 8 * j);                            \
+            *reinterpret_cast<uint4 *>(arow + (c) * A_CHUNK_BYTES + (((4 * half + j) ^ (row & 7)) << 4)) = o; \
+        }                                                                                                \
+        fence_async_smem();                                                                              \
+        if ((c) < 3) {                                                                                   \
+            tmem_wait_ld();                                                                              \
+            REG_FENCE32(nxt);                                                                            \
+        }                                                                                                \
+        tc_before_sync();                                                                                \
+        __syncwarp();                                                                                    \
+        if (lane == 0) mbar_arrive(BAR_A + 8 * (c));                                                     \
+    }
+                    EPI_CHUNK(0, va, vb)
+                    EPI_CHUNK(1, vb, va)
+                    EPI_CHUNK(2, va, vb)
+                    EPI_CHUNK(3, vb, va)
+#undef EPI_CHUNK
                 }
                 if (!ok) break;
                 // layer 4 and the residual update
                 ok = __all_sync(0xffffffffu, mbar_wait(BAR_D, nd++ & 1, abort_flag));
                 if (!ok) break;
-                tc_after_sync();
-                uint32_t f[16];
-                TMEM_LD16(lane_base + 256, f);
-                tmem_wait_ld();
-                tc_before_sync();
-                if (act) {
-                    float y[4];
+                if (half == 0) {
+                    tc_after_sync();
+                    uint32_t f[16];
+                    TMEM_LD16(lane_base + 256, f);
+                    tmem_wait_ld();
+                    REG_FENCE16(f);
+                    tc_before_sync();
+                    if (act) {
+                        float y[4], q[15];
+                        quad_features(x, q);
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        float lin = stail[72 + c];
+                        for (int c = 0; c < 4; ++c) {
+                            float lin = stail[72 + c];
 #pragma unroll
-                        for (int k = 0; k < 6; ++k) lin = fmaf(x[k], stail[8 + k * NOUT + c], lin);
-                        y[c] = x[c] + (lin + (__uint_as_float(f[c]) + stail[c]));
+                            for (int k = 0; k < 6; ++k) lin = fmaf(x[k], stail[8 + k * NOUT + c], lin);
+#pragma unroll
+                            for (int m = 0; m < 15; ++m) lin = fmaf(q[m], stail[80 + m * NOUT + c], lin);
+                            y[c] = x[c] + (lin + (__uint_as_float(f[c]) + stail[c]));
+                        }
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) x[c] = y[c];
+                        ++cnt;
                     }
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) x[c] = y[c];
-                    ++cnt;
                 }
             }
-            if (p < n && ok) {
+            if (half == 0 && p < n && ok) {
                 reinterpret_cast<float4 *>(state)[2 * p] = make_float4(x[0], x[1], x[2], x[3]);
                 reinterpret_cast<float4 *>(state)[2 * p + 1] = make_float4(x[4], x[5], x[6], x[7]);
                 if (applied) applied[p] = cnt;
@@ -723,7 +840,7 @@ extern "C" int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B,
     if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return FFA_ERR_INVALID;
     dim3 grid((unsigned)((N + GT_N - 1) / GT_N), (unsigned)((M + GT_M - 1) / GT_M));
     if (grid.y > 65535) return FFA_ERR_UNSUPPORTED;
-    gemm_tc<<<grid, 128, 0, (cudaStream_t)stream>>>(A, lda, transA, B, ldb, transB, C, ldc, M, N, K, bias);
+    gemm_tc<<<grid, 128, 0, (cudaStream_t)stream>>>(A, lda, transA, B, ldb, transB, C, ldc, M, N, K, bias, K);
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }
 
@@ -740,13 +857,29 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     float *f = h3 + B * H, *y = f + B * NOUT, *dd = y + B * NOUT, *dh = dd + B * NOUT, *dz = dh + B * H;
     const int ew = blocks_for(B * H, 256);
     const int Bi = (int)B;
+    float *part = dz + B * H;                                    // split-K partials
     auto gemm = [&](const float *A_, int lda_, int tA_, const float *B_, int ldb_, int tB_, float *C_, int ldc_,
                     int M_, int N_, int K_, const float *bias_) {
         const dim3 grid((unsigned)((N_ + GT_N - 1) / GT_N), (unsigned)((M_ + GT_M - 1) / GT_M));
-        gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, tA_, B_, ldb_, tB_, C_, ldc_, M_, N_, K_, bias_);
+        gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, tA_, B_, ldb_, tB_, C_, ldc_, M_, N_, K_, bias_, K_);
+    };
+    // weight gradients (K = batch): split K over up to SPLITS_MAX blocks per
+    // output tile, partials summed in a fixed order
+    auto gemm_wgrad = [&](const float *A_, int lda_, const float *B_, int ldb_, float *C_, int ldc_, int M_, int N_) {
+        int splits = (int)((B + 1023) / 1024);
+        splits = splits < 1 ? 1 : splits > SPLITS_MAX ? SPLITS_MAX : splits;
+        const int kc = (int)(((B + splits - 1) / splits + GT_K - 1) / GT_K * GT_K);
+        splits = (int)((B + kc - 1) / kc);
+        const dim3 grid((unsigned)((N_ + GT_N - 1) / GT_N), (unsigned)((M_ + GT_M - 1) / GT_M), (unsigned)splits);
+        if (splits == 1) {
+            gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, 1, B_, ldb_, 0, C_, ldc_, M_, N_, (int)B, nullptr, kc);
+        } else {
+            gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, 1, B_, ldb_, 0, part, N_, M_, N_, (int)B, nullptr, kc);
+            split_sum_kernel<<<(M_ * N_ + 255) / 256, 256, 0, s>>>(part, splits, M_, N_, C_, ldc_);
+        }
     };
     // forward
-    gemm(d->x, NOUT, 0, P + P_W1, H, 0, z1, H, Bi, H, 6, P + P_B1);
+    layer1_kernel<<<ew, 256, 0, s>>>(d->x, P, z1, B);
     silu_kernel<<<ew, 256, 0, s>>>(z1, h1, B * H);
     gemm(h1, H, 0, P + P_W2, H, 0, z2, H, Bi, H, H, P + P_B2);
     silu_kernel<<<ew, 256, 0, s>>>(z2, h2, B * H);
@@ -756,9 +889,9 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     out_grad_kernel<<<148, 256, 0, s>>>(d->x, d->target, f, P, y, dd, B, d->n_fit, d->loss_part);
     // backward
     FFA_CHECK_CUDA(cudaMemsetAsync(G, 0, sizeof(float) * P_TOTAL, s));
-    skip_grad_kernel<<<NOUT, 256, 0, s>>>(d->x, dd, B, G);
+    skip_grad_kernel<<<NOUT + 16, 256, 0, s>>>(d->x, dd, B, G);
     colsum_kernel<<<1, 256, 0, s>>>(dd, B, NOUT, NOUT, G + P_BS);
-    gemm(h3, H, 1, dd, NOUT, 0, G + P_W4, NOUT, H, NOUT, Bi, nullptr);
+    gemm_wgrad(h3, H, dd, NOUT, G + P_W4, NOUT, H, NOUT);
     colsum_kernel<<<1, 256, 0, s>>>(dd, B, NOUT, NOUT, G + P_B4);
     gemm(dd, NOUT, 0, P + P_W4, NOUT, 1, dh, H, Bi, H, NOUT, nullptr);
     const float *zs[3] = {z3, z2, z1};
@@ -767,7 +900,7 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     const int ldin[3] = {H, H, NOUT}, kin[3] = {H, H, 6};
     for (int l = 0; l < 3; ++l) {
         dsilu_kernel<<<ew, 256, 0, s>>>(dh, zs[l], B * H);   // dh -> dz in place
-        gemm(hin[l], ldin[l], 1, dh, H, 0, G + wofs[l], H, kin[l], H, Bi, nullptr);
+        gemm_wgrad(hin[l], ldin[l], dh, H, G + wofs[l], H, kin[l], H);
         colsum_kernel<<<H / 32, 256, 0, s>>>(dh, B, H, H, G + bofs[l]);
         if (l < 2) {
             gemm(dh, H, 0, P + wofs[l], H, 1, dz, H, Bi, H, H, nullptr);
@@ -808,7 +941,7 @@ extern "C" int ffa_mlp_infer(const ffa_mlp_infer_desc *d, void *stream)
     const int64_t tiles = (d->n + TC_M - 1) / TC_M;
     const int grid = (int)(tiles < sms ? tiles : sms);
     FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-    mlp_infer_tc_kernel<<<grid, 192, TC_SMEM, (cudaStream_t)stream>>>(
+    mlp_infer_tc_kernel<<<grid, 320, TC_SMEM, (cudaStream_t)stream>>>(
         d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n, d->n_apply,
         d->radius2);
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;

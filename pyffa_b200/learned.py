@@ -15,9 +15,10 @@ plain tracker as the arbiter:
   "amplitudes up to A_x / A_p" is the unit disc in each transverse plane:
   s = (u, pu, v, pv, e) with e the energy mapped to [-1, 1];
 - the network (ffa_mlp_*; widths 6 -> 256 -> 256 -> 256 -> 6, SiLU, bfloat16
-  operands with float32 accumulation, a float32 linear skip) maps s at one
-  sector entrance to s at the next; the skip layer is the least-squares
-  linear map, the MLP learns what the linear map misses;
+  operands with float32 accumulation, a float32 skip connection of first
+  and second order) maps s at one sector entrance to s at the next; the skip
+  connection is the least-squares second-order map, the MLP learns what it
+  misses (the third and higher orders);
 - tracking applies the map K times per launch on float32 states; states
   outside the domain go to the plain tracker for the rest of the run, and
   every `audit_every` turns a random `audit_frac` of the learned states is
@@ -50,7 +51,7 @@ LOSS_PARTS = 148
 
 def _layout():
     shapes = [("W1", (16, 256)), ("b1", (256,)), ("W2", (256, 256)), ("b2", (256,)), ("W3", (256, 256)),
-              ("b3", (256,)), ("W4", (256, 8)), ("b4", (8,)), ("Ws", (8, 8)), ("bs", (8,))]
+              ("b3", (256,)), ("W4", (256, 8)), ("b4", (8,)), ("Ws", (8, 8)), ("bs", (8,)), ("Wq", (16, 8))]
     out, o = {}, 0
     for k, sh in shapes:
         out[k] = (o, sh)
@@ -62,7 +63,10 @@ def _layout():
 LAYOUT = _layout()
 # the used part of each padded block (6 inputs, 6 outputs)
 USED = {"W1": (6, 256), "b1": (256,), "W2": (256, 256), "b2": (256,), "W3": (256, 256), "b3": (256,),
-        "W4": (256, 6), "b4": (6,), "Ws": (6, 6), "bs": (6,)}
+        "W4": (256, 6), "b4": (6,), "Ws": (6, 6), "bs": (6,), "Wq": (15, 6)}
+# the quadratic skip features s_i s_j, i <= j < 5, in the kernels' order
+QUAD = [(i, j) for i in range(5) for j in range(i, 5)]
+SKIP = ("Ws", "bs", "Wq")
 
 
 def block(p, name):
@@ -332,20 +336,29 @@ def make_dataset(frame, tracker, n, seed=0, radius=1.05, chunk=1 << 21):
 
 
 # ------------------------------------------------------------- training
-def fit_linear(params, X, T, n_fit=4, max_rows=1 << 22):
-    """Least-squares skip layer (float64 normal equations over up to
-    max_rows samples): T[:, :n_fit] - X[:, :n_fit] ~ X[:, :5] Ws + bs."""
+def skip_features(x):
+    """[s0..s4, 1, s_i s_j (QUAD order)] of inputs x (n, >=5), float64."""
     torch = _torch()
-    x = X[:max_rows, :5].double()
-    A = torch.cat([x, torch.ones_like(x[:, :1])], 1)
+    x = x[:, :5].double()
+    return torch.cat([x, torch.ones_like(x[:, :1])] + [(x[:, i] * x[:, j])[:, None] for i, j in QUAD], 1)
+
+
+def fit_skip(params, X, T, n_fit=4, max_rows=1 << 22, order=2):
+    """Least-squares skip connection (float64 normal equations over up to
+    max_rows samples): T[:, :n_fit] - X[:, :n_fit] ~ X Ws + bs (+ q(X) Wq
+    for order 2)."""
+    torch = _torch()
+    A = skip_features(X[:max_rows])
+    if order < 2:
+        A = A[:, :6]
     Bm = (T[:max_rows, :n_fit] - X[:max_rows, :n_fit]).double()
     sol = torch.linalg.solve(A.T @ A, A.T @ Bm)
-    Ws = block(params, "Ws")
-    bs = block(params, "bs")
-    Ws.zero_()
-    bs.zero_()
-    Ws[:5, :n_fit] = sol[:5].float()
-    bs[:n_fit] = sol[5].float()
+    for k in SKIP:
+        block(params, k).zero_()
+    block(params, "Ws")[:5, :n_fit] = sol[:5].float()
+    block(params, "bs")[:n_fit] = sol[5].float()
+    if order >= 2:
+        block(params, "Wq")[:15, :n_fit] = sol[6:].float()
 
 
 class Trainer:
@@ -361,9 +374,10 @@ class Trainer:
         self.v = torch.zeros_like(params)
         self.mask = torch.ones(N_PARAMS, dtype=torch.uint8, device=dev)
         if freeze_skip:
-            for k in ("Ws", "bs"):
+            for k in SKIP:
                 block(self.mask, k).zero_()
-        self.work = torch.empty(8 * self.B * HIDDEN + 24 * self.B, dtype=torch.float32, device=dev)
+        self.work = torch.empty(8 * self.B * HIDDEN + 24 * self.B + _lib.MLP_SPLIT_WORK, dtype=torch.float32,
+                                device=dev)
         self.loss_part = torch.zeros(LOSS_PARTS, dtype=torch.float64, device=dev)
         self.beta1, self.beta2, self.eps = beta1, beta2, eps
         self.t = 0
@@ -394,13 +408,13 @@ class Trainer:
 
 
 def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200, seed=0, n_fit=4,
-          log_every=0, time_limit=None):
-    """Linear skip by least squares, then Adam on the MLP with a cosine
-    learning rate.  Returns the history [(step, mse)] (sampled when
-    log_every > 0) and the trainer."""
+          log_every=0, time_limit=None, eps=1e-8):
+    """Second-order skip connection by least squares, then Adam on the MLP
+    with a cosine learning rate.  Returns the history [(step, mse)] (sampled
+    when log_every > 0) and the trainer."""
     torch = _torch()
-    fit_linear(params, X, T, n_fit)
-    tr = Trainer(params, batch=batch, n_fit=n_fit)
+    fit_skip(params, X, T, n_fit)
+    tr = Trainer(params, batch=batch, n_fit=n_fit, eps=eps)
     n = X.shape[0]
     nb = n // batch
     total = max(1, epochs * nb)
@@ -596,6 +610,14 @@ def tunes(record, nsectors=None):
         dphi = np.angle(z[1:] / z[:-1]) % (2 * np.pi)
         out.append(dphi.mean(0) / (2 * np.pi))
     return np.stack(out, 1)
+
+
+def betatron_emittance(frame, s4):
+    """rms emittances of the betatron motion from normalised transverse
+    coordinates s4 (n, 4) (closed orbit of each energy removed, mid-energy
+    Twiss frame): R^2 times the rms emittance of (X, PX) and (Y, PY)."""
+    s4 = np.asarray(s4, np.float64)
+    return rms_emittance(s4) * np.array([frame.R["x"] ** 2, frame.R["z"] ** 2])
 
 
 def rms_emittance(phys):

@@ -19,6 +19,7 @@ def _params(seed, scale_out=0.05):
     d["b4"] = 0.01 * rng.standard_normal(6)
     d["Ws"] = 0.1 * rng.standard_normal((6, 6))
     d["bs"] = 0.01 * rng.standard_normal(6)
+    d["Wq"] = 0.05 * rng.standard_normal((15, 6))
     return d
 
 
@@ -46,7 +47,7 @@ def test_oracle_gradients_match_finite_differences():
     def loss(p):
         return M.loss_and_grads(p, x, t, n_fit=4)[0] / n
     for name, idx in (("W1", (2, 17)), ("b1", (5,)), ("W2", (100, 3)), ("b2", (77,)), ("W3", (9, 250)),
-                      ("b3", (0,)), ("W4", (31, 2)), ("b4", (3,)), ("Ws", (4, 1)), ("bs", (0,))):
+                      ("b3", (0,)), ("W4", (31, 2)), ("b4", (3,)), ("Ws", (4, 1)), ("bs", (0,)), ("Wq", (7, 2))):
         h = 1e-6
         p1 = {k: v.copy() for k, v in d.items()}
         p2 = {k: v.copy() for k, v in d.items()}
