@@ -407,14 +407,48 @@ class Trainer:
         return float(self.loss_part.sum().item()) / (self.B * self.n_fit)
 
 
+def skip_map(params, X, n_fit=4):
+    """The skip connection's output s + s Ws + bs + q(s) Wq (float64, first
+    n_fit columns) for inputs X."""
+    torch = _torch()
+    W = torch.cat([block(params, "Ws")[:5, :n_fit], block(params, "bs")[None, :n_fit],
+                   block(params, "Wq")[:15, :n_fit]], 0).double()
+    return X[:, :n_fit].double() + skip_features(X) @ W
+
+
+def residual_scale(params, X, T, n_fit=4, chunk=1 << 21):
+    """Power of two nearest the rms of what the skip connection misses."""
+    acc, cnt = 0.0, 0
+    for a in range(0, X.shape[0], chunk):
+        r = T[a:a + chunk, :n_fit].double() - skip_map(params, X[a:a + chunk], n_fit)
+        acc += float((r * r).sum())
+        cnt += r.numel()
+    rms = math.sqrt(acc / max(cnt, 1))
+    return 2.0 ** round(math.log2(rms)) if rms > 0 else 1.0
+
+
 def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200, seed=0, n_fit=4,
-          log_every=0, time_limit=None, eps=1e-8):
+          log_every=0, time_limit=None, eps=1e-8, out_scale="auto", chunk=1 << 21):
     """Second-order skip connection by least squares, then Adam on the MLP
-    with a cosine learning rate.  Returns the history [(step, mse)] (sampled
-    when log_every > 0) and the trainer."""
+    with a cosine learning rate.
+
+    The network is trained on what the skip connection misses divided by
+    `out_scale` (by default the power of two nearest its rms), so that its
+    output is of order one and the optimiser's step noise on W4 and b4 is
+    not of the residual's own size; the scale is folded into W4 and b4 at the
+    end (exactly: a power of two).  Returns the history [(step, mse)] of the
+    scaled problem (sampled when log_every > 0) and the trainer."""
     torch = _torch()
     fit_skip(params, X, T, n_fit)
+    sigma = residual_scale(params, X, T, n_fit, chunk) if out_scale == "auto" else float(out_scale or 1.0)
+    if sigma != 1.0:
+        Tn = T.clone()
+        for a in range(0, X.shape[0], chunk):
+            sk = skip_map(params, X[a:a + chunk], n_fit)
+            Tn[a:a + chunk, :n_fit] = (sk + (T[a:a + chunk, :n_fit].double() - sk) / sigma).float()
+        T = Tn
     tr = Trainer(params, batch=batch, n_fit=n_fit, eps=eps)
+    tr.out_scale = sigma
     n = X.shape[0]
     nb = n // batch
     total = max(1, epochs * nb)
@@ -423,6 +457,7 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
     hist = []
     t0 = time.perf_counter()
     k = 0
+    done = False
     for ep in range(epochs):
         perm = torch.randperm(n, device=X.device, generator=g)
         Xs, Ts = X[perm].contiguous(), T[perm].contiguous()
@@ -436,7 +471,13 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
             if log_every and k % log_every == 0:
                 hist.append((k, tr.mse()))
             if time_limit is not None and k % 64 == 0 and time.perf_counter() - t0 > time_limit:
-                return hist, tr
+                done = True
+                break
+        if done:
+            break
+    if sigma != 1.0:
+        block(params, "W4").mul_(sigma)
+        block(params, "b4").mul_(sigma)
     return hist, tr
 
 
