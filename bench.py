@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--no-fp32c", action="store_true")
     ap.add_argument("--no-mapgen", action="store_true")
     ap.add_argument("--no-scan", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned-samples", type=int, default=20_000_000)
+    ap.add_argument("--learned-epochs", type=int, default=8)
+    ap.add_argument("--learned-n", type=int, default=10_000_000)
     return ap.parse_args()
 
 
@@ -328,6 +332,132 @@ def seo_scan_bench(dev, n_energies=256):
             "cpu_port_sample": f"{len(sample)} of the energies with the oracle tracker, scaled"}
 
 
+# algorithmic flops of one map application: 5 inputs (the sixth is zero),
+# two 256 x 256 hidden layers, 4 fitted outputs
+LEARNED_FLOP_PER_MAP = 2 * (5 * 256 + 2 * 256 * 256 + 256 * 4)
+# executed on the tensor cores (K = 16 layer-1 tile, N = 16 layer-4 tile)
+LEARNED_MMA_FLOP_PER_MAP = 2 * (16 * 256 + 2 * 256 * 256 + 256 * 16)
+
+
+def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=10_000_000, turns_per_step=50,
+                  steps=2, check_n=512, check_turns=1000):
+    """Learned sector map: train on `samples` one-sector crossings of the
+    plain azimuth-domain tracker (300-600 MeV, amplitudes up to 10 mm / 5
+    mrad, uniform in normalised phase space), then track an n-particle bunch
+    with audits every 50 turns on 1% of the states (one step = 50 turns), and
+    compare a check bunch over 1000 turns with the FP64 plain tracker."""
+    import torch
+    from pyffa_b200 import learned, synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools, FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical
+    cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
+    bm = FFAG_Bfield_analytical(config=cfg, max_order=0, AddNumricalMap=False)
+    bm.UpdataConfig()
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(bm)
+    tracker = learned.SectorTracker(gp.Bmap, gp.q, steps_per_sector=128, device=dev)
+    d0 = synthetic.design(300.0)
+    conv = FFAG_ConversionTools()
+    nodes = np.cos(np.pi * (np.arange(17) + 0.5) / 17)[::-1]
+    P = conv.Ek2P(450.0 + 150.0 * nodes)
+    r_guess = d0["r0"] * (P / conv.Ek2P(300.0)) ** (1 / (cfg["Bmap"]["coefficients_tupel"][1] + 1))
+    frame = learned.SectorFrame.build(tracker, (300.0, 600.0), (10e-3, 5e-3), r_guess=r_guess, pr_guess=d0["pr0"])
+    t0 = time.perf_counter()
+    X, T = learned.make_dataset(frame, tracker, samples, seed=1)
+    Xv, Tv = learned.make_dataset(frame, tracker, 1 << 16, seed=2)
+    torch.cuda.synchronize(dev)
+    t_data = time.perf_counter() - t0
+    p = torch.from_numpy(learned.init_params(3)).to(dev)
+    t0 = time.perf_counter()
+    _, tr = learned.train(p, X, T, epochs=epochs, batch=8192, lr=2e-3, time_limit=90.0)
+    torch.cuda.synchronize(dev)
+    t_train = time.perf_counter() - t0
+    mse = learned.evaluate(p, Xv, Tv)
+    del X, T
+    torch.cuda.empty_cache()
+
+    # the n-particle bunch: Gaussian (sigma 0.3) inside radius 0.9, energies across the range
+    def bunch(m, seed):
+        rng = np.random.default_rng(seed)
+        s = np.zeros((m, 5))
+        s[:, :4] = 0.3 * rng.standard_normal((m, 4))
+        for j in (0, 2):
+            r = np.hypot(s[:, j], s[:, j + 1])
+            s[:, j:j + 2] *= np.minimum(1.0, 0.9 / np.maximum(r, 1e-12))[:, None]
+        s[:, 4] = rng.uniform(-0.9, 0.9, m)
+        st = torch.from_numpy(s).to(dev)
+        Pm = torch.as_tensor(frame.P_of_Ek(frame.Ek_of(s[:, 4])), device=dev)
+        return torch.cat([frame.to_phys(st, st[:, 4]), Pm[:, None]], 1)
+
+    lm = learned.LearnedSectorMap(frame, tracker, p, audit_every=50, audit_frac=0.01, audit_tol=1e-5)
+    phys = bunch(n, 5)
+    lm.track(phys, turns_per_step)                      # warm-up
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = lm.launches
+    audits = []
+    for k in range(steps):
+        ev[k][0].record()
+        res = lm.track(phys, turns_per_step)
+        ev[k][1].record()
+        audits += res["audits"]
+    torch.cuda.synchronize(dev)
+    mlp_launches = (lm.launches - launches0) // max(steps, 1)
+    ms = [a.elapsed_time(b) for a, b in ev]
+    value = n * turns_per_step * steps / (sum(ms) * 1e-3)
+    # the inference kernel alone: 50 turns of maps in one launch, states resident
+    st = torch.zeros((n, 8), dtype=torch.float32, device=dev)
+    st[:, :5] = frame.to_norm(phys).float()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lm.apply(st, 12)
+    e0.record()
+    lm.apply(st, turns_per_step * 12)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    k_s = e0.elapsed_time(e1) * 1e-3
+    maps = n * turns_per_step * 12
+    peaks = {}
+    try:
+        mp = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
+        peaks = {"burst": mp["bf16_tflops"], "sustained": mp["bf16_tflops_sustained"]}
+    except Exception:
+        peaks = {"burst": 1590.0, "sustained": 1400.0, "source": "fallback"}
+    ach = LEARNED_FLOP_PER_MAP * maps / k_s / 1e12
+    # accuracy: a check bunch over 1000 turns against the FP64 plain tracker
+    cb = bunch(check_n, 4)
+    ref = learned.plain_track(frame, tracker, cb, check_turns, record=True)
+    got = learned.LearnedSectorMap(frame, tracker, p, audit_every=50, audit_frac=0.01,
+                                   audit_tol=1e-5).track(cb, check_turns, record=True)
+    dq = np.abs(learned.tunes(got["record"]) - learned.tunes(ref["record"]))
+    de = np.abs(learned.betatron_emittance(frame, got["record"][-1]) /
+                learned.betatron_emittance(frame, ref["record"][-1]) - 1)
+    return {
+        "value": value, "unit": "particle-turns/s",
+        "speedup_vs_fp64": value / fp64_value if fp64_value else None,
+        "speedup_vs_fp32c": value / fp32c_value if fp32c_value else None,
+        "ms_per_step": statistics.mean(ms), "turns_per_step": turns_per_step, "particles": n,
+        "audit": {"every_turns": 50, "fraction": 0.01, "tol": 1e-5,
+                  "sampled": int(sum(a[1] for a in audits)), "failed": int(sum(a[2] for a in audits)),
+                  "max_error": max((a[3] for a in audits), default=None)},
+        "plain_fallback_states": int(res["plain"].sum()),
+        "kernel": {"maps_per_launch": turns_per_step * 12, "s": k_s, "particle_turns_per_s": n * turns_per_step / k_s,
+                   "roofline": {"bound": "tensor", "achieved": ach, "unit": "TFLOP/s",
+                                "peak": peaks["sustained"], "frac": ach / peaks["sustained"],
+                                "peak_burst": peaks["burst"], "frac_of_burst": ach / peaks["burst"],
+                                "flop_per_map": LEARNED_FLOP_PER_MAP,
+                                "mma_flop_per_map": LEARNED_MMA_FLOP_PER_MAP,
+                                "peak_source": "MEASURED_PEAKS.json bf16 cuBLAS (sustained: seconds-long launch)"}},
+        "accuracy": {"check_bunch": check_n, "turns": check_turns, "tune_error_max": float(dq.max()),
+                     "tune_error_rms": float(np.sqrt(np.mean(dq ** 2))),
+                     "emittance_error_max": float(de.max()), "vs": "FP64 azimuth-domain RK4 tracker, 128 steps/sector"},
+        "training": {"samples": samples, "epochs": epochs, "batch": 8192, "s": t_train, "data_s": t_data,
+                     "steps": tr.t, "samples_per_s": tr.t * 8192 / t_train, "validation_mse": mse,
+                     "residual_scale": tr.out_scale},
+        "mlp_launches_per_step": mlp_launches,
+        "dtype": "bf16 tensor-core hidden layers, f32 accumulation, f32 skip and state",
+    }
+
+
 def run_reference(args):
     """--impl reference: the oracle port on the host cores, each step one turn
     of a bounded sample."""
@@ -514,6 +644,10 @@ def main():
         scan = None
         if not args.no_scan:
             scan = seo_scan_bench(dev)
+        lrn = None
+        if not args.no_learned:
+            lrn = learned_bench(dev, value / world, fp32c["value"] / world if fp32c else None,
+                                samples=args.learned_samples, epochs=args.learned_epochs, n=args.learned_n)
         line = {
             "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
             "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
@@ -534,6 +668,7 @@ def main():
             "fp32c": fp32c,
             "mapgen": mg,
             "co_scan": scan,
+            "learned_map": lrn,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)
