@@ -416,12 +416,13 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
     torch.cuda.synchronize(dev)
     k_s = e0.elapsed_time(e1) * 1e-3
     maps = n * turns_per_step * 12
-    peaks = {}
     try:
         mp = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
-        peaks = {"burst": mp["bf16_tflops"], "sustained": mp["bf16_tflops_sustained"]}
+        peaks = {"burst": mp["bf16_tflops"], "sustained": mp["bf16_tflops_sustained"],
+                 "source": "MEASURED_PEAKS.json bf16 cuBLAS (of measured; sustained: seconds-long launch)"}
     except Exception:
-        peaks = {"burst": 1590.0, "sustained": 1400.0, "source": "fallback"}
+        peaks = {"burst": 1590.0, "sustained": 1400.0,
+                 "source": "fallback (MEASURED_PEAKS.json absent): 1.59 PF/s burst, 1.4 sustained"}
     ach = LEARNED_FLOP_PER_MAP * maps / k_s / 1e12
     # accuracy: a check bunch over 1000 turns against the FP64 plain tracker
     cb = bunch(check_n, 4)
@@ -446,7 +447,7 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
                                 "peak_burst": peaks["burst"], "frac_of_burst": ach / peaks["burst"],
                                 "flop_per_map": LEARNED_FLOP_PER_MAP,
                                 "mma_flop_per_map": LEARNED_MMA_FLOP_PER_MAP,
-                                "peak_source": "MEASURED_PEAKS.json bf16 cuBLAS (sustained: seconds-long launch)"}},
+                                "peak_source": peaks["source"]}},
         "accuracy": {"check_bunch": check_n, "turns": check_turns, "tune_error_max": float(dq.max()),
                      "tune_error_rms": float(np.sqrt(np.mean(dq ** 2))),
                      "emittance_error_max": float(de.max()), "vs": "FP64 azimuth-domain RK4 tracker, 128 steps/sector"},
