@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-mapgen", action="store_true")
     ap.add_argument("--no-scan", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-coscan", action="store_true")
     ap.add_argument("--learned-samples", type=int, default=20_000_000)
     ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--learned-n", type=int, default=10_000_000)
@@ -330,6 +331,45 @@ def seo_scan_bench(dev, n_energies=256):
             "Qz_range": [float(res["table"][:, 3].min()), float(res["table"][:, 3].max())],
             "cpu_port_s_est": cpu_s, "cpu_port_threads": O.num_threads(),
             "cpu_port_sample": f"{len(sample)} of the energies with the oracle tracker, scaled"}
+
+
+def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0):
+    """Batched closed-orbit / tune scan (c3): 256 instances at energies
+    300-600 MeV (linspace), ceil(exp(U(0, ln 4096))) particles each with
+    0.5 mm Gaussian offsets, all in one bunch through the FP32C Boris pusher
+    (RF off), 200 turns of the slowest instance per iteration, float64
+    one-turn-map fit and fixed-point update per instance."""
+    import torch
+    from pyffa_b200 import coscan, synthetic
+    from pyffa_b200.constants import FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_EField_new
+    gp2 = FFAG_GlobalParameters()
+    gp2.AddBMap(gp.Bmap)
+    gp2.AddEMap(FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=False))
+    E = np.linspace(300.0, 600.0, n_instances)
+    counts = coscan.instance_counts(n_instances, 4096, seed)
+    d = synthetic.design(300.0)
+    k = float(gp.Bmap.k_value)
+    scale = (synthetic.momentum(E) / synthetic.momentum(300.0)) ** (1 / (k + 1))
+    r_sc = d["r0"] * scale
+    scan = coscan.BatchedOrbitScan(gp2, E, counts, r_sc + 1e-4, np.full(n_instances, np.arctan(d["pr0"])),
+                                   d["perimeter"] * scale, sigma=0.5e-3, turns=turns, seed=seed, device=dev)
+    recs = [scan.iterate() for _ in range(iterations)]
+    torch.cuda.synchronize(dev)
+    pt = sum(r["particle_turns"] for r in recs)
+    ms = sum(r["ms"] for r in recs)
+    q = recs[-1]["tunes"]
+    return {"value": pt / (ms * 1e-3), "unit": "particle-turns/s (sum over instances)",
+            "instances": n_instances, "particles": scan.N, "turns_per_iteration": turns,
+            "steps_per_iteration": scan.steps, "iterations": iterations,
+            "ms_per_iteration": [r["ms"] for r in recs], "launches_per_iteration": recs[-1]["launches"],
+            "max_abs_dr_m": [r["max_abs_dr"] for r in recs],
+            "orbit_vs_scaling_law_m": float(np.abs(scan.r - r_sc).max()),
+            "Qr_frac_range": [float(np.nanmin(q[:, 0])), float(np.nanmax(q[:, 0]))],
+            "Qz_frac_range": [float(np.nanmin(q[:, 1])), float(np.nanmax(q[:, 1]))],
+            "padding_waste": scan.padding(), "valid_instances": int(recs[-1]["good"].sum()),
+            "dtype": "f32c push, f64 fit and update",
+            "not_built": "CUDA-graph capture of the iteration and a tile autotuner"}
 
 
 # algorithmic flops of one map application: 5 inputs (the sixth is zero),
@@ -645,6 +685,9 @@ def main():
         scan = None
         if not args.no_scan:
             scan = seo_scan_bench(dev)
+        csp = None
+        if not args.no_coscan:
+            csp = coscan_bench(gp, dev)
         lrn = None
         if not args.no_learned:
             lrn = learned_bench(dev, value / world, fp32c["value"] / world if fp32c else None,
@@ -670,6 +713,7 @@ def main():
             "mapgen": mg,
             "co_scan": scan,
             "learned_map": lrn,
+            "co_scan_particles": csp,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)

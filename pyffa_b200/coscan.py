@@ -1,0 +1,216 @@
+"""Batched closed-orbit and tune scan with the compensated float32 pusher.
+
+Many independent instances (one energy each, a few to thousands of
+particles with small offsets around a guessed orbit) run as ONE bunch
+through the FP32C Boris pusher: every launch advances all instances, so the
+load of small and large instances is balanced particle by particle.  Per
+iteration the bunch is pushed for `turns` turns of the slowest instance, the
+azimuth-0 crossings of every particle (ffa_push_crossing, interpolated to
+the azimuth) are paired turn to turn on the device, and for every instance
+and transverse plane the least-squares one-turn map x' = M x + b over all of
+its particles and turns is formed in float64.  Its fixed point
+(I - M)^-1 b is the Newton update of the closed orbit; the phase advance of
+M (trace, with the sign of M12 fixing the half plane) is the fractional tune.
+The next iteration restarts the instances around the updated orbits.
+
+The reference's counterpart is the per-energy closed-orbit search in the
+azimuth domain (FFAG_SearchSEO, src/FFAG_track.py:1142-1586: fixed-point
+averaging and a finite-difference Newton step on the one-sector map, tunes
+from the transfer-matrix trace, GetQrQz src/FFAG_track.py:1257-1309); this
+scan does the same with time-domain tracking of particle ensembles, which is
+what a tracking code sees, for all energies in one launch sequence.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .constants import FFAG_ConversionTools
+
+
+def accumulate_crossings(rec, gv, inst, nsteps, last, has, S, Y, crossings):
+    """Adds one launch's crossing records (k, 23) to the per-instance sums.
+
+    The state at the target azimuth is interpolated from the pre- and
+    post-step states with the record's ratio, taken relative to the guessed
+    orbit gv[instance] (v-format r, vr, z, vz), and paired with the same
+    particle's previous crossing (this launch, or `last` from earlier ones).
+    S[plane, i] += f f^T and Y[plane, i] += x' f^T with f = (x, x_dot, 1) of
+    the earlier crossing and x' the later one; crossings[i] counts records."""
+    import torch
+    k = rec.shape[0]
+    p = rec[:, 1].long()
+    x = rec[:, 4:8] + rec[:, 3:4] * (rec[:, 11:15] - rec[:, 4:8])
+    x = x - gv[inst[p]]
+    order = torch.argsort(p * (nsteps + 2) + rec[:, 2].long())
+    p, x = p[order], x[order]
+    same = torch.zeros(k, dtype=torch.bool, device=rec.device)
+    same[1:] = p[1:] == p[:-1]
+    prev = torch.empty_like(x)
+    prev[1:] = x[:-1]
+    first = ~same
+    prev[first] = last[p[first]]
+    ok = same | (first & has[p])
+    xp, xn, ip = prev[ok], x[ok], inst[p[ok]]
+    for pl in (0, 1):
+        f = torch.cat([xp[:, 2 * pl:2 * pl + 2], torch.ones_like(xp[:, :1])], 1)
+        S[pl].index_add_(0, ip, f[:, :, None] * f[:, None, :])
+        Y[pl].index_add_(0, ip, xn[:, 2 * pl:2 * pl + 2, None] * f[:, None, :])
+    crossings.index_add_(0, inst[p], torch.ones(k, dtype=crossings.dtype, device=rec.device))
+    lastocc = torch.ones(k, dtype=torch.bool, device=rec.device)
+    lastocc[:-1] = p[1:] != p[:-1]
+    last[p[lastocc]] = x[lastocc]
+    has[p[lastocc]] = True
+
+
+def fit_one_turn(S, Y, cond_max=1e14):
+    """float64 least-squares one-turn map per instance and plane from the sums
+    of accumulate_crossings: returns the fixed point offsets (I, 4), the
+    fractional tunes (I, 2) and a validity mask (I,)."""
+    I = S.shape[1]
+    tunes = np.full((I, 2), np.nan)
+    fix = np.zeros((I, 4))
+    good = np.ones(I, dtype=bool)
+    for i in range(I):
+        for pl in (0, 1):
+            A, B = S[pl, i], Y[pl, i]
+            if not np.all(np.isfinite(A)) or np.linalg.cond(A) > cond_max:
+                good[i] = False
+                continue
+            W = np.linalg.solve(A.T, B.T).T                       # B A^-1
+            M, bb = W[:, :2], W[:, 2]
+            fix[i, 2 * pl:2 * pl + 2] = np.linalg.solve(np.eye(2) - M, bb)
+            c = np.clip(0.5 * np.trace(M), -1.0, 1.0)
+            mu = math.acos(c) if M[0, 1] > 0 else 2 * math.pi - math.acos(c)
+            tunes[i, pl] = mu / (2 * math.pi)
+    return fix, tunes, good
+
+
+def instance_counts(n_instances=256, max_count=4096, seed=0):
+    """ceil(exp(U(0, ln max_count))) particles per instance (seeded)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.ceil(np.exp(rng.uniform(0.0, math.log(max_count), n_instances))).astype(np.int64)
+
+
+class BatchedOrbitScan:
+    """All instances of a scan in one device bunch.
+
+    gp: FFAG_GlobalParameters with the field map and an Emap (RF off);
+    energies (I,) MeV; counts (I,) particles per instance; guesses r0 (I,)
+    [m] and pr0 (I,) (p-format angle) of the closed orbit at azimuth 0 and
+    its length `perimeter` (I,) [m]; sigma: Gaussian offset in r and z [m].
+    The time step is the fastest instance's revolution time / steps_per_turn;
+    an iteration lasts `turns` turns of the slowest instance."""
+
+    def __init__(self, gp, energies, counts, r0, pr0, perimeter, sigma=0.5e-3, steps_per_turn=720, turns=200,
+                 seed=0, device=None):
+        import torch
+        self.gp = gp
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.E = np.asarray(energies, np.float64)
+        self.counts = np.asarray(counts, np.int64)
+        self.I = len(self.E)
+        self.r = np.asarray(r0, np.float64).copy()
+        self.pr = np.asarray(pr0, np.float64).copy()
+        self.z = np.zeros(self.I)
+        self.pz = np.zeros(self.I)
+        self.conv = FFAG_ConversionTools()
+        v = self.conv.Ek2v(self.E)
+        self.T = np.asarray(perimeter, np.float64) / v
+        self.dt = float(self.T.min() / steps_per_turn)
+        self.turns = int(turns)
+        self.steps = int(math.ceil(self.turns * self.T.max() / self.dt))
+        self.inst = np.repeat(np.arange(self.I), self.counts)
+        self.N = int(self.counts.sum())
+        rng = np.random.Generator(np.random.PCG64(seed))
+        self.g = sigma * rng.standard_normal((self.N, 2))    # r and z offsets, fixed over the iterations
+        self.history = []
+
+    # ------------------------------------------------------------ bunch
+    def _vformat(self):
+        a = np.zeros((self.N, 16))
+        i = self.inst
+        a[:, 0] = self.r[i] + self.g[:, 0]
+        a[:, 1] = self.pr[i]
+        a[:, 2] = self.z[i] + self.g[:, 1]
+        a[:, 3] = self.pz[i]
+        a[:, 5] = self.E[i]
+        a[:, 15] = np.arange(self.N)
+        v = self.conv.ConvertPrzek2Vrzek_boris(a)
+        v[:, 7] = 1.0
+        v[:, 8] = 1.0
+        return v
+
+    def _guess_v(self):
+        """v-format (r, vr, z, vz) of the guessed orbits."""
+        a = np.zeros((self.I, 16))
+        a[:, 0], a[:, 1], a[:, 2], a[:, 3], a[:, 5] = self.r, self.pr, self.z, self.pz, self.E
+        v = self.conv.ConvertPrzek2Vrzek_boris(a)
+        return v[:, [0, 1, 2, 3]]
+
+    # ------------------------------------------------------------ one iteration
+    def iterate(self):
+        """One push of all instances and the float64 update; returns the
+        iteration record (orbit change, tunes, particle-turns, device time)."""
+        import torch
+        from .track import CrossingCapture, Pusher, StepClock, _EphemeralBunch
+        dev = self.dev
+        f64 = dict(dtype=torch.float64, device=dev)
+        b = _EphemeralBunch(self._vformat(), "Boris", dev)
+        pusher = Pusher(b, self.gp, "Boris", "fp32c")
+        clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
+        clock.ensure(self.steps + 1)
+        cap = CrossingCapture(b, [0.0], self.gp, self.dt)
+        L = cap.max_steps()
+        gv = torch.as_tensor(self._guess_v(), **f64)               # (I, 4)
+        inst = torch.as_tensor(self.inst, device=dev)
+        last = torch.zeros((self.N, 4), **f64)
+        has = torch.zeros(self.N, dtype=torch.bool, device=dev)
+        S = torch.zeros((2, self.I, 3, 3), **f64)                  # planes x, z: sum f f^T
+        Y = torch.zeros((2, self.I, 2, 3), **f64)                  # sum x' f^T
+        crossings = torch.zeros(self.I, **f64)
+        launches = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(pusher.stream)
+        for s0 in range(0, self.steps, L):
+            ns = min(L, self.steps - s0)
+            pusher.push(clock, s0, ns, 0, xing=cap.prepare(ns))
+            launches += 1
+            k = int(cap.count.item())
+            if k > cap.x.capacity:
+                raise RuntimeError(f"crossing records overflowed: {k} > {cap.x.capacity}")
+            if k == 0:
+                continue
+            accumulate_crossings(cap.buf[:k * 23].view(k, 23), gv, inst, self.steps, last, has, S, Y, crossings)
+        e1.record(pusher.stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        gvn = gv.cpu().numpy()
+        fix, tunes, good = fit_one_turn(S.cpu().numpy(), Y.cpu().numpy())
+        new = gvn + fix
+        dr = np.where(good, fix[:, 0], 0.0)
+        # back to p-format orbit parameters at azimuth 0 (vphi from the speed)
+        vtot = self.conv.Ek2v(self.E)
+        for i in np.nonzero(good)[0]:
+            vr, vz = new[i, 1], new[i, 3]
+            vf = math.sqrt(max(vtot[i] ** 2 - vr * vr - vz * vz, 0.0))
+            self.r[i], self.z[i] = new[i, 0], new[i, 2]
+            self.pr[i], self.pz[i] = math.atan2(vr, vf), math.atan2(vz, vf)
+        pt = float(crossings.sum().item())
+        rec_ = {"ms": ms, "launches": launches, "particle_turns": pt, "max_abs_dr": float(np.abs(dr).max()),
+                "dr": dr, "tunes": tunes, "good": good, "crossings": crossings.cpu().numpy()}
+        self.history.append(rec_)
+        return rec_
+
+    def run(self, iterations=3, tol=1e-6):
+        """Iterates until the largest orbit change is below `tol` [m]."""
+        for _ in range(iterations):
+            rec = self.iterate()
+            if rec["max_abs_dr"] < tol:
+                break
+        return self.history[-1]
+
+    def padding(self, block=32):
+        """Launch slots per particle: the push kernel's blocks over the whole bunch."""
+        return math.ceil(self.N / block) * block / self.N

@@ -1,0 +1,69 @@
+"""Batched orbit scan, host side (no GPU): crossing records of known
+one-turn maps, shuffled and split over two launches, are paired turn to turn
+and fitted back to their fixed points and tunes."""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from pyffa_b200 import coscan  # noqa: E402
+
+
+def _map(q, beta, alpha):
+    mu = 2 * math.pi * q
+    g = (1 + alpha * alpha) / beta
+    c, s = math.cos(mu), math.sin(mu)
+    return np.array([[c + alpha * s, beta * s], [-g * s, c - alpha * s]])
+
+
+def test_records_fit_back_to_fixed_points_and_tunes():
+    rng = np.random.default_rng(1)
+    counts = [1, 3, 17]
+    tunes = [(0.5951, 0.7813), (0.31, 0.12), (0.87, 0.44)]
+    fixed = rng.normal(0, 1e-3, (3, 4))
+    guess = fixed + rng.normal(0, 1e-4, (3, 4))
+    inst = np.repeat(np.arange(3), counts)
+    N, T = len(inst), 40
+    rec, ratio = [], 0.3
+    state = fixed[inst] + rng.normal(0, 5e-4, (N, 4))
+    Ms = [[_map(qx, 2.0, 0.4), _map(qz, 11.0, -1.3)] for qx, qz in tunes]
+    for t in range(T):
+        for pidx in range(N):
+            x = state[pidx]
+            d = rng.normal(0, 1e-4, 4)
+            row = np.zeros(23)
+            row[1], row[2], row[3] = pidx, 100 * t + pidx % 7, ratio
+            row[4:8] = x - ratio * d
+            row[11:15] = x + (1 - ratio) * d
+            rec.append(row)
+        for pidx in range(N):
+            i = inst[pidx]
+            for pl in (0, 1):
+                sl = slice(2 * pl, 2 * pl + 2)
+                state[pidx, sl] = Ms[i][pl] @ (state[pidx, sl] - fixed[i, sl]) + fixed[i, sl]
+    rec = np.array(rec)
+    f64 = dict(dtype=torch.float64)
+    S = torch.zeros((2, 3, 3, 3), **f64)
+    Y = torch.zeros((2, 3, 2, 3), **f64)
+    cr = torch.zeros(3, **f64)
+    last = torch.zeros((N, 4), **f64)
+    has = torch.zeros(N, dtype=torch.bool)
+    gv = torch.as_tensor(guess)
+    it = torch.as_tensor(inst)
+    # two launches (turns 0..17 and 18..39), each in shuffled order
+    for part in (rec[rec[:, 2] < 1800], rec[rec[:, 2] >= 1800]):
+        part = part[rng.permutation(len(part))]
+        coscan.accumulate_crossings(torch.as_tensor(part), gv, it, 100 * T, last, has, S, Y, cr)
+    fix, q, good = coscan.fit_one_turn(S.numpy(), Y.numpy())
+    assert good.all()
+    assert np.allclose(guess + fix, fixed, atol=1e-12, rtol=0)
+    assert np.allclose(q, np.array(tunes), atol=1e-10)
+    assert cr.numpy().tolist() == [c * T for c in counts]
+
+
+def test_instance_counts_log_uniform():
+    c = coscan.instance_counts(256, 4096, seed=0)
+    assert c.min() >= 1 and c.max() <= 4096 and len(c) == 256
+    assert 300 < c.mean() < 700
