@@ -29,12 +29,14 @@ import numpy as np
 from .constants import FFAG_ConversionTools
 
 
-def accumulate_crossings(rec, gv, inst, nsteps, last, has, S, Y, crossings):
+def accumulate_crossings(rec, gv, inst, nsteps, last, has, S, Y, crossings, scale=None):
     """Adds one launch's crossing records (k, 23) to the per-instance sums.
 
     The state at the target azimuth is interpolated from the pre- and
     post-step states with the record's ratio, taken relative to the guessed
-    orbit gv[instance] (v-format r, vr, z, vz), and paired with the same
+    orbit gv[instance] (v-format r, vr, z, vz) and multiplied by
+    scale[instance] (4 factors that make the coordinates of order one and the
+    normal equations well conditioned; None: 1), and paired with the same
     particle's previous crossing (this launch, or `last` from earlier ones).
     S[plane, i] += f f^T and Y[plane, i] += x' f^T with f = (x, x_dot, 1) of
     the earlier crossing and x' the later one; crossings[i] counts records."""
@@ -43,6 +45,8 @@ def accumulate_crossings(rec, gv, inst, nsteps, last, has, S, Y, crossings):
     p = rec[:, 1].long()
     x = rec[:, 4:8] + rec[:, 3:4] * (rec[:, 11:15] - rec[:, 4:8])
     x = x - gv[inst[p]]
+    if scale is not None:
+        x = x * scale[inst[p]]
     order = torch.argsort(p * (nsteps + 2) + rec[:, 2].long())
     p, x = p[order], x[order]
     same = torch.zeros(k, dtype=torch.bool, device=rec.device)
@@ -164,6 +168,11 @@ class BatchedOrbitScan:
         cap = CrossingCapture(b, [0.0], self.gp, self.dt)
         L = cap.max_steps()
         gv = torch.as_tensor(self._guess_v(), **f64)               # (I, 4)
+        # fit coordinates: offsets in mm and in mrad of the speed
+        unit = np.empty((self.I, 4))
+        unit[:, 0] = unit[:, 2] = 1e-3
+        unit[:, 1] = unit[:, 3] = 1e-3 * self.conv.Ek2v(self.E)
+        sc = torch.as_tensor(1.0 / unit, **f64)
         inst = torch.as_tensor(self.inst, device=dev)
         last = torch.zeros((self.N, 4), **f64)
         has = torch.zeros(self.N, dtype=torch.bool, device=dev)
@@ -182,12 +191,13 @@ class BatchedOrbitScan:
                 raise RuntimeError(f"crossing records overflowed: {k} > {cap.x.capacity}")
             if k == 0:
                 continue
-            accumulate_crossings(cap.buf[:k * 23].view(k, 23), gv, inst, self.steps, last, has, S, Y, crossings)
+            accumulate_crossings(cap.buf[:k * 23].view(k, 23), gv, inst, self.steps, last, has, S, Y, crossings, sc)
         e1.record(pusher.stream)
         torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
         gvn = gv.cpu().numpy()
         fix, tunes, good = fit_one_turn(S.cpu().numpy(), Y.cpu().numpy())
+        fix = fix * unit
         new = gvn + fix
         dr = np.where(good, fix[:, 0], 0.0)
         # back to p-format orbit parameters at azimuth 0 (vphi from the speed)

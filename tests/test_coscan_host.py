@@ -22,17 +22,20 @@ def test_records_fit_back_to_fixed_points_and_tunes():
     rng = np.random.default_rng(1)
     counts = [1, 3, 17]
     tunes = [(0.5951, 0.7813), (0.31, 0.12), (0.87, 0.44)]
-    fixed = rng.normal(0, 1e-3, (3, 4))
-    guess = fixed + rng.normal(0, 1e-4, (3, 4))
+    # physical scales: positions ~ 8.5 m and mm offsets, velocities ~ 1e8 m/s
+    # and 1e4 m/s offsets (the fit has to rescale them to stay conditioned)
+    unit = np.array([1e-3, 2e5, 1e-3, 2e5])
+    fixed = np.array([8.5, 2e7, 0.0, 0.0]) + rng.normal(0, 1, (3, 4)) * unit
+    guess = fixed + rng.normal(0, 0.1, (3, 4)) * unit
     inst = np.repeat(np.arange(3), counts)
     N, T = len(inst), 40
     rec, ratio = [], 0.3
-    state = fixed[inst] + rng.normal(0, 5e-4, (N, 4))
-    Ms = [[_map(qx, 2.0, 0.4), _map(qz, 11.0, -1.3)] for qx, qz in tunes]
+    state = fixed[inst] + rng.normal(0, 0.5, (N, 4)) * unit
+    Ms = [[_map(qx, 2e-8, 0.4), _map(qz, 11e-8, -1.3)] for qx, qz in tunes]
     for t in range(T):
         for pidx in range(N):
             x = state[pidx]
-            d = rng.normal(0, 1e-4, 4)
+            d = rng.normal(0, 0.1, 4) * unit
             row = np.zeros(23)
             row[1], row[2], row[3] = pidx, 100 * t + pidx % 7, ratio
             row[4:8] = x - ratio * d
@@ -55,10 +58,12 @@ def test_records_fit_back_to_fixed_points_and_tunes():
     # two launches (turns 0..17 and 18..39), each in shuffled order
     for part in (rec[rec[:, 2] < 1800], rec[rec[:, 2] >= 1800]):
         part = part[rng.permutation(len(part))]
-        coscan.accumulate_crossings(torch.as_tensor(part), gv, it, 100 * T, last, has, S, Y, cr)
+        coscan.accumulate_crossings(torch.as_tensor(part), gv, it, 100 * T, last, has, S, Y, cr,
+                                    torch.as_tensor(np.tile(1.0 / unit, (3, 1))))
     fix, q, good = coscan.fit_one_turn(S.numpy(), Y.numpy())
     assert good.all()
-    assert np.allclose(guess + fix, fixed, atol=1e-12, rtol=0)
+    assert np.allclose(guess + fix * unit, fixed, atol=0, rtol=1e-12)
+    assert np.all(np.abs(guess + fix * unit - fixed) <= 1e-9 * unit)
     assert np.allclose(q, np.array(tunes), atol=1e-10)
     assert cr.numpy().tolist() == [c * T for c in counts]
 
