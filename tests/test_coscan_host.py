@@ -57,8 +57,9 @@ def test_records_fit_back_to_fixed_points_and_tunes():
     it = torch.as_tensor(inst)
     # two launches (turns 0..17 and 18..39), each in shuffled order
     for part in (rec[rec[:, 2] < 1800], rec[rec[:, 2] >= 1800]):
-        part = part[rng.permutation(len(part))]
-        coscan.accumulate_crossings(torch.as_tensor(part), gv, it, 100 * T, last, has, S, Y, cr,
+        part = torch.as_tensor(part[rng.permutation(len(part))])
+        x = part[:, 4:8] + part[:, 3:4] * (part[:, 11:15] - part[:, 4:8])
+        coscan.accumulate_crossings(part[:, 1].long(), part[:, 2].long(), x, gv, it, 100 * T, last, has, S, Y, cr,
                                     torch.as_tensor(np.tile(1.0 / unit, (3, 1))))
     fix, q, good = coscan.fit_one_turn(S.numpy(), Y.numpy())
     assert good.all()
@@ -72,3 +73,41 @@ def test_instance_counts_log_uniform():
     c = coscan.instance_counts(256, 4096, seed=0)
     assert c.min() >= 1 and c.max() <= 4096 and len(c) == 256
     assert 300 < c.mean() < 700
+
+
+def _record(pre, post):
+    row = np.zeros(23)
+    row[4:10], row[11:17] = pre, post
+    return row
+
+
+def test_crossing_states_exact_on_straight_lines():
+    """A drift crossing azimuth 0 at any point of the step: r, vr, z, vz of
+    the crossing come out exact (a linear interpolation in the azimuth
+    misses r by up to r'' dphi^2 / 8)."""
+    dt = 3.7e-10
+    rng = np.random.default_rng(5)
+    rows, want = [], []
+    for frac in rng.uniform(0.01, 0.99, 50):
+        # straight line through (8.13 m, 0) at the crossing, 6.7 deg off the tangent
+        v, a = 1.9e8, 0.1171
+        vx, vy, vz = v * math.sin(a), v * math.cos(a), 2e5
+        X, Yc, Zc = 8.13 + rng.normal(0, 1e-3), 0.0, rng.normal(0, 1e-3)
+        def polar(t):
+            x, y, z = X + vx * t, Yc + vy * t, Zc + vz * t
+            r, fi = math.hypot(x, y), math.atan2(y, x)
+            vr = (x * vx + y * vy) / r
+            f5 = (x * vy - y * vx) / (r * r)
+            return [r, vr, z, vz, fi % (2 * math.pi), f5]
+        rows.append(_record(polar(-frac * dt), polar((1 - frac) * dt)))
+        want.append([X, vx, Zc, vz])
+    rec = torch.as_tensor(np.array(rows))
+    got = coscan.crossing_states(rec, dt).numpy()
+    want = np.array(want)
+    assert np.abs(got[:, 0] - want[:, 0]).max() < 1e-12
+    assert np.abs(got[:, 2] - want[:, 2]).max() < 1e-12
+    assert np.abs(got[:, 1] / want[:, 1] - 1).max() < 1e-10
+    # the azimuth-linear interpolation of r is off by tens of micrometres here
+    lin = rec[:, 4] + (rec[:, 11] - rec[:, 4]) * (-(rec[:, 8] - 2 * math.pi * (rec[:, 8] > 3)) /
+                                                  (rec[:, 15] - rec[:, 8] + 2 * math.pi * (rec[:, 8] > 3)))
+    assert np.abs(lin.numpy() - want[:, 0]).max() > 1e-5
