@@ -333,12 +333,14 @@ def seo_scan_bench(dev, n_energies=256):
             "cpu_port_sample": f"{len(sample)} of the energies with the oracle tracker, scaled"}
 
 
-def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0):
+def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, steps_per_turn=2880):
     """Batched closed-orbit / tune scan (c3): 256 instances at energies
     300-600 MeV (linspace), ceil(exp(U(0, ln 4096))) particles each with
     0.5 mm Gaussian offsets, all in one bunch through the FP32C Boris pusher
     (RF off), 200 turns of the slowest instance per iteration, float64
-    one-turn-map fit and fixed-point update per instance."""
+    one-turn-map fit and fixed-point update per instance.  2880 steps per
+    turn of the fastest instance: at 720 the 2.8-degree D magnet gets five
+    steps and the motion is not regular enough for a tune."""
     import torch
     from pyffa_b200 import coscan, synthetic
     from pyffa_b200.constants import FFAG_GlobalParameters
@@ -353,7 +355,8 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0):
     scale = (synthetic.momentum(E) / synthetic.momentum(300.0)) ** (1 / (k + 1))
     r_sc = d["r0"] * scale
     scan = coscan.BatchedOrbitScan(gp2, E, counts, r_sc + 1e-4, np.full(n_instances, np.arctan(d["pr0"])),
-                                   d["perimeter"] * scale, sigma=0.5e-3, turns=turns, seed=seed, device=dev)
+                                   d["perimeter"] * scale, sigma=0.5e-3, turns=turns, seed=seed, device=dev,
+                                   steps_per_turn=steps_per_turn)
     recs = [scan.iterate() for _ in range(iterations)]
     torch.cuda.synchronize(dev)
     pt = sum(r["particle_turns"] for r in recs)
@@ -361,7 +364,7 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0):
     q = recs[-1]["tunes"]
     return {"value": pt / (ms * 1e-3), "unit": "particle-turns/s (sum over instances)",
             "instances": n_instances, "particles": scan.N, "turns_per_iteration": turns,
-            "steps_per_iteration": scan.steps, "iterations": iterations,
+            "steps_per_iteration": scan.steps, "steps_per_turn_fastest": steps_per_turn, "iterations": iterations,
             "ms_per_iteration": [r["ms"] for r in recs], "launches_per_iteration": recs[-1]["launches"],
             "max_abs_dr_m": [r["max_abs_dr"] for r in recs],
             "orbit_vs_scaling_law_m": float(np.abs(scan.r - r_sc).max()),

@@ -38,14 +38,14 @@ def test_batched_scan_orbits_and_tunes():
     # start 0.2 mm off the orbit
     counts = [1, 4, 30, 120, 9]
     scan = coscan.BatchedOrbitScan(gp, E, counts, r_exp + 2e-4, pr_exp, d["perimeter"] * scale,
-                                   sigma=0.5e-3, turns=60, seed=3)
+                                   sigma=0.5e-3, turns=60, seed=3, steps_per_turn=2880)
     first = scan.iterate()
     second = scan.iterate()
     assert first["good"].all() and second["good"].all()
     # the first update takes the orbit most of the way, the second is small
     assert first["max_abs_dr"] > 1e-4 and second["max_abs_dr"] < 2e-5, (first["max_abs_dr"], second["max_abs_dr"])
-    # the time-domain orbit (Boris, 720-830 steps per turn) is the azimuth-domain one to discretisation error
-    assert np.abs(scan.r - r_exp).max() < 5e-4, scan.r - r_exp
+    # the time-domain orbit (Boris, 2880-3330 steps per turn) is the azimuth-domain one to discretisation error
+    assert np.abs(scan.r - r_exp).max() < 1e-4, scan.r - r_exp
     assert np.abs(scan.z).max() < 1e-6
     q = second["tunes"]
     assert np.abs(q[:, 0] - (d["Qx"] % 1)).max() < 2e-3, q
@@ -54,6 +54,6 @@ def test_batched_scan_orbits_and_tunes():
     assert (second["crossings"] >= 60 * np.array(counts)).all()
     # self-consistency: 10 um offsets around the orbit found come back to it
     check = coscan.BatchedOrbitScan(gp, E, [8] * 5, scan.r, scan.pr, d["perimeter"] * scale,
-                                    sigma=1e-5, turns=60, seed=4)
+                                    sigma=1e-5, turns=60, seed=4, steps_per_turn=2880)
     rec = check.iterate()
     assert rec["good"].all() and rec["max_abs_dr"] < 3e-6, rec["max_abs_dr"]
