@@ -363,6 +363,7 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     ms = sum(r["ms"] for r in recs)
     q = recs[-1]["tunes"]
     return {"value": pt / (ms * 1e-3), "unit": "particle-turns/s (sum over instances)",
+            "particle_steps_per_s": scan.N * scan.steps * iterations / (ms * 1e-3),
             "instances": n_instances, "particles": scan.N, "turns_per_iteration": turns,
             "steps_per_iteration": scan.steps, "steps_per_turn_fastest": steps_per_turn, "iterations": iterations,
             "ms_per_iteration": [r["ms"] for r in recs], "launches_per_iteration": recs[-1]["launches"],
