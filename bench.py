@@ -163,6 +163,27 @@ def fp64_peak_tflops(dev_index):
     return best
 
 
+def fp32_peak_tflops(dev_index):
+    """FP32 FMA pipe peak measured live with the probe kernel."""
+    import ctypes
+    import torch
+    from pyffa_b200 import build
+    L = ctypes.CDLL(build.build_probe())
+    L.ffa_probe_fp32_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_float)]
+    sms = torch.cuda.get_device_properties(dev_index).multi_processor_count
+    blocks, iters = sms * 8, 8192
+    out = torch.zeros(blocks, dtype=torch.float32, device="cuda")
+    ms = ctypes.c_float()
+    best = 0.0
+    for _ in range(3):
+        L.ffa_probe_fp32_fma(blocks, iters, ctypes.c_void_p(out.data_ptr()),
+                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), ctypes.byref(ms))
+        flops = 2.0 * 8 * iters * blocks * 256
+        best = max(best, flops / (ms.value * 1e-3) / 1e12)
+    return best
+
+
 def cpu_baseline(gp, v, dt, sample_n=100_000, steps=8 * STEPS_PER_TURN):
     """The reference algorithm on the host cores (oracle port, all threads):
     particle-turns/s on a bounded sample of the workload."""
@@ -656,6 +677,10 @@ def main():
 
     if rank == 0:
         peak64 = fp64_peak_tflops(local)
+        if fp32c is not None:
+            peak32 = fp32_peak_tflops(local)
+            fp32c["fma_peaks_tflops"] = {"fp64": peak64, "fp32": peak32, "fp32_over_fp64": peak32 / peak64,
+                                         "source": "measured live: FMA probe kernels (libffa_probe.so)"}
         avg_launch_s = (t_ms / args.steps) * 1e-3
         pstep = n * STEPS_PER_TURN
         roof = {"bound": "fp64", "unit": "TFLOP/s", "peak": peak64,
