@@ -334,14 +334,14 @@ __global__ void adam_kernel(float *P, const float *G, float *m, float *v, int64_
 // D0 = columns 0..255, D1 = columns 256..511, layers 1..4 alternate D0, D1.
 // Warp roles: warp 0 streams W2 / W3 from global (L2-resident) into a ring
 // of three 32 KB shared-memory slots with cp.async.bulk; warp 1 owns tensor
-// memory and issues the MMAs (one thread); warps 2..9 are the epilogue, two
-// threads per state (its tensor-memory lane), one per half of each 64-column
-// chunk.  They read the accumulator row, add the bias, apply SiLU, round to
-// bfloat16 and write the next layer's A operand one chunk at a time (the
-// next chunk's tensor-memory load in flight meanwhile), so the next layer's
-// MMAs on chunk c start while chunk c + 1 is still being written.  The
-// state, the domain check and the float32 skip layer stay in the registers
-// of the half-0 thread for all n_apply maps.
+// memory and issues the MMAs (one thread); warps 2..17 are the epilogue, four
+// threads per state (its tensor-memory lane), one per 16-column quarter of
+// each 64-column chunk.  They read the accumulator row, add the bias, apply
+// SiLU, round to bfloat16 and write the next layer's A operand one chunk at
+// a time (the next chunk's tensor-memory load in flight meanwhile), so the
+// next layer's MMAs on chunk c start while chunk c + 1 is still being
+// written.  The state, the domain check and the float32 skip connection stay
+// in the registers of the quarter-0 thread for all n_apply maps.
 //
 // Shared-memory operand layouts (K-major):
 //  - A (activations, 128 x 256) and W2 / W3 / W4 (B operand, N x 256): four
@@ -567,7 +567,9 @@ __device__ __forceinline__ uint4 silu8(const uint32_t *v, const float *hb)
     return o;
 }
 
-__global__ void __launch_bounds__(320, 1)
+constexpr int TC_THREADS = 32 * (2 + 16);
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
     mlp_infer_tc_kernel(const float *__restrict__ P, const unsigned char *__restrict__ wp, float *__restrict__ state,
                         int32_t *__restrict__ applied, int32_t *__restrict__ error, int64_t n, int n_apply,
                         float radius2)
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(320, 1)
         stail[i] = i < 8 ? P[P_B4 + i] : i < 72 ? P[P_WS + (i - 8)] : i < 80 ? P[P_BS + (i - 72)] : P[P_WQ + (i - 80)];
     if (threadIdx.x == 0) {
         mbar_init(BAR_X, 4);
-        for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * c, 8);
+        for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * c, 16);
         mbar_init(BAR_D, 1);
         for (int s = 0; s < RING; ++s) {
             mbar_init(BAR_FULL + 8 * s, 1);
@@ -693,13 +695,13 @@ __global__ void __launch_bounds__(320, 1)
         }
     } else {
         // ---------------------------------------------------- epilogue
-        // warps 2..9: tensor-memory lane quarter warp % 4, column half
-        // (warp - 2) / 4 of every 64-column chunk; the half-0 thread of a row
-        // owns that state
+        // warps 2..17: tensor-memory lane quarter warp % 4, column quarter
+        // (warp - 2) / 4 of every 64-column chunk; the quarter-0 thread of a
+        // row owns that state
         const int quarter = warp & 3;
-        const int half = (warp - 2) >> 2;
+        const int half = (warp - 2) >> 2;          // column quarter 0..3
         const int row = quarter * 32 + lane;
-        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + 32 * half;
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + 16 * half;
         uint32_t nd = 0;
         bool ok = true;
         for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -747,25 +749,25 @@ __global__ void __launch_bounds__(320, 1)
                     if (!ok) break;
                     tc_after_sync();
                     const uint32_t src = lane_base + ((l == 1) ? 256u : 0u);
-                    const float *hb = sbias + l * H + 32 * half;
+                    const float *hb = sbias + l * H + 16 * half;
                     unsigned char *arow = sm + SM_A + row * 128;
-                    uint32_t va[32], vb[32];
-                    TMEM_LD32(src, va);
+                    uint32_t va[16], vb[16];
+                    TMEM_LD16(src, va);
                     tmem_wait_ld();
-                    REG_FENCE32(va);
+                    REG_FENCE16(va);
                     // chunk c is converted while chunk c + 1 is in flight
 #define EPI_CHUNK(c, cur, nxt)                                                                           \
     {                                                                                                    \
-        if ((c) < 3) TMEM_LD32(src + ((c) + 1) * TC_CHUNK, nxt);                                         \
-        _Pragma("unroll") for (int j = 0; j < 4; ++j)                                                    \
+        if ((c) < 3) TMEM_LD16(src + ((c) + 1) * TC_CHUNK, nxt);                                         \
+        _Pragma("unroll") for (int j = 0; j < 2; ++j)                                                    \
         {                                                                                                \
             const uint4 o = silu8(cur + 8 * j, hb + (c) * TC_CHUNK + 8 * j);                            \
-            *reinterpret_cast<uint4 *>(arow + (c) * A_CHUNK_BYTES + (((4 * half + j) ^ (row & 7)) << 4)) = o; \
+            *reinterpret_cast<uint4 *>(arow + (c) * A_CHUNK_BYTES + (((2 * half + j) ^ (row & 7)) << 4)) = o; \
         }                                                                                                \
         fence_async_smem();                                                                              \
         if ((c) < 3) {                                                                                   \
             tmem_wait_ld();                                                                              \
-            REG_FENCE32(nxt);                                                                            \
+            REG_FENCE16(nxt);                                                                            \
         }                                                                                                \
         tc_before_sync();                                                                                \
         __syncwarp();                                                                                    \
@@ -941,7 +943,7 @@ extern "C" int ffa_mlp_infer(const ffa_mlp_infer_desc *d, void *stream)
     const int64_t tiles = (d->n + TC_M - 1) / TC_M;
     const int grid = (int)(tiles < sms ? tiles : sms);
     FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-    mlp_infer_tc_kernel<<<grid, 320, TC_SMEM, (cudaStream_t)stream>>>(
+    mlp_infer_tc_kernel<<<grid, TC_THREADS, TC_SMEM, (cudaStream_t)stream>>>(
         d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n, d->n_apply,
         d->radius2);
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
