@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-scan", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-coscan", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--learned-samples", type=int, default=20_000_000)
     ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--learned-n", type=int, default=10_000_000)
@@ -627,6 +628,30 @@ def main():
     status = b.status.cpu().numpy()
     value = n * world * args.steps / (t_ms * 1e-3)
 
+    # the same FP64 kernel on a 1e6-particle bunch (fills the GPU: the 1e5
+    # bunch gives 21 warps per SM), 10 one-turn launches
+    large = None
+    if not args.no_large and args.n == N_PARTICLES and args.precision == "fp64" and world == 1:
+        from pyffa_b200 import synthetic
+        from pyffa_b200.constants import FFAG_ConversionTools
+        vl = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(synthetic.centred_bunch(1_000_000, seed=17))
+        vl[:, 7] = 1.0
+        vl[:, 8] = 1.0
+        bl = _EphemeralBunch(vl, "Boris", dev)
+        pul = Pusher(bl, gp, "Boris", "fp64")
+        pul.push(clock, 0, STEPS_PER_TURN, 0)
+        torch.cuda.synchronize()
+        el = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(10)]
+        for k in range(10):
+            el[k][0].record(stream)
+            pul.push(clock, (k + 1) * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+            el[k][1].record(stream)
+        torch.cuda.synchronize()
+        lms = statistics.mean(a.elapsed_time(bb) for a, bb in el)
+        large = {"particles": 1_000_000, "value": 1_000_000 / (lms * 1e-3), "unit": "particle-turns/s",
+                 "ms_per_turn": lms, "fp64_tflops": FP64_FLOP_PER_PARTICLE_STEP * 1e6 * STEPS_PER_TURN / (lms * 1e-3) / 1e12}
+        del bl, pul
+
     # the compensated float32 pusher on the same workload
     fp32c = None
     if args.precision == "fp64" and not args.no_fp32c:
@@ -677,6 +702,8 @@ def main():
 
     if rank == 0:
         peak64 = fp64_peak_tflops(local)
+        if large is not None:
+            large["fp64_frac"] = large["fp64_tflops"] / peak64
         if fp32c is not None:
             peak32 = fp32_peak_tflops(local)
             fp32c["fma_peaks_tflops"] = {"fp64": peak64, "fp32": peak32, "fp32_over_fp64": peak32 / peak64,
@@ -743,6 +770,7 @@ def main():
             "co_scan": scan,
             "learned_map": lrn,
             "co_scan_particles": csp,
+            "fp64_1e6_particles": large,
             "launch_ms": {"mean": statistics.mean(launch_ms), "min": min(launch_ms), "max": max(launch_ms)},
         }
         print(json.dumps(line), flush=True)
