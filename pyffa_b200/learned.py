@@ -639,6 +639,26 @@ def plain_track(frame, tracker, phys, turns, record=False):
     return res
 
 
+# ------------------------------------------------------------- persistence
+def save(path, params, frame):
+    """Writes a trained network and its coordinate frame to one .npz file."""
+    p = params.detach().cpu().numpy() if hasattr(params, "detach") else np.asarray(params, np.float32)
+    np.savez(path, params=p.astype(np.float32), Ek_range=np.array(frame.Ek_range), cheb_r=frame.cr,
+             cheb_pr=frame.cpr, twiss_x=np.array(frame.twiss["x"]), twiss_z=np.array(frame.twiss["z"]),
+             amp=np.array(frame.amp), nsectors=np.array(frame.nsectors),
+             tunes=np.array(frame.tunes if frame.tunes is not None else [np.nan, np.nan]))
+
+
+def load(path):
+    """(params float32 numpy (N_PARAMS,), SectorFrame) from a file of save()."""
+    d = np.load(path)
+    if d["params"].shape != (N_PARAMS,):
+        raise ValueError(f"{path}: {d['params'].shape[0]} parameters, this library uses {N_PARAMS}")
+    frame = SectorFrame(tuple(d["Ek_range"]), d["cheb_r"], d["cheb_pr"], tuple(d["twiss_x"]), tuple(d["twiss_z"]),
+                        tuple(d["amp"]), int(d["nsectors"]), tunes=list(d["tunes"]))
+    return d["params"].copy(), frame
+
+
 # ------------------------------------------------------------- diagnostics
 def tunes(record, nsectors=None):
     """Fractional tunes per state from turn-by-turn Floquet coordinates

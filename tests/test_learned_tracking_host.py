@@ -116,3 +116,16 @@ def test_failed_audit_hands_states_over():
     a1, a2 = res["audits"]
     assert a1[:3] == (10, 20, 20) and a2[:3] == (20, 10, 10)
     assert int(res["plain"].sum()) == 30
+
+
+def test_save_and_load_round_trip(tmp_path):
+    frame = _frame()
+    p = learned.init_params(5)
+    path = str(tmp_path / "map.npz")
+    learned.save(path, torch.from_numpy(p), frame)
+    p2, f2 = learned.load(path)
+    assert np.array_equal(p2, p)
+    s = torch.from_numpy(learned.sample_domain(50, np.random.default_rng(6)))
+    a = frame.to_phys(s, s[:, 4])
+    b = f2.to_phys(s, s[:, 4])
+    assert torch.equal(a, b) and f2.R == frame.R and f2.nsectors == 12
