@@ -360,7 +360,8 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     300-600 MeV (linspace), ceil(exp(U(0, ln 4096))) particles each with
     0.5 mm Gaussian offsets, all in one bunch through the FP32C Boris pusher
     (RF off), 200 turns of the slowest instance per iteration, float64
-    one-turn-map fit and fixed-point update per instance.  2880 steps per
+    one-turn-map fit and fixed-point update per instance, every iteration
+    after the first a replay of one captured CUDA graph.  2880 steps per
     turn of the fastest instance: at 720 the 2.8-degree D magnet gets five
     steps and the motion is not regular enough for a tune."""
     import torch
@@ -388,14 +389,16 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
             "particle_steps_per_s": scan.N * scan.steps * iterations / (ms * 1e-3),
             "instances": n_instances, "particles": scan.N, "turns_per_iteration": turns,
             "steps_per_iteration": scan.steps, "steps_per_turn_fastest": steps_per_turn, "iterations": iterations,
-            "ms_per_iteration": [r["ms"] for r in recs], "launches_per_iteration": recs[-1]["launches"],
+            "ms_per_iteration": [r["ms"] for r in recs], "modes": [r["mode"] for r in recs],
+            "push_launches_per_iteration": recs[-1]["launches"],
             "max_abs_dr_m": [r["max_abs_dr"] for r in recs],
             "orbit_vs_scaling_law_m": float(np.abs(scan.r - r_sc).max()),
             "Qr_frac_range": [float(np.nanmin(q[:, 0])), float(np.nanmax(q[:, 0]))],
             "Qz_frac_range": [float(np.nanmin(q[:, 1])), float(np.nanmax(q[:, 1]))],
             "padding_waste": scan.padding(), "valid_instances": int(recs[-1]["good"].sum()),
             "dtype": "f32c push, f64 fit and update",
-            "not_built": "CUDA-graph capture of the iteration and a tile autotuner"}
+            "graph": "iteration 1 runs directly and is captured; later iterations replay the CUDA graph",
+            "not_built": "a tile autotuner (one bunch, 32-thread blocks over all particles)"}
 
 
 # algorithmic flops of one map application: 5 inputs (the sixth is zero),

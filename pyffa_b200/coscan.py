@@ -102,6 +102,45 @@ def accumulate_crossings(p, step, x, gv, inst, nsteps, last, has, S, Y, crossing
     has[p[lastocc]] = True
 
 
+def accumulate_crossings_fixed(rec, count, dt, gv, inst_ext, nsteps, last, has, S, Y, crossings, scale):
+    """accumulate_crossings over a whole record buffer (C, 23) of which the
+    first `count` (device scalar) rows are valid, with no host read-back and
+    no data-dependent shapes (capturable in a CUDA graph).  Invalid rows go to
+    a dummy particle N (inst_ext[N] = I, the dummy instance: gv[I] = 0,
+    scale[I] = 1, rows I of S, Y, crossings and N of last, has unused)."""
+    import torch
+    C = rec.shape[0]
+    N = inst_ext.shape[0] - 1
+    I = gv.shape[0] - 1
+    valid = torch.arange(C, device=rec.device) < count
+    p = torch.where(valid, rec[:, 1].long(), N)
+    step = torch.where(valid, rec[:, 2].long(), 0)
+    x = torch.where(valid[:, None], crossing_states(rec, dt), torch.zeros((), dtype=rec.dtype, device=rec.device))
+    ii = inst_ext[p]
+    x = (x - gv[ii]) * scale[ii]
+    order = torch.argsort(p * (nsteps + 2) + step)
+    p, x = p[order], x[order]
+    ii = inst_ext[p]
+    same = torch.zeros(C, dtype=torch.bool, device=rec.device)
+    same[1:] = p[1:] == p[:-1]
+    prev = torch.empty_like(x)
+    prev[1:] = x[:-1]
+    first = ~same
+    prev = torch.where(first[:, None], last[p], prev)
+    ok = same | (first & has[p])
+    ip = torch.where(ok, ii, I)
+    for pl in (0, 1):
+        f = torch.cat([prev[:, 2 * pl:2 * pl + 2], torch.ones_like(prev[:, :1])], 1)
+        S[pl].index_add_(0, ip, f[:, :, None] * f[:, None, :])
+        Y[pl].index_add_(0, ip, x[:, 2 * pl:2 * pl + 2, None] * f[:, None, :])
+    crossings.index_add_(0, ii, torch.ones(C, dtype=crossings.dtype, device=rec.device))
+    lastocc = torch.ones(C, dtype=torch.bool, device=rec.device)
+    lastocc[:-1] = p[1:] != p[:-1]
+    idx = torch.where(lastocc, p, N)
+    last.index_copy_(0, idx, x)
+    has.index_fill_(0, idx, True)
+
+
 def fit_one_turn(S, Y, cond_max=1e14):
     """float64 least-squares one-turn map per instance and plane from the sums
     of accumulate_crossings: returns the fixed point offsets (I, 4), the
@@ -164,6 +203,8 @@ class BatchedOrbitScan:
         rng = np.random.Generator(np.random.PCG64(seed))
         self.g = sigma * rng.standard_normal((self.N, 2))    # r and z offsets, fixed over the iterations
         self.history = []
+        self._dev_state = None
+        self._graph = None
 
     # ------------------------------------------------------------ bunch
     def _vformat(self):
@@ -188,52 +229,99 @@ class BatchedOrbitScan:
         return v[:, [0, 1, 2, 3]]
 
     # ------------------------------------------------------------ one iteration
-    def iterate(self):
-        """One push of all instances and the float64 update; returns the
-        iteration record (orbit change, tunes, particle-turns, device time)."""
+    def _setup(self):
+        """Device buffers of an iteration, allocated once: the bunch, the
+        pusher on a private stream, the crossing buffer for the longest
+        launch, the per-instance sums (with a dummy instance I and a dummy
+        particle N for the fixed-shape accumulation)."""
         import torch
         from .track import CrossingCapture, Pusher, StepClock, _EphemeralBunch
         dev = self.dev
         f64 = dict(dtype=torch.float64, device=dev)
-        b = _EphemeralBunch(self._vformat(), "Boris", dev)
-        pusher = Pusher(b, self.gp, "Boris", "fp32c")
-        clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
-        clock.ensure(self.steps + 1)
-        cap = CrossingCapture(b, [0.0], self.gp, self.dt)
-        L = cap.max_steps()
-        gv = torch.as_tensor(self._guess_v(), **f64)               # (I, 4)
-        # fit coordinates: offsets in mm and in mrad of the speed
-        unit = np.empty((self.I, 4))
-        unit[:, 0] = unit[:, 2] = 1e-3
-        unit[:, 1] = unit[:, 3] = 1e-3 * self.conv.Ek2v(self.E)
-        sc = torch.as_tensor(1.0 / unit, **f64)
-        inst = torch.as_tensor(self.inst, device=dev)
-        last = torch.zeros((self.N, 4), **f64)
-        has = torch.zeros(self.N, dtype=torch.bool, device=dev)
-        S = torch.zeros((2, self.I, 3, 3), **f64)                  # planes x, z: sum f f^T
-        Y = torch.zeros((2, self.I, 2, 3), **f64)                  # sum x' f^T
-        crossings = torch.zeros(self.I, **f64)
-        launches = 0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(pusher.stream)
-        for s0 in range(0, self.steps, L):
-            ns = min(L, self.steps - s0)
-            pusher.push(clock, s0, ns, 0, xing=cap.prepare(ns))
-            launches += 1
-            k = int(cap.count.item())
-            if k > cap.x.capacity:
-                raise RuntimeError(f"crossing records overflowed: {k} > {cap.x.capacity}")
-            if k == 0:
-                continue
-            rec = cap.buf[:k * 23].view(k, 23)
-            accumulate_crossings(rec[:, 1].long(), rec[:, 2].long(), crossing_states(rec, self.dt), gv, inst,
-                                 self.steps, last, has, S, Y, crossings, sc)
-        e1.record(pusher.stream)
-        torch.cuda.synchronize(dev)
+        st = type("ScanState", (), {})()
+        st.stream = torch.cuda.Stream(dev)
+        st.bunch = _EphemeralBunch(self._vformat(), "Boris", dev)
+        st.pusher = Pusher(st.bunch, self.gp, "Boris", "fp32c")
+        st.pusher.stream = st.stream
+        st.clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
+        st.clock.ensure(self.steps + 1)
+        st.cap = CrossingCapture(st.bunch, [0.0], self.gp, self.dt)
+        st.L = st.cap.max_steps()
+        st.xing = st.cap.prepare(st.L)
+        st.rows = st.cap.buf.view(-1, 23)[:st.cap.x.capacity]
+        unit = np.ones((self.I + 1, 4))
+        unit[:self.I, 0] = unit[:self.I, 2] = 1e-3
+        unit[:self.I, 1] = unit[:self.I, 3] = 1e-3 * self.conv.Ek2v(self.E)
+        st.unit = unit[:self.I]
+        st.scale = torch.as_tensor(1.0 / unit, **f64)
+        st.gv = torch.zeros((self.I + 1, 4), **f64)
+        st.inst = torch.as_tensor(np.concatenate([self.inst, [self.I]]), device=dev)
+        st.last = torch.zeros((self.N + 1, 4), **f64)
+        st.has = torch.zeros(self.N + 1, dtype=torch.bool, device=dev)
+        st.S = torch.zeros((2, self.I + 1, 3, 3), **f64)
+        st.Y = torch.zeros((2, self.I + 1, 2, 3), **f64)
+        st.crossings = torch.zeros(self.I + 1, **f64)
+        st.maxk = torch.zeros(1, dtype=torch.int64, device=dev)
+        st.launches = len(range(0, self.steps, st.L))
+        self._dev_state = st
+
+    def _body(self):
+        """The work of one iteration, enqueued on the scan's stream: AoS ->
+        SoA, then for every launch the push with crossing capture and the
+        accumulation of its records."""
+        import ctypes
+        from . import _lib
+        st = self._dev_state
+        b = st.bunch
+        _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), st.stream.cuda_stream),
+                   "ffa_aos_to_soa")
+        for t in (st.S, st.Y, st.crossings, st.last, st.has, st.maxk):
+            t.zero_()
+        for s0 in range(0, self.steps, st.L):
+            ns = min(st.L, self.steps - s0)
+            st.cap.count.zero_()
+            st.pusher.push(st.clock, s0, ns, 0, xing=st.xing)
+            st.maxk.copy_(st.maxk.maximum(st.cap.count))
+            accumulate_crossings_fixed(st.rows, st.cap.count, self.dt, st.gv, st.inst, self.steps, st.last, st.has,
+                                       st.S, st.Y, st.crossings, st.scale)
+
+    def iterate(self, graph=True):
+        """One push of all instances and the float64 update; returns the
+        iteration record (orbit change, tunes, particle-turns, device time).
+        With graph=True the first iteration runs the work directly (it is
+        also the warm-up) and captures it in a CUDA graph; later iterations
+        replay that graph after uploading their starting states and guesses."""
+        import torch
+        if self._dev_state is None:
+            self._setup()
+        st = self._dev_state
+        with torch.cuda.stream(st.stream):
+            st.bunch.aos.copy_(torch.from_numpy(self._vformat()))
+            st.gv[:self.I].copy_(torch.from_numpy(self._guess_v()))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st.stream)
+            if self._graph is not None:
+                self._graph.replay()
+                mode = "graph"
+            else:
+                self._body()
+                mode = "direct"
+            e1.record(st.stream)
+        st.stream.synchronize()
         ms = e0.elapsed_time(e1)
-        gvn = gv.cpu().numpy()
-        fix, tunes, good = fit_one_turn(S.cpu().numpy(), Y.cpu().numpy())
-        fix = fix * unit
+        if int(st.maxk.item()) > st.cap.x.capacity:
+            raise RuntimeError(f"crossing records overflowed: {int(st.maxk.item())} > {st.cap.x.capacity}")
+        S = st.S[:, :self.I].cpu().numpy()
+        Y = st.Y[:, :self.I].cpu().numpy()
+        crossings = st.crossings[:self.I].cpu().numpy()
+        gvn = st.gv[:self.I].cpu().numpy()
+        if graph and self._graph is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=st.stream):
+                self._body()
+            self._graph = g
+        fix, tunes, good = fit_one_turn(S, Y)
+        fix = fix * st.unit
         new = gvn + fix
         dr = np.where(good, fix[:, 0], 0.0)
         # back to p-format orbit parameters at azimuth 0 (vphi from the speed)
@@ -243,16 +331,16 @@ class BatchedOrbitScan:
             vf = math.sqrt(max(vtot[i] ** 2 - vr * vr - vz * vz, 0.0))
             self.r[i], self.z[i] = new[i, 0], new[i, 2]
             self.pr[i], self.pz[i] = math.atan2(vr, vf), math.atan2(vz, vf)
-        pt = float(crossings.sum().item())
-        rec_ = {"ms": ms, "launches": launches, "particle_turns": pt, "max_abs_dr": float(np.abs(dr).max()),
-                "dr": dr, "tunes": tunes, "good": good, "crossings": crossings.cpu().numpy()}
+        rec_ = {"ms": ms, "launches": st.launches, "mode": mode, "particle_turns": float(crossings.sum()),
+                "max_abs_dr": float(np.abs(dr).max()), "dr": dr, "tunes": tunes, "good": good,
+                "crossings": crossings}
         self.history.append(rec_)
         return rec_
 
-    def run(self, iterations=3, tol=1e-6):
+    def run(self, iterations=3, tol=1e-6, graph=True):
         """Iterates until the largest orbit change is below `tol` [m]."""
         for _ in range(iterations):
-            rec = self.iterate()
+            rec = self.iterate(graph)
             if rec["max_abs_dr"] < tol:
                 break
         return self.history[-1]

@@ -2,7 +2,8 @@
 300-600 MeV) through the compensated float32 pusher in one bunch; the
 fitted closed orbits agree with the scaling-law orbit of the azimuth-domain
 search and the fractional tunes with its one-sector transfer matrix, and a
-second iteration changes the orbits by less than the first."""
+second iteration (a replay of the iteration's CUDA graph) changes the
+orbits by less than the first."""
 import os
 import tempfile
 
@@ -40,7 +41,8 @@ def test_batched_scan_orbits_and_tunes():
     scan = coscan.BatchedOrbitScan(gp, E, counts, r_exp + 2e-4, pr_exp, d["perimeter"] * scale,
                                    sigma=0.5e-3, turns=60, seed=3, steps_per_turn=2880)
     first = scan.iterate()
-    second = scan.iterate()
+    second = scan.iterate()           # the captured CUDA graph of an iteration, replayed
+    assert (first["mode"], second["mode"]) == ("direct", "graph")
     assert first["good"].all() and second["good"].all()
     # the first update takes the orbit most of the way, the second is small
     assert first["max_abs_dr"] > 1e-4 and second["max_abs_dr"] < 2e-5, (first["max_abs_dr"], second["max_abs_dr"])
