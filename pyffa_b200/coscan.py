@@ -285,12 +285,39 @@ class BatchedOrbitScan:
             accumulate_crossings_fixed(st.rows, st.cap.count, self.dt, st.gv, st.inst, self.steps, st.last, st.has,
                                        st.S, st.Y, st.crossings, st.scale)
 
+    def _body_direct(self):
+        """The iteration without a graph: each launch's record count is read
+        back and only those records are accumulated."""
+        import ctypes
+        from . import _lib
+        st = self._dev_state
+        b = st.bunch
+        _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), st.stream.cuda_stream),
+                   "ffa_aos_to_soa")
+        for t in (st.S, st.Y, st.crossings, st.last, st.has, st.maxk):
+            t.zero_()
+        for s0 in range(0, self.steps, st.L):
+            ns = min(st.L, self.steps - s0)
+            st.cap.count.zero_()
+            st.pusher.push(st.clock, s0, ns, 0, xing=st.xing)
+            k = int(st.cap.count.item())
+            st.maxk.fill_(max(int(st.maxk.item()), k))
+            if k == 0 or k > st.cap.x.capacity:
+                continue
+            rec = st.rows[:k]
+            accumulate_crossings(rec[:, 1].long(), rec[:, 2].long(), crossing_states(rec, self.dt), st.gv, st.inst,
+                                 self.steps, st.last, st.has, st.S, st.Y, st.crossings, st.scale)
+
     def iterate(self, graph=True):
         """One push of all instances and the float64 update; returns the
         iteration record (orbit change, tunes, particle-turns, device time).
-        With graph=True the first iteration runs the work directly (it is
-        also the warm-up) and captures it in a CUDA graph; later iterations
-        replay that graph after uploading their starting states and guesses."""
+        graph=False: the launches run directly, each launch's records counted
+        on the host and accumulated ("direct").  graph=True: the fixed-shape
+        accumulation over the whole record buffer, which has no host
+        read-back; the first such iteration runs directly (it is also the
+        warm-up, "captured") and is captured as one CUDA graph, which later
+        iterations replay after uploading their starting states and guesses
+        ("graph")."""
         import torch
         if self._dev_state is None:
             self._setup()
@@ -300,12 +327,15 @@ class BatchedOrbitScan:
             st.gv[:self.I].copy_(torch.from_numpy(self._guess_v()))
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st.stream)
-            if self._graph is not None:
+            if not graph:
+                self._body_direct()
+                mode = "direct"
+            elif self._graph is not None:
                 self._graph.replay()
                 mode = "graph"
             else:
                 self._body()
-                mode = "direct"
+                mode = "captured"
             e1.record(st.stream)
         st.stream.synchronize()
         ms = e0.elapsed_time(e1)

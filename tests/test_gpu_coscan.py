@@ -42,7 +42,7 @@ def test_batched_scan_orbits_and_tunes():
                                    sigma=0.5e-3, turns=60, seed=3, steps_per_turn=2880)
     first = scan.iterate()
     second = scan.iterate()           # the captured CUDA graph of an iteration, replayed
-    assert (first["mode"], second["mode"]) == ("direct", "graph")
+    assert (first["mode"], second["mode"]) == ("captured", "graph")
     assert first["good"].all() and second["good"].all()
     # the first update takes the orbit most of the way, the second is small
     assert first["max_abs_dr"] > 1e-4 and second["max_abs_dr"] < 2e-5, (first["max_abs_dr"], second["max_abs_dr"])
@@ -57,5 +57,6 @@ def test_batched_scan_orbits_and_tunes():
     # self-consistency: 10 um offsets around the orbit found come back to it
     check = coscan.BatchedOrbitScan(gp, E, [8] * 5, scan.r, scan.pr, d["perimeter"] * scale,
                                     sigma=1e-5, turns=60, seed=4, steps_per_turn=2880)
-    rec = check.iterate()
+    rec = check.iterate(graph=False)  # the direct path: per-launch record counts
+    assert rec["mode"] == "direct"
     assert rec["good"].all() and rec["max_abs_dr"] < 3e-6, rec["max_abs_dr"]
