@@ -360,8 +360,9 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     300-600 MeV (linspace), ceil(exp(U(0, ln 4096))) particles each with
     0.5 mm Gaussian offsets, all in one bunch through the FP32C Boris pusher
     (RF off), 200 turns of the slowest instance per iteration, float64
-    one-turn-map fit and fixed-point update per instance, every iteration
-    after the first a replay of one captured CUDA graph.  2880 steps per
+    one-turn-map fit and fixed-point update per instance; the push's launch
+    shape picked by the autotuner on the scan's bunch first; iteration 1
+    direct, iteration 2 captured as a CUDA graph, later ones replays.  2880 steps per
     turn of the fastest instance: at 720 the 2.8-degree D magnet gets five
     steps and the motion is not regular enough for a tune."""
     import torch
@@ -400,7 +401,16 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
             "padding_waste": scan.padding(), "valid_instances": int(recs[-1]["good"].sum()),
             "dtype": "f32c push, f64 fit and update",
             "graph": "iteration 1 direct; iteration 2 fixed-shape and captured as one CUDA graph; iteration 3 a replay",
-            "not_built": "a tile autotuner (one bunch, 32-thread blocks over all particles)"}
+            "autotune": None if scan.tuning is None else
+            {"shape": scan.tuning.report()["chosen"], "speedup_vs_default_shape": scan.tuning.speedup,
+             "tune_steps": scan.tune_steps, "rtol": scan.tune_rtol, "candidates": _tune_rows(scan.tuning)}}
+
+
+def _tune_rows(res):
+    """Autotuner table, compact: [threads, register cap, warps per SM, ms,
+    largest relative state difference from the default shape, accepted]."""
+    return [[r["threads"], r["max_regs"], r.get("warps_per_sm"), round(r["ms"], 4), r.get("max_rel_diff"),
+             r.get("accepted")] for r in res.rows]
 
 
 # algorithmic flops of one map application: 5 inputs (the sixth is zero),
@@ -675,6 +685,24 @@ def main():
         fp32c = {"value": v32, "unit": "particle-turns/s", "ms_per_step": float(t32.item()) / args.steps,
                  "speedup_vs_fp64": v32 / value,
                  "dtype": "f32 field exponentials and map lookup, f64 push and state"}
+        # the launch-shape autotuner on this bunch (one-turn launches); the
+        # chosen shape timed like the default one
+        from pyffa_b200 import autotune
+        tune = autotune.tune_push(pu32, clock, args.warmup * STEPS_PER_TURN, STEPS_PER_TURN, reset=restore)
+        tuned = {"shape": tune.report()["chosen"], "tuner_speedup": tune.speedup,
+                 "candidates": _tune_rows(tune)}
+        if tune.best != (0, 0):
+            pu32.shape = tune.best
+            mst = timed_turns(pu32, args.steps)
+            tt = torch.tensor([sum(mst)], dtype=torch.float64, device=dev)
+            if world > 1:
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            vt = n * world * args.steps / (float(tt.item()) * 1e-3)
+            pu32.shape = (0, 0)
+        else:
+            vt = v32
+        tuned.update({"value": vt, "speedup_vs_fp64": vt / value})
+        fp32c["autotuned"] = tuned
     clocks = cs.summary()
 
     # end to end through the host-buffer API: host matrix in, one turn, host matrix out

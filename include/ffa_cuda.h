@@ -49,7 +49,16 @@ enum ffa_push_flags {
     FFA_RK4 = 1,                  /* 4th-order Runge-Kutta (solver_type 0) */
     FFA_FP64 = 0,                 /* all arithmetic in float64 */
     FFA_FP32C = 2,                /* Boris: float32 field exponentials and map lookup, float64 push */
-    FFA_RF_PHYSICAL_SUM = 4       /* sum every RF gap (reference: last gap wins) */
+    FFA_RF_PHYSICAL_SUM = 4,      /* sum every RF gap (reference: last gap wins) */
+    /* Launch shape of the Boris pushers, bits 8-11 (0: the default shape).
+     * Bits 8-9: threads per block 32 << v (32, 64, 128, 256).  Bits 10-11:
+     * register cap per thread 80, 72, 64, 56; caps below 80 are built for the
+     * FFA_FP32C pusher without space charge (else FFA_ERR_UNSUPPORTED).  The
+     * shape sets how many warps are resident per SM, not the arithmetic: the
+     * results are the same for every shape.  RK4 takes the default only. */
+    FFA_SHAPE_TB_SHIFT = 8,
+    FFA_SHAPE_NREG_SHIFT = 10,
+    FFA_SHAPE_MASK = 0xF00
 };
 
 /* Device status words, int64 each, accumulated with atomics. */
@@ -188,6 +197,13 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
              const ffa_consts *cs, const ffa_step_table *tab, ffa_state_soa *st,
              int64_t n, int64_t step0, int32_t nsteps, double dt, int32_t sc_step,
              int32_t flags, void *stream, int64_t *status);
+
+/* Resident blocks per SM and threads per block of the push kernel that
+ * ffa_push / ffa_push_crossing (crossing != 0) would launch for `flags` and
+ * a field map of `max_order`, without space charge (the runtime's occupancy
+ * calculator; needs a device).  For the launch-shape autotuner's report. */
+int ffa_push_occupancy(int32_t flags, int32_t max_order, int32_t crossing, int32_t *blocks_per_sm,
+                       int32_t *threads_per_block);
 
 /* Converts between the reference's N x 16 row-major matrix (device) and the
  * SoA state.  soa_to_aos writes cols 0-5 and 7-12 and leaves 6, 13-15.

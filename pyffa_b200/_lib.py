@@ -23,6 +23,18 @@ FFA_RK4 = 1
 FFA_FP64 = 0
 FFA_FP32C = 2
 FFA_RF_PHYSICAL_SUM = 4
+FFA_SHAPE_TB_SHIFT = 8
+FFA_SHAPE_NREG_SHIFT = 10
+FFA_SHAPE_MASK = 0xF00
+SHAPE_THREADS = (32, 64, 128, 256)   # threads per block, bits 8-9
+SHAPE_NREGS = (80, 72, 64, 56)       # register cap per thread, bits 10-11
+
+
+def shape_flags(tb_sel: int, nreg_sel: int) -> int:
+    """ffa_push flag bits of a Boris launch shape (0, 0: the default)."""
+    if not (0 <= tb_sel < 4 and 0 <= nreg_sel < 4):
+        raise ValueError(f"launch shape ({tb_sel}, {nreg_sel}) out of range")
+    return (tb_sel << FFA_SHAPE_TB_SHIFT) | (nreg_sel << FFA_SHAPE_NREG_SHIFT)
 
 STATUS_LOST = 0
 STATUS_NAN = 1
@@ -158,6 +170,7 @@ EXPORTS = {
     "ffa_theta_track": [d_p, C.POINTER(ThetaTrackDesc), d_p],
     "ffa_soa_to_aos": [C.POINTER(StateSoA), C.c_int64, d_p, d_p],
     "ffa_mean_fi": [C.POINTER(StateSoA), C.c_int64, d_p, d_p, d_p],
+    "ffa_push_occupancy": [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
     "ffa_sc_plan_create": [C.POINTER(SCDesc), d_p, C.POINTER(d_p)],
     "ffa_sc_plan_destroy": [d_p],
     "ffa_sc_step": [d_p, C.POINTER(StateSoA), C.c_int64, C.c_int32, C.c_int32, d_p, d_p, d_p],

@@ -42,19 +42,35 @@ def needs_rebuild() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every .cu under csrc/ into pyffa_b200/libffa_cuda.so."""
+    """Compile every .cu under csrc/ into pyffa_b200/libffa_cuda.so: one nvcc
+    per source, run in parallel, then one link."""
     if not force and not needs_rebuild():
         return LIB_PATH
+    import tempfile
+    from concurrent.futures import ThreadPoolExecutor
     tmp = LIB_PATH + ".tmp"
-    cmd = [nvcc_path(), *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
-           "-Xptxas", "-v" if verbose else "-O3", "-shared", "-o", tmp,
-           "-I", os.path.join(REPO_DIR, "include"), *sources()]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libffa_cuda.so")
-    if verbose:
-        sys.stderr.write(res.stderr)
+    nvcc = nvcc_path()
+    with tempfile.TemporaryDirectory(prefix="ffa_build_") as work:
+        def compile_one(src):
+            obj = os.path.join(work, os.path.basename(src) + ".o")
+            cmd = [nvcc, *ARCH_FLAGS, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
+                   "-Xptxas", "-v" if verbose else "-O3", "-I", os.path.join(REPO_DIR, "include"),
+                   "-c", src, "-o", obj]
+            return obj, subprocess.run(cmd, capture_output=True, text=True)
+        srcs = sources()
+        with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+            results = list(ex.map(compile_one, srcs))
+        for _, res in results:
+            if res.returncode != 0:
+                sys.stderr.write(res.stdout + res.stderr)
+                raise RuntimeError("nvcc failed building libffa_cuda.so")
+            if verbose:
+                sys.stderr.write(res.stderr)
+        res = subprocess.run([nvcc, *ARCH_FLAGS, "-shared", "-o", tmp, *[o for o, _ in results]],
+                             capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("nvcc failed linking libffa_cuda.so")
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 

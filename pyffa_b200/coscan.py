@@ -178,12 +178,22 @@ class BatchedOrbitScan:
     [m] and pr0 (I,) (p-format angle) of the closed orbit at azimuth 0 and
     its length `perimeter` (I,) [m]; sigma: Gaussian offset in r and z [m].
     The time step is the fastest instance's revolution time / steps_per_turn;
-    an iteration lasts `turns` turns of the slowest instance."""
+    an iteration lasts `turns` turns of the slowest instance.  autotune: the
+    push's launch shape (threads per block, register cap) is picked by
+    timing the candidates on the scan's own bunch before the first iteration
+    (autotune.tune_push; `tuning` holds the table), else the default; shapes
+    whose states differ from the default's by more than tune_rtol (relative)
+    on the tuning run are not chosen.  The scan fits maps to many crossings,
+    so rounding-level differences (1e-11) are accepted by default."""
 
     def __init__(self, gp, energies, counts, r0, pr0, perimeter, sigma=0.5e-3, steps_per_turn=720, turns=200,
-                 seed=0, device=None):
+                 seed=0, device=None, autotune=True, tune_steps=1000, tune_rtol=1e-9):
         import torch
         self.gp = gp
+        self.autotune = bool(autotune)
+        self.tune_steps = int(tune_steps)
+        self.tune_rtol = float(tune_rtol)
+        self.tuning = None
         self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.E = np.asarray(energies, np.float64)
         self.counts = np.asarray(counts, np.int64)
@@ -264,6 +274,25 @@ class BatchedOrbitScan:
         st.maxk = torch.zeros(1, dtype=torch.int64, device=dev)
         st.launches = len(range(0, self.steps, st.L))
         self._dev_state = st
+        if self.autotune:
+            self._tune()
+
+    def _tune(self):
+        """Times every launch shape on the first `tune_steps` steps of the
+        scan's starting bunch, with crossing capture as in an iteration, and
+        sets the fastest on the pusher."""
+        import ctypes
+        from . import _lib, autotune
+        st = self._dev_state
+        b = st.bunch
+
+        def reset():
+            _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()),
+                                                 st.stream.cuda_stream), "ffa_aos_to_soa")
+        res = autotune.tune_push(st.pusher, st.clock, 0, min(st.L, self.tune_steps, self.steps), xing=st.xing,
+                                 reset=reset, count=st.cap.count, rtol=self.tune_rtol)
+        st.pusher.shape = res.best
+        self.tuning = res
 
     def _body(self):
         """The work of one iteration, enqueued on the scan's stream: AoS ->

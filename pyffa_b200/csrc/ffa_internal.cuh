@@ -96,9 +96,11 @@ struct ffa_fieldmap {
 
 // Launchers implemented in ffa_push.cu
 namespace ffa {
-cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s);
+// tb: threads per block; nreg_sel: register cap 80, 72, 64, 56 (0..3)
+cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s, int tb);
 cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s);
-cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s);
+cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel);
+cudaError_t push_occupancy(bool rk4, bool f32, int max_order, bool xing, int tb, int nreg_sel, int *blocks);
 cudaError_t launch_theta_track(const FieldK &f, const ffa_theta_track_desc &d, cudaStream_t s);
 cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, float *n32, cudaStream_t s);
 }  // namespace ffa

@@ -433,8 +433,12 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
 // 720-step turn at 88 registers, 3.81 ms at 80).
 constexpr int BORIS_TB = 32;
 
-template <int MAXO, bool SC, bool XING, bool F32>
-__global__ void __maxnreg__(80) boris_f64_kernel(const PushK p)
+// NREG: the register cap.  80 is the default launch shape; the compensated
+// float32 pusher without space charge is also built with 72, 64 and 56
+// (more resident warps, more spills) for the launch-shape autotuner.  The
+// cap changes register allocation only, not the arithmetic.
+template <int MAXO, bool SC, bool XING, bool F32, int NREG = 80>
+__global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -774,9 +778,8 @@ cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, fl
 }
 
 template <int MAXO, bool SC>
-static void boris_launch(const PushK &p, cudaStream_t s)
+static void boris_launch(const PushK &p, cudaStream_t s, int tb, int)
 {
-    const int tb = BORIS_TB;
     if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
     else boris_f64_kernel<MAXO, SC, false, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
@@ -789,21 +792,21 @@ static void rk4_launch(const PushK &p, cudaStream_t s)
     else rk4_f64_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
-#define FFA_DISPATCH(FN, p, s)                                                   \
-    do {                                                                         \
-        const bool sc_ = (p).st.sc_pre != nullptr && (p).sc_step > 0;            \
-        switch ((p).f.max_order) {                                               \
-        case 0: sc_ ? FN<0, true>(p, s) : FN<0, false>(p, s); break;             \
-        case 1: sc_ ? FN<1, true>(p, s) : FN<1, false>(p, s); break;             \
-        case 2: sc_ ? FN<2, true>(p, s) : FN<2, false>(p, s); break;             \
-        case 3: sc_ ? FN<3, true>(p, s) : FN<3, false>(p, s); break;             \
-        default: sc_ ? FN<4, true>(p, s) : FN<4, false>(p, s); break;            \
-        }                                                                        \
+#define FFA_DISPATCH(FN, p, ...)                                                       \
+    do {                                                                               \
+        const bool sc_ = (p).st.sc_pre != nullptr && (p).sc_step > 0;                  \
+        switch ((p).f.max_order) {                                                     \
+        case 0: sc_ ? FN<0, true>(p, __VA_ARGS__) : FN<0, false>(p, __VA_ARGS__); break; \
+        case 1: sc_ ? FN<1, true>(p, __VA_ARGS__) : FN<1, false>(p, __VA_ARGS__); break; \
+        case 2: sc_ ? FN<2, true>(p, __VA_ARGS__) : FN<2, false>(p, __VA_ARGS__); break; \
+        case 3: sc_ ? FN<3, true>(p, __VA_ARGS__) : FN<3, false>(p, __VA_ARGS__); break; \
+        default: sc_ ? FN<4, true>(p, __VA_ARGS__) : FN<4, false>(p, __VA_ARGS__); break; \
+        }                                                                              \
     } while (0)
 
-cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s)
+cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s, int tb)
 {
-    FFA_DISPATCH(boris_launch, p, s);
+    FFA_DISPATCH(boris_launch, p, s, tb, 0);
     return cudaGetLastError();
 }
 
@@ -813,18 +816,61 @@ cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <int MAXO, bool SC>
-static void boris32_launch(const PushK &p, cudaStream_t s)
+template <int MAXO, bool XING, int NREG>
+static void boris32_shaped(const PushK &p, cudaStream_t s, int tb)
 {
-    const int tb = BORIS_TB;
+    boris_f64_kernel<MAXO, false, XING, true, NREG><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+}
+
+template <int MAXO, bool SC>
+static void boris32_launch(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
+{
+    if constexpr (!SC) {
+        if (nreg_sel != 0) {   // the caller has checked: no space charge
+            const bool x = p.xing.buf != nullptr;
+            switch (nreg_sel) {
+            case 1: x ? boris32_shaped<MAXO, true, 72>(p, s, tb) : boris32_shaped<MAXO, false, 72>(p, s, tb); break;
+            case 2: x ? boris32_shaped<MAXO, true, 64>(p, s, tb) : boris32_shaped<MAXO, false, 64>(p, s, tb); break;
+            default: x ? boris32_shaped<MAXO, true, 56>(p, s, tb) : boris32_shaped<MAXO, false, 56>(p, s, tb); break;
+            }
+            return;
+        }
+    }
     if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
     else boris_f64_kernel<MAXO, SC, false, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
 }
 
-cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s)
+cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
 {
-    FFA_DISPATCH(boris32_launch, p, s);
+    FFA_DISPATCH(boris32_launch, p, s, tb, nreg_sel);
     return cudaGetLastError();
+}
+
+// Resident blocks per SM of a push kernel (no space charge), from the runtime.
+template <int MAXO, bool X>
+static const void *push_kernel_fn(bool rk4, bool f32, int nreg_sel)
+{
+    if (rk4) return (const void *)rk4_f64_kernel<MAXO, false, X>;
+    if (!f32) return (const void *)boris_f64_kernel<MAXO, false, X, false>;
+    switch (nreg_sel) {
+    case 0: return (const void *)boris_f64_kernel<MAXO, false, X, true, 80>;
+    case 1: return (const void *)boris_f64_kernel<MAXO, false, X, true, 72>;
+    case 2: return (const void *)boris_f64_kernel<MAXO, false, X, true, 64>;
+    default: return (const void *)boris_f64_kernel<MAXO, false, X, true, 56>;
+    }
+}
+
+cudaError_t push_occupancy(bool rk4, bool f32, int max_order, bool xing, int tb, int nreg_sel, int *blocks)
+{
+    const void *fn;
+    switch (max_order) {
+    case 0: fn = xing ? push_kernel_fn<0, true>(rk4, f32, nreg_sel) : push_kernel_fn<0, false>(rk4, f32, nreg_sel); break;
+    case 1: fn = xing ? push_kernel_fn<1, true>(rk4, f32, nreg_sel) : push_kernel_fn<1, false>(rk4, f32, nreg_sel); break;
+    case 2: fn = xing ? push_kernel_fn<2, true>(rk4, f32, nreg_sel) : push_kernel_fn<2, false>(rk4, f32, nreg_sel); break;
+    case 3: fn = xing ? push_kernel_fn<3, true>(rk4, f32, nreg_sel) : push_kernel_fn<3, false>(rk4, f32, nreg_sel); break;
+    default: fn = xing ? push_kernel_fn<4, true>(rk4, f32, nreg_sel) : push_kernel_fn<4, false>(rk4, f32, nreg_sel); break;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, fn, tb, 0);
 }
 
 }  // namespace ffa

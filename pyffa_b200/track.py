@@ -124,13 +124,17 @@ class Pusher:
         if getattr(gp.Emap, "physical_sum", False):
             self.flags |= _lib.FFA_RF_PHYSICAL_SUM
         self.stream = torch.cuda.current_stream(bunch.device)
+        # launch shape (threads-per-block index, register-cap index) of the
+        # Boris kernels; (0, 0) is the default, autotune.tune_push picks others
+        self.shape = (0, 0)
 
     def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0, xing=None) -> None:
         L = _lib.lib()
         b = self.bunch
+        flags = self.flags | _lib.shape_flags(*self.shape)
         args = (self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
                 ctypes.byref(clock.table), ctypes.byref(b.soa()), b.n, step0, nsteps, clock.dt,
-                sc_step, self.flags, self.stream.cuda_stream, b.status.data_ptr())
+                sc_step, flags, self.stream.cuda_stream, b.status.data_ptr())
         if xing is None:
             _lib.check(L.ffa_push(*args), "ffa_push")
         else:
