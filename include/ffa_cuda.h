@@ -395,6 +395,11 @@ int ffa_mlp_train_step(const ffa_mlp_train_desc *desc, void *stream);
 int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, int transB, float *C, int ldc,
                  int M, int N, int K, const float *bias, void *stream);
 
+/* Tensor-core GEMM tiles (ffa_mlp_gemm, ffa_mlp_train_step) whose bounded
+ * pipeline waits ran out since the last call (their output tiles hold NaN);
+ * reads and clears the device counter, synchronising the device. */
+int ffa_mlp_gemm_timeouts(int32_t *count);
+
 /* Inference weights: the bfloat16 packing of a parameter block into `wpack`
  * (FFA_MLP_WPACK_BYTES, 16-byte aligned).  Call again after the parameters
  * change. */

@@ -180,6 +180,7 @@ EXPORTS = {
     "ffa_mlp_train_step": [C.POINTER(MlpTrainDesc), d_p],
     "ffa_mlp_gemm": [d_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int, d_p,
                      d_p],
+    "ffa_mlp_gemm_timeouts": [C.POINTER(C.c_int32)],
     "ffa_mlp_pack": [d_p, d_p, d_p],
     "ffa_mlp_infer": [C.POINTER(MlpInferDesc), d_p],
 }

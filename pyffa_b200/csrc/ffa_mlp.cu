@@ -123,27 +123,36 @@ __global__ void __launch_bounds__(128) gemm_tc(const float *__restrict__ A, int 
     for (int k0 = kb; k0 < ke; k0 += GT_K) {
         // staging: the index that is contiguous in global memory runs fastest
         // across threads (coalesced loads), converted to bfloat16
+        // fixed trip counts (128 threads): the loads of a stage are issued together
         if (!transA) {
-            for (int e = threadIdx.x; e < GT_M * GT_K; e += blockDim.x) {
+#pragma unroll
+            for (int it = 0; it < GT_M * GT_K / 128; ++it) {
+                const int e = threadIdx.x + 128 * it;
                 const int mm = e / GT_K, kk = e - mm * GT_K;
                 const int gm = m0 + mm, gk = k0 + kk;
                 sA[mm][kk] = __float2bfloat16_rn((gm < M && gk < ke) ? A[(int64_t)gm * lda + gk] : 0.0f);
             }
         } else {
-            for (int e = threadIdx.x; e < GT_M * GT_K; e += blockDim.x) {
+#pragma unroll
+            for (int it = 0; it < GT_M * GT_K / 128; ++it) {
+                const int e = threadIdx.x + 128 * it;
                 const int kk = e / GT_M, mm = e - kk * GT_M;
                 const int gm = m0 + mm, gk = k0 + kk;
                 sA[mm][kk] = __float2bfloat16_rn((gm < M && gk < ke) ? A[(int64_t)gk * lda + gm] : 0.0f);
             }
         }
         if (transB) {
-            for (int e = threadIdx.x; e < GT_N * GT_K; e += blockDim.x) {
+#pragma unroll
+            for (int it = 0; it < GT_N * GT_K / 128; ++it) {
+                const int e = threadIdx.x + 128 * it;
                 const int nn = e / GT_K, kk = e - nn * GT_K;
                 const int gn = n0 + nn, gk = k0 + kk;
                 sB[nn][kk] = __float2bfloat16_rn((gn < N && gk < ke) ? B[(int64_t)gn * ldb + gk] : 0.0f);
             }
         } else {
-            for (int e = threadIdx.x; e < GT_N * GT_K; e += blockDim.x) {
+#pragma unroll
+            for (int it = 0; it < GT_N * GT_K / 128; ++it) {
+                const int e = threadIdx.x + 128 * it;
                 const int kk = e / GT_N, nn = e - kk * GT_N;
                 const int gn = n0 + nn, gk = k0 + kk;
                 sB[nn][kk] = __float2bfloat16_rn((gn < N && gk < ke) ? B[(int64_t)gk * ldb + gn] : 0.0f);
@@ -186,13 +195,13 @@ __global__ void __launch_bounds__(128) gemm_tc(const float *__restrict__ A, int 
 
 // C[m][n] = sum over the splits of part[z][m][n], in split order
 __global__ void split_sum_kernel(const float *__restrict__ part, int splits, int M, int N, float *__restrict__ C,
-                                 int ldc)
+                                 int ldc, const float *__restrict__ bias)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M * N) return;
     float s = 0.0f;
     for (int z = 0; z < splits; ++z) s += part[(int64_t)z * M * N + i];
-    C[(int64_t)(i / N) * ldc + (i % N)] = s;
+    C[(int64_t)(i / N) * ldc + (i % N)] = s + (bias ? bias[i % N] : 0.0f);
 }
 
 constexpr int SPLITS_MAX = 16;
@@ -264,21 +273,48 @@ __global__ void out_grad_kernel(const float *x, const float *t, const float *f, 
 
 // column sums g[c] = sum_i d[i][c]: one block per 32 columns, eight warps
 // over interleaved rows, then a fixed-order reduction (deterministic).
-__global__ void __launch_bounds__(256) colsum_kernel(const float *d, int64_t B, int ncol, int ld, float *g)
+// Column sums g[c] = sum_i d[i][c] (bias gradients) in two fixed-order
+// passes: block (x, y) sums 32 columns over the rows [y rows_per, (y + 1)
+// rows_per) into part[y][c] (8 warps, 4 rows each per step), then one
+// thread per column adds the partial sums in row-chunk order.
+__global__ void __launch_bounds__(256) colsum_part_kernel(const float *__restrict__ d, int64_t B, int ncol, int ld,
+                                                          int64_t rows_per, float *__restrict__ part)
 {
     __shared__ float sh[8][33];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int c = blockIdx.x * 32 + lane;
-    float s = 0.0f;
-    if (c < ncol)
-        for (int64_t i = w; i < B; i += 8) s += d[i * ld + c];
-    sh[w][lane] = s;
+    const int64_t i0 = blockIdx.y * rows_per, i1 = min(B, i0 + rows_per);
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+    if (c < ncol) {
+        int64_t i = i0 + w;
+        for (; i + 24 < i1; i += 32) {
+            s0 += d[i * ld + c];
+            s1 += d[(i + 8) * ld + c];
+            s2 += d[(i + 16) * ld + c];
+            s3 += d[(i + 24) * ld + c];
+        }
+        for (; i < i1; i += 8) s0 += d[i * ld + c];
+    }
+    sh[w][lane] = (s0 + s1) + (s2 + s3);
     __syncthreads();
     if (w == 0 && c < ncol) {
         float t = 0.0f;
         for (int k = 0; k < 8; ++k) t += sh[k][lane];
-        g[c] = t;
+        part[(int64_t)blockIdx.y * ncol + c] = t;
     }
+}
+
+// one warp per column: lane l adds chunks l, l + 32, ..., then a fixed
+// shuffle tree (the same order every call)
+__global__ void colsum_final_kernel(const float *__restrict__ part, int chunks, int ncol, float *__restrict__ g)
+{
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (c >= ncol) return;
+    float t = 0.0f;
+    for (int y = lane; y < chunks; y += 32) t += part[(int64_t)y * ncol + c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) g[c] = t;
 }
 
 // skip-layer gradients: block k < 8 forms gWs[k][c] = sum_i x[i][k] d[i][c],
@@ -825,6 +861,236 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (threadIdx.x == 0 && *abort_flag && error) atomicExch(error, 1);
 }
 
+// ------------------------------------------------- GEMM (training, tcgen05)
+// The training products of at least 128 x 128 x 64 on the 5th-generation
+// tensor cores: C[M][N] = op(A) op(B) (+ bias) with the operands and the
+// meaning of transA / transB of gemm_tc.  One CTA of sixteen warps per
+// 128 x 128 output tile (and per K split, gridDim.z, as in gemm_tc); K is
+// staged 64 at a time: every thread loads its 16 + 16 float32 of the step
+// from global memory along the index that is contiguous there (into
+// registers, one step ahead), rounds to bfloat16 (as gemm_tc does) and
+// stores into a 128-byte-swizzled K-major tile (A: 128 m-rows, B: 128
+// n-rows, 128 bytes of k each), two stages; one thread issues the four
+// K = 16 MMAs of a stage into a 128-column TMEM accumulator and commits them
+// to that stage's mbarrier, which frees the stage for the store two steps
+// later.  Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its 32 output
+// rows) and 32 columns, adds the bias and stores float32.  Waits are
+// bounded: on a timeout the tile is written as NaN and g_gemm_timeouts is
+// counted.
+constexpr int G5_BM = 128, G5_BN = 128, G5_BK = 64, G5_STAGES = 2, G5_THREADS = 512;
+constexpr uint32_t G5_TILE = 128 * 128;                               // one operand stage: 16 KB
+constexpr uint32_t G5_SM_A = 0;
+constexpr uint32_t G5_SM_B = G5_SM_A + G5_STAGES * G5_TILE;
+constexpr uint32_t G5_SM_BAR = G5_SM_B + G5_STAGES * G5_TILE;        // one mbarrier per stage
+constexpr uint32_t G5_SM_MISC = G5_SM_BAR + 8 * G5_STAGES;            // tmem base, abort flag
+constexpr size_t G5_SMEM = G5_SM_MISC + 16 + 1024;                    // + alignment slack
+constexpr uint32_t G5_TMEM_COLS = 128;
+constexpr int G5_PER = G5_BM * G5_BK / G5_THREADS;                    // floats per thread per operand: 16
+static_assert(G5_PER == 16, "staging split");
+
+__device__ int g_gemm_timeouts;
+
+// This thread's share of rows [r0, r0 + 128) x k [k0, k0 + 64) of op(X)
+// (X[r ld + k] when kcont, else X[k ld + r]) into registers; rows >= nrows
+// and k >= kend read as 0.  kcont: 8 threads per row, two runs of 8
+// consecutive k each (a row's 256 bytes over 8 lanes); otherwise one row per
+// thread and 16 consecutive k (every load 32 consecutive rows of one k).
+__device__ __forceinline__ void g5_load(float v[G5_PER], const float *__restrict__ X, int ld, bool kcont, bool vec,
+                                        int r0, int nrows, int k0, int kend)
+{
+    const int t = threadIdx.x;
+    if (kcont) {
+#pragma unroll
+        for (int it = 0; it < 2; ++it) {
+            const int id = t + G5_THREADS * it;
+            const int gr = r0 + (id >> 3), gk = k0 + 8 * (id & 7);
+            if (gr < nrows && vec && gk + 8 <= kend) {
+                const float4 *src = reinterpret_cast<const float4 *>(X + (int64_t)gr * ld + gk);
+                const float4 a = __ldg(src), b = __ldg(src + 1);
+                v[8 * it + 0] = a.x; v[8 * it + 1] = a.y; v[8 * it + 2] = a.z; v[8 * it + 3] = a.w;
+                v[8 * it + 4] = b.x; v[8 * it + 5] = b.y; v[8 * it + 6] = b.z; v[8 * it + 7] = b.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    v[8 * it + j] = (gr < nrows && gk + j < kend) ? __ldg(X + (int64_t)gr * ld + gk + j) : 0.0f;
+            }
+        }
+    } else {
+        const int gr = r0 + (t & 127), kq = k0 + 16 * (t >> 7);
+        const bool rok = gr < nrows;
+#pragma unroll
+        for (int j = 0; j < G5_PER; ++j) v[j] = (rok && kq + j < kend) ? __ldg(X + (int64_t)(kq + j) * ld + gr) : 0.0f;
+    }
+}
+
+// the registers of g5_load as bfloat16 into a 128-byte-swizzled K-major stage
+__device__ __forceinline__ void g5_store(unsigned char *dst, const float v[G5_PER], bool kcont)
+{
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        int row, c;
+        if (kcont) {
+            const int id = t + G5_THREADS * h;
+            row = id >> 3;
+            c = id & 7;
+        } else {
+            row = t & 127;
+            c = 2 * (t >> 7) + h;
+        }
+        *reinterpret_cast<uint4 *>(dst + row * 128 + ((c ^ (row & 7)) << 4)) =
+            make_uint4(pack_bf16(v[8 * h], v[8 * h + 1]), pack_bf16(v[8 * h + 2], v[8 * h + 3]),
+                       pack_bf16(v[8 * h + 4], v[8 * h + 5]), pack_bf16(v[8 * h + 6], v[8 * h + 7]));
+    }
+}
+
+__global__ void __launch_bounds__(G5_THREADS) gemm_tc05(const float *__restrict__ A, int lda, int transA,
+                                                        const float *__restrict__ B, int ldb, int transB,
+                                                        float *__restrict__ C, int ldc, int M, int N, int K,
+                                                        const float *__restrict__ bias, int k_chunk, int vecA, int vecB)
+{
+    extern __shared__ unsigned char g5_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(g5_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t s0 = smem_u32(sm);
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(sm + G5_SM_MISC);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + G5_SM_MISC + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * G5_BM, n0 = blockIdx.x * G5_BN;
+    const int kb = blockIdx.z * k_chunk, ke = min(K, kb + k_chunk);
+    if (gridDim.z > 1) {
+        C += (int64_t)blockIdx.z * M * N;
+        ldc = N;
+        bias = nullptr;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < G5_STAGES; ++s) mbar_init(s0 + G5_SM_BAR + 8 * s, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                     "r"(G5_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const int nk = ke > kb ? (ke - kb + G5_BK - 1) / G5_BK : 0;
+    const bool kcA = !transA, kcB = transB != 0;
+    float va[G5_PER], vb[G5_PER];
+    if (nk > 0) {                                  // the first K step's loads overlap the set-up barrier
+        g5_load(va, A, lda, kcA, vecA != 0, m0, M, kb, ke);
+        g5_load(vb, B, ldb, kcB, vecB != 0, n0, N, kb, ke);
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *tmem_holder;
+    constexpr uint32_t IDESC = idesc_bf16(G5_BM, G5_BN);
+    int issued = 0;                                // commits made (thread 0)
+    for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % G5_STAGES;
+        const uint32_t bar = s0 + G5_SM_BAR + 8 * s;
+        if (kt >= G5_STAGES) {
+            // the MMAs that read this stage two steps ago have completed
+            if (threadIdx.x == 0) mbar_wait(bar, ((kt / G5_STAGES) - 1) & 1, abort_flag);
+            __syncthreads();
+            if (*abort_flag) break;                // read by every thread after the barrier
+        }
+        g5_store(sm + G5_SM_A + s * G5_TILE, va, kcA);
+        g5_store(sm + G5_SM_B + s * G5_TILE, vb, kcB);
+        if (kt + 1 < nk) {                         // next K step in flight during the MMAs
+            const int k1 = kb + (kt + 1) * G5_BK;
+            g5_load(va, A, lda, kcA, vecA != 0, m0, M, k1, ke);
+            g5_load(vb, B, ldb, kcB, vecB != 0, n0, N, k1, ke);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_after_sync();
+            const uint32_t a0 = s0 + G5_SM_A + s * G5_TILE, b0 = s0 + G5_SM_B + s * G5_TILE;
+#pragma unroll
+            for (int kk = 0; kk < G5_BK / 16; ++kk)
+                umma(tmem, sdesc(a0 + 32 * kk, 16, 1024, 2), sdesc(b0 + 32 * kk, 16, 1024, 2), IDESC, (kt | kk) != 0);
+            umma_commit(bar);
+            ++issued;
+        }
+    }
+    // the last commit covers every MMA of the tile
+    if (threadIdx.x == 0 && issued > 0) {
+        const int last = issued - 1;
+        const uint32_t bar = s0 + G5_SM_BAR + 8 * (last % G5_STAGES);
+        if (*abort_flag) mbar_wait_bounded(bar, (last / G5_STAGES) & 1);   // drain what is in flight
+        else mbar_wait(bar, (last / G5_STAGES) & 1, abort_flag);
+    }
+    __syncthreads();
+    tc_after_sync();
+    const bool failed = *abort_flag != 0;
+    // warp w: TMEM lanes 32 (w % 4) .. + 31 (its output rows), columns 32 (w / 4) .. + 31
+    const int quarter = warp & 3, cg = warp >> 2;
+    const int row = m0 + 32 * quarter + lane;
+    const bool vecC = ((ldc & 3) == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+    uint32_t v[32];
+    if (nk > 0 && !failed) {
+        TMEM_LD32(tmem + ((uint32_t)(32 * quarter) << 16) + 32 * cg, v);
+        tmem_wait_ld();
+        REG_FENCE32(v);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = failed ? 0x7FC00000u : 0u;
+    }
+    const int gn0 = n0 + 32 * cg;
+    if (row < M && gn0 < N) {
+        float *dst = C + (int64_t)row * ldc + gn0;
+        if (vecC && gn0 + 32 <= N) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4) {
+                float4 o = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]),
+                                       __uint_as_float(v[j + 3]));
+                if (bias) {
+                    o.x += bias[gn0 + j]; o.y += bias[gn0 + j + 1]; o.z += bias[gn0 + j + 2]; o.w += bias[gn0 + j + 3];
+                }
+                *reinterpret_cast<float4 *>(dst + j) = o;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (gn0 + j < N) dst[j] = __uint_as_float(v[j]) + (bias ? bias[gn0 + j] : 0.0f);
+        }
+    }
+    tc_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G5_TMEM_COLS));
+    }
+    if (threadIdx.x == 0 && failed) atomicAdd(&g_gemm_timeouts, 1);
+}
+
+bool g5_fits(int M, int N, int K) { return M >= G5_BM && N >= G5_BN && K >= G5_BK; }
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// one GEMM launch: the tcgen05 kernel for products of at least one full
+// tile, gemm_tc for the narrow ones (N = 8 outputs, K = 8 inputs, M = 6)
+cudaError_t launch_gemm(const float *A, int lda, int tA, const float *B, int ldb, int tB, float *C, int ldc, int M,
+                        int N, int K, const float *bias, int k_chunk, int splits, cudaStream_t s)
+{
+    if (g5_fits(M, N, K)) {
+        static bool attr = false;
+        if (!attr) {
+            const cudaError_t e = cudaFuncSetAttribute(gemm_tc05, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)G5_SMEM);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        const dim3 grid((unsigned)((N + G5_BN - 1) / G5_BN), (unsigned)((M + G5_BM - 1) / G5_BM), (unsigned)splits);
+        const int vA = !tA && (lda & 3) == 0 && aligned16(A), vB = tB && (ldb & 3) == 0 && aligned16(B);
+        gemm_tc05<<<grid, G5_THREADS, G5_SMEM, s>>>(A, lda, tA, B, ldb, tB, C, ldc, M, N, K, bias, k_chunk, vA, vB);
+    } else {
+        const dim3 grid((unsigned)((N + GT_N - 1) / GT_N), (unsigned)((M + GT_M - 1) / GT_M), (unsigned)splits);
+        gemm_tc<<<grid, 128, 0, s>>>(A, lda, tA, B, ldb, tB, C, ldc, M, N, K, bias, k_chunk);
+    }
+    return cudaGetLastError();
+}
+
 int blocks_for(int64_t n, int tb) { return (int)((n + tb - 1) / tb < 4096 ? (n + tb - 1) / tb : 4096); }
 
 }  // namespace
@@ -840,10 +1106,20 @@ extern "C" int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B,
                             int ldc, int M, int N, int K, const float *bias, void *stream)
 {
     if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0) return FFA_ERR_INVALID;
-    dim3 grid((unsigned)((N + GT_N - 1) / GT_N), (unsigned)((M + GT_M - 1) / GT_M));
-    if (grid.y > 65535) return FFA_ERR_UNSUPPORTED;
-    gemm_tc<<<grid, 128, 0, (cudaStream_t)stream>>>(A, lda, transA, B, ldb, transB, C, ldc, M, N, K, bias, K);
-    return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
+    if ((M + GT_M - 1) / GT_M > 65535) return FFA_ERR_UNSUPPORTED;
+    return launch_gemm(A, lda, transA ? 1 : 0, B, ldb, transB ? 1 : 0, C, ldc, M, N, K, bias, K, 1,
+                       (cudaStream_t)stream) == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
+}
+
+extern "C" int ffa_mlp_gemm_timeouts(int32_t *count)
+{
+    if (!count) return FFA_ERR_INVALID;
+    int v = 0;
+    FFA_CHECK_CUDA(cudaMemcpyFromSymbol(&v, g_gemm_timeouts, sizeof(int)));
+    const int zero = 0;
+    FFA_CHECK_CUDA(cudaMemcpyToSymbol(g_gemm_timeouts, &zero, sizeof(int)));
+    *count = v;
+    return FFA_OK;
 }
 
 extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
@@ -860,25 +1136,55 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     const int ew = blocks_for(B * H, 256);
     const int Bi = (int)B;
     float *part = dz + B * H;                                    // split-K partials
+    // split K over `splits` blocks per output tile (chunks a multiple of
+    // `kq`), partials in the split-K area, summed in a fixed order (+ bias)
+    auto gemm_split = [&](const float *A_, int lda_, int tA_, const float *B_, int ldb_, int tB_, float *C_, int ldc_,
+                          int M_, int N_, int K_, const float *bias_, int splits, int kq) {
+        const int kc = ((K_ + splits - 1) / splits + kq - 1) / kq * kq;
+        splits = (K_ + kc - 1) / kc;
+        if (splits <= 1) {
+            launch_gemm(A_, lda_, tA_, B_, ldb_, tB_, C_, ldc_, M_, N_, K_, bias_, K_, 1, s);
+        } else {
+            launch_gemm(A_, lda_, tA_, B_, ldb_, tB_, part, N_, M_, N_, K_, nullptr, kc, splits, s);
+            split_sum_kernel<<<(M_ * N_ + 255) / 256, 256, 0, s>>>(part, splits, M_, N_, C_, ldc_, bias_);
+        }
+    };
+    auto max_splits = [&](int M_, int N_, int cap) {
+        const int64_t room = SPLIT_WORK / ((int64_t)M_ * N_);
+        return (int)(room < cap ? room : cap);
+    };
+    // products: the tcgen05 kernel whole; the narrow ones (N = 8 outputs)
+    // split in K chunks of 64, as the partial-product area allows
     auto gemm = [&](const float *A_, int lda_, int tA_, const float *B_, int ldb_, int tB_, float *C_, int ldc_,
                     int M_, int N_, int K_, const float *bias_) {
-        const dim3 grid((unsigned)((N_ + GT_N - 1) / GT_N), (unsigned)((M_ + GT_M - 1) / GT_M));
-        gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, tA_, B_, ldb_, tB_, C_, ldc_, M_, N_, K_, bias_, K_);
-    };
-    // weight gradients (K = batch): split K over up to SPLITS_MAX blocks per
-    // output tile, partials summed in a fixed order
-    auto gemm_wgrad = [&](const float *A_, int lda_, const float *B_, int ldb_, float *C_, int ldc_, int M_, int N_) {
-        int splits = (int)((B + 1023) / 1024);
-        splits = splits < 1 ? 1 : splits > SPLITS_MAX ? SPLITS_MAX : splits;
-        const int kc = (int)(((B + splits - 1) / splits + GT_K - 1) / GT_K * GT_K);
-        splits = (int)((B + kc - 1) / kc);
-        const dim3 grid((unsigned)((N_ + GT_N - 1) / GT_N), (unsigned)((M_ + GT_M - 1) / GT_M), (unsigned)splits);
-        if (splits == 1) {
-            gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, 1, B_, ldb_, 0, C_, ldc_, M_, N_, (int)B, nullptr, kc);
-        } else {
-            gemm_tc<<<grid, 128, 0, s>>>(A_, lda_, 1, B_, ldb_, 0, part, N_, M_, N_, (int)B, nullptr, kc);
-            split_sum_kernel<<<(M_ * N_ + 255) / 256, 256, 0, s>>>(part, splits, M_, N_, C_, ldc_);
+        int splits = 1;
+        if (!g5_fits(M_, N_, K_) && K_ >= 128) {
+            splits = (K_ + 63) / 64;
+            const int cap = max_splits(M_, N_, 64);
+            splits = splits < cap ? splits : cap;
         }
+        gemm_split(A_, lda_, tA_, B_, ldb_, tB_, C_, ldc_, M_, N_, K_, bias_, splits < 1 ? 1 : splits, GT_K);
+    };
+    // weight gradients (K = batch): chunks of 512 on the tcgen05 path (up to
+    // 16 splits), 256 on gemm_tc (up to 64)
+    auto gemm_wgrad = [&](const float *A_, int lda_, const float *B_, int ldb_, float *C_, int ldc_, int M_, int N_) {
+        const bool tc05 = g5_fits(M_, N_, (int)B);
+        const int64_t per = tc05 ? 512 : 256;
+        int splits = (int)((B + per - 1) / per);
+        const int cap = max_splits(M_, N_, tc05 ? SPLITS_MAX : 64);
+        splits = splits < 1 ? 1 : splits > cap ? cap : splits;
+        gemm_split(A_, lda_, 1, B_, ldb_, 0, C_, ldc_, M_, N_, (int)B, nullptr, splits, tc05 ? G5_BK : GT_K);
+    };
+    // bias gradients: column sums in two fixed-order passes (scratch: the
+    // split-K area, free between products)
+    auto colsum = [&](const float *d_, int ncol, int ld_, float *g_) {
+        int chunks = (int)((B + 127) / 128);
+        chunks = chunks > 64 ? 64 : chunks;
+        const int64_t rows_per = (B + chunks - 1) / chunks;
+        chunks = (int)((B + rows_per - 1) / rows_per);
+        colsum_part_kernel<<<dim3((unsigned)((ncol + 31) / 32), (unsigned)chunks), 256, 0, s>>>(d_, B, ncol, ld_,
+                                                                                              rows_per, part);
+        colsum_final_kernel<<<(ncol + 7) / 8, 256, 0, s>>>(part, chunks, ncol, g_);
     };
     // forward
     layer1_kernel<<<ew, 256, 0, s>>>(d->x, P, z1, B);
@@ -892,9 +1198,9 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     // backward
     FFA_CHECK_CUDA(cudaMemsetAsync(G, 0, sizeof(float) * P_TOTAL, s));
     skip_grad_kernel<<<NOUT + 16, 256, 0, s>>>(d->x, dd, B, G);
-    colsum_kernel<<<1, 256, 0, s>>>(dd, B, NOUT, NOUT, G + P_BS);
+    colsum(dd, NOUT, NOUT, G + P_BS);
     gemm_wgrad(h3, H, dd, NOUT, G + P_W4, NOUT, H, NOUT);
-    colsum_kernel<<<1, 256, 0, s>>>(dd, B, NOUT, NOUT, G + P_B4);
+    colsum(dd, NOUT, NOUT, G + P_B4);
     gemm(dd, NOUT, 0, P + P_W4, NOUT, 1, dh, H, Bi, H, NOUT, nullptr);
     const float *zs[3] = {z3, z2, z1};
     const float *hin[3] = {h2, h1, d->x};
@@ -903,7 +1209,7 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
     for (int l = 0; l < 3; ++l) {
         dsilu_kernel<<<ew, 256, 0, s>>>(dh, zs[l], B * H);   // dh -> dz in place
         gemm_wgrad(hin[l], ldin[l], dh, H, G + wofs[l], H, kin[l], H);
-        colsum_kernel<<<H / 32, 256, 0, s>>>(dh, B, H, H, G + bofs[l]);
+        colsum(dh, H, H, G + bofs[l]);
         if (l < 2) {
             gemm(dh, H, 0, P + wofs[l], H, 1, dz, H, Bi, H, H, nullptr);
             float *t = dh;

@@ -41,10 +41,13 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("tA,tB", [(0, 0), (1, 0), (0, 1), (1, 1)])
-def test_gemm_matches_bf16_products(tA, tB):
+@pytest.mark.parametrize("Mm,Nn,Kk", [(100, 72, 40),        # narrow: the mma.sync kernel
+                                      (300, 260, 200),      # tcgen05, ragged tiles and K
+                                      (512, 256, 1024)])    # tcgen05, full tiles
+def test_gemm_matches_bf16_products(tA, tB, Mm, Nn, Kk):
+    import ctypes
     from pyffa_b200 import _lib
-    rng = np.random.default_rng(10 + 2 * tA + tB)
-    Mm, Nn, Kk = 100, 72, 40
+    rng = np.random.default_rng(10 + 2 * tA + tB + Mm)
     A = rng.standard_normal((Kk, Mm) if tA else (Mm, Kk)).astype(np.float32)
     B = rng.standard_normal((Nn, Kk) if tB else (Kk, Nn)).astype(np.float32)
     bias = rng.standard_normal(Nn).astype(np.float32)
@@ -60,6 +63,8 @@ def test_gemm_matches_bf16_products(tA, tB):
     got = C.cpu().numpy()
     assert np.all(np.isfinite(got))
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+    cnt = ctypes.c_int32(-1)
+    assert _lib.lib().ffa_mlp_gemm_timeouts(ctypes.byref(cnt)) == 0 and cnt.value == 0
 
 
 def _train_inputs(seed, B):
