@@ -361,8 +361,10 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     0.5 mm Gaussian offsets, all in one bunch through the FP32C Boris pusher
     (RF off), 200 turns of the slowest instance per iteration, float64
     one-turn-map fit and fixed-point update per instance; the push's launch
-    shape picked by the autotuner on the scan's bunch first; iteration 1
-    direct, iteration 2 captured as a CUDA graph, later ones replays.  2880 steps per
+    shape picked by the autotuner on the scan's bunch first; each iteration
+    one push launch over all its steps (crossing records in one device
+    buffer); iteration 1 direct, iteration 2 captured as a CUDA graph, later
+    ones replays.  2880 steps per
     turn of the fastest instance: at 720 the 2.8-degree D magnet gets five
     steps and the motion is not regular enough for a tune."""
     import torch
@@ -394,6 +396,8 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
             "steps_per_iteration": scan.steps, "steps_per_turn_fastest": steps_per_turn, "iterations": len(recs),
             "ms_per_iteration": [r["ms"] for r in recs], "modes": [r["mode"] for r in recs],
             "push_launches_per_iteration": recs[-1]["launches"],
+            "steps_per_launch": scan._dev_state.L,
+            "crossing_buffer_gb": scan._dev_state.cap.buf.numel() * 8 / 1e9,
             "max_abs_dr_m": [r["max_abs_dr"] for r in recs],
             "orbit_vs_scaling_law_m": float(np.abs(scan.r - r_sc).max()),
             "Qr_frac_range": [float(np.nanmin(q[:, 0])), float(np.nanmax(q[:, 0]))],

@@ -65,6 +65,11 @@ def crossing_states(rec, dt, iterations=3):
     return torch.stack([X, VX, Z, VZ], 1)
 
 
+def _lib_record_bytes():
+    from . import _lib
+    return 8 * _lib.CROSSING_RECORD
+
+
 def accumulate_crossings(p, step, x, gv, inst, nsteps, last, has, S, Y, crossings, scale=None):
     """Adds one launch's crossings to the per-instance sums.
 
@@ -184,12 +189,20 @@ class BatchedOrbitScan:
     (autotune.tune_push; `tuning` holds the table), else the default; shapes
     whose states differ from the default's by more than tune_rtol (relative)
     on the tuning run are not chosen.  The scan fits maps to many crossings,
-    so rounding-level differences (1e-11) are accepted by default."""
+    so rounding-level differences (1e-11) are accepted by default.
+    persistent: the whole iteration is one push launch, its crossing records
+    held in one device buffer (about 1.8 KB per particle and turn-bound of
+    crossings: 10 GB for 162k particles over 200 turns), when that buffer and
+    the accumulation's temporaries (taken as 3x the buffer) fit in half the
+    free device memory; otherwise, and with persistent=False, launches of the
+    longest length whose records fit that memory (at most 5 records per
+    particle without `persistent`)."""
 
     def __init__(self, gp, energies, counts, r0, pr0, perimeter, sigma=0.5e-3, steps_per_turn=720, turns=200,
-                 seed=0, device=None, autotune=True, tune_steps=1000, tune_rtol=1e-9):
+                 seed=0, device=None, autotune=True, tune_steps=1000, tune_rtol=1e-9, persistent=True):
         import torch
         self.gp = gp
+        self.persistent = bool(persistent)
         self.autotune = bool(autotune)
         self.tune_steps = int(tune_steps)
         self.tune_rtol = float(tune_rtol)
@@ -256,7 +269,7 @@ class BatchedOrbitScan:
         st.clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
         st.clock.ensure(self.steps + 1)
         st.cap = CrossingCapture(st.bunch, [0.0], self.gp, self.dt)
-        st.L = st.cap.max_steps()
+        st.L = self._launch_steps(st.cap)
         st.xing = st.cap.prepare(st.L)
         st.rows = st.cap.buf.view(-1, 23)[:st.cap.x.capacity]
         unit = np.ones((self.I + 1, 4))
@@ -293,6 +306,27 @@ class BatchedOrbitScan:
                                  reset=reset, count=st.cap.count, rtol=self.tune_rtol)
         st.pusher.shape = res.best
         self.tuning = res
+
+    def _launch_steps(self, cap):
+        """Steps per push launch: the whole iteration when its records fit
+        (see the class notes), else the longest launch that fits."""
+        import torch
+        short = cap.max_steps()
+        if not self.persistent:
+            return min(short, self.steps)
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        budget = free // 2
+
+        def need(L):    # record buffer + 3x for the accumulation's temporaries
+            per = 2 + int(np.ceil(L * cap.dt * cap.f_max / (2 * np.pi)))
+            return 4 * cap.bunch.n * cap.x.ntargets * per * _lib_record_bytes()
+        if need(self.steps) <= budget:
+            return self.steps
+        lo, hi = min(short, self.steps), self.steps
+        while hi - lo > 1:                  # longest launch within the budget
+            mid = (lo + hi) // 2
+            lo, hi = (mid, hi) if need(mid) <= budget else (lo, mid)
+        return lo
 
     def _body(self):
         """The work of one iteration, enqueued on the scan's stream: AoS ->

@@ -60,3 +60,34 @@ def test_batched_scan_orbits_and_tunes():
     rec = check.iterate(graph=False)  # the direct path: per-launch record counts
     assert rec["mode"] == "direct"
     assert rec["good"].all() and rec["max_abs_dr"] < 3e-6, rec["max_abs_dr"]
+
+
+def test_one_launch_and_many_launches_agree():
+    """The persistent iteration (one push launch, all records in one buffer)
+    and the same iteration in launches of at most 5 records per particle give
+    the same orbit update (to rounding: a launch boundary re-forms 1 / r)."""
+    from pyffa_b200 import coscan, synthetic
+    from pyffa_b200.constants import FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical, FFAG_EField_new
+    cfg = synthetic.lattice_bmap(r_range=(7.9, 9.3, 0.002), theta_step_deg=0.02)
+    bm = FFAG_Bfield_analytical(config=cfg, max_order=2, stacks=synthetic.taylor_stacks(cfg, 2))
+    em = FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=False)
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(bm)
+    gp.AddEMap(em)
+    d = synthetic.design(300.0)
+    E = np.array([300.0, 450.0, 600.0])
+    k = cfg["Bmap"]["coefficients_tupel"][1]
+    scale = (synthetic.momentum(E) / synthetic.momentum(300.0)) ** (1 / (k + 1))
+    out = []
+    for persistent in (True, False):
+        scan = coscan.BatchedOrbitScan(gp, E, [16, 40, 9], d["r0"] * scale + 2e-4, np.full(3, np.arctan(d["pr0"])),
+                                       d["perimeter"] * scale, sigma=0.5e-3, turns=20, seed=6, steps_per_turn=2880,
+                                       autotune=False, persistent=persistent)
+        rec = scan.iterate(graph=False)
+        out.append((rec, scan.r.copy(), scan._dev_state.launches))
+    (a, ra, la), (b, rb, lb) = out
+    assert la == 1 and lb > 1, (la, lb)
+    assert np.array_equal(a["crossings"], b["crossings"])
+    assert np.abs(ra - rb).max() < 1e-9, ra - rb
+    assert np.abs(a["tunes"] - b["tunes"]).max() < 1e-7
