@@ -111,3 +111,41 @@ def test_crossing_states_exact_on_straight_lines():
     lin = rec[:, 4] + (rec[:, 11] - rec[:, 4]) * (-(rec[:, 8] - 2 * math.pi * (rec[:, 8] > 3)) /
                                                   (rec[:, 15] - rec[:, 8] + 2 * math.pi * (rec[:, 8] > 3)))
     assert np.abs(lin.numpy() - want[:, 0]).max() > 1e-5
+
+
+def test_launch_steps_persistent_and_memory_bound(monkeypatch):
+    """One launch per iteration when the records fit half the free device
+    memory (with 3x for the accumulation), else the longest launch that
+    does; persistent=False keeps the 5-records-per-particle launches."""
+    import torch
+    from pyffa_b200 import _lib
+
+    class Cap:                       # a CrossingCapture's sizing fields
+        def __init__(self, n, dt, f_max):
+            self.bunch = type("B", (), {"n": n})()
+            self.x = type("X", (), {"ntargets": 1})()
+            self.dt, self.f_max = dt, f_max
+
+        def max_steps(self):
+            return max(1, int(3 * 2 * np.pi / (self.dt * self.f_max)))
+
+    def need(cap, L):
+        per = 2 + int(np.ceil(L * cap.dt * cap.f_max / (2 * np.pi)))
+        return 4 * cap.bunch.n * per * 8 * _lib.CROSSING_RECORD
+
+    cap = Cap(162321, 8.2e-11, 3.79e7)
+    scan = object.__new__(coscan.BatchedOrbitScan)
+    scan.dev, scan.steps = "cuda:0", 666804
+    scan.persistent = True
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (180 << 30, 180 << 30))
+    assert scan._launch_steps(cap) == scan.steps                       # 180 GB free: one launch
+    free = 2 * need(cap, 100000)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (free, free))
+    L = scan._launch_steps(cap)
+    assert cap.max_steps() < L < scan.steps
+    assert need(cap, L) <= free // 2 < need(cap, L + 1)                # the longest that fits
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (0, 0))
+    assert scan._launch_steps(cap) == cap.max_steps()                  # nothing free: the short launches
+    scan.persistent = False
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (180 << 30, 180 << 30))
+    assert scan._launch_steps(cap) == cap.max_steps()
