@@ -87,6 +87,19 @@ class StateSoA(C.Structure):
     ]
 
 
+_SOA_ELEM = {"inj": 1, "surv": 1, "sc_pre": 1, "sc_pp": 1, "inj_step": 4}   # bytes; the rest float64
+
+
+def soa_offset(st: "StateSoA", start: int) -> "StateSoA":
+    """The SoA view of particles start.. of `st` (every non-null column
+    pointer advanced by start elements)."""
+    out = StateSoA()
+    for name, _ in StateSoA._fields_:
+        p = getattr(st, name)
+        setattr(out, name, None if not p else p + start * _SOA_ELEM.get(name, 8))
+    return out
+
+
 class StepTable(C.Structure):
     _fields_ = [("drf", d_p), ("acc", d_p), ("nsteps", C.c_int64)]
 

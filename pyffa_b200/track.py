@@ -128,13 +128,21 @@ class Pusher:
         # Boris kernels; (0, 0) is the default, autotune.tune_push picks others
         self.shape = (0, 0)
 
-    def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0, xing=None) -> None:
+    def push(self, clock: StepClock, step0: int, nsteps: int, sc_step: int = 0, xing=None, start: int = 0,
+             count=None, stream=None) -> None:
+        """Advances particles [start, start + count) (default: all) by nsteps
+        steps from absolute step step0 on `stream` (default: the pusher's)."""
         L = _lib.lib()
         b = self.bunch
         flags = self.flags | _lib.shape_flags(*self.shape)
+        n = b.n - start if count is None else count
+        if start < 0 or n < 0 or start + n > b.n:
+            raise ValueError(f"particle range [{start}, {start + n}) outside the bunch of {b.n}")
+        soa = b.soa() if start == 0 else _lib.soa_offset(b.soa(), start)
+        s = (self.stream if stream is None else stream).cuda_stream
         args = (self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
-                ctypes.byref(clock.table), ctypes.byref(b.soa()), b.n, step0, nsteps, clock.dt,
-                sc_step, flags, self.stream.cuda_stream, b.status.data_ptr())
+                ctypes.byref(clock.table), ctypes.byref(soa), n, step0, nsteps, clock.dt,
+                sc_step, flags, s, b.status.data_ptr())
         if xing is None:
             _lib.check(L.ffa_push(*args), "ffa_push")
         else:
@@ -456,9 +464,15 @@ class MatrixTracker:
     in host memory by `nsteps` fused steps and writes the result back (the
     call a host-side caller of Boris_solve / rk4_step makes, batched over
     steps).  Device buffers are allocated once; each call copies the matrix
-    in, converts it to SoA, pushes, converts back and copies it out."""
+    in, converts it to SoA, pushes, converts back and copies it out.
 
-    def __init__(self, n, gp, solver="Boris", precision="fp64", device=None):
+    chunks > 1 splits the bunch into that many particle ranges (multiples of
+    32), each on its own stream: one range's host copies overlap another's
+    push, and the pushes of all ranges are resident together, so the push
+    itself is not slowed.  Every particle sees the same arithmetic either
+    way."""
+
+    def __init__(self, n, gp, solver="Boris", precision="fp64", device=None, chunks=2):
         import torch
         self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.n = n
@@ -469,19 +483,47 @@ class MatrixTracker:
         self.pusher = Pusher(self.b, gp, solver, precision)
         self.clock = None
         self.launches = 0
+        k = max(1, min(int(chunks), max(1, n // 32)))
+        edges = [0] + [((n * c) // k) // 32 * 32 for c in range(1, k)] + [n]
+        self.spans = [(a, e) for a, e in zip(edges[:-1], edges[1:]) if e > a]
+        self.streams = [torch.cuda.Stream(self.dev) for _ in self.spans] if len(self.spans) > 1 else []
 
     def bind_clock(self, t_start, dt, nsteps_total):
         self.clock = StepClock(t_start, dt, self.gp.Emap, self.solver, self.dev)
         self.clock.ensure(nsteps_total)
 
     def run(self, host_in, host_out, step0, nsteps):
-        """host_in / host_out: pinned (or pageable) float64 torch tensors (n, 16)."""
+        """host_in / host_out: pinned (or pageable) float64 torch tensors (n, 16).
+        The work is ordered after what the pusher's stream holds, and that
+        stream waits for it (synchronise it to read host_out)."""
+        import torch
         L = _lib.lib()
         b = self.b
-        s = self.pusher.stream.cuda_stream
-        b.aos.copy_(host_in, non_blocking=True)
-        _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), s), "ffa_aos_to_soa")
-        self.pusher.push(self.clock, step0, nsteps, 0)
-        _lib.check(L.ffa_soa_to_aos(ctypes.byref(b.soa()), b.n, b.aos.data_ptr(), s), "ffa_soa_to_aos")
-        host_out.copy_(b.aos, non_blocking=True)
-        self.launches += 3
+        main = self.pusher.stream
+        if not self.streams:
+            s = main.cuda_stream
+            b.aos.copy_(host_in, non_blocking=True)
+            _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), s), "ffa_aos_to_soa")
+            self.pusher.push(self.clock, step0, nsteps, 0)
+            _lib.check(L.ffa_soa_to_aos(ctypes.byref(b.soa()), b.n, b.aos.data_ptr(), s), "ffa_soa_to_aos")
+            host_out.copy_(b.aos, non_blocking=True)
+            self.launches += 3
+            return
+        ready = torch.cuda.Event()
+        ready.record(main)
+        row = b.aos.stride(0) * b.aos.element_size()
+        for (a, e), st in zip(self.spans, self.streams):
+            st.wait_event(ready)
+            soa = _lib.soa_offset(b.soa(), a)
+            with torch.cuda.stream(st):
+                b.aos[a:e].copy_(host_in[a:e], non_blocking=True)
+                _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr() + a * row, e - a, ctypes.byref(soa), st.cuda_stream),
+                           "ffa_aos_to_soa")
+                self.pusher.push(self.clock, step0, nsteps, 0, start=a, count=e - a, stream=st)
+                _lib.check(L.ffa_soa_to_aos(ctypes.byref(soa), e - a, b.aos.data_ptr() + a * row, st.cuda_stream),
+                           "ffa_soa_to_aos")
+                host_out[a:e].copy_(b.aos[a:e], non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(st)
+            main.wait_event(done)
+            self.launches += 3

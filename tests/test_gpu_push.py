@@ -190,3 +190,47 @@ def test_status_counts_losses(golden):
     ref = golden["borisloop_out"]
     assert rk.last_run["status"]["lost"] == int(((ref[:, 7] == 1) & (ref[:, 8] == 0)).sum())
     assert rk.last_run["status"]["nan"] == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_host_matrix_entry_point_matches_device_push(full_lattice, precision):
+    """MatrixTracker (host matrix in, one call, host matrix out) gives the
+    device push's result bit for bit, with one stream and with the bunch
+    split over two streams (copies of one half overlapping the other's
+    push); a ragged size exercises the split at a multiple of 32."""
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.track import MatrixTracker, Pusher, StepClock, _EphemeralBunch
+    gp = full_lattice
+    n = 3001
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(synthetic.centred_bunch(n, seed=11))
+    v[:, 7] = 1.0
+    v[:, 8] = 1.0
+    v[:, 9] = 0.3
+    dt = synthetic.design_dt(300.0, 720)
+    dev = torch.device("cuda", 0)
+    b = _EphemeralBunch(v.copy(), "Boris", dev)
+    pu = Pusher(b, gp, "Boris", precision)
+    clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
+    clock.ensure(2 * 720)
+    pu.push(clock, 0, 720, 0)
+    pu.push(clock, 720, 720, 0)
+    torch.cuda.synchronize()
+    ref = b.matrix()
+    for chunks in (1, 2):
+        mt = MatrixTracker(n, gp, "Boris", precision, device=dev, chunks=chunks)
+        mt.bind_clock(0.0, dt, 2 * 720)
+        assert len(mt.spans) == chunks and all(a % 32 == 0 for a, _ in mt.spans)
+        h = [torch.from_numpy(v.copy()).pin_memory(), torch.zeros((n, 16), dtype=torch.float64).pin_memory()]
+        mt.run(h[0], h[1], 0, 720)
+        mt.run(h[1], h[0], 720, 720)
+        mt.pusher.stream.synchronize()
+        got = h[0].numpy()
+        cols = [0, 1, 2, 3, 4, 5, 7, 8, 9, 10, 11, 12]
+        assert np.array_equal(got[:, cols], ref[:, cols]), chunks
+        assert int(mt.b.status[_lib_status_lost()].item()) == int(b.status[_lib_status_lost()].item())
+
+
+def _lib_status_lost():
+    from pyffa_b200 import _lib
+    return _lib.STATUS_LOST
