@@ -384,6 +384,14 @@ typedef struct ffa_mlp_train_desc {
     const float *x, *target;      /* device [batch][8] */
     float *work;
     double *loss_part;
+    /* Optional device schedule (both or neither): the step takes its
+     * learning rate from lr_table[*counter] and is Adam step *counter + 1
+     * (bias corrections formed on the device), then increments *counter;
+     * lr and step above are then ignored and the update always runs.  With
+     * nothing read from the host per step, the call can be captured once in
+     * a CUDA graph and replayed. */
+    const float *lr_table;
+    int32_t *counter;
 } ffa_mlp_train_desc;
 
 int ffa_mlp_train_step(const ffa_mlp_train_desc *desc, void *stream);

@@ -141,7 +141,8 @@ class MlpTrainDesc(C.Structure):
     _fields_ = [("batch", C.c_int64), ("n_fit", C.c_int32), ("step", C.c_int32),
                 ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
                 ("params", d_p), ("grads", d_p), ("adam_m", d_p), ("adam_v", d_p), ("mask", d_p),
-                ("x", d_p), ("target", d_p), ("work", d_p), ("loss_part", d_p)]
+                ("x", d_p), ("target", d_p), ("work", d_p), ("loss_part", d_p),
+                ("lr_table", d_p), ("counter", d_p)]
 
 
 class MlpInferDesc(C.Structure):

@@ -359,6 +359,27 @@ __global__ void adam_kernel(float *P, const float *G, float *m, float *v, int64_
     }
 }
 
+// Adam with the step read from the device: learning rate lr_table[*counter],
+// bias corrections of step *counter + 1
+__global__ void adam_sched_kernel(float *P, const float *G, float *m, float *v, int64_t n, const float *lr_table,
+                                  const int32_t *counter, float b1, float b2, float eps, const uint8_t *mask)
+{
+    const int k = *counter;
+    const float lr = lr_table[k], t = (float)(k + 1);
+    const float c1 = 1.0f - powf(b1, t), c2 = 1.0f - powf(b2, t);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (mask && !mask[i]) continue;
+        const float g = G[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * g;
+        const float vi = b2 * v[i] + (1.0f - b2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        P[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void counter_advance_kernel(int32_t *counter) { *counter += 1; }
+
 // ------------------------------------------------------- fused inference
 // 8 warps x 16 particles.  Shared: W2^T as bf16 [n][k + 8] (k padded against
 // bank conflicts), W1^T [n][16], W4^T [8][k + 8], biases, skip layer, the
@@ -1125,8 +1146,11 @@ extern "C" int ffa_mlp_gemm_timeouts(int32_t *count)
 extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
 {
     if (!d || !d->params || !d->grads || !d->adam_m || !d->adam_v || !d->x || !d->target || !d->work ||
-        !d->loss_part || d->batch <= 0 || d->n_fit < 1 || d->n_fit > 6 || (d->lr > 0.0f && d->step < 1))
+        !d->loss_part || d->batch <= 0 || d->n_fit < 1 || d->n_fit > 6)
         return FFA_ERR_INVALID;
+    const bool sched = d->lr_table != nullptr;
+    if (sched != (d->counter != nullptr)) return FFA_ERR_INVALID;
+    if (!sched && d->lr > 0.0f && d->step < 1) return FFA_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t B = d->batch;
     if (B > 65535LL * GT_M || B * H > INT32_MAX) return FFA_ERR_UNSUPPORTED;
@@ -1217,7 +1241,11 @@ extern "C" int ffa_mlp_train_step(const ffa_mlp_train_desc *d, void *stream)
             dz = t;
         }
     }
-    if (d->lr > 0.0f) {
+    if (sched) {
+        adam_sched_kernel<<<blocks_for(P_TOTAL, 256), 256, 0, s>>>(P, G, d->adam_m, d->adam_v, P_TOTAL, d->lr_table,
+                                                                   d->counter, d->beta1, d->beta2, d->eps, d->mask);
+        counter_advance_kernel<<<1, 1, 0, s>>>(d->counter);
+    } else if (d->lr > 0.0f) {
         const float c1 = 1.0f - powf(d->beta1, (float)d->step), c2 = 1.0f - powf(d->beta2, (float)d->step);
         adam_kernel<<<blocks_for(P_TOTAL, 256), 256, 0, s>>>(P, G, d->adam_m, d->adam_v, P_TOTAL, d->lr, d->beta1,
                                                              d->beta2, d->eps, c1, c2, d->mask);

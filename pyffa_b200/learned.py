@@ -362,12 +362,22 @@ def fit_skip(params, X, T, n_fit=4, max_rows=1 << 22, order=2):
 
 
 class Trainer:
-    """Adam on the tensor-core forward/backward (ffa_mlp_train_step)."""
+    """Adam on the tensor-core forward/backward (ffa_mlp_train_step).
 
-    def __init__(self, params, batch=8192, n_fit=4, freeze_skip=True, beta1=0.9, beta2=0.999, eps=1e-8):
+    lr_table (device float32, one learning rate per step) switches to the
+    device schedule: step k takes lr_table[k] and Adam's bias corrections of
+    step k + 1 from a device counter, so that graph_step can replay one
+    captured CUDA graph of the whole step (about 30 launches) with nothing
+    read from the host; step() then ignores its lr argument."""
+
+    def __init__(self, params, batch=8192, n_fit=4, freeze_skip=True, beta1=0.9, beta2=0.999, eps=1e-8,
+                 lr_table=None):
         torch = _torch()
         self.p = params
         dev = params.device
+        self.lr_table = None if lr_table is None else lr_table.to(device=dev, dtype=torch.float32).contiguous()
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev) if lr_table is not None else None
+        self._graph = None
         self.B, self.n_fit = int(batch), int(n_fit)
         self.g = torch.zeros_like(params)
         self.m = torch.zeros_like(params)
@@ -385,10 +395,10 @@ class Trainer:
 
     def step(self, x, t, lr):
         """One step on the batch x, t ((B, 8) float32, contiguous); lr = 0
-        computes loss and gradients only."""
+        computes loss and gradients only (host schedule)."""
         torch = _torch()
         assert x.shape[0] == self.B and x.is_contiguous() and t.is_contiguous()
-        if lr > 0:
+        if lr > 0 or self.lr_table is not None:
             self.t += 1
         d = _lib.MlpTrainDesc()
         d.batch, d.n_fit, d.step = self.B, self.n_fit, max(self.t, 1)
@@ -398,8 +408,35 @@ class Trainer:
         d.mask = self.mask.data_ptr()
         d.x, d.target = x.data_ptr(), t.data_ptr()
         d.work, d.loss_part = self.work.data_ptr(), self.loss_part.data_ptr()
+        if self.lr_table is not None:
+            d.lr_table, d.counter = self.lr_table.data_ptr(), self.counter.data_ptr()
         stream = torch.cuda.current_stream(self.p.device).cuda_stream
         _lib.check(_lib.lib().ffa_mlp_train_step(ctypes.byref(d), stream), "ffa_mlp_train_step")
+        self.launches += 1
+
+    def graph_step(self, x, t):
+        """step() under the device schedule through a CUDA graph: the batch
+        is copied into fixed buffers and the graph of one step replayed.  The
+        first call runs the step directly (it also sets the kernels up) and
+        captures the next one."""
+        torch = _torch()
+        if self.lr_table is None:
+            raise ValueError("graph_step needs the device schedule (lr_table)")
+        if self._graph is None:
+            self._xb, self._tb = x.clone(), t.clone()
+            self.step(self._xb, self._tb, 0.0)
+            torch.cuda.current_stream(self.p.device).synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.step(self._xb, self._tb, 0.0)
+            self.t -= 1                       # capturing ran nothing
+            self.launches -= 1
+            self._graph = g
+            return
+        self._xb.copy_(x)
+        self._tb.copy_(t)
+        self._graph.replay()
+        self.t += 1
         self.launches += 1
 
     def mse(self):
@@ -428,7 +465,7 @@ def residual_scale(params, X, T, n_fit=4, chunk=1 << 21):
 
 
 def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200, seed=0, n_fit=4,
-          log_every=0, time_limit=None, eps=1e-8, out_scale="auto", chunk=1 << 21):
+          log_every=0, time_limit=None, eps=1e-8, out_scale="auto", chunk=1 << 21, graph=True):
     """Second-order skip connection by least squares, then Adam on the MLP
     with a cosine learning rate.
 
@@ -436,8 +473,11 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
     `out_scale` (by default the power of two nearest its rms), so that its
     output is of order one and the optimiser's step noise on W4 and b4 is
     not of the residual's own size; the scale is folded into W4 and b4 at the
-    end (exactly: a power of two).  Returns the history [(step, mse)] of the
-    scaled problem (sampled when log_every > 0) and the trainer."""
+    end (exactly: a power of two).  graph: the learning-rate schedule as a
+    device table and every step after the first a replay of one captured
+    CUDA graph (Trainer.graph_step); else one host-scheduled call per step.
+    Returns the history [(step, mse)] of the scaled problem (sampled when
+    log_every > 0) and the trainer."""
     torch = _torch()
     fit_skip(params, X, T, n_fit)
     sigma = residual_scale(params, X, T, n_fit, chunk) if out_scale == "auto" else float(out_scale or 1.0)
@@ -447,11 +487,16 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
             sk = skip_map(params, X[a:a + chunk], n_fit)
             Tn[a:a + chunk, :n_fit] = (sk + (T[a:a + chunk, :n_fit].double() - sk) / sigma).float()
         T = Tn
-    tr = Trainer(params, batch=batch, n_fit=n_fit, eps=eps)
-    tr.out_scale = sigma
     n = X.shape[0]
     nb = n // batch
     total = max(1, epochs * nb)
+    # the learning-rate schedule (cosine with a linear warm-up) as a device table
+    kk = np.arange(total)
+    sched = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * kk / total))
+    sched = np.where(kk < warmup, sched * (kk + 1) / warmup, sched)
+    tr = Trainer(params, batch=batch, n_fit=n_fit, eps=eps,
+                 lr_table=torch.from_numpy(sched.astype(np.float32)) if graph else None)
+    tr.out_scale = sigma
     g = torch.Generator(device=X.device)
     g.manual_seed(seed)
     hist = []
@@ -462,11 +507,10 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
         perm = torch.randperm(n, device=X.device, generator=g)
         Xs, Ts = X[perm].contiguous(), T[perm].contiguous()
         for i in range(nb):
-            frac = k / total
-            lr_k = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * frac))
-            if k < warmup:
-                lr_k *= (k + 1) / warmup
-            tr.step(Xs[i * batch:(i + 1) * batch], Ts[i * batch:(i + 1) * batch], lr_k)
+            if graph:
+                tr.graph_step(Xs[i * batch:(i + 1) * batch], Ts[i * batch:(i + 1) * batch])
+            else:
+                tr.step(Xs[i * batch:(i + 1) * batch], Ts[i * batch:(i + 1) * batch], float(sched[k]))
             k += 1
             if log_every and k % log_every == 0:
                 hist.append((k, tr.mse()))

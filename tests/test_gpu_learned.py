@@ -250,3 +250,36 @@ def test_learned_map_gain_tunes_and_emittance(lattice):
     assert out["learned"][0] <= 1e-4, out
     assert out["learned"][2] <= 1e-2, out
     assert out["learned"][0] < out["second-order"][0] / 5, out
+
+
+def test_graph_training_matches_eager():
+    """The device-scheduled step replayed from one captured CUDA graph gives
+    the parameters of the same steps run directly, bit for bit, and the
+    device counter has advanced once per step."""
+    from pyffa_b200 import learned
+    B, steps = 512, 9
+    rng = np.random.default_rng(21)
+    X = np.zeros((B * steps, 8), np.float32)
+    X[:, :5] = rng.uniform(-1, 1, (B * steps, 5))
+    T = X.copy()
+    T[:, :5] += 0.05 * rng.standard_normal((B * steps, 5)).astype(np.float32)
+    dX, dT = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    p0 = torch.from_numpy(learned.init_params(3)).cuda()
+    table = torch.linspace(1e-3, 2e-4, steps)
+    out = []
+    for graph in (False, True):
+        p = p0.clone()
+        tr = learned.Trainer(p, batch=B, lr_table=table)
+        for i in range(steps):
+            xb, tb = dX[i * B:(i + 1) * B], dT[i * B:(i + 1) * B]
+            if graph:
+                tr.graph_step(xb, tb)
+            else:
+                tr.step(xb.contiguous(), tb.contiguous(), 0.0)
+        torch.cuda.synchronize()
+        assert int(tr.counter.item()) == steps and tr.t == steps
+        out.append((p.cpu().numpy(), tr.m.cpu().numpy(), tr.loss_part.cpu().numpy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert not np.array_equal(out[0][0], p0.cpu().numpy())          # the steps did move the parameters
