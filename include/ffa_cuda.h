@@ -201,7 +201,8 @@ int ffa_push(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *
 /* Resident blocks per SM and threads per block of the push kernel that
  * ffa_push / ffa_push_crossing (crossing != 0) would launch for `flags` and
  * a field map of `max_order`, without space charge (the runtime's occupancy
- * calculator; needs a device).  For the launch-shape autotuner's report. */
+ * calculator; needs a device).  For the launch-shape autotuner's report.
+ * No counterpart in the reference, whose Numba kernels have no launch shape. */
 int ffa_push_occupancy(int32_t flags, int32_t max_order, int32_t crossing, int32_t *blocks_per_sm,
                        int32_t *threads_per_block);
 
@@ -405,7 +406,9 @@ int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, i
 
 /* Tensor-core GEMM tiles (ffa_mlp_gemm, ffa_mlp_train_step) whose bounded
  * pipeline waits ran out since the last call (their output tiles hold NaN);
- * reads and clears the device counter, synchronising the device. */
+ * reads and clears the device counter, synchronising the device.  No
+ * counterpart in the reference (its training path does not exist; the
+ * learned map is new). */
 int ffa_mlp_gemm_timeouts(int32_t *count);
 
 /* Inference weights: the bfloat16 packing of a parameter block into `wpack`
