@@ -464,6 +464,14 @@ def residual_scale(params, X, T, n_fit=4, chunk=1 << 21):
     return 2.0 ** round(math.log2(rms)) if rms > 0 else 1.0
 
 
+def lr_schedule(total, lr, lr_min, warmup):
+    """Learning rate of steps 0..total-1: cosine from lr to lr_min over the
+    run, times (k + 1) / warmup for the first `warmup` steps (float64)."""
+    kk = np.arange(int(total))
+    sched = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * kk / max(int(total), 1)))
+    return np.where(kk < warmup, sched * (kk + 1) / warmup, sched)
+
+
 def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200, seed=0, n_fit=4,
           log_every=0, time_limit=None, eps=1e-8, out_scale="auto", chunk=1 << 21, graph=True):
     """Second-order skip connection by least squares, then Adam on the MLP
@@ -490,10 +498,7 @@ def train(params, X, T, epochs=10, batch=8192, lr=2e-3, lr_min=1e-5, warmup=200,
     n = X.shape[0]
     nb = n // batch
     total = max(1, epochs * nb)
-    # the learning-rate schedule (cosine with a linear warm-up) as a device table
-    kk = np.arange(total)
-    sched = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * kk / total))
-    sched = np.where(kk < warmup, sched * (kk + 1) / warmup, sched)
+    sched = lr_schedule(total, lr, lr_min, warmup)
     tr = Trainer(params, batch=batch, n_fit=n_fit, eps=eps,
                  lr_table=torch.from_numpy(sched.astype(np.float32)) if graph else None)
     tr.out_scale = sigma

@@ -137,3 +137,16 @@ def test_sample_domain_uniform_in_disc():
         # uniform in the disc: r^2 is uniform on [0, 1]
         assert abs(np.mean(r2) - 0.5) < 0.01
     assert s[:, 4].min() >= -1 and s[:, 4].max() <= 1
+
+
+def test_lr_schedule_cosine_with_warmup():
+    total, lr, lr_min, warmup = 1000, 2e-3, 1e-5, 200
+    s = learned.lr_schedule(total, lr, lr_min, warmup)
+    assert s.shape == (total,)
+    for k in (0, 1, 199, 200, 500, 999):
+        ref = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * k / total))
+        if k < warmup:
+            ref *= (k + 1) / warmup
+        assert abs(s[k] - ref) <= 1e-15 * lr
+    assert s[warmup - 1] > s[0] and np.all(np.diff(s[warmup:]) < 0)
+    assert s.min() > 0
