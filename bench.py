@@ -693,6 +693,11 @@ def main():
         # chosen shape timed like the default one
         from pyffa_b200 import autotune
         tune = autotune.tune_push(pu32, clock, args.warmup * STEPS_PER_TURN, STEPS_PER_TURN, reset=restore)
+        if world > 1:    # every rank times rank 0's choice (the same collectives on every rank)
+            choice = torch.tensor(list(tune.best), dtype=torch.int64, device=dev)
+            dist.broadcast(choice, 0)
+            tune.best = (int(choice[0].item()), int(choice[1].item()))
+            tune.best_ms = next(r["ms"] for r in tune.rows if r["shape"] == tune.best)
         tuned = {"shape": tune.report()["chosen"], "tuner_speedup": tune.speedup,
                  "candidates": _tune_rows(tune)}
         if tune.best != (0, 0):
@@ -766,23 +771,26 @@ def main():
                        "traffic": None}
         roof["traffic"] = BORIS_TRAFFIC_PER_LAUNCH if args.n == N_PARTICLES and args.precision == "fp64" else None
         roof["hbm"]["traffic"] = roof["traffic"]
+        # the CPU baseline and the other workloads' legs at N = 1 only: with
+        # more ranks they would hold every GPU while the others wait
+        solo = world == 1
         cpu = None
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and solo:
             cpu = cpu_baseline(gp, v, dt)
         sc = None
-        if not args.no_sc:
+        if not args.no_sc and solo:
             sc = sc_bench(gp, dt, dev)
         mg = None
-        if not args.no_mapgen:
+        if not args.no_mapgen and solo:
             mg = mapgen_bench(dev, hbm_peak)
         scan = None
-        if not args.no_scan:
+        if not args.no_scan and solo:
             scan = seo_scan_bench(dev)
         csp = None
-        if not args.no_coscan:
+        if not args.no_coscan and solo:
             csp = coscan_bench(gp, dev)
         lrn = None
-        if not args.no_learned:
+        if not args.no_learned and solo:
             lrn = learned_bench(dev, value / world, fp32c["value"] / world if fp32c else None,
                                 samples=args.learned_samples, epochs=args.learned_epochs, n=args.learned_n)
         line = {
