@@ -459,6 +459,16 @@ class _EphemeralBunch:
         return self.aos.cpu().numpy()
 
 
+def split_spans(n: int, chunks: int) -> list:
+    """[start, end) ranges that cover 0..n in order: every start a multiple
+    of 32 (edges rounded down to whole warps, the last range taking the
+    remainder, so sizes differ by less than 64), no empty range, at most
+    `chunks` of them (fewer when n has fewer warps)."""
+    k = max(1, min(int(chunks), max(1, n // 32)))
+    edges = [0] + [((n * c) // k) // 32 * 32 for c in range(1, k)] + [n]
+    return [(a, e) for a, e in zip(edges[:-1], edges[1:]) if e > a]
+
+
 class MatrixTracker:
     """Host-buffer entry point: advances an N x 16 v-format matrix that lives
     in host memory by `nsteps` fused steps and writes the result back (the
@@ -483,9 +493,7 @@ class MatrixTracker:
         self.pusher = Pusher(self.b, gp, solver, precision)
         self.clock = None
         self.launches = 0
-        k = max(1, min(int(chunks), max(1, n // 32)))
-        edges = [0] + [((n * c) // k) // 32 * 32 for c in range(1, k)] + [n]
-        self.spans = [(a, e) for a, e in zip(edges[:-1], edges[1:]) if e > a]
+        self.spans = split_spans(n, chunks)
         self.streams = [torch.cuda.Stream(self.dev) for _ in self.spans] if len(self.spans) > 1 else []
 
     def bind_clock(self, t_start, dt, nsteps_total):

@@ -181,3 +181,16 @@ def test_two_rank_split_and_reductions_gloo():
     for rank, vals, tmax in res:
         assert vals == [1001, 1001 - expect_lost]
         assert tmax == 2.0
+
+
+@pytest.mark.parametrize("n,chunks", [(1, 2), (31, 2), (64, 2), (100000, 2), (3001, 2), (3001, 4), (5000, 1),
+                                      (97, 8)])
+def test_host_matrix_split_spans(n, chunks):
+    from pyffa_b200.track import split_spans
+    sp = split_spans(n, chunks)
+    assert sp[0][0] == 0 and sp[-1][1] == n
+    assert all(a < e for a, e in sp) and all(sp[i][1] == sp[i + 1][0] for i in range(len(sp) - 1))
+    assert all(a % 32 == 0 for a, _ in sp)
+    assert 1 <= len(sp) <= chunks
+    if n >= 32 * chunks:
+        assert len(sp) == chunks and max(e - a for a, e in sp) - min(e - a for a, e in sp) < 64
