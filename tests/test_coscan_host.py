@@ -149,3 +149,57 @@ def test_launch_steps_persistent_and_memory_bound(monkeypatch):
     scan.persistent = False
     monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (180 << 30, 180 << 30))
     assert scan._launch_steps(cap) == cap.max_steps()
+
+
+def test_fixed_shape_accumulation_equals_direct():
+    """The graph mode's fixed-shape accumulation (whole record buffer, rows
+    past the count sent to a dummy particle and instance) gives the direct
+    accumulation's sums, pairs and last states, whatever the stale rows hold
+    (NaN included), over two launches in shuffled order."""
+    rng = np.random.default_rng(5)
+    f64 = dict(dtype=torch.float64)
+    I, counts = 3, [2, 5, 4]
+    inst = np.repeat(np.arange(I), counts)
+    N, turns, dt = len(inst), 6, 2e-10
+    rows = []
+    for t in range(turns):
+        for p in range(N):
+            r = 8.5 + 1e-3 * rng.standard_normal()
+            f5 = 2.3e7 / r                       # rad/s
+            row = np.zeros(23)
+            row[1], row[2] = p, 3000 * t + 17 * p
+            d0 = rng.uniform(0.1, 0.9) * f5 * dt  # the step crosses azimuth 0
+            for o, fi in ((4, -d0), (11, f5 * dt - d0)):
+                row[o:o + 6] = [r + 1e-6 * rng.standard_normal(), 1e4 * rng.standard_normal(),
+                                1e-3 * rng.standard_normal(), 1e4 * rng.standard_normal(), fi, f5]
+            rows.append(row)
+    rec = np.array(rows)
+    launches = [rec[rec[:, 2] < 3000 * 3], rec[rec[:, 2] >= 3000 * 3]]
+    scale = torch.as_tensor(np.vstack([np.tile([1e3, 1e-4, 1e3, 1e-4], (I, 1)), np.ones((1, 4))]))
+    gv = torch.zeros((I + 1, 4), **f64)
+    gv[:I, 0] = 8.5
+    inst_ext = torch.as_tensor(np.concatenate([inst, [I]]))
+
+    def state(n_inst, n_part):
+        return (torch.zeros((2, n_inst, 3, 3), **f64), torch.zeros((2, n_inst, 2, 3), **f64),
+                torch.zeros(n_inst, **f64), torch.zeros((n_part, 4), **f64),
+                torch.zeros(n_part, dtype=torch.bool))
+    S1, Y1, c1, last1, has1 = state(I, N)
+    S2, Y2, c2, last2, has2 = state(I + 1, N + 1)
+    C = max(len(x) for x in launches) + 7
+    for part in launches:
+        part = part[rng.permutation(len(part))]
+        pt = torch.as_tensor(part)
+        coscan.accumulate_crossings(pt[:, 1].long(), pt[:, 2].long(), coscan.crossing_states(pt, dt),
+                                    gv[:I], inst_ext[:N], 3000 * turns, last1, has1, S1, Y1, c1, scale[:I])
+        buf = rng.standard_normal((C, 23))           # stale rows past the count
+        buf[len(part):len(part) + 3] = np.nan
+        buf[:len(part)] = part
+        coscan.accumulate_crossings_fixed(torch.as_tensor(buf), torch.tensor(len(part)), dt, gv, inst_ext,
+                                          3000 * turns, last2, has2, S2, Y2, c2, scale)
+    assert torch.allclose(S2[:, :I], S1, rtol=1e-13, atol=0) and torch.allclose(Y2[:, :I], Y1, rtol=1e-13, atol=0)
+    assert torch.equal(c2[:I], c1) and c1.tolist() == [float(turns * c) for c in counts]
+    assert torch.equal(has2[:N], has1) and bool(has1.all())
+    assert torch.allclose(last2[:N], last1, rtol=1e-15, atol=0)
+    # (turns - 1) pairs per particle in the normal equations' constant term
+    assert S1[0, :, 2, 2].tolist() == [float((turns - 1) * c) for c in counts]
