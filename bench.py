@@ -584,7 +584,6 @@ def main():
         return run_reference(args)
     import torch
     import torch.distributed as dist
-    from pyffa_b200 import _lib
     from pyffa_b200.track import MatrixTracker, Pusher, StepClock, _EphemeralBunch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

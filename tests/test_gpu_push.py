@@ -6,8 +6,6 @@ float64 coordinates are compared at 1e-12 relative per turn of tracking (the
 bar of the tracking path).  Flags (injection, aperture loss) and map cell
 indices are compared exactly.
 """
-import ctypes
-
 import numpy as np
 import pytest
 
