@@ -1095,6 +1095,8 @@ cudaError_t launch_gemm(const float *A, int lda, int tA, const float *B, int ldb
                         int N, int K, const float *bias, int k_chunk, int splits, cudaStream_t s)
 {
     if (g5_fits(M, N, K)) {
+        // once per process (one process per GPU); set outside any graph
+        // capture: the first training step runs directly before the capture
         static bool attr = false;
         if (!attr) {
             const cudaError_t e = cudaFuncSetAttribute(gemm_tc05, cudaFuncAttributeMaxDynamicSharedMemorySize,
