@@ -115,3 +115,70 @@ def test_state_comparison():
     c = a.clone()
     c[0] = float("nan")                                      # a NaN where there was none
     assert autotune.compare(c, a) == (False, float("inf"))
+
+
+class _FakeEvent:
+    """Stands in for torch.cuda.Event: the tuner reads e0.elapsed_time(e1)."""
+    clock = [0.0]
+    times = {}
+
+    def __init__(self, enable_timing=False):
+        self.t = None
+
+    def record(self, stream=None):
+        self.t = _FakeEvent.clock[0]
+
+    def elapsed_time(self, other):
+        return other.t - self.t
+
+
+class _FakePusher:
+    def __init__(self, times, differs):
+        import torch
+        self.flags = _lib.FFA_FP32C
+        self.shape = (1, 1)                   # the caller's own shape, restored afterwards
+        self.stream = type("S", (), {"synchronize": lambda s: None})()
+        self.gp = type("G", (), {"Bmap": type("B", (), {"max_order": 2})()})()
+        self.times, self.differs = times, differs
+        self.calls = []
+        self.state = torch.zeros(4, dtype=torch.float64)
+
+    def push(self, clock, step0, nsteps, sc_step, xing=None):
+        import torch
+        self.calls.append(self.shape)
+        _FakeEvent.clock[0] += self.times(self.shape, len(self.calls))
+        self.state = torch.full((4,), 1.0 + (1e-12 if self.shape in self.differs else 0.0), dtype=torch.float64)
+
+
+def _patch(monkeypatch):
+    import contextlib
+    import torch
+    monkeypatch.setattr(torch.cuda, "Event", _FakeEvent)
+    monkeypatch.setattr(torch.cuda, "stream", lambda s: contextlib.nullcontext())
+    monkeypatch.setattr(autotune, "occupancy", lambda flags, order, xing: (12, 64))
+
+
+def test_tune_push_bookkeeping(monkeypatch):
+    _patch(monkeypatch)
+    times = lambda shape, k: {(0, 0): 10.0, (2, 1): 8.0, (3, 3): 6.0}.get(shape, 9.9) + (5.0 if k % 3 == 1 else 0)
+    pu = _FakePusher(times, differs={(3, 3)})
+    resets = []
+    res = autotune.tune_push(pu, None, 0, 100, reset=lambda: resets.append(1), snapshot=lambda: pu.state,
+                             repeats=2)
+    assert pu.shape == (1, 1)                                  # restored
+    assert pu.calls[:3] == [(0, 0)] * 3 and len(pu.calls) == 3 * 16 and len(resets) == 3 * 16
+    rows = {r["shape"]: r for r in res.rows}
+    assert rows[(0, 0)]["ms"] == 10.0                          # the untimed first launch (+5) is not counted
+    assert rows[(3, 3)]["identical"] is False and rows[(3, 3)]["max_rel_diff"] > 0
+    assert rows[(3, 3)]["accepted"] is False and rows[(2, 1)]["accepted"] is True
+    assert res.best == (2, 1) and abs(res.speedup - 10.0 / 8.0) < 1e-12
+    # a tolerance admits the rounding-level shape, which is then the fastest
+    pu2 = _FakePusher(times, differs={(3, 3)})
+    res2 = autotune.tune_push(pu2, None, 0, 100, reset=lambda: None, snapshot=lambda: pu2.state, rtol=1e-9)
+    assert res2.best == (3, 3)
+    # cached by key: no launches the second time
+    pu3 = _FakePusher(times, differs=set())
+    r1 = autotune.tune_push(pu3, None, 0, 100, reset=lambda: None, snapshot=lambda: pu3.state, cache_key="k")
+    n = len(pu3.calls)
+    assert autotune.tune_push(pu3, None, 0, 100, cache_key="k") is r1 and len(pu3.calls) == n
+    autotune._CACHE.clear()
