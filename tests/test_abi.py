@@ -81,3 +81,23 @@ def test_invalid_arguments_rejected_without_gpu():
     t.batch = 16
     t.n_fit = 9
     assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
+
+
+def test_train_schedule_fields_checked_without_gpu():
+    """The device schedule needs both lr_table and counter; the host
+    schedule needs step >= 1 when it updates (checked before any launch)."""
+    L = _lib.lib()
+    keep = ctypes.create_string_buffer(64)
+    fake = ctypes.addressof(keep)
+    t = _lib.MlpTrainDesc()
+    t.batch, t.n_fit = 16, 4
+    for name in ("params", "grads", "adam_m", "adam_v", "x", "target", "work", "loss_part"):
+        setattr(t, name, fake)
+    t.lr_table = fake                      # counter missing
+    assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
+    t.lr_table, t.counter = None, fake     # lr_table missing
+    assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
+    t.counter = None
+    t.lr, t.step = 1e-3, 0                 # host schedule, update without a step number
+    assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
+    assert L.ffa_mlp_gemm_timeouts(None) == 1
