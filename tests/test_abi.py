@@ -101,3 +101,21 @@ def test_train_schedule_fields_checked_without_gpu():
     t.lr, t.step = 1e-3, 0                 # host schedule, update without a step number
     assert L.ffa_mlp_train_step(ctypes.byref(t), None) == 1
     assert L.ffa_mlp_gemm_timeouts(None) == 1
+
+
+def test_soa_offset_advances_each_column_by_its_element_size():
+    st = _lib.StateSoA()
+    base = 1 << 20
+    for k, (name, _) in enumerate(_lib.StateSoA._fields_):
+        if name not in ("sc_pp", "e_pp_fi"):           # two columns left null
+            setattr(st, name, base + (k << 16))
+    out = _lib.soa_offset(st, 10)
+    sizes = {"inj": 1, "surv": 1, "sc_pre": 1, "sc_pp": 1, "inj_step": 4}
+    for k, (name, _) in enumerate(_lib.StateSoA._fields_):
+        if name in ("sc_pp", "e_pp_fi"):
+            assert getattr(out, name) is None
+        else:
+            assert getattr(out, name) == base + (k << 16) + 10 * sizes.get(name, 8), name
+    # the header's column types: uint8 flags, int32 injection steps, double otherwise
+    text = open(HEADER).read()
+    assert "uint8_t *inj, *surv;" in text and "const int32_t *inj_step;" in text and "uint8_t *sc_pre, *sc_pp;" in text
