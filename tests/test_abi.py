@@ -119,3 +119,9 @@ def test_soa_offset_advances_each_column_by_its_element_size():
     # the header's column types: uint8 flags, int32 injection steps, double otherwise
     text = open(HEADER).read()
     assert "uint8_t *inj, *surv;" in text and "const int32_t *inj_step;" in text and "uint8_t *sc_pre, *sc_pp;" in text
+
+
+def test_integration_guide_covers_every_entry_point():
+    guide = open(os.path.join(build.REPO_DIR, "INTEGRATION.md")).read()
+    missing = [n for n in declared_entry_points() if n not in guide]
+    assert not missing, missing
