@@ -87,6 +87,12 @@ def test_residency_model():
     assert m(32, 56) == 32          # one-warp blocks: 32 blocks per SM at most
     assert m(256, 80) == 24
     assert m(256, 56) == 32         # 36 warps' registers, but whole 8-warp blocks: 4
+    # every candidate against the runtime's occupancy calculator on a B200
+    # (ffa_push_occupancy, FP32C Boris with crossing capture, map order 2)
+    runtime = {(32, 80): 24, (64, 80): 24, (128, 80): 24, (256, 80): 24, (32, 72): 28, (64, 72): 28,
+               (128, 72): 28, (256, 72): 24, (32, 64): 32, (64, 64): 32, (128, 64): 32, (256, 64): 32,
+               (32, 56): 32, (64, 56): 36, (128, 56): 36, (256, 56): 32}
+    assert {k: m(*k) for k in runtime} == runtime
     # the 256-energy scan bunch: 1.43 waves of the default shape, one of 36 warps
     assert abs(autotune.waves(162321, 24, 148) - 1.428) < 1e-3
     assert autotune.waves(162321, 36, 148) <= 1.0
