@@ -167,7 +167,9 @@ typedef struct ffa_crossing {
     int64_t *count;               /* device */
 } ffa_crossing;
 
-/* ffa_push with azimuth-crossing capture (all three pushers). */
+/* ffa_push with azimuth-crossing capture (all three pushers).  Replaces the
+ * per-step PositionDumpBunch.check_and_dump of the step loop
+ * (src/FFAG_dump.py:1098-1130, called from src/FFAG_track.py:297-579). */
 int ffa_push_crossing(const struct ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_aperture *ap,
                       const ffa_consts *cs, const ffa_step_table *tab, ffa_state_soa *st,
                       int64_t n, int64_t step0, int32_t nsteps, double dt, int32_t sc_step,
@@ -250,12 +252,16 @@ typedef struct ffa_sc_diag {
 
 typedef struct ffa_sc_plan ffa_sc_plan;
 
+/* Plan of ffa_sc_step for one bunch capacity and grid: owns the device
+ * scratch.  Replaces the grid and FFT set-up of the step loop
+ * (pyfftw plans and buffers, src/FFAG_track.py:319-328). */
 int ffa_sc_plan_create(const ffa_sc_desc *desc, void *stream, ffa_sc_plan **out);
 int ffa_sc_plan_destroy(ffa_sc_plan *plan);
 
 /* One space-charge update over the particles with surv != 0: coordinates,
  * slice arc and moments, CIC deposit, Poisson solve per slice, field and
- * gather into esc_*.  Replaces Build_2_5D_SliceGrid_sbs.  When `roll` is
+ * gather into esc_*.  Replaces Build_2_5D_SliceGrid_sbs
+ * (src/FFAG_Bunch.py:1157-1352) and the endpoint roll of src/FFAG_track.py:341-400.  When `roll` is
  * nonzero the extrapolation endpoints are rolled afterwards as the step loop
  * does (first != 0 at step 0).  diag: device ffa_sc_diag or NULL. */
 int ffa_sc_step(ffa_sc_plan *plan, ffa_state_soa *st, int64_t n, int32_t roll, int32_t first,
@@ -268,14 +274,15 @@ int ffa_sc_step(ffa_sc_plan *plan, ffa_state_soa *st, int64_t n, int32_t roll, i
  * in a control system where an allocation could fail or stall the device.
  * Same inputs, outputs and results as ffa_sc_plan_create + ffa_sc_step, but
  * all scratch lives in one fixed device array compiled into the library
- * (about 31 MB, held by every device that loads the library until exit).
+ * (about 30 MB, held by every device that loads the library until exit).
  * Limits: n <= FFA_SC_STATIC_MAX_PARTICLES (else FFA_ERR_INVALID);
  * ns * nz * nx <= FFA_SC_STATIC_MAX_CELLS, nx, nz <= 128, periodic boundary
  * (else FFA_ERR_UNSUPPORTED).  Every call on a device shares the array and
  * finds the previous call's contents there (the charge accumulator is
- * cleared each call); calls that overlap on the GPU race and must be
- * serialised by the caller.  The first call on a device looks up the array's
- * address and fills its FFT tables: make it before any stream capture. */
+ * cleared each call, the FFT twiddles are formed inside the kernels); calls
+ * that overlap on the GPU race and must be serialised by the caller.  Each
+ * call looks up the array's address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing). */
 #define FFA_SC_STATIC_MAX_PARTICLES 524288
 #define FFA_SC_STATIC_MAX_CELLS 524288
 int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *st, int64_t n, int32_t roll, int32_t first,
@@ -283,7 +290,9 @@ int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *st, int64_t n, in
 
 /* Device views of the plan's last charge, potential and field cubes
  * (float32, (ns, nz, nx)), and of the per-particle slice / cell indices
- * (int32 slice, int64 cell = (s*nz + iz)*nx + ix, -1 when not deposited). */
+ * (int32 slice, int64 cell = (s*nz + iz)*nx + ix, -1 when not deposited):
+ * the rho / phi / Ex / Ez grids Build_2_5D_SliceGrid_sbs returns
+ * (src/FFAG_Bunch.py:1346-1352). */
 int ffa_sc_buffers(const ffa_sc_plan *plan, const float **rho, const float **phi,
                    const float **ex, const float **ez, const int32_t **slice_idx,
                    const int64_t **cell_idx);
@@ -309,6 +318,8 @@ typedef struct ffa_theta_track_desc {
     double *traj;                 /* device [m][n_points][traj_cols] at every point, or NULL */
 } ffa_theta_track_desc;
 
+/* Runs the m tracks in one launch (one thread each); replaces the per-orbit
+ * rk4_solve / rk4_solve_vect calls of FFAG_SearchSEO (src/FFAG_track.py:1245-1371). */
 int ffa_theta_track(const struct ffa_fieldmap *fm, const ffa_theta_track_desc *desc, void *stream);
 
 /* ---------------------------------------------------------- map generation
@@ -344,6 +355,7 @@ typedef struct ffa_mapgen_desc {
     double *bz, *br, *bfi;        /* device [n_orders][n_r][n_theta] */
 } ffa_mapgen_desc;
 
+/* Fills bz, br, bfi; replaces Generate_Bmaps (src/FFAG_HighOrder.py:828-998). */
 int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
 
 /* ------------------------------------------------------ learned sector map
@@ -369,7 +381,8 @@ int ffa_mapgen(const ffa_mapgen_desc *desc, void *stream);
 #define FFA_MLP_WPACK_BYTES 278528   /* bfloat16 copies of W1..W4 for inference */
 #define FFA_MLP_SPLIT_WORK 1048576    /* floats of split-K partial products in the training work area */
 
-/* One optimiser step: forward, mean-squared error over the first n_fit
+/* One optimiser step (no counterpart in the reference, whose tracker has no
+ * learned map): forward, mean-squared error over the first n_fit
  * outputs, backward into `grads` (every parameter, same layout), then Adam
  * on the entries whose `mask` byte is non-zero (mask NULL: all) when lr > 0.
  * `step` is the 1-based Adam step (bias correction).  `work` holds
@@ -397,7 +410,8 @@ typedef struct ffa_mlp_train_desc {
 
 int ffa_mlp_train_step(const ffa_mlp_train_desc *desc, void *stream);
 
-/* C[M][N] = op(A) op(B) (+ bias[N]) in bfloat16 x bfloat16 -> float32 on
+/* No counterpart in the reference (part of the learned map's training).
+ * C[M][N] = op(A) op(B) (+ bias[N]) in bfloat16 x bfloat16 -> float32 on
  * the tensor cores; op(A)[m][k] = A[m lda + k] (transA 0) or A[k lda + m],
  * op(B)[k][n] = B[k ldb + n] (transB 0) or B[n ldb + k].  The training step's
  * building block, exported for tests. */
@@ -411,12 +425,15 @@ int ffa_mlp_gemm(const float *A, int lda, int transA, const float *B, int ldb, i
  * learned map is new). */
 int ffa_mlp_gemm_timeouts(int32_t *count);
 
-/* Inference weights: the bfloat16 packing of a parameter block into `wpack`
+/* No counterpart in the reference (learned map).
+ * Inference weights: the bfloat16 packing of a parameter block into `wpack`
  * (FFA_MLP_WPACK_BYTES, 16-byte aligned).  Call again after the parameters
  * change. */
 int ffa_mlp_pack(const float *params, void *wpack, void *stream);
 
-/* Applies the map n_apply times to each state in place (tcgen05 tensor
+/* No counterpart in the reference (learned map; it stands in for the
+ * per-sector steps of the tracking loop, src/FFAG_track.py:297-579).
+ * Applies the map n_apply times to each state in place (tcgen05 tensor
  * cores, one CTA per SM).  A state takes a map only while it is inside the
  * training domain, u^2 + pu^2 <= radius2, v^2 + pv^2 <= radius2 and
  * |e| <= 1 (radius2 <= 0: no check); the first state outside it is kept, and

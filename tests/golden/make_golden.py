@@ -2,11 +2,11 @@
 tracker (PyFFA, pure Python + Numba) on seeded synthetic inputs.
 
 Run in the development container, where the reference source is available:
-    python tests/golden/make_golden.py [--ref /root/reference]              # tracking
-    python tests/golden/make_golden.py --crossing [--ref /root/reference]   # crossing dumps
-    python tests/golden/make_golden.py --mapgen [--ref /root/reference]     # z-Taylor maps
-    python tests/golden/make_golden.py --seo [--ref /root/reference]        # closed orbits
-    python tests/golden/make_golden.py --bunch [--ref /root/reference]      # injected bunches
+    python tests/golden/make_golden.py --ref REFERENCE_CHECKOUT              # tracking
+    python tests/golden/make_golden.py --crossing --ref REFERENCE_CHECKOUT   # crossing dumps
+    python tests/golden/make_golden.py --mapgen --ref REFERENCE_CHECKOUT     # z-Taylor maps
+    python tests/golden/make_golden.py --seo --ref REFERENCE_CHECKOUT        # closed orbits
+    python tests/golden/make_golden.py --bunch --ref REFERENCE_CHECKOUT      # injected bunches
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -68,12 +68,9 @@ def p_bunch(n, seed, inj_spread_ns=0.0, dt=None):
     return a
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    args = ap.parse_args()
+def main(ref):
     sys.path.insert(0, os.path.join(HERE, "shims"))
-    sys.path.insert(0, os.path.join(args.ref, "src"))
+    sys.path.insert(0, os.path.join(ref, "src"))
     import FFAG_track
     from FFAG_Bunch import FFAG_Bunch
     from FFAG_dump import Dumps
@@ -432,21 +429,22 @@ def bunch_main(ref):
 
 
 if __name__ == "__main__":
-    if "--bunch" in sys.argv:
-        sys.argv.remove("--bunch")
-        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
-        bunch_main(ref)
-    elif "--seo" in sys.argv:
-        sys.argv.remove("--seo")
-        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
-        seo_main(ref)
-    elif "--mapgen" in sys.argv:
-        sys.argv.remove("--mapgen")
-        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
-        mapgen_main(ref)
-    elif "--crossing" in sys.argv:
-        sys.argv.remove("--crossing")
-        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
-        crossing_main(ref)
+    ap = argparse.ArgumentParser(description="Generate golden vectors by running the reference's own code.")
+    ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"),
+                    help="checkout of the reference project (or set PYFFA_REFERENCE)")
+    kind = ap.add_mutually_exclusive_group()
+    for k in ("bunch", "seo", "mapgen", "crossing"):
+        kind.add_argument("--" + k, action="store_true")
+    args = ap.parse_args()
+    if not args.ref:
+        ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
+    if args.bunch:
+        bunch_main(args.ref)
+    elif args.seo:
+        seo_main(args.ref)
+    elif args.mapgen:
+        mapgen_main(args.ref)
+    elif args.crossing:
+        crossing_main(args.ref)
     else:
-        main()
+        main(args.ref)

@@ -121,7 +121,18 @@ def test_soa_offset_advances_each_column_by_its_element_size():
     assert "uint8_t *inj, *surv;" in text and "const int32_t *inj_step;" in text and "uint8_t *sc_pre, *sc_pp;" in text
 
 
-def test_integration_guide_covers_every_entry_point():
-    guide = open(os.path.join(build.REPO_DIR, "INTEGRATION.md")).read()
-    missing = [n for n in declared_entry_points() if n not in guide]
-    assert not missing, missing
+def test_every_entry_point_cites_what_it_replaces():
+    """Each declaration's doc block (the last comment starting at column 0
+    before it) cites the reference file it replaces or says that it has no
+    counterpart there."""
+    text = open(HEADER).read()
+    bad = []
+    for m in re.finditer(r"\bint\s+(ffa_\w+)\s*\(", text):
+        before = text[:m.start()]
+        if before.rfind("/*") > before.rfind("*/"):
+            continue                      # a mention inside a comment
+        start = before.rfind("\n/*")
+        doc = before[start:before.find("*/", start)]
+        if not any(key in doc for key in ("src/", "examples/", "benchmarks/", "counterpart")):
+            bad.append(m.group(1))
+    assert not bad, bad

@@ -80,44 +80,17 @@ def _track(gp, v, dt, nsteps, precision, target=None):
 def at_azimuth(d, n, dt):
     """Per particle (NaN where it did not cross): r, vr, z, vz interpolated
     to the target azimuth, the post-step speed and the crossing time."""
+    from pyffa_b200 import diagnostics
     rec = d.crossing_records
-    out = np.full((n, 6), np.nan)
-    if rec.shape[0] == 0:
-        return out
     idx = rec[:, 1].astype(np.int64)
     assert np.unique(idx).size == idx.size, "one crossing per particle in the window"
-    a = rec[:, 3:4]
-    pre, post = rec[:, 4:11], rec[:, 11:18]
-    x = pre + a * (post - pre)
-    out[idx, 0:4] = x[:, 0:4]
-    out[idx, 4] = np.sqrt(post[:, 1] ** 2 + post[:, 3] ** 2 + (post[:, 0] * post[:, 5]) ** 2)
-    out[idx, 5] = rec[:, 23] - dt + rec[:, 3] * dt
-    return out
+    return diagnostics.at_azimuth(rec, n, dt)
 
 
-def _emittance(x, xp):
-    x = x - x.mean()
-    xp = xp - xp.mean()
-    return np.sqrt(np.mean(x * x) * np.mean(xp * xp) - np.mean(x * xp) ** 2)
-
-
-def azimuth_errors(s64, s32, c=2.99792458e8):
+def azimuth_errors(s64, s32):
     """Errors of s32 against s64 (rows of at_azimuth)."""
-    ok = np.isfinite(s64[:, 0]) & np.isfinite(s32[:, 0])
-    a, b = s64[ok], s32[ok]
-    g = lambda v: 1.0 / np.sqrt(1.0 - (v / c) ** 2)
-    p64, p32 = g(a[:, 4]) * a[:, 4], g(b[:, 4]) * b[:, 4]
-    dr = np.abs(b[:, 0] - a[:, 0]) / a[:, 0]
-    e = {"n": int(ok.sum()), "r": float(dr.max()), "r_median": float(np.median(dr)),
-         "t": float(np.max(np.abs(b[:, 5] - a[:, 5]) / a[:, 5])),
-         "p": float(np.max(np.abs(p32 - p64) / p64))}
-    for name, col in (("vr", 1), ("z", 2), ("vz", 3)):
-        e[name + "_amp"] = float(np.abs(b[:, col] - a[:, col]).max() / np.abs(a[:, col]).max())
-    for name, (cx, cv) in (("emit_x", (0, 1)), ("emit_z", (2, 3))):
-        e64 = _emittance(a[:, cx], a[:, cv] / a[:, 4])
-        e32 = _emittance(b[:, cx], b[:, cv] / b[:, 4])
-        e[name] = float(abs(e32 - e64) / e64)
-    return e
+    from pyffa_b200 import diagnostics
+    return diagnostics.azimuth_errors(s64, s32)
 
 
 def _bunch(seed, n=2048):
