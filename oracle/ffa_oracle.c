@@ -31,6 +31,7 @@
 #define MAXG 8
 #define MAXSEG 16
 #define MAXPOLY 16
+#define MAXHARM 16
 
 /* ---------------------------------------------------------------- types */
 
@@ -52,6 +53,12 @@ typedef struct {
     const double *bz_stack;     /* (max_order+1, r_size, fi_size) */
     const double *bfi_stack;
     const double *br_stack;
+    /* field-error harmonics (FFAG_BField_Error, src/FFAG_Field.py:947-993):
+     * m, amplitude [T], phase [rad], radial band */
+    int32_t n_harm;
+    int32_t pad1;
+    double harm_m[MAXHARM], harm_amp[MAXHARM], harm_ph[MAXHARM];
+    double harm_rmin[MAXHARM], harm_rmax[MAXHARM];
 } orc_field;
 
 typedef struct {
@@ -95,6 +102,20 @@ void orc_freq_curve(const orc_emap *em, double xi, double *freq, double *volt)
     double z0 = em->fc_volt[i], z1 = em->fc_volt[i + 1];
     *freq = y0 + (xi - x0) / (x1 - x0) * (y1 - y0);
     *volt = z0 + (xi - x0) / (x1 - x0) * (z1 - z0);
+}
+
+/* bharmonics_kernel_1d, src/FFAG_Field.py:1541-1587, for one particle: the
+ * Bz sum of the harmonics whose radial band holds r (fi unwrapped), which
+ * the caller adds to Bz afterwards; Br and Bfi take nothing. */
+static double harmonics_Bz(const orc_field *f, double r, double fi)
+{
+    if (r <= 0.0) return 0.0;
+    double Bz = 0.0;
+    for (int k = 0; k < f->n_harm; ++k) {
+        if (f->harm_rmin[k] <= r && r <= f->harm_rmax[k])
+            Bz += f->harm_amp[k] * cos(f->harm_m[k] * fi + f->harm_ph[k]);
+    }
+    return Bz;
 }
 
 /* GetBfields_Njit body, src/FFAG_Field.py:1333-1426 (alive particles only) */
@@ -262,6 +283,7 @@ void orc_boris_step(double t, double *mat, int64_t N, double dt,
             analytic_B(f, r, fi_mod, z, &Bz, &Br, &Bfi);
             if (f->max_order >= 1) high_order_B(f, r, fi_mod, z, &Bz, &Bfi, &Br);
         }
+        if (f->n_harm > 0) Bz += harmonics_Bz(f, r, fi);   /* src/FFAG_track.py:1007 */
         double Er = 0.0, Efi = 0.0;
         rf_field(em, acc_Etot, r, fi, row[9], &Er, &Efi);
         double Ez = 0.0;
@@ -360,6 +382,7 @@ static void rk4_rhs_row(const double *row, double dRF_rate, double acc_Etot,
     double Bz = 0.0, Br = 0.0, Bfi = 0.0;
     analytic_B(f, r, fi_mod, z, &Bz, &Br, &Bfi);
     if (f->max_order >= 1) high_order_B(f, r, fi_mod, z, &Bz, &Bfi, &Br);
+    if (f->n_harm > 0) Bz += harmonics_Bz(f, r, fi);       /* src/FFAG_track.py:1782 */
     double Er = 0.0, Efi = 0.0;
     rf_field(em, acc_Etot, r, fi, row[9], &Er, &Efi);
     double Ez = 0.0;

@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libffa_oracle.so")
-MAXG, MAXSEG, MAXPOLY = 8, 16, 16
+MAXG, MAXSEG, MAXPOLY, MAXHARM = 8, 16, 16, 16
 
 
 def build(force: bool = False) -> str:
@@ -33,7 +33,11 @@ class OrcField(C.Structure):
                 ("convex", C.c_double * (MAXSEG * 5)),
                 ("r_min", C.c_double), ("r_step", C.c_double), ("r_size", C.c_int64),
                 ("fi_min", C.c_double), ("fi_step", C.c_double), ("fi_size", C.c_int64),
-                ("bz_stack", C.c_void_p), ("bfi_stack", C.c_void_p), ("br_stack", C.c_void_p)]
+                ("bz_stack", C.c_void_p), ("bfi_stack", C.c_void_p), ("br_stack", C.c_void_p),
+                ("n_harm", C.c_int32), ("pad1", C.c_int32),
+                ("harm_m", C.c_double * MAXHARM), ("harm_amp", C.c_double * MAXHARM),
+                ("harm_ph", C.c_double * MAXHARM), ("harm_rmin", C.c_double * MAXHARM),
+                ("harm_rmax", C.c_double * MAXHARM)]
 
 
 class OrcEmap(C.Structure):
@@ -147,6 +151,17 @@ class Setup:
     def __init__(self, bmap, emap, gp):
         self._keep = []
         self.field = _orc_field(bmap, self._keep)
+        bh = getattr(gp, "BHarmonics", None)
+        if bh is not None and bh.enable_flag and bh.Nharm > 0:
+            if bh.Nharm > MAXHARM:
+                raise ValueError(f"at most {MAXHARM} field-error harmonics")
+            self.field.n_harm = bh.Nharm
+            for k in range(bh.Nharm):
+                self.field.harm_m[k] = float(bh.m_arr[k])
+                self.field.harm_amp[k] = float(bh.amp_arr[k])
+                self.field.harm_ph[k] = float(bh.phase_arr[k])
+                self.field.harm_rmin[k] = float(bh.rmin_arr[k])
+                self.field.harm_rmax[k] = float(bh.rmax_arr[k])
         e = OrcEmap()
         e.enable = 1 if emap.EnableFlag else 0
         e.ngaps = len(emap.gap_azimuths)

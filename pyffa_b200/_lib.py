@@ -172,6 +172,7 @@ class SCDiag(C.Structure):
 EXPORTS = {
     "ffa_fieldmap_create": [C.POINTER(FieldDesc), d_p, C.POINTER(d_p)],
     "ffa_fieldmap_destroy": [d_p],
+    "ffa_fieldmap_set_harmonics": [d_p, C.c_int32, d_p, d_p, d_p, d_p, d_p],
     "ffa_inject": [C.POINTER(StateSoA), C.c_int64, C.c_int64, d_p],
     "ffa_push": [d_p, C.POINTER(RFDesc), C.POINTER(Aperture), C.POINTER(Consts), C.POINTER(StepTable),
                  C.POINTER(StateSoA), C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32,

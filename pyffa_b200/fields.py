@@ -211,6 +211,27 @@ class DeviceFieldMap:
             _lib.check(_lib.lib().ffa_fieldmap_create(ctypes.byref(desc), _lib.stream_ptr(None), ctypes.byref(h)),
                        "ffa_fieldmap_create")
         self.handle = h
+        self._harm_key = ()
+
+    def set_harmonics(self, harmonics) -> None:
+        """Makes the map carry the field-error harmonics of an
+        FFAG_BField_Error (None or disabled: none).  The library copies them
+        to the device synchronously, so this is done only when they change."""
+        import ctypes
+        import torch
+        if harmonics is not None and harmonics.active():
+            arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                    (harmonics.m_arr, harmonics.amp_arr, harmonics.phase_arr, harmonics.rmin_arr, harmonics.rmax_arr)]
+        else:
+            arrs = []
+        key = tuple(tuple(a.tolist()) for a in arrs)
+        if key == self._harm_key:
+            return
+        ptrs = [ctypes.c_void_p(a.ctypes.data) for a in arrs] if arrs else [None] * 5
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().ffa_fieldmap_set_harmonics(self.handle, len(arrs[0]) if arrs else 0, *ptrs),
+                       "ffa_fieldmap_set_harmonics")
+        self._harm_key = key
 
     def __del__(self):
         try:
@@ -335,12 +356,39 @@ class FFAG_EField_new:
 
 
 class FFAG_BField_Error:
-    """Field-error harmonics switch (src/FFAG_Field.py:947-1042).  The
-    harmonic sum is not part of the GPU push; enabling it is rejected."""
+    """Field-error harmonics (src/FFAG_Field.py:947-993): Bz(r, fi) gains
+    sum_k amp_k cos(m_k fi + phase_k) for rmin_k <= r <= rmax_k, with fi the
+    unwrapped azimuth; Br and Bfi are unchanged.  `harmonics_cfg` is a list
+    of dicts {"m", "amp_Gs", "phase_deg", "rmin", "rmax"} (gauss, degrees,
+    metres), as in the reference.  The push kernels add the sum after the
+    mid-plane map (Boris_solve src/FFAG_track.py:1007, the RK4 field
+    FunctionForAccelerationBunch_dt :1782)."""
+
+    MAX_HARMONICS = 16
 
     def __init__(self, harmonics_cfg, EnableFlag):
         self.harmonics_cfg = harmonics_cfg
         self.enable_flag = bool(EnableFlag)
         self.Nharm = len(harmonics_cfg)
-        if self.enable_flag and self.Nharm > 0:
-            raise NotImplementedError("field-error harmonics are not supported by the GPU pushers")
+        if self.Nharm > self.MAX_HARMONICS:
+            raise ValueError(f"at most {self.MAX_HARMONICS} field-error harmonics")
+        self.m_arr = np.array([int(h["m"]) for h in harmonics_cfg], dtype=np.int64)
+        self.amp_arr = np.array([float(h["amp_Gs"]) * 1e-4 for h in harmonics_cfg], dtype=np.float64)
+        self.phase_arr = np.array([np.deg2rad(float(h["phase_deg"])) for h in harmonics_cfg], dtype=np.float64)
+        self.rmin_arr = np.array([float(h["rmin"]) for h in harmonics_cfg], dtype=np.float64)
+        self.rmax_arr = np.array([float(h["rmax"]) for h in harmonics_cfg], dtype=np.float64)
+
+    def active(self) -> bool:
+        return self.enable_flag and self.Nharm > 0
+
+    def GetBzHarmonics(self, r, phi):
+        """Bz of the harmonics at (r, phi), numpy, broadcasting."""
+        r = np.asarray(r, np.float64)
+        phi = np.asarray(phi, np.float64)
+        out = np.zeros(np.broadcast(r, phi).shape)
+        if not self.enable_flag:
+            return out
+        for k in range(self.Nharm):
+            band = (self.rmin_arr[k] <= r) & (r <= self.rmax_arr[k])
+            out = out + np.where(band, self.amp_arr[k] * np.cos(self.m_arr[k] * phi + self.phase_arr[k]), 0.0)
+        return out

@@ -113,9 +113,9 @@ class Pusher:
         self.rf = gp.Emap.rf_desc()
         self.ap = _aperture(gp)
         self.cs = _consts(gp)
-        bh = getattr(gp, "BHarmonics", None)
-        if bh is not None and getattr(bh, "enable_flag", False) and getattr(bh, "Nharm", 0) > 0:
-            raise NotImplementedError("field-error harmonics are not supported by the GPU pushers")
+        # field-error harmonics (FFAG_BField_Error): carried by the device map
+        # and set on it before each push, since maps are shared between pushers
+        self.harmonics = getattr(gp, "BHarmonics", None)
         self.flags = _lib.FFA_RK4 if solver == "RK4" else _lib.FFA_BORIS
         if precision == "fp32c":
             if solver == "RK4":
@@ -139,6 +139,7 @@ class Pusher:
         if start < 0 or n < 0 or start + n > b.n:
             raise ValueError(f"particle range [{start}, {start + n}) outside the bunch of {b.n}")
         soa = b.soa() if start == 0 else _lib.soa_offset(b.soa(), start)
+        self.fm.set_harmonics(self.harmonics)
         s = (self.stream if stream is None else stream).cuda_stream
         args = (self.fm.handle, ctypes.byref(self.rf), ctypes.byref(self.ap), ctypes.byref(self.cs),
                 ctypes.byref(clock.table), ctypes.byref(soa), n, step0, nsteps, clock.dt,

@@ -14,6 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "golden_tracking.npz")
+GOLDEN_HARMONICS = os.path.join(HERE, "golden", "golden_harmonics.npz")
 
 
 class Golden:
@@ -47,11 +48,14 @@ class Golden:
 
     def gp(self, aperture=True):
         from pyffa_b200.constants import FFAG_GlobalParameters
+        from pyffa_b200.fields import FFAG_BField_Error
         g = FFAG_GlobalParameters()
         g.AddBMap(self.bmap())
         g.AddEMap(self.emap())
         if aperture:
             g.AddAperture(*self.aperture)
+        if "harmonics_json" in self.z:
+            g.AddBHarmonics(FFAG_BField_Error(json.loads(bytes(self.z["harmonics_json"]).decode()), True))
         return g
 
 
@@ -62,6 +66,14 @@ def load_golden():
     if "g" not in _cache:
         _cache["g"] = Golden()
     return _cache["g"]
+
+
+def load_golden_harmonics():
+    """The harmonics fixture: the tracking fixture's lattice with field-error
+    harmonics enabled (FFAG_BField_Error), single steps and loops."""
+    if "h" not in _cache:
+        _cache["h"] = Golden(GOLDEN_HARMONICS)
+    return _cache["h"]
 
 
 def rel_err(a, b, scale=None):

@@ -7,6 +7,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py --mapgen --ref REFERENCE_CHECKOUT     # z-Taylor maps
     python tests/golden/make_golden.py --seo --ref REFERENCE_CHECKOUT        # closed orbits
     python tests/golden/make_golden.py --bunch --ref REFERENCE_CHECKOUT      # injected bunches
+    python tests/golden/make_golden.py --harmonics --ref REFERENCE_CHECKOUT  # field-error harmonics
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -428,17 +429,128 @@ def bunch_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# field-error harmonics of the harmonics fixture: one band covering the whole
+# map band, one inside it (band edges crossed by the bunch), one high mode
+HARMONICS = [{"m": 1, "amp_Gs": 20.0, "phase_deg": 30.0, "rmin": 8.0, "rmax": 8.5},
+             {"m": 3, "amp_Gs": 8.0, "phase_deg": -45.0, "rmin": 8.12, "rmax": 8.3},
+             {"m": 12, "amp_Gs": 5.0, "phase_deg": 90.0, "rmin": 8.2, "rmax": 8.6}]
+
+
+def harmonics_main(ref):
+    """Boris and RK4 single steps and tracking loops with field-error
+    harmonics enabled (FFAG_BField_Error, added by Boris_solve and the RK4
+    field function after the map), on the tracking fixture's lattice."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    import FFAG_track
+    from FFAG_Bunch import FFAG_Bunch
+    from FFAG_dump import Dumps
+    from FFAG_Field import FFAG_BField_Error
+    from FFAG_MathTools import RK4_Post_Step_njit
+    from FFAG_ParasAndConversion import FFAG_ConversionTools
+
+    conv = FFAG_ConversionTools()
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg_path, emap_path = build_inputs(tmp)
+        cfg_text, emap_text = open(cfg_path).read(), open(emap_path).read()
+        stacks = {}
+        for comp in ("Bz", "Bfi", "Br"):
+            stacks[comp] = np.stack([np.load(os.path.join(os.path.dirname(cfg_path), f"{comp}_order_{n}.npz"))
+                                     [f"{comp}_Taylor_coeff"] for n in range(MAX_ORDER + 1)])
+        aperture = (8.02, 8.48, -0.006, 0.006)
+        dt = synthetic.design_dt(300.0, 720)
+        t0 = 1.0e-9
+
+        def gp_h():
+            gp = ref_objects(cfg_path, emap_path, aperture)
+            gp.AddBHarmonics(FFAG_BField_Error(HARMONICS, True))
+            return gp
+
+        pa = p_bunch(64, seed=31)
+        pa[4:8, 4] = np.deg2rad([0.95, 1.0, 1.05, 4.0])    # inside the RF gaps
+        pa[8:16, 0] = np.linspace(8.10, 8.32, 8)            # across the inner band's edges
+        va = conv.ConvertPrzek2Vrzek_boris(pa)
+        va[:, 9] = 0.3
+        va[:, 7] = 1.0
+        va[:, 8] = 1.0
+        bunch = FFAG_Bunch(va.copy(), BunchType="Boris")
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        FFAG_track.FFAG_RungeKutta().Boris_solve(
+            t0, m, dt, bunch.Malloc_x_cart, bunch.Malloc_y_cart, bunch.Malloc_z_cart,
+            bunch.Malloc_vx_cart, bunch.Malloc_vy_cart, bunch.Malloc_vz_cart,
+            bunch.Malloc_Ex_cart, bunch.Malloc_Ey_cart, bunch.Malloc_Ez_cart,
+            bunch.Malloc_Bx_cart, bunch.Malloc_By_cart, bunch.Malloc_Bz_cart,
+            bunch.Malloc_RF_phase, bunch.Malloc_mod_fi,
+            bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+            bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+            bunch.Step_SurviveFlag, bunch.Malloc_RF_shift,
+            bunch.SurvivedNum_Local, bunch.LostNum_Local, gp_h())
+        out["boris1_in"], out["boris1_out"], out["boris1_t"] = m_in, m.copy(), np.array([t0, dt])
+
+        vr = conv.ConvertPrzek2Vrzek(pa)
+        vr[:, 9] = 0.3
+        vr[:, 7] = 1.0
+        vr[:, 8] = 1.0
+        bunch = FFAG_Bunch(vr.copy(), BunchType="RK4")
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        dr, _, _, _ = FFAG_track.FFAG_RungeKutta().rk4_step_malloc(
+            FFAG_track.FunctionForAccelerationBunch_dt, t0, m, dt, gp_h(),
+            bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+            bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+            bunch.Malloc_mod_fi, bunch.Malloc_RF_shift, bunch.Malloc_RK_dxdt,
+            bunch.SurvivedNum_Local, bunch.LostNum_Local)
+        RK4_Post_Step_njit(m, dr)
+        out["rk41_in"], out["rk41_out"] = m_in, m.copy()
+
+        for solver, nsteps in (("Boris", 240), ("RK4", 120)):
+            pl = p_bunch(64, seed=37, inj_spread_ns=4 * dt * 1e9)
+            v = conv.ConvertPrzek2Vrzek_boris(pl) if solver == "Boris" else conv.ConvertPrzek2Vrzek(pl)
+            v[:, 9] = 0.3
+            v[:, 15] = np.arange(v.shape[0])
+            b = FFAG_Bunch(v.copy(), BunchType=solver)
+            lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+                  "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+            v_in = b.LocalBunch.copy()
+            ts = -0.5 * dt
+            if solver == "Boris":
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC_boris(None, ts, b, gp_h(), lp)
+            else:
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC(FFAG_track.FunctionForAccelerationBunch_dt,
+                                                                       ts, b, gp_h(), lp)
+            key = "borisloop" if solver == "Boris" else "rk4loop"
+            out[key + "_in"], out[key + "_out"], out[key + "_t"] = v_in, b.LocalBunch.copy(), np.array([ts, dt, nsteps])
+
+        out["harmonics_json"] = np.frombuffer(json.dumps(HARMONICS).encode(), dtype=np.uint8)
+        out["cfg_json"] = np.frombuffer(cfg_text.encode(), dtype=np.uint8)
+        out["emap_text"] = np.frombuffer(emap_text.encode(), dtype=np.uint8)
+        for comp in ("Bz", "Bfi", "Br"):
+            out[f"stack_{comp}"] = stacks[comp][1:]
+        out["aperture"] = np.array(aperture)
+        from pyffa_b200 import orbit
+        seo = orbit.seo_tables(synthetic.lattice_bmap(), np.linspace(290.0, 310.0, 5), nfi=181)
+        for k in ("Ek_axis", "fi_axis", "r", "pr", "perimeter"):
+            out["seo_" + k] = seo[k]
+    path = os.path.join(HERE, "golden_harmonics.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="Generate golden vectors by running the reference's own code.")
     ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"),
                     help="checkout of the reference project (or set PYFFA_REFERENCE)")
     kind = ap.add_mutually_exclusive_group()
-    for k in ("bunch", "seo", "mapgen", "crossing"):
+    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics"):
         kind.add_argument("--" + k, action="store_true")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
-    if args.bunch:
+    if args.harmonics:
+        harmonics_main(args.ref)
+    elif args.bunch:
         bunch_main(args.ref)
     elif args.seo:
         seo_main(args.ref)

@@ -71,6 +71,7 @@ def test_invalid_arguments_rejected_without_gpu():
     d.max_order = 9
     assert L.ffa_fieldmap_create(ctypes.byref(d), None, ctypes.byref(out)) == 4
     assert L.ffa_push(None, None, None, None, None, None, 0, 0, 0, 0.0, 0, 0, None, None) == 1
+    assert L.ffa_fieldmap_set_harmonics(None, 0, None, None, None, None, None) == 1
     assert L.ffa_aos_to_soa(None, 0, None, None) == 1
     # learned sector map entry points
     assert L.ffa_mlp_train_step(None, None) == 1
