@@ -31,6 +31,7 @@ sys.path.insert(0, HERE)
 
 N_PARTICLES = 100_000
 STEPS_PER_TURN = 720
+REF_SAMPLE_STEPS = 72       # steps of a turn the reference arm runs per step
 MAX_ORDER = 2
 # float64 operations per particle-step of the Boris kernel (2 per DFMA,
 # 1 per DADD / DMUL), counted from the kernel's executed instruction mix by
@@ -62,6 +63,8 @@ def parse():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-coscan", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-rk4", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--learned-samples", type=int, default=20_000_000)
     ap.add_argument("--learned-epochs", type=int, default=8)
     ap.add_argument("--learned-n", type=int, default=10_000_000)
@@ -218,22 +221,47 @@ def sc_workload(n=1_000_000, seed=11):
     return v, seo
 
 
-def sc_bench(gp, dt, dev, updates=20, warmup=3, turns=2):
-    """Space-charge update time (ms) for the periodic and the open-boundary
-    solve, and particle-turns/s of the c2 cycle: per turn 12 x (update + 60
-    Boris steps with the field extrapolated between updates)."""
+# Compulsory HBM bytes of one space-charge update of this design, per
+# particle: pass 1 reads r, vr, z, vz, fi, f5 and the survival flag and writes
+# x = r - r0 and pr0 (65 B); the deposit reads the flag, fi, x and z and
+# writes the slice and cell indices (37 B); gather + roll read the slice, x,
+# z, pr0, the flag, the pre mask and the three pre endpoints and write the
+# three fields, both endpoint triples and both masks (128 B).  Per cell: the
+# float32 charge, potential and field cubes, written once (16 B).  The
+# fixed-point accumulator and the slices' spectra stay in L2 / shared memory.
+SC_BYTES_PER_PARTICLE = 65 + 37 + 128
+SC_BYTES_PER_CELL = 16
+SC_GRID = (64, 128, 128)
+
+
+def sc_bench(gp, dt, dev, hbm_peak, updates=20, warmup=3, turns=2):
+    """c2 space charge: update time (ms) and HBM roofline of the periodic and
+    the open-boundary solve on 1e6 macroparticles, 64 slices, 128 x 128;
+    the c2 cycle (per turn 12 x (open-boundary update + 60 Boris steps, the
+    field extrapolated between updates)) with the FP32C pusher, and with the
+    FP64 pusher for comparison; and the fraction of the bunch that survives
+    one cycle turn at the full charge, at 1e-3 of it, and without space
+    charge (the aperture losses of the space-charge defocusing)."""
     import torch
     from pyffa_b200.bunch import FFAG_Bunch
     from pyffa_b200.space_charge import SpaceCharge
     from pyffa_b200.track import Pusher, StepClock
     v, seo = sc_workload()
     n = v.shape[0]
-    out = {"particles": n, "grid": [64, 128, 128], "sigma_ratio": 12.0}
-    for mode in ("periodic", "hockney"):
-        b = FFAG_Bunch(v, marcosize=1e13 / n, sc_grid_size=(64, 128, 128, 12.0), BunchType="Boris", device=dev)
+    cells = SC_GRID[0] * SC_GRID[1] * SC_GRID[2]
+    nbytes = SC_BYTES_PER_PARTICLE * n + SC_BYTES_PER_CELL * cells
+    out = {"particles": n, "grid": list(SC_GRID), "sigma_ratio": 12.0,
+           "bytes_per_update": nbytes, "bytes_basis": f"{SC_BYTES_PER_PARTICLE} B per particle + "
+                                                     f"{SC_BYTES_PER_CELL} B per cell (compulsory HBM traffic)"}
+
+    def make(mode, qscale=1.0):
+        b = FFAG_Bunch(v, marcosize=1e13 / n * qscale, sc_grid_size=(*SC_GRID, 12.0), BunchType="Boris", device=dev)
         b.SEO_fi_axis, b.SEO_Ek_axis, b.SEO_r_matrix = seo["fi_axis"], seo["Ek_axis"], seo["r"]
         b.SEO_pr_matrix, b.SEO_perimeter = seo["pr"], seo["perimeter"]
-        sc = SpaceCharge(b, hockney=(mode == "hockney"))
+        return b, SpaceCharge(b, hockney=(mode == "hockney"))
+
+    for mode in ("periodic", "hockney"):
+        b, sc = make(mode)
         for k in range(warmup):
             sc.update(first=(k == 0))
         torch.cuda.synchronize()
@@ -243,25 +271,151 @@ def sc_bench(gp, dt, dev, updates=20, warmup=3, turns=2):
             sc.update(first=False)
         e1.record(sc.stream)
         torch.cuda.synchronize()
-        out[f"{mode}_ms_per_update"] = e0.elapsed_time(e1) / updates
-        if mode == "hockney":
-            sc_steps = STEPS_PER_TURN // 12
-            pusher = Pusher(b, gp, "Boris", "fp64")
-            clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
-            clock.ensure(STEPS_PER_TURN * (turns + 1))
-            step = 0
-            torch.cuda.synchronize()
-            e0.record(sc.stream)
-            for _ in range(turns * 12):
-                sc.update(first=False)
-                pusher.push(clock, step, sc_steps, sc_steps)
-                step += sc_steps
-            e1.record(sc.stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            out["cycle_particle_turns_per_s"] = n * turns / (ms * 1e-3)
-            out["cycle"] = "12 x (open-boundary update + 60 Boris fp64 steps) per turn"
-            out["alive_fraction"] = float((b.cols["surv"] == 1).float().mean().item())
+        ms = e0.elapsed_time(e1) / updates
+        out[f"{mode}_ms_per_update"] = ms
+        out[f"{mode}_roofline"] = {"bound": "hbm", "achieved": nbytes / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                                   "unit": "GB/s", "frac": nbytes / (ms * 1e-3) / 1e9 / hbm_peak}
+        del sc, b
+
+    sc_steps = STEPS_PER_TURN // 12
+
+    def cycle(precision, nturns, qscale=1.0, with_sc=True):
+        b, sc = make("hockney", qscale)
+        pusher = Pusher(b, gp, "Boris", precision)
+        clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
+        clock.ensure(STEPS_PER_TURN * (nturns + 1))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(sc.stream)
+        step = 0
+        for k in range(nturns * 12):
+            if with_sc:     # an update every 60 steps from step 0, as the step loop does
+                sc.update(first=(k == 0))
+            pusher.push(clock, step, sc_steps, sc_steps if with_sc else 0)
+            step += sc_steps
+        e1.record(sc.stream)
+        torch.cuda.synchronize()
+        alive = float((b.cols["surv"] == 1).float().mean().item())
+        return e0.elapsed_time(e1), alive
+
+    cycle("fp32c", 1)                   # warm-up
+    ms32, _ = cycle("fp32c", turns)
+    ms64, _ = cycle("fp64", turns)
+    out["cycle"] = "12 x (open-boundary update + 60 Boris FP32C steps) per turn"
+    out["cycle_particle_turns_per_s"] = n * turns / (ms32 * 1e-3)
+    out["cycle_fp64_particle_turns_per_s"] = n * turns / (ms64 * 1e-3)
+    out["cycle_ms_per_turn"] = {"fp32c": ms32 / turns, "fp64": ms64 / turns}
+    _, a1 = cycle("fp32c", 1)
+    _, a3 = cycle("fp32c", 1, qscale=1e-3)
+    _, a0 = cycle("fp32c", 1, with_sc=False)
+    out["alive_fraction_after_one_turn"] = {"full_charge": a1, "charge_x1e-3": a3, "no_space_charge": a0}
+    return out
+
+
+def rk4_bench(gp, dt, dev, steps, warmup, flush, n=N_PARTICLES, seed=7):
+    """c1 with the float64 RK4 pusher: the same lattice, RF and bunch (RK4
+    columns: f5 = total energy), 720 steps per turn, one turn per launch,
+    L2 flushed and the bunch restored between launches (outside the events)."""
+    import torch
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.track import Pusher, StepClock, _EphemeralBunch
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek(synthetic.centred_bunch(n, seed=seed))
+    v[:, 7] = 1.0
+    v[:, 8] = 1.0
+    b = _EphemeralBunch(v, "RK4", dev)
+    pristine = {k: t.clone() for k, t in b.cols.items()}
+    pu = Pusher(b, gp, "RK4", "fp64")
+    clock = StepClock(0.0, dt, gp.Emap, "RK4", dev)
+    clock.ensure(STEPS_PER_TURN * (warmup + steps + 1))
+    stream = pu.stream
+
+    def restore():
+        for k, t in b.cols.items():
+            t.copy_(pristine[k])
+
+    for k in range(warmup):
+        restore()
+        pu.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        restore()
+        flush.zero_()
+        ev[k][0].record(stream)
+        pu.push(clock, (warmup + k) * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.mean(a.elapsed_time(bb) for a, bb in ev)
+    return {"value": n / (ms * 1e-3), "unit": "particle-turns/s", "ms_per_turn": ms, "particles": n,
+            "steps_per_turn": STEPS_PER_TURN, "launches": steps}
+
+
+def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=7):
+    """c1's accuracy report: the c1 bunch tracked for 1000 turns with the RF
+    on by the float64 Boris pusher (the reference for the errors), the FP32C
+    Boris pusher and the float64 RK4 pusher, and by the float64 Boris pusher
+    from every radius times 1 + 2^-24 (the dynamics' own response to a
+    float32-sized input change).  Coordinates and rms emittances are compared
+    where the particles cross the azimuth half a turn from the bunch in the
+    last turn; tunes (FFT, the reference's estimator) from 1000 turns of
+    crossings of the first `tune_n` particles."""
+    import tempfile
+    import torch
+    from pyffa_b200 import diagnostics as D
+    from pyffa_b200 import synthetic
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.constants import E0_J, FFAG_ConversionTools
+    from pyffa_b200.dump import Dumps, PositionDumpBunch
+    from pyffa_b200.track import FFAG_RungeKutta
+    p = synthetic.centred_bunch(n, seed=seed)
+    conv = FFAG_ConversionTools()
+    target = (np.pi + np.mean(p[:, 4])) % (2 * np.pi)
+    nsteps = turns * STEPS_PER_TURN
+
+    def run(solver, precision, m, window_turns):
+        b = FFAG_Bunch(m, BunchType=solver, device=dev)
+        d = PositionDumpBunch(np.rad2deg(target), (nsteps - window_turns * STEPS_PER_TURN - 0.05 * STEPS_PER_TURN) * dt,
+                              (nsteps - 0.05 * STEPS_PER_TURN) * dt, save_folder=os.path.join(tempfile.mkdtemp(), "x"))
+        dumps = Dumps()
+        dumps.add_dump(d)
+        lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+              "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": dumps}
+        rk = FFAG_RungeKutta(precision=precision, verbose=False)
+        getattr(rk, "rk4_solve_dt_bunch3_withSC" if solver == "RK4" else "rk4_solve_dt_bunch3_withSC_boris")(
+            None, 0.0, b, gp, lp)
+        torch.cuda.synchronize()
+        return d.crossing_records, b.LocalBunch
+
+    vb = conv.ConvertPrzek2Vrzek_boris(p)
+    vr = conv.ConvertPrzek2Vrzek(p)
+    vb32 = vb.copy()
+    vb32[:, 0] *= 1 + 2.0 ** -24
+    cases = {"fp64_boris": ("Boris", "fp64", vb), "fp32c_boris": ("Boris", "fp32c", vb),
+             "fp64_rk4": ("RK4", "fp64", vr), "fp64_boris_r_1_2e-24": ("Boris", "fp64", vb32)}
+    last, tun, alive = {}, {}, {}
+    for name, (solver, prec, m) in cases.items():
+        t0 = time.perf_counter()
+        rec, end = run(solver, prec, m.copy(), 0.9)
+        last[name] = D.at_azimuth(rec, n, dt, solver, E0_J)
+        alive[name] = int((end[:, 8] == 1).sum())
+        rec_t, _ = run(solver, prec, m[:tune_n].copy(), turns)
+        tun[name] = D.tunes(D.crossing_table(rec_t, tune_n, dt, solver, E0_J))
+        last[name + "_s"] = time.perf_counter() - t0
+    out = {"particles": n, "turns": turns, "steps_per_turn": STEPS_PER_TURN, "rf": "2 gaps, last-gap semantics",
+           "vs": "fp64_boris", "tune_particles": tune_n, "alive": alive}
+    for name in ("fp32c_boris", "fp64_rk4", "fp64_boris_r_1_2e-24"):
+        e = D.azimuth_errors(last["fp64_boris"], last[name])
+        dq = np.abs(tun[name] - tun["fp64_boris"])
+        dq = np.minimum(dq, 1.0 - dq)
+        ok = np.isfinite(dq).all(1)
+        e["tune_max"] = [float(dq[ok, 0].max()), float(dq[ok, 1].max())] if ok.any() else None
+        e["tune_rms"] = [float(np.sqrt(np.mean(dq[ok, 0] ** 2))), float(np.sqrt(np.mean(dq[ok, 1] ** 2)))] \
+            if ok.any() else None
+        e["wall_s"] = last[name + "_s"]
+        out[name] = e
+    q = tun["fp64_boris"]
+    out["fp64_boris_tunes_median"] = [float(np.nanmedian(q[:, 0])), float(np.nanmedian(q[:, 1]))]
     return out
 
 
@@ -424,8 +578,51 @@ LEARNED_FLOP_PER_MAP = 2 * (5 * 256 + 2 * 256 * 256 + 256 * 4)
 LEARNED_MMA_FLOP_PER_MAP = 2 * (16 * 256 + 2 * 256 * 256 + 256 * 16)
 
 
+def same_lattice_push(gp_l, phys, dev, turns=2):
+    """The plain time-domain Boris pushers (FP64, FP32C) on the learned map's
+    own lattice (analytic field, no z-Taylor map, no RF) and bunch (the
+    learned map's states as Boris states at fi = 0), 720 steps of the
+    300 MeV design dt per launch.  The bunch spans 300-600 MeV, so a launch
+    carries each particle through a different fraction of a turn: the
+    particle-turns are counted from each particle's azimuth advance."""
+    import torch
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_EField_new
+    from pyffa_b200.learned import phys_to_boris
+    from pyffa_b200.track import Pusher, StepClock, _EphemeralBunch
+    gp2 = FFAG_GlobalParameters()
+    gp2.AddBMap(gp_l.Bmap)
+    gp2.AddEMap(FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=False))
+    m = phys_to_boris(phys)
+    dt = synthetic.design_dt(300.0, STEPS_PER_TURN)
+    out = {"particles": m.shape[0], "launches": turns, "steps_per_launch": STEPS_PER_TURN,
+           "lattice": "the learned map's: analytic field, no z-Taylor map, no RF"}
+    for prec in ("fp64", "fp32c"):
+        b = _EphemeralBunch(m, "Boris", dev)
+        pu = Pusher(b, gp2, "Boris", prec)
+        clock = StepClock(0.0, dt, gp2.Emap, "Boris", dev)
+        clock.ensure(STEPS_PER_TURN * (turns + 2))
+        pu.push(clock, 0, STEPS_PER_TURN, 0)
+        torch.cuda.synchronize()
+        fi0 = b.cols["fi"].clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(pu.stream)
+        for k in range(turns):
+            pu.push(clock, (k + 1) * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+        e1.record(pu.stream)
+        torch.cuda.synchronize()
+        pturns = float(((b.cols["fi"] - fi0) / (2 * np.pi)).sum().item())
+        ms = e0.elapsed_time(e1)
+        out[prec] = {"value": pturns / (ms * 1e-3), "unit": "particle-turns/s", "ms_per_launch": ms / turns,
+                     "particle_turns": pturns}
+        del b, pu
+        torch.cuda.empty_cache()
+    return out, gp2, dt
+
+
 def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=10_000_000, turns_per_step=50,
-                  steps=2, check_n=512, check_turns=1000):
+                  steps=10, check_n=512, check_turns=1000):
     """Learned sector map: train on `samples` one-sector crossings of the
     plain azimuth-domain tracker (300-600 MeV, amplitudes up to 10 mm / 5
     mrad, uniform in normalised phase space), then track an n-particle bunch
@@ -509,6 +706,12 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
         peaks = {"burst": 1590.0, "sustained": 1400.0,
                  "source": "fallback (MEASURED_PEAKS.json absent): 1.59 PF/s burst, 1.4 sustained"}
     ach = LEARNED_FLOP_PER_MAP * maps / k_s / 1e12
+    # the plain time-domain pushers on the same lattice and bunch
+    same, gp_same, dt_same = same_lattice_push(gp, phys, dev)
+    same["speedup_vs_fp64_same_lattice"] = value / same["fp64"]["value"]
+    same["speedup_vs_fp32c_same_lattice"] = value / same["fp32c"]["value"]
+    del phys
+    torch.cuda.empty_cache()
     # accuracy: a check bunch over 1000 turns against the FP64 plain tracker
     cb = bunch(check_n, 4)
     ref = learned.plain_track(frame, tracker, cb, check_turns, record=True)
@@ -517,6 +720,17 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
     dq = np.abs(learned.tunes(got["record"]) - learned.tunes(ref["record"]))
     de = np.abs(learned.betatron_emittance(frame, got["record"][-1]) /
                 learned.betatron_emittance(frame, ref["record"][-1]) - 1)
+    # and against the FP64 time-domain Boris pusher (60 steps per sector of
+    # the 300 MeV design), whose own truncation error shows as its
+    # difference from the azimuth-domain RK4
+    rb = learned.boris_record(frame, gp_same, cb, check_turns, dt_same, "fp64", dev)
+    ok = np.isfinite(rb).all(axis=(0, 2))
+    qb = learned.tunes(rb[:, ok])
+    dqb = np.abs(learned.tunes(got["record"][:, ok]) - qb)
+    dqbr = np.abs(learned.tunes(ref["record"][:, ok]) - qb)
+    eb = learned.betatron_emittance(frame, rb[-1][ok])
+    deb = np.abs(learned.betatron_emittance(frame, got["record"][-1][ok]) / eb - 1)
+    debr = np.abs(learned.betatron_emittance(frame, ref["record"][-1][ok]) / eb - 1)
     return {
         "value": value, "unit": "particle-turns/s",
         "speedup_vs_fp64": value / fp64_value if fp64_value else None,
@@ -535,7 +749,14 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
                                 "peak_source": peaks["source"]}},
         "accuracy": {"check_bunch": check_n, "turns": check_turns, "tune_error_max": float(dq.max()),
                      "tune_error_rms": float(np.sqrt(np.mean(dq ** 2))),
-                     "emittance_error_max": float(de.max()), "vs": "FP64 azimuth-domain RK4 tracker, 128 steps/sector"},
+                     "emittance_error_max": float(de.max()), "vs": "FP64 azimuth-domain RK4 tracker, 128 steps/sector",
+                     "vs_fp64_boris": {"states": int(ok.sum()), "tune_error_max": float(dqb.max()),
+                                       "tune_error_rms": float(np.sqrt(np.mean(dqb ** 2))),
+                                       "emittance_error_max": float(deb.max()),
+                                       "rk4_vs_boris_tune_max": float(dqbr.max()),
+                                       "rk4_vs_boris_emittance_max": float(debr.max()),
+                                       "boris": "FP64 time-domain Boris, 720 steps per turn at 300 MeV"}},
+        "same_lattice": same,
         "training": {"samples": samples, "epochs": epochs, "batch": 8192, "s": t_train, "data_s": t_data,
                      "steps": tr.t, "samples_per_s": tr.t * 8192 / t_train, "validation_mse": mse,
                      "residual_scale": tr.out_scale},
@@ -544,9 +765,23 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
     }
 
 
+def bench_config(n, precision, world):
+    """The workload both arms report (identical dicts)."""
+    return {"workload": "c1: 12-sector FFAG, 300 MeV, 1301x6000 map z-Taylor order 2, 2 RF gaps "
+                        "(last-gap semantics), Boris, 720 steps/turn, 1 turn per step",
+            "particles_per_gpu": n, "steps_per_turn": STEPS_PER_TURN, "precision": precision,
+            "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"}
+
+
+METRIC = "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)"
+
+
 def run_reference(args):
-    """--impl reference: the oracle port on the host cores, each step one turn
-    of a bounded sample."""
+    """--impl reference: the reference's algorithm on the host cores (the
+    oracle's C port, every thread; on one host it runs at 1.07x the
+    reference's own Numba path, oracle/time_reference_numba.py), on the same
+    bunch as the GPU arm; each step a bounded sample of one turn: the whole
+    bunch through REF_SAMPLE_STEPS of the turn's 720 steps, scaled."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -554,26 +789,27 @@ def run_reference(args):
     from oracle import oracle as O
     O.build()
     S = O.Setup(gp.Bmap, gp.Emap, gp)
-    sample_n = 10_000
+    O.boris_step(S, np.ascontiguousarray(v[:64].copy()), 0.0, dt)    # warm the library
     times = []
     for k in range(args.warmup + args.steps):
-        m = np.ascontiguousarray(v[:sample_n].copy())
+        m = np.ascontiguousarray(v.copy())
         t0 = time.perf_counter()
-        O.track(S, "Boris", m, 0.0, dt, STEPS_PER_TURN)
+        O.track(S, "Boris", m, 0.0, dt, REF_SAMPLE_STEPS)
         el = time.perf_counter() - t0
         if k >= args.warmup:
             times.append(el)
-    tot = sum(times)
-    val = sample_n * len(times) / tot
-    line = {"metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
-            "value": val, "unit": "particle-turns/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+    n = v.shape[0]
+    per_turn_s = sum(times) / len(times) * STEPS_PER_TURN / REF_SAMPLE_STEPS
+    val = n / per_turn_s
+    sample = (f"{n} particles (the GPU arm's bunch) x {REF_SAMPLE_STEPS} of the {STEPS_PER_TURN} steps of a turn "
+              f"per step, scaled to a turn")
+    line = {"metric": METRIC, "value": val, "unit": "particle-turns/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_turn_s,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded)", "config": {"workload": "c1: 12-sector FFAG, 300 MeV, 1301x6000 map, "
-                                                                 "2 RF gaps, Boris fp64, 720 steps/turn",
-                                                     "sample_particles": sample_n},
+            "data": "synthetic (seeded 6D Gaussian bunch, analytic lattice)",
+            "config": bench_config(n, "fp64", args.gpus),
             "cpu_baseline": {"value": val, "unit": "particle-turns/s", "cores": O.num_threads(), "kind": "port",
-                             "sample": f"{sample_n} particles x one turn per step"},
+                             "sample": sample},
             "e2e": {"value": val, "unit": "particle-turns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -778,7 +1014,13 @@ def main():
             cpu = cpu_baseline(gp, v, dt)
         sc = None
         if not args.no_sc and solo:
-            sc = sc_bench(gp, dt, dev)
+            sc = sc_bench(gp, dt, dev, hbm_peak)
+        rk4 = None
+        if not args.no_rk4 and solo:
+            rk4 = rk4_bench(gp, dt, dev, min(args.steps, 10), args.warmup, flush)
+        acc = None
+        if not args.no_accuracy and solo:
+            acc = c1_accuracy_bench(gp, dt, dev)
         mg = None
         if not args.no_mapgen and solo:
             mg = mapgen_bench(dev, hbm_peak)
@@ -793,15 +1035,12 @@ def main():
             lrn = learned_bench(dev, value / world, fp32c["value"] / world if fp32c else None,
                                 samples=args.learned_samples, epochs=args.learned_epochs, n=args.learned_n)
         line = {
-            "metric": "particle-turns/s (Boris FP64, 1e5-particle bunch, 2 RF gaps, z-Taylor order 2)",
+            "metric": METRIC,
             "value": value, "unit": "particle-turns/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32c",
             "data": "synthetic (seeded 6D Gaussian bunch, analytic lattice)",
-            "config": {"workload": "c1: 12-sector FFAG, 300 MeV, 1301x6000 map z-Taylor order 2, 2 RF gaps "
-                                   "(last-gap semantics), Boris, 720 steps/turn, 1 turn per step",
-                       "particles_per_gpu": n, "steps_per_turn": STEPS_PER_TURN, "precision": args.precision,
-                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "config": bench_config(n, args.precision, world),
             "gpu_launches": args.steps,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -809,6 +1048,8 @@ def main():
             "clocks": clocks,
             "status": {"lost": int(status[0]), "nan": int(status[1]), "out_of_map": int(status[2])},
             "space_charge": sc,
+            "rk4": rk4,
+            "c1_accuracy": acc,
             "fp32c": fp32c,
             "mapgen": mg,
             "co_scan": scan,

@@ -34,6 +34,7 @@ extern "C" {
 #define FFA_MAX_SEG 16
 #define FFA_MAX_GAPS 8
 #define FFA_MAX_ORDER 4
+#define FFA_MAX_HARMONICS 16
 
 enum ffa_error {
     FFA_OK = 0,
@@ -53,7 +54,8 @@ enum ffa_push_flags {
     /* Launch shape of the Boris pushers, bits 8-11 (0: the default shape).
      * Bits 8-9: threads per block 32 << v (32, 64, 128, 256).  Bits 10-11:
      * register cap per thread 80, 72, 64, 56; caps below 80 are built for the
-     * FFA_FP32C pusher without space charge (else FFA_ERR_UNSUPPORTED).  The
+     * FFA_FP32C pusher without space charge or field-error harmonics (else
+     * FFA_ERR_UNSUPPORTED).  The
      * shape sets how many warps are resident per SM, not the arithmetic: the
      * results are the same for every shape.  RK4 takes the default only. */
     FFA_SHAPE_TB_SHIFT = 8,
@@ -182,6 +184,19 @@ typedef struct ffa_fieldmap ffa_fieldmap;
  * loading (src/FFAG_Field.py:636-711). */
 int ffa_fieldmap_create(const ffa_field_desc *desc, void *stream, ffa_fieldmap **out);
 int ffa_fieldmap_destroy(ffa_fieldmap *fm);
+
+/* Field-error harmonics of a field map: every pusher then adds
+ * Bz += sum_k amp[k] cos(m[k] fi + phase[k]) over the k with
+ * rmin[k] <= r <= rmax[k] (fi the unwrapped azimuth; Br, Bfi unchanged) after
+ * the mid-plane map.  Replaces FFAG_BField_Error + AddBHarmonics_to_Bmap_njit
+ * (src/FFAG_Field.py:947-1042, bharmonics_kernel_1d :1541-1587) as called by
+ * Boris_solve (src/FFAG_track.py:1007) and FunctionForAccelerationBunch_dt
+ * (:1782).  Host arrays of n <= FFA_MAX_HARMONICS values (amp in tesla, phase
+ * in rad, m an integer), copied to a small device table (allocated on the
+ * first call, synchronous copy); n = 0 removes them.  The closed-orbit tracks
+ * (ffa_theta_track) do not take them.  Takes effect for later pushes. */
+int ffa_fieldmap_set_harmonics(ffa_fieldmap *fm, int32_t n, const double *m, const double *amp,
+                               const double *phase, const double *rmin, const double *rmax);
 
 /* Applies the injection of absolute step `step` (flags only).
  * Replaces FFAG_Bunch.InjectParticles (src/FFAG_Bunch.py:265-303). */

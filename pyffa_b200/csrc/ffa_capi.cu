@@ -123,6 +123,10 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
         return FFA_ERR_INVALID;
     for (int j = 0; j < d->n_convex; ++j)
         if (!(d->convex[5 * j + 2] != 0.0)) return FFA_ERR_INVALID;
+    // the push kernels index the node table with 32-bit offsets (12 values per
+    // node at most): larger tables are refused
+    if (d->max_order > 0 && (double)d->r_size * (double)d->fi_size * 12.0 >= 2147483647.0)
+        return FFA_ERR_UNSUPPORTED;
 
     ffa_fieldmap *fm = (ffa_fieldmap *)calloc(1, sizeof(ffa_fieldmap));
     if (!fm) return FFA_ERR_NOMEM;
@@ -216,11 +220,36 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
     return FFA_OK;
 }
 
+int ffa_fieldmap_set_harmonics(ffa_fieldmap *fm, int32_t n, const double *m, const double *amp,
+                               const double *phase, const double *rmin, const double *rmax)
+{
+    if (!fm || n < 0) return FFA_ERR_INVALID;
+    if (n > FFA_MAX_HARMONICS) return FFA_ERR_UNSUPPORTED;
+    if (n > 0 && (!m || !amp || !phase || !rmin || !rmax)) return FFA_ERR_INVALID;
+    double rows[5 * FFA_MAX_HARMONICS] = {0};
+    for (int k = 0; k < n; ++k) {
+        if (m[k] != floor(m[k]) || !isfinite(amp[k]) || !isfinite(phase[k])) return FFA_ERR_INVALID;
+        rows[5 * k] = m[k];
+        rows[5 * k + 1] = amp[k];
+        rows[5 * k + 2] = phase[k];
+        rows[5 * k + 3] = rmin[k];
+        rows[5 * k + 4] = rmax[k];
+    }
+    if (n > 0) {
+        if (!fm->harm && cudaMalloc(&fm->harm, sizeof(rows)) != cudaSuccess) return FFA_ERR_NOMEM;
+        FFA_CHECK_CUDA(cudaMemcpy(fm->harm, rows, sizeof(rows), cudaMemcpyHostToDevice));
+    }
+    fm->k.harm = fm->harm;
+    fm->k.n_harm = n;
+    return FFA_OK;
+}
+
 int ffa_fieldmap_destroy(ffa_fieldmap *fm)
 {
     if (!fm) return FFA_OK;
     if (fm->nodes64) cudaFree(fm->nodes64);
     if (fm->nodes32) cudaFree(fm->nodes32);
+    if (fm->harm) cudaFree(fm->harm);
     free(fm);
     return FFA_OK;
 }
@@ -250,7 +279,8 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
     const int tb_sel = (flags >> FFA_SHAPE_TB_SHIFT) & 3, nreg_sel = (flags >> FFA_SHAPE_NREG_SHIFT) & 3;
     if ((flags & FFA_RK4) && (tb_sel | nreg_sel)) return FFA_ERR_UNSUPPORTED;
-    if (nreg_sel && (!(flags & FFA_FP32C) || (sc_step > 0 && st->sc_pre))) return FFA_ERR_UNSUPPORTED;
+    if (nreg_sel && (!(flags & FFA_FP32C) || (sc_step > 0 && st->sc_pre) || fm->k.n_harm > 0))
+        return FFA_ERR_UNSUPPORTED;
     if (n == 0 || nsteps == 0) return FFA_OK;
 
     PushK p;

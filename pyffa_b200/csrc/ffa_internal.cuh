@@ -47,6 +47,11 @@ struct FieldK {
     // (truncation below 2^-56 relative); pw_tlim = -1 disables it
     double pw_r0, pw_inv_r0, pw_tlim, pw_r0m;
     double pw_c[16];
+    // field-error harmonics: Bz += sum_k amp cos(m fi + phase) over the n_harm
+    // rows (m, amp, phase, rmin, rmax) of the device table `harm` with
+    // rmin <= r <= rmax (fi unwrapped)
+    int32_t n_harm, pad2;
+    const double *harm;
 };
 
 struct RFK {
@@ -92,6 +97,7 @@ struct ffa_fieldmap {
     ffa::FieldK k;
     double *nodes64;
     float *nodes32;
+    double *harm;         // device, FFA_MAX_HARMONICS rows of 5
 };
 
 // Launchers implemented in ffa_push.cu

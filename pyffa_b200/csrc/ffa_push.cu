@@ -35,10 +35,19 @@ namespace ffa {
 __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double ir, double fim, double zi,
                                              double &Bz, double &Br, double &Bfi)
 {
-    double spiral = 0.0, spiral_p = 0.0;
-    if (!f.spiral_zero) {   // all-zero coefficients evaluate to exactly 0
+    // theta' = (fi mod P) - s(r), reduced mod P again.  Without a spiral
+    // (all-zero coefficients evaluate to exactly 0) the callers' fim is
+    // reduced already: the second reduction would only map a fim within an
+    // ulp of P to about 0 (a step lands there with probability ~1e-16), so
+    // it is skipped with the polynomials.
+    double spiral_p = 0.0;
+    double fs = fim;
+    if (!f.spiral_zero) {
+        double spiral = 0.0;
         for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * ri + f.spoly[a];
         for (int a = 0; a < f.n_spolyp; ++a) spiral_p = spiral_p * ri + f.spolyp[a];
+        fs = fim - spiral;
+        fs -= f.period * floor(fs * f.inv_period);
     }
     double B0r, B0r_p;
     if (f.k == 0.0) {
@@ -62,8 +71,6 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0r_p = f.B0k * pk1;
         B0r = f.B0 * (pk1 * ri);
     }
-    double fs = fim - spiral;
-    fs -= f.period * floor(fs * f.inv_period);
     double B0F = 0.0, B0Fp = 0.0;
     for (int j = 0; j < f.n_seg; ++j) {
         const double ks = f.seg_k[j];
@@ -111,6 +118,11 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
 
 // Bilinear lookup of the z-Taylor coefficients: int() truncation, index
 // clamped to [0, n-2], weights not clamped (linear extrapolation).
+// Node indices are 32-bit (the largest table offset, NX * NY * 12 values, is
+// below 2^31): the truncation saturates outside the int range, where the
+// clamp applies anyway, and a NaN coordinate truncates to node 0.
+__device__ __forceinline__ int trunc_index(double q) { return __double2int_rz(q); }
+
 template <int MAXO>
 __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double y, double z,
                                                double &Bz, double &Bfi, double &Br, int &clamped)
@@ -121,12 +133,13 @@ __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double
     // changes by rounding only
     const double qx = (x - f.r_min) * f.inv_r_step;
     const double qy = (y - f.fi_min) * f.inv_fi_step;
-    int64_t i = (int64_t)qx;
-    int64_t j = (int64_t)qy;
+    const int nr = (int)f.r_size, nf = (int)f.fi_size;
+    int i = trunc_index(qx);
+    int j = trunc_index(qy);
     if (i < 0) { i = 0; ++clamped; }
-    else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
+    else if (i >= nr - 1) { i = nr - 2; ++clamped; }
     if (j < 0) { j = 0; ++clamped; }
-    else if (j >= f.fi_size - 1) { j = f.fi_size - 2; ++clamped; }
+    else if (j >= nf - 1) { j = nf - 2; ++clamped; }
     const double tx = qx - (double)i;
     const double ty = qy - (double)j;
     const double w00 = (1.0 - tx) * (1.0 - ty), w01 = (1.0 - tx) * ty;
@@ -134,10 +147,10 @@ __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double
     constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
     constexpr int NV = 3 * MAXO;
     const double *nd[4];
-    nd[0] = f.nodes64 + (i * f.fi_size + j) * NP;  // (i, j)
-    nd[1] = nd[0] + NP;                            // (i, j+1)
-    nd[2] = nd[0] + f.fi_size * NP;                // (i+1, j)
-    nd[3] = nd[2] + NP;                            // (i+1, j+1)
+    nd[0] = f.nodes64 + (i * nf + j) * NP;    // (i, j)
+    nd[1] = nd[0] + NP;                       // (i, j+1)
+    nd[2] = nd[0] + nf * NP;                  // (i+1, j)
+    nd[3] = nd[2] + NP;                       // (i+1, j+1)
     const double w[4] = {w00, w01, w10, w11};
     // accumulate node by node in the reference's order w00, w01, w10, w11;
     // a node's coefficients are 16 B aligned pairs
@@ -166,6 +179,23 @@ __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double
         ze *= z2;
         zo *= z2;
     }
+}
+
+// bharmonics_kernel_1d (src/FFAG_Field.py:1541-1587) for one particle: the
+// Bz sum of the field-error harmonics (rows m, amp, phase, rmin, rmax of the
+// device table h) whose radial band holds r, fi the unwrapped azimuth; the
+// caller adds it to Bz after the map as the reference does, Br and Bfi take
+// nothing.  Compiled only into the kernel variants launched for a map with
+// harmonics, so the others keep their registers.
+__device__ __forceinline__ double harmonics_bz(const double *h, int n, double r, double fi)
+{
+    if (!(r > 0.0)) return 0.0;
+    double b = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double *row = h + 5 * k;
+        if (row[3] <= r && r <= row[4]) b += row[1] * cos(row[0] * fi + row[2]);
+    }
+    return b;
 }
 
 // One gap of emap_kernel: inside test on (x, y) = r (cos fi, sin fi).
@@ -344,17 +374,18 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
     if constexpr (MAXO >= 1) {
         const double qx = (r - f.r_min) * f.inv_r_step;
         const double qy = (fim - f.fi_min) * f.inv_fi_step;
-        int64_t i = (int64_t)qx, jj = (int64_t)qy;
-        if (i < 0) { i = 0; ++clamped; } else if (i >= f.r_size - 1) { i = f.r_size - 2; ++clamped; }
-        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= f.fi_size - 1) { jj = f.fi_size - 2; ++clamped; }
+        const int nr = (int)f.r_size, nf = (int)f.fi_size;
+        int i = trunc_index(qx), jj = trunc_index(qy);
+        if (i < 0) { i = 0; ++clamped; } else if (i >= nr - 1) { i = nr - 2; ++clamped; }
+        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= nf - 1) { jj = nf - 2; ++clamped; }
         const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
         const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
         constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
         constexpr int NV = 3 * MAXO;
         const float *nd[4];
-        nd[0] = f.nodes32 + (i * f.fi_size + jj) * NP;
+        nd[0] = f.nodes32 + (i * nf + jj) * NP;
         nd[1] = nd[0] + NP;
-        nd[2] = nd[0] + f.fi_size * NP;
+        nd[2] = nd[0] + nf * NP;
         nd[3] = nd[2] + NP;
         float acc[NV];
 #pragma unroll
@@ -396,8 +427,11 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
         B0r_p = f.kc1 * g;
         B0r = f.c1 * g * r;
     }
-    double fs = fim - spiral;
-    fs -= f.period * floor(fs * f.inv_period);
+    double fs = fim;
+    if (!f.spiral_zero) {   // as in analytic_b64
+        fs = fim - spiral;
+        fs -= f.period * floor(fs * f.inv_period);
+    }
     double F = 0.0, Fp = 0.0;
     for (int j = 0; j < f.n_seg; ++j) {
         const float a1 = (float)(f.seg_k[j] * (fs - f.seg_x0[j]));
@@ -437,7 +471,7 @@ constexpr int BORIS_TB = 32;
 // float32 pusher without space charge is also built with 72, 64 and 56
 // (more resident warps, more spills) for the launch-shape autotuner.  The
 // cap changes register allocation only, not the arithmetic.
-template <int MAXO, bool SC, bool XING, bool F32, int NREG = 80>
+template <int MAXO, bool SC, bool XING, bool F32, int NREG = 80, bool HARM = false>
 __global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -487,6 +521,7 @@ __global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
                 Bfi += hf;
                 Br += hr;
             }
+            if constexpr (HARM) Bz += harmonics_bz(f.harm, f.n_harm, r, fi);
             double Er, Efi;
             rf_field64(p.rf, acc, r, fi, rfph, Er, Efi);
             double Ez = 0.0;
@@ -575,7 +610,7 @@ struct Y7 {
 };
 
 // RK4_equations_of_motion_njit for one live particle at stage state y.
-template <int MAXO>
+template <int MAXO, bool HARM>
 __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double rate, double acc,
                                           double esr, double esz, double esf, Y7 &d, int &oob)
 {
@@ -585,6 +620,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     double Bz, Br, Bfi;
     analytic_b64(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi);
     if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
+    if constexpr (HARM) Bz += harmonics_bz(f.harm, f.n_harm, y.r, y.fi);
     double Er, Efi;
     rf_field64(p.rf, acc, y.r, y.fi, y.rf, Er, Efi);
     double Ez = 0.0;
@@ -607,7 +643,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     d.rf = rate;
 }
 
-template <int MAXO, bool SC, bool XING>
+template <int MAXO, bool SC, bool XING, bool HARM = false>
 __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -644,18 +680,18 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
             continue;
         }
         Y7 d, k1, k2, k3, k4, ys;
-        rk4_rhs64<MAXO>(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM>(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
         k1 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k1.r, y.vr + 0.5 * k1.vr, y.z + 0.5 * k1.z, y.vz + 0.5 * k1.vz,
               y.fi + 0.5 * k1.fi, y.E + 0.5 * k1.E, y.rf + 0.5 * k1.rf};
-        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
         k2 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k2.r, y.vr + 0.5 * k2.vr, y.z + 0.5 * k2.z, y.vz + 0.5 * k2.vz,
               y.fi + 0.5 * k2.fi, y.E + 0.5 * k2.E, y.rf + 0.5 * k2.rf};
-        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
         k3 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + k3.r, y.vr + k3.vr, y.z + k3.z, y.vz + k3.vz, y.fi + k3.fi, y.E + k3.E, y.rf + k3.rf};
-        rk4_rhs64<MAXO>(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
         k4 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         y.r += (k1.r + 2 * k2.r + 2 * k3.r + k4.r) / 6;
         y.vr += (k1.vr + 2 * k2.vr + 2 * k3.vr + k4.vr) / 6;
@@ -777,19 +813,41 @@ cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, fl
     return cudaGetLastError();
 }
 
+// Field-error harmonics select their own kernel variants (HARM), so that
+// the harmonic sum costs the common case nothing.
+template <int MAXO, bool SC, bool F32>
+static void boris_default(const PushK &p, cudaStream_t s, int tb)
+{
+    const unsigned g = (unsigned)((p.n + tb - 1) / tb);
+    const bool x = p.xing.buf != nullptr;
+    if (p.f.n_harm > 0) {
+        if (x) boris_f64_kernel<MAXO, SC, true, F32, 80, true><<<g, tb, 0, s>>>(p);
+        else boris_f64_kernel<MAXO, SC, false, F32, 80, true><<<g, tb, 0, s>>>(p);
+    } else {
+        if (x) boris_f64_kernel<MAXO, SC, true, F32><<<g, tb, 0, s>>>(p);
+        else boris_f64_kernel<MAXO, SC, false, F32><<<g, tb, 0, s>>>(p);
+    }
+}
+
 template <int MAXO, bool SC>
 static void boris_launch(const PushK &p, cudaStream_t s, int tb, int)
 {
-    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
-    else boris_f64_kernel<MAXO, SC, false, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    boris_default<MAXO, SC, false>(p, s, tb);
 }
 
 template <int MAXO, bool SC>
 static void rk4_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = 128;
-    if (p.xing.buf) rk4_f64_kernel<MAXO, SC, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
-    else rk4_f64_kernel<MAXO, SC, false><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    const unsigned g = (unsigned)((p.n + tb - 1) / tb);
+    const bool x = p.xing.buf != nullptr;
+    if (p.f.n_harm > 0) {
+        if (x) rk4_f64_kernel<MAXO, SC, true, true><<<g, tb, 0, s>>>(p);
+        else rk4_f64_kernel<MAXO, SC, false, true><<<g, tb, 0, s>>>(p);
+    } else {
+        if (x) rk4_f64_kernel<MAXO, SC, true><<<g, tb, 0, s>>>(p);
+        else rk4_f64_kernel<MAXO, SC, false><<<g, tb, 0, s>>>(p);
+    }
 }
 
 #define FFA_DISPATCH(FN, p, ...)                                                       \
@@ -826,7 +884,7 @@ template <int MAXO, bool SC>
 static void boris32_launch(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
 {
     if constexpr (!SC) {
-        if (nreg_sel != 0) {   // the caller has checked: no space charge
+        if (nreg_sel != 0) {   // the caller has checked: no space charge, no harmonics
             const bool x = p.xing.buf != nullptr;
             switch (nreg_sel) {
             case 1: x ? boris32_shaped<MAXO, true, 72>(p, s, tb) : boris32_shaped<MAXO, false, 72>(p, s, tb); break;
@@ -836,8 +894,7 @@ static void boris32_launch(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
             return;
         }
     }
-    if (p.xing.buf) boris_f64_kernel<MAXO, SC, true, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
-    else boris_f64_kernel<MAXO, SC, false, true><<<(unsigned)((p.n + tb - 1) / tb), tb, 0, s>>>(p);
+    boris_default<MAXO, SC, true>(p, s, tb);
 }
 
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel)

@@ -1,34 +1,37 @@
 // ffa_sc.cu -- 2.5D slice-by-slice space charge on the GPU.
 //
 // One update (FFAG_Bunch.Build_2_5D_SliceGrid_sbs, src/FFAG_Bunch.py:1157-1352)
-// runs as a chain of stream-ordered kernels with every intermediate scalar
-// kept on the device, so the host never waits inside an update:
+// runs as a short chain of stream-ordered kernels with every intermediate
+// scalar kept on the device, so the host never waits inside an update:
 //   pass1   per particle: gamma, fi mod 2pi, closed-orbit lookup r0 / pr0,
-//           x = r - r0; per-block partial count, sum(gamma) and the extreme
-//           azimuths under 4 trial shifts   (GetLocalCoordinates_2p5,
-//           src/FFAG_SC_new.py:74-147; divide_arc2 :534-567; lookup
-//           src/FFAG_Bunch.py:1227-1244)
-//   reduce1 one block: arc [fi_s, fi_e], slice width, mean gamma
-//           (merge_multiple_arcs :577-606 for one rank)
-//   pass2   slice index and the moment sums   (ComputeSliceBoundsAndCoordsSBS_merged
-//           :449-531)
-//   reduce2 one block: box mean +- sigma_ratio * sigma, bunch length, cell
-//           charge   (src/FFAG_Bunch.py:1265-1294)
-//   deposit CIC weights accumulated as 2^-40 fixed-point integers with 64-bit
-//           atomics: the sum is exact, so the charge cube is identical for any
-//           particle order and launch (DistributeChargeSBS_Njit :244-312
-//           accumulates float32 in particle order)
-//   solve   per slice: 2D FFT, multiply by the periodic 1/(eps0 k^2) kernel
-//           (make_fft_kernel_open_numba :731-760) or by the FFT of the
-//           open-boundary Green's function on the doubled grid (Hockney),
-//           inverse FFT.  The FFTs are batched radix-2 transforms of whole
-//           lines held in shared memory, one kernel per axis, with the cube
-//           resident in L2 between passes.
-//   field   central differences of the potential / gamma^2
+//           x = r - r0, the moment sums and the extreme azimuths under 4
+//           trial shifts (GetLocalCoordinates_2p5, src/FFAG_SC_new.py:74-147;
+//           divide_arc2 :534-567; lookup src/FFAG_Bunch.py:1227-1244; sums of
+//           ComputeSliceBoundsAndCoordsSBS_merged :449-531).  The last block
+//           to finish folds the block partials in a fixed order: arc
+//           [fi_s, fi_e], slice width, mean gamma (merge_multiple_arcs
+//           :577-606 for one rank), box mean +- sigma_ratio * sigma, bunch
+//           length and cell charge (src/FFAG_Bunch.py:1265-1294).
+//   deposit slice index, then CIC weights accumulated as 2^-40 fixed-point
+//           integers with 64-bit atomics: the sum is exact, so the charge cube
+//           is identical for any particle order and launch
+//           (DistributeChargeSBS_Njit :244-312 accumulates float32 in
+//           particle order)
+//   green   open boundary only: the transform of the free-space Green's
+//           function on the doubled grid, float64, as a sum of cosines
+//   solve   ONE block per slice, the slice resident in shared memory: real
+//           FFT of the charge (rows paired as real and imaginary parts),
+//           per column the z transform, the kernel multiply (periodic
+//           1/(eps0 k^2) of make_fft_kernel_open_numba :731-760, or the Green
+//           transform) and the inverse, inverse real FFT of the rows, and the
+//           central-difference field / gamma^2
 //           (compute_field_from_potential_numba_SBS :672-728)
 //   gather  bilinear field at each particle, projected on the orbit
-//           direction (interpolate_fields_to_particles_SBS_numba :870-972)
-//   roll    the two extrapolation endpoints (src/FFAG_track.py:341-400)
+//           direction (interpolate_fields_to_particles_SBS_numba :870-972),
+//           and the roll of the two extrapolation endpoints
+//           (src/FFAG_track.py:341-400) in the same pass
+// Grids the fused solve does not cover (nx != nz, or sizes other than 32, 64
+// and 128) take a chain of batched line FFTs through a global work cube.
 // Block partial sums use a fixed grid and fixed reduction order, so every
 // update is bit-for-bit reproducible run to run.
 #include <math.h>
@@ -48,21 +51,17 @@ constexpr double EPS0 = 8.854187817e-12;
 
 struct SCState {
     ffa_sc_diag diag;
-    double amin[4], amax[4];
-    double sum_gamma;
     double inv_dx, inv_dz;
     int32_t degenerate;   // dx <= 0 or dz <= 0: fields are not updated
     int32_t bad;          // degenerate or bunch length <= 0: gathered field = 0
 };
 
-struct Partial1 {
+// per-block partial sums of pass1
+struct Partial {
     double sum_gamma;
     double amin[4], amax[4];
-    long long count;
-};
-
-struct Partial2 {
     double sx, sz, sx2, sz2;
+    long long count;
 };
 
 __device__ __forceinline__ double fast_mod(double a, double b) { return a - b * floor(a / b); }
@@ -97,178 +96,104 @@ __device__ __forceinline__ double seo_lookup(const double *Z, double X0, double 
     return (1 - tx) * (1 - ty) * z00 + (1 - tx) * ty * z01 + tx * (1 - ty) * z10 + tx * ty * z11;
 }
 
-template <typename T>
-__device__ T block_sum(T v, T *sh)
+// Warp tree (shuffle down) then warp 0's values folded in warp order by
+// thread 0: the same order on every run.
+template <typename T, typename Op>
+__device__ __forceinline__ T warp_fold(T v, Op op)
 {
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    T r = 0;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r += sh[k];
-    return r;  // valid in thread 0
+    for (int off = 16; off > 0; off >>= 1) v = op(v, __shfl_down_sync(0xffffffffu, v, off));
+    return v;
 }
 
-__device__ double block_min(double v, double *sh)
+struct OpSum { template <typename T> __device__ T operator()(T a, T b) const { return a + b; } };
+struct OpMin { __device__ double operator()(double a, double b) const { return fmin(a, b); } };
+struct OpMax { __device__ double operator()(double a, double b) const { return fmax(a, b); } };
+
+// Block reduction of one Partial per thread (valid in thread 0).  Per value:
+// warp tree, then thread 0 folds the warps' results starting from the
+// identity (0, +1e300 / -1e300 for min / max), in warp order.
+__device__ Partial block_partial(const Partial &p)
 {
-    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, off));
+    constexpr int NW = SC_TB / 32;
+    __shared__ double sh[NW][13];
+    __shared__ long long shc[NW];
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    double r = 1e300;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = fmin(r, sh[k]);
-    return r;
-}
-
-__device__ double block_max(double v, double *sh)
-{
-    for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    __syncthreads();
-    if (l == 0) sh[w] = v;
-    __syncthreads();
-    double r = -1e300;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = fmax(r, sh[k]);
-    return r;
-}
-
-// ----------------------------------------------------------------- passes
-
-__global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ffa_sc_desc d, double *x_out,
-                                                  double *pr0_out, int32_t *slice, int64_t *cell, Partial1 *part)
-{
-    __shared__ double shd[32];
-    __shared__ long long shl[32];
-    const double shifts[4] = {0.0, PI, PI * 0.5, PI * 1.5};
-    double sg = 0.0;
-    long long cnt = 0;
-    double mn[4] = {1e30, 1e30, 1e30, 1e30}, mx[4] = {-1e30, -1e30, -1e30, -1e30};
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        slice[i] = -1;
-        cell[i] = -1;
-        if (S.surv[i] == 0) continue;
-        const double g = gamma_of(S, i, d.boris, d.speed_c, d.E0_J);
-        const double fi = S.fi[i];
-        const double fm = fi - 2 * PI * floor(fi / (2 * PI));
-        const double Ek = (g - 1) * d.E0_rest_MeV;
-        const double r0 = seo_lookup(d.seo_r, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
-        pr0_out[i] = seo_lookup(d.seo_pr, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
-        x_out[i] = S.r[i] - r0;
-        sg += g;
-        ++cnt;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const double v = fast_mod(fm + shifts[k], 2 * PI);
-            mn[k] = fmin(mn[k], v);
-            mx[k] = fmax(mx[k], v);
-        }
-    }
-    const double bsg = block_sum(sg, shd);
-    const long long bcnt = block_sum(cnt, shl);
-    double bmn[4], bmx[4];
+    double v[13];
+    v[0] = warp_fold(p.sum_gamma, OpSum());
     for (int k = 0; k < 4; ++k) {
-        bmn[k] = block_min(mn[k], shd);
-        bmx[k] = block_max(mx[k], shd);
+        v[1 + k] = warp_fold(p.amin[k], OpMin());
+        v[5 + k] = warp_fold(p.amax[k], OpMax());
     }
+    v[9] = warp_fold(p.sx, OpSum());
+    v[10] = warp_fold(p.sz, OpSum());
+    v[11] = warp_fold(p.sx2, OpSum());
+    v[12] = warp_fold(p.sz2, OpSum());
+    const long long c = warp_fold(p.count, OpSum());
+    __syncthreads();
+    if (l == 0) {
+        for (int k = 0; k < 13; ++k) sh[w][k] = v[k];
+        shc[w] = c;
+    }
+    __syncthreads();
+    Partial r;
+    r.sum_gamma = 0.0; r.sx = r.sz = r.sx2 = r.sz2 = 0.0; r.count = 0;
+    for (int k = 0; k < 4; ++k) { r.amin[k] = 1e300; r.amax[k] = -1e300; }
     if (threadIdx.x == 0) {
-        Partial1 &P = part[blockIdx.x];
-        P.sum_gamma = bsg;
-        P.count = bcnt;
-        for (int k = 0; k < 4; ++k) { P.amin[k] = bmn[k]; P.amax[k] = bmx[k]; }
-    }
-}
-
-// One block of SC_TB threads: each thread folds a fixed strided subset of the
-// block partials, then a fixed-shape tree -- the same order on every run.
-__global__ void __launch_bounds__(SC_TB) sc_reduce1(const Partial1 *part, int nblk, ffa_sc_desc d, SCState *st)
-{
-    __shared__ double shd[32];
-    __shared__ long long shl[32];
-    double sg = 0.0;
-    long long cnt = 0;
-    double mn[4] = {1e30, 1e30, 1e30, 1e30}, mx[4] = {-1e30, -1e30, -1e30, -1e30};
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-        sg += part[b].sum_gamma;
-        cnt += part[b].count;
-        for (int k = 0; k < 4; ++k) {
-            mn[k] = fmin(mn[k], part[b].amin[k]);
-            mx[k] = fmax(mx[k], part[b].amax[k]);
+        for (int q = 0; q < NW; ++q) {
+            r.sum_gamma += sh[q][0];
+            for (int k = 0; k < 4; ++k) {
+                r.amin[k] = fmin(r.amin[k], sh[q][1 + k]);
+                r.amax[k] = fmax(r.amax[k], sh[q][5 + k]);
+            }
+            r.sx += sh[q][9]; r.sz += sh[q][10]; r.sx2 += sh[q][11]; r.sz2 += sh[q][12];
+            r.count += shc[q];
         }
     }
-    sg = block_sum(sg, shd);
-    cnt = block_sum(cnt, shl);
-    for (int k = 0; k < 4; ++k) {
-        mn[k] = block_min(mn[k], shd);
-        mx[k] = block_max(mx[k], shd);
+    return r;
+}
+
+// The final state from the block partials, by one block: each thread folds a
+// fixed strided subset of the partials, then the block reduction above.
+__device__ void finalize_state(const Partial *part, int nblk, const ffa_sc_desc &d, SCState *st, int64_t *status)
+{
+    Partial a;
+    a.sum_gamma = 0.0; a.sx = a.sz = a.sx2 = a.sz2 = 0.0; a.count = 0;
+    for (int k = 0; k < 4; ++k) { a.amin[k] = 1e30; a.amax[k] = -1e30; }
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+        const Partial *q = part + b;
+        a.sum_gamma += __ldcg(&q->sum_gamma);
+        a.count += __ldcg(&q->count);
+        for (int k = 0; k < 4; ++k) {
+            a.amin[k] = fmin(a.amin[k], __ldcg(&q->amin[k]));
+            a.amax[k] = fmax(a.amax[k], __ldcg(&q->amax[k]));
+        }
+        a.sx += __ldcg(&q->sx); a.sz += __ldcg(&q->sz); a.sx2 += __ldcg(&q->sx2); a.sz2 += __ldcg(&q->sz2);
     }
+    const Partial t = block_partial(a);
     if (threadIdx.x != 0) return;
+    ffa_sc_diag &D = st->diag;
+    // arc: the trial shift with the smallest span (merge_multiple_arcs)
     const double shifts[4] = {0.0, PI, PI * 0.5, PI * 1.5};
     int best = 0;
-    double best_span = mx[0] - mn[0];
+    double best_span = t.amax[0] - t.amin[0];
     for (int k = 1; k < 4; ++k)
-        if (mx[k] - mn[k] < best_span) { best_span = mx[k] - mn[k]; best = k; }
-    double arc_s = mn[best] - shifts[best], arc_e = mx[best] - shifts[best];
+        if (t.amax[k] - t.amin[k] < best_span) { best_span = t.amax[k] - t.amin[k]; best = k; }
+    double arc_s = t.amin[best] - shifts[best], arc_e = t.amax[best] - shifts[best];
     if (arc_e < arc_s) arc_e += 2 * PI;
     double fi_s = py_mod(arc_s, 2 * PI), fi_e = py_mod(arc_e, 2 * PI);
     if (fi_e <= fi_s) fi_e += 2 * PI;
-    ffa_sc_diag &D = st->diag;
+    const long long cnt = t.count;
     D.fi_s = fi_s;
     D.fi_e = fi_e;
     D.slice_step = (fi_e - fi_s) / (d.ns - 1);
     D.count = cnt;
-    D.mean_gamma_m1 = cnt > 0 ? sg / (double)cnt - 1.0 : 0.0;
-    st->sum_gamma = sg;
-}
-
-__global__ void __launch_bounds__(SC_TB) sc_pass2(ffa_state_soa S, int64_t n, ffa_sc_desc d, const double *x,
-                                                  int32_t *slice, const SCState *st, Partial2 *part)
-{
-    __shared__ double shd[32];
-    const double fi_s = st->diag.fi_s, step = st->diag.slice_step;
-    double sx = 0, sz = 0, sx2 = 0, sz2 = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (S.surv[i] == 0) continue;
-        const double xi = x[i], zi = S.z[i];
-        sx += xi;
-        sz += zi;
-        sx2 += xi * xi;
-        sz2 += zi * zi;
-        double fi = S.fi[i];
-        fi = fi - 2 * PI * floor(fi / (2 * PI));
-        if (fi < fi_s) fi += 2 * PI;
-        int64_t s = (int64_t)((fi - fi_s) / step);
-        if (s < 0) s = 0; else if (s >= d.ns) s = d.ns - 1;
-        slice[i] = (int32_t)s;
-    }
-    const double a = block_sum(sx, shd), b = block_sum(sz, shd), c = block_sum(sx2, shd), e = block_sum(sz2, shd);
-    if (threadIdx.x == 0) part[blockIdx.x] = Partial2{a, b, c, e};
-}
-
-__global__ void __launch_bounds__(SC_TB) sc_reduce2(const Partial2 *part, int nblk, ffa_sc_desc d, SCState *st,
-                                                    int64_t *status)
-{
-    __shared__ double shd[32];
-    double sx = 0, sz = 0, sx2 = 0, sz2 = 0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-        sx += part[b].sx; sz += part[b].sz; sx2 += part[b].sx2; sz2 += part[b].sz2;
-    }
-    sx = block_sum(sx, shd);
-    sz = block_sum(sz, shd);
-    sx2 = block_sum(sx2, shd);
-    sz2 = block_sum(sz2, shd);
-    if (threadIdx.x != 0) return;
-    ffa_sc_diag &D = st->diag;
-    const long long cnt = D.count;
+    D.mean_gamma_m1 = cnt > 0 ? t.sum_gamma / (double)cnt - 1.0 : 0.0;
+    // box from the moments
     double mx = 0, mz = 0, sgx = 0, sgz = 0;
     if (cnt > 1) {
-        mx = sx / (double)cnt;
-        mz = sz / (double)cnt;
-        const double vx = sx2 / (double)cnt - mx * mx, vz = sz2 / (double)cnt - mz * mz;
+        mx = t.sx / (double)cnt;
+        mz = t.sz / (double)cnt;
+        const double vx = t.sx2 / (double)cnt - mx * mx, vz = t.sz2 / (double)cnt - mz * mz;
         sgx = sqrt(vx > 0.0 ? vx : 0.0);
         sgz = sqrt(vz > 0.0 ? vz : 0.0);
     }
@@ -303,22 +228,85 @@ __global__ void __launch_bounds__(SC_TB) sc_reduce2(const Partial2 *part, int nb
     if (st->degenerate && status) atomicAdd((unsigned long long *)&status[FFA_STATUS_SC_DEGENERATE], 1ull);
 }
 
+// ----------------------------------------------------------------- passes
+
+// `done` counts finished blocks; it must be zero at launch (it sits in the
+// slot after the charge accumulator, which is cleared before every update).
+__global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ffa_sc_desc d, double *x_out,
+                                                  double *pr0_out, Partial *part, unsigned long long *done,
+                                                  SCState *st, int64_t *status)
+{
+    const double shifts[4] = {0.0, PI, PI * 0.5, PI * 1.5};
+    Partial p;
+    p.sum_gamma = 0.0; p.sx = p.sz = p.sx2 = p.sz2 = 0.0; p.count = 0;
+    for (int k = 0; k < 4; ++k) { p.amin[k] = 1e30; p.amax[k] = -1e30; }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (S.surv[i] == 0) continue;
+        const double g = gamma_of(S, i, d.boris, d.speed_c, d.E0_J);
+        const double fi = S.fi[i];
+        const double fm = fi - 2 * PI * floor(fi / (2 * PI));
+        const double Ek = (g - 1) * d.E0_rest_MeV;
+        const double r0 = seo_lookup(d.seo_r, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
+        pr0_out[i] = seo_lookup(d.seo_pr, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
+        const double xi = S.r[i] - r0, zi = S.z[i];
+        x_out[i] = xi;
+        p.sum_gamma += g;
+        ++p.count;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double v = fast_mod(fm + shifts[k], 2 * PI);
+            p.amin[k] = fmin(p.amin[k], v);
+            p.amax[k] = fmax(p.amax[k], v);
+        }
+        p.sx += xi;
+        p.sz += zi;
+        p.sx2 += xi * xi;
+        p.sz2 += zi * zi;
+    }
+    const Partial b = block_partial(p);
+    __shared__ int last;
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = b;
+        __threadfence();
+        last = atomicAdd(done, 1ull) == (unsigned long long)(gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    finalize_state(part, gridDim.x, d, st, status);
+}
+
+// slice index of every live particle (-1 otherwise), then the CIC deposit
 __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, ffa_sc_desc d, const double *x,
-                                                    const int32_t *slice, int64_t *cell, const SCState *st,
+                                                    int32_t *slice, int64_t *cell, const SCState *st,
                                                     unsigned long long *acc)
 {
-    if (st->bad) return;
+    const int bad = st->bad;
+    const double fi_s = st->diag.fi_s, step = st->diag.slice_step;
     const double xmin = st->diag.xmin, zmin = st->diag.zmin, inv_dx = st->inv_dx, inv_dz = st->inv_dz;
     const int nx = d.nx, nz = d.nz;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int s = slice[i];
-        if (s < 0) continue;
+        if (S.surv[i] == 0) {
+            slice[i] = -1;
+            cell[i] = -1;
+            continue;
+        }
+        double fi = S.fi[i];
+        fi = fi - 2 * PI * floor(fi / (2 * PI));
+        if (fi < fi_s) fi += 2 * PI;
+        int64_t s = (int64_t)((fi - fi_s) / step);
+        if (s < 0) s = 0; else if (s >= d.ns) s = d.ns - 1;
+        slice[i] = (int32_t)s;
+        if (bad) {
+            cell[i] = -1;
+            continue;
+        }
         const double rx = (x[i] - xmin) * inv_dx, rz = (S.z[i] - zmin) * inv_dz;
         int64_t ix = (int64_t)floor(rx), iz = (int64_t)floor(rz);
         double fx = rx - (double)ix, fz = rz - (double)iz;
         if (ix < 0) { ix = 0; fx = 0.0; } else if (ix >= nx - 1) { ix = nx - 2; fx = 1.0; }
         if (iz < 0) { iz = 0; fz = 0.0; } else if (iz >= nz - 1) { iz = nz - 2; fz = 1.0; }
-        const int64_t c0 = ((int64_t)s * nz + iz) * nx + ix;
+        const int64_t c0 = (s * nz + iz) * nx + ix;
         cell[i] = c0;
         atomicAdd(acc + c0, (unsigned long long)llrint((1.0 - fx) * (1.0 - fz) * FIX_SCALE));
         atomicAdd(acc + c0 + 1, (unsigned long long)llrint(fx * (1.0 - fz) * FIX_SCALE));
@@ -327,12 +315,512 @@ __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, 
     }
 }
 
-// fixed point -> float32 charge cube, and the complex work buffer of the
+// --------------------------------------------------- open-boundary Green's
+//
+// G(x, z) = -ln(x^2 + z^2) / (4 pi eps0) on the doubled (NZ, NX) grid with
+// x = dx * min(i, NX - i), z = dz * min(j, NZ - j) (the cell average at the
+// origin), times dx dz.  G is real and even in both indices, so its 2D DFT is
+// real, even, and a double cosine sum over the first quadrant:
+//   T[j][kx]  = sum_{i=0}^{NX/2} w_i G[j][i] cos(2 pi i kx / NX)
+//   Gk[kz][kx] = sum_{j=0}^{NZ/2} w_j T[j][kx] cos(2 pi j kz / NZ)
+// with w = 1 at 0 and N/2, 2 elsewhere.  Both sums in float64; the solve
+// reads the (NZ/2 + 1) x (NX/2 + 1) quadrant of Gk rounded to float32.
+__device__ __forceinline__ double green_point(int j, int i, double dx, double dz)
+{
+    const double K = -1.0 / (4.0 * PI * EPS0);
+    double v;
+    if (i == 0 && j == 0) {
+        const double a = 0.5 * dx, b = 0.5 * dz;
+        const double F = a * b * (log(a * a + b * b) - 3.0) + a * a * atan(b / a) + b * b * atan(a / b);
+        v = K * (F / (a * b));
+    } else {
+        const double x = dx * (double)i, z = dz * (double)j;
+        v = K * log(x * x + z * z);
+    }
+    return v * dx * dz;
+}
+
+__global__ void __launch_bounds__(256) sc_green_rows(int NZ, int NX, const SCState *st, double *T)
+{
+    if (st->bad) return;
+    extern __shared__ double gsh[];
+    const int hx = NX / 2;
+    double *g = gsh;                 // hx + 1 weighted values of row j
+    double *c = gsh + (hx + 1);      // cos(2 pi m / NX), m < NX
+    const int j = blockIdx.x;        // 0 .. NZ / 2
+    const double dx = st->diag.dx, dz = st->diag.dz;
+    for (int i = threadIdx.x; i <= hx; i += blockDim.x)
+        g[i] = ((i == 0 || i == hx) ? 1.0 : 2.0) * green_point(j, i, dx, dz);
+    for (int m = threadIdx.x; m < NX; m += blockDim.x) c[m] = cospi(2.0 * (double)m / (double)NX);
+    __syncthreads();
+    for (int kx = threadIdx.x; kx <= hx; kx += blockDim.x) {
+        double a = 0.0;
+        for (int i = 0; i <= hx; ++i) a += g[i] * c[(i * kx) & (NX - 1)];
+        T[(int64_t)j * (hx + 1) + kx] = a;
+    }
+}
+
+__global__ void __launch_bounds__(256) sc_green_cols(int NZ, int NX, const SCState *st, const double *T, float *gk)
+{
+    if (st->bad) return;
+    extern __shared__ double gsh[];
+    const int hx = NX / 2, hz = NZ / 2;
+    double *c = gsh;                 // cos(2 pi m / NZ), m < NZ
+    const int kz = blockIdx.x;       // 0 .. NZ / 2
+    for (int m = threadIdx.x; m < NZ; m += blockDim.x) c[m] = cospi(2.0 * (double)m / (double)NZ);
+    __syncthreads();
+    for (int kx = threadIdx.x; kx <= hx; kx += blockDim.x) {
+        double a = 0.0;
+        for (int j = 0; j <= hz; ++j)
+            a += ((j == 0 || j == hz) ? 1.0 : 2.0) * T[(int64_t)j * (hx + 1) + kx] * c[(j * kz) & (NZ - 1)];
+        gk[(int64_t)kz * (hx + 1) + kx] = (float)a;
+    }
+}
+
+// ------------------------------------------------------- fused slice solve
+//
+// Line transforms in registers.  A line of N = N1 * N2 points is held by a
+// group of N1 threads of one warp, N2 points per thread; the four-step
+// factorisation
+//   X[k2 + N2 k1] = sum_n1 W_N1^(n1 k1) W_N^(n1 k2) sum_n2 x[n1 + N1 n2] W_N2^(n2 k2)
+// runs the inner DFTs of length N2 in registers (thread n1 holds
+// x[n1 + N1 n2]), multiplies by the twiddles, exchanges through a
+// per-group shared-memory scratch (row k2, pitch N1 + 1, conflict-free both
+// ways), and runs the outer DFTs of length N1 in registers: thread t ends
+// with X[(t + N1 q) + N2 k1].  The inverse runs the same two steps in reverse
+// order, so a forward transform followed by an inverse leaves every thread
+// with its own input points again.
+
+template <int N> struct Split;
+template <> struct Split<32> { static constexpr int N1 = 4, N2 = 8; };
+template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Split<128> { static constexpr int N1 = 8, N2 = 16; };
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+
+constexpr int SOLVE_TB = 512;
+
+// group scratch stride (float2): N2 rows of N1 + 1, padded so that the
+// groups sharing a half-warp land on disjoint banks
+template <int N1, int N2>
+__host__ __device__ constexpr int scratch_stride()
+{
+    return N2 * (N1 + 1) + (((N1 % 16) - (N2 * (N1 + 1)) % 16 + 16) % 16);
+}
+
+// cos(2 pi m / 16)
+__device__ __forceinline__ float cos16(int m)
+{
+    switch (m & 15) {
+    case 0: return 1.0f;
+    case 1: case 15: return 0.92387953251128674f;
+    case 2: case 14: return 0.70710678118654752f;
+    case 3: case 13: return 0.38268343236508977f;
+    case 4: case 12: return 0.0f;
+    case 5: case 11: return -0.38268343236508977f;
+    case 6: case 10: return -0.70710678118654752f;
+    case 7: case 9: return -0.92387953251128674f;
+    default: return -1.0f;
+    }
+}
+
+// b * W_R^m, W = exp(-2 pi i m / R) forward, exp(+2 pi i m / R) inverse;
+// m is a constant after unrolling, so the branches and constants fold
+template <int R, bool INV>
+__device__ __forceinline__ float2 rot(float2 b, int m)
+{
+    const int m16 = (m * (16 / R)) & 15;
+    if (m16 == 0) return b;
+    if (m16 == 8) return make_float2(-b.x, -b.y);
+    if (m16 == 4) return INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+    if (m16 == 12) return INV ? make_float2(b.y, -b.x) : make_float2(-b.y, b.x);
+    const float c = cos16(m16), sn = cos16(m16 - 4);
+    const float wi = INV ? sn : -sn;
+    return make_float2(b.x * c - b.y * wi, b.x * wi + b.y * c);
+}
+
+template <int R>
+__host__ __device__ constexpr int brev_c(int k)
+{
+    int r = 0;
+    for (int b = 1, rb = R >> 1; b < R; b <<= 1, rb >>= 1)
+        if (k & b) r |= rb;
+    return r;
+}
+
+template <int R> struct Log2;
+template <> struct Log2<4> { static constexpr int v = 2; };
+template <> struct Log2<8> { static constexpr int v = 3; };
+template <> struct Log2<16> { static constexpr int v = 4; };
+
+// in-register DFT of length R (radix-2, decimation in time), natural order in and out
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&v)[R])
+{
+    float2 t[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) t[k] = v[brev_c<R>(k)];
+#pragma unroll
+    for (int st = 0; st < Log2<R>::v; ++st) {
+        const int h = 1 << st;
+#pragma unroll
+        for (int g = 0; g < R; g += 2 * h) {
+#pragma unroll
+            for (int j = 0; j < h; ++j) {
+                const float2 a = t[g + j];
+                const float2 b = rot<R, INV>(t[g + j + h], j * (R / (2 * h)));
+                t[g + j] = make_float2(a.x + b.x, a.y + b.y);
+                t[g + j + h] = make_float2(a.x - b.x, a.y - b.y);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = t[k];
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 w) { return make_float2(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
+__device__ __forceinline__ float2 cmulc(float2 a, float2 w) { return make_float2(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y); }
+
+// forward: in v[n2] = x[t + N1 n2]; out v[q N1 + k1] = X[(t + N1 q) + N2 k1].
+// tw[m] = exp(-2 pi i m / N).  Every lane of the warp must call it.
+template <int N1, int N2>
+__device__ __forceinline__ void fft_fwd(float2 (&v)[N2], int t, float2 *S, const float2 *tw)
+{
+    constexpr int N = N1 * N2;
+    dft<N2, false>(v);
+    __syncwarp();
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) S[k2 * (N1 + 1) + t] = cmul(v[k2], tw[(t * k2) & (N - 1)]);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < N2 / N1; ++q) {
+        float2 u[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) u[n1] = S[(t + N1 * q) * (N1 + 1) + n1];
+        dft<N1, false>(u);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) v[q * N1 + k1] = u[k1];
+    }
+}
+
+// inverse (unnormalised): in v[q N1 + k1] = X[(t + N1 q) + N2 k1]; out
+// v[n2] = x[t + N1 n2].  Every lane of the warp must call it.
+template <int N1, int N2>
+__device__ __forceinline__ void fft_inv(float2 (&v)[N2], int t, float2 *S, const float2 *tw)
+{
+    constexpr int N = N1 * N2;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < N2 / N1; ++q) {
+        float2 u[N1];
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) u[k1] = v[q * N1 + k1];
+        dft<N1, true>(u);
+        const int k2 = t + N1 * q;
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) S[k2 * (N1 + 1) + n1] = cmulc(u[n1], tw[(n1 * k2) & (N - 1)]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) v[k2] = S[k2 * (N1 + 1) + t];
+    dft<N2, true>(v);
+}
+
+// Thread -> (line group, point) map for lines of N1 threads.  Lines in one
+// half-warp are N1 apart so that their column points fall on disjoint banks.
+template <int N1>
+struct Grp {
+    int t, gid, line;
+    __device__ Grp()
+    {
+        const int tid = threadIdx.x;
+        const int h = tid >> 4;
+        const int e = (tid & 15) / N1;
+        t = tid & (N1 - 1);
+        gid = tid / N1;
+        line = (h / N1) * 16 + (h % N1) + N1 * e;
+    }
+};
+
+template <int NX, int NZ, bool HOCK>
+constexpr size_t solve_smem()
+{
+    constexpr int nz = HOCK ? NZ / 2 : NZ;
+    constexpr int P = NX / 2 + 1;
+    constexpr int SX = scratch_stride<Split<NX>::N1, Split<NX>::N2>();
+    constexpr int SZ = scratch_stride<Split<NZ>::N1, Split<NZ>::N2>();
+    constexpr int GX = SOLVE_TB / Split<NX>::N1 * SX, GZ = SOLVE_TB / Split<NZ>::N1 * SZ;
+    return sizeof(float2) * (size_t)(nz * P + NX + NZ + (GX > GZ ? GX : GZ));
+}
+
+// One block per slice.  Charge rows (2p, 2p + 1) are the real and imaginary
+// parts of one complex line; their x transforms give the two half spectra
+// (kx = 0 .. NX/2).  Each half-spectrum column then goes through the z
+// transform, the kernel and the inverse z transform in registers, and row
+// pairs come back through one inverse complex line transform each.  The
+// inverse takes the real parts of the kx = 0 and kx = NX/2 bins, which is
+// what the real part of a full complex inverse transform keeps.  Output: the
+// potential (scaled by 1 / (NX NZ) as the normalised inverse does) and the
+// field cubes; the charge cube as float32 on the way in.
+template <int NX, int NZ, bool HOCK>
+__global__ void __launch_bounds__(SOLVE_TB, 1)
+    sc_solve_fused(const unsigned long long *__restrict__ acc, const SCState *st, const float *__restrict__ gk,
+                   float *__restrict__ rho, float *__restrict__ phi, float *__restrict__ Ex, float *__restrict__ Ez)
+{
+    constexpr int nx = HOCK ? NX / 2 : NX, nz = HOCK ? NZ / 2 : NZ;
+    constexpr int P = NX / 2 + 1;     // half-spectrum pitch (float2)
+    constexpr int NCOL = NX / 2 + 1;
+    constexpr int X1 = Split<NX>::N1, X2 = Split<NX>::N2, Z1 = Split<NZ>::N1, Z2 = Split<NZ>::N2;
+    constexpr int SX = scratch_stride<X1, X2>(), SZ = scratch_stride<Z1, Z2>();
+    extern __shared__ float4 sm_solve[];
+    float2 *spec = reinterpret_cast<float2 *>(sm_solve);
+    float2 *twx = spec + nz * P;
+    float2 *twz = twx + NX;
+    float2 *scr = twz + NZ;
+    const int tid = threadIdx.x;
+    const int64_t cube0 = (int64_t)blockIdx.x * nz * nx;
+    const int degenerate = st->degenerate, bad = st->bad;
+    if (bad) {
+        for (int e = tid; e < nz * nx; e += SOLVE_TB) {
+            rho[cube0 + e] = 0.0f;
+            phi[cube0 + e] = 0.0f;
+            if (!degenerate) { Ex[cube0 + e] = 0.0f; Ez[cube0 + e] = 0.0f; }
+        }
+        return;
+    }
+    const double qd = st->diag.q_density / FIX_SCALE;
+    for (int m = tid; m < NX; m += SOLVE_TB) {
+        double sv, cv;
+        sincospi(2.0 * (double)m / (double)NX, &sv, &cv);
+        twx[m] = make_float2((float)cv, (float)(-sv));
+    }
+    for (int m = tid; m < NZ; m += SOLVE_TB) {
+        double sv, cv;
+        sincospi(2.0 * (double)m / (double)NZ, &sv, &cv);
+        twz[m] = make_float2((float)cv, (float)(-sv));
+    }
+    __syncthreads();
+
+    // (1) forward row transforms, two real rows per complex line
+    {
+        const Grp<X1> g;
+        float2 *S = scr + g.gid * SX;
+        constexpr int NPAIR = nz / 2, G = SOLVE_TB / X1;
+        for (int base = 0; base < NPAIR; base += G) {
+            const int p = base + g.line;
+            const bool act = p < NPAIR;
+            float2 v[X2];
+#pragma unroll
+            for (int n2 = 0; n2 < X2; ++n2) {
+                const int nn = g.t + X1 * n2;
+                float a = 0.0f, b = 0.0f;
+                if (act && nn < nx) {
+                    const int64_t ca = cube0 + (int64_t)(2 * p) * nx + nn;
+                    a = (float)((double)acc[ca] * qd);
+                    b = (float)((double)acc[ca + nx] * qd);
+                    rho[ca] = a;
+                    rho[ca + nx] = b;
+                }
+                v[n2] = make_float2(a, b);
+            }
+            fft_fwd<X1, X2>(v, g.t, S, twx);
+            // natural order into the scratch, then split the pair:
+            // A[k] = (Z[k] + conj Z[N-k]) / 2, B[k] = (Z[k] - conj Z[N-k]) / 2i
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < X2 / X1; ++q)
+#pragma unroll
+                for (int k1 = 0; k1 < X1; ++k1) S[(g.t + X1 * q) + X2 * k1] = v[q * X1 + k1];
+            __syncwarp();
+            if (act) {
+                for (int k = g.t; k <= NX / 2; k += X1) {
+                    const float2 zk = S[k], zn = S[(NX - k) & (NX - 1)];
+                    spec[(2 * p) * P + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                    spec[(2 * p + 1) * P + k] = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // (2) per half-spectrum column: z transform, kernel, inverse z transform
+    {
+        const Grp<Z1> g;
+        float2 *S = scr + g.gid * SZ;
+        constexpr int G = SOLVE_TB / Z1;
+        float dkx = 0.0f, dkz = 0.0f;
+        if (!HOCK) {
+            dkx = (float)(2.0 * PI / (nx * st->diag.dx));
+            dkz = (float)(2.0 * PI / (nz * st->diag.dz));
+        }
+        for (int base = 0; base < NCOL; base += G) {
+            const int c = base + g.line;
+            const bool act = c < NCOL;
+            float2 v[Z2];
+#pragma unroll
+            for (int n2 = 0; n2 < Z2; ++n2) {
+                const int row = g.t + Z1 * n2;
+                v[n2] = (act && row < nz) ? spec[row * P + c] : make_float2(0.0f, 0.0f);
+            }
+            fft_fwd<Z1, Z2>(v, g.t, S, twz);
+#pragma unroll
+            for (int q = 0; q < Z2 / Z1; ++q) {
+#pragma unroll
+                for (int k1 = 0; k1 < Z1; ++k1) {
+                    const int kz = (g.t + Z1 * q) + Z2 * k1;
+                    float kern = 0.0f;
+                    if (act) {
+                        if (HOCK) {
+                            kern = __ldg(gk + (kz <= NZ / 2 ? kz : NZ - kz) * NCOL + c);
+                        } else {
+                            // make_fft_kernel_open_numba in float32: bin n/2 is +n/2
+                            const float kxf = (float)((double)dkx * (double)c);
+                            const float kzf = (float)((double)dkz * (double)(kz <= nz / 2 ? kz : kz - nz));
+                            const float kz2 = __fmul_rn(kzf, kzf);
+                            const float k2 = __fadd_rn(__fmul_rn(kxf, kxf), kz2);
+                            kern = (k2 == 0.0f) ? 0.0f : (float)(1.0 / (EPS0 * (double)k2));
+                        }
+                    }
+                    float2 &w = v[q * Z1 + k1];
+                    w.x = __fmul_rn(w.x, kern);
+                    w.y = __fmul_rn(w.y, kern);
+                }
+            }
+            fft_inv<Z1, Z2>(v, g.t, S, twz);
+            if (act) {
+#pragma unroll
+                for (int n2 = 0; n2 < Z2; ++n2) {
+                    const int row = g.t + Z1 * n2;
+                    if (row < nz) spec[row * P + c] = v[n2];
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // (3) inverse row transforms: half spectra A (row 2p), B (row 2p + 1)
+    // -> Z[k] = A[k] + i B[k] over all k (Hermitian extension) -> a + i b
+    {
+        const Grp<X1> g;
+        float2 *S = scr + g.gid * SX;
+        constexpr int NPAIR = nz / 2, G = SOLVE_TB / X1;
+        const float scale = (float)(1.0 / ((double)NX * (double)NZ));
+        for (int base = 0; base < NPAIR; base += G) {
+            const int p = base + g.line;
+            const bool act = p < NPAIR;
+            float2 v[X2];
+#pragma unroll
+            for (int q = 0; q < X2 / X1; ++q) {
+#pragma unroll
+                for (int k1 = 0; k1 < X1; ++k1) {
+                    const int k = (g.t + X1 * q) + X2 * k1;
+                    float2 A = make_float2(0.0f, 0.0f), B = A;
+                    if (act) {
+                        const int kk = k <= NX / 2 ? k : NX - k;
+                        A = spec[(2 * p) * P + kk];
+                        B = spec[(2 * p + 1) * P + kk];
+                        if (k > NX / 2) { A.y = -A.y; B.y = -B.y; }
+                        else if (k == 0 || k == NX / 2) { A.y = 0.0f; B.y = 0.0f; }
+                    }
+                    v[q * X1 + k1] = make_float2(A.x - B.y, A.y + B.x);
+                }
+            }
+            fft_inv<X1, X2>(v, g.t, S, twx);
+            // the group has read rows 2p, 2p + 1 before fft_inv's first
+            // barrier: they now hold the two potential rows (float32)
+            if (act) {
+                float *pa = reinterpret_cast<float *>(spec + (2 * p) * P);
+                float *pb = reinterpret_cast<float *>(spec + (2 * p + 1) * P);
+#pragma unroll
+                for (int n2 = 0; n2 < X2; ++n2) {
+                    const int nn = g.t + X1 * n2;
+                    if (nn < nx) {
+                        const float fa = __fmul_rn(v[n2].x, scale), fb = __fmul_rn(v[n2].y, scale);
+                        pa[nn] = fa;
+                        pb[nn] = fb;
+                        phi[cube0 + (int64_t)(2 * p) * nx + nn] = fa;
+                        phi[cube0 + (int64_t)(2 * p + 1) * nx + nn] = fb;
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // (4) compute_field_from_potential_numba_SBS for every cell (each cell
+    // takes the value of the last loop of the reference that writes it)
+    {
+        const double dr = st->diag.dx, dz = st->diag.dz, BL = st->diag.bunch_length;
+        const double gm = st->diag.mean_gamma_m1 + 1.0;
+        const double ig2 = 1.0 / (gm * gm);
+        const double inv2dr = 0.5 / dr, inv2dz = 0.5 / dz;
+        const bool zero = (dr == 0.0 || dz == 0.0 || BL == 0);
+        for (int e = tid; e < nz * nx; e += SOLVE_TB) {
+            if (zero) { Ex[cube0 + e] = 0.0f; Ez[cube0 + e] = 0.0f; continue; }
+            const int j = e / nx, i = e - j * nx;
+#define PH(jj, ii) reinterpret_cast<const float *>(spec + (jj) * P)[(ii)]
+            double ex, ez;
+            if (i == 0 || i == nx - 1) {
+                const int jp = j + 1 < nz - 1 ? j + 1 : nz - 1, jm = j - 1 > 0 ? j - 1 : 0;
+                ex = (i == 0) ? -(double)__fsub_rn(PH(j, 1), PH(j, 0)) / dr * ig2
+                              : -(double)__fsub_rn(PH(j, nx - 1), PH(j, nx - 2)) / dr * ig2;
+                ez = -(double)__fsub_rn(PH(jp, i), PH(jm, i)) / dz * ig2;
+            } else if (j == 0) {
+                ex = -(double)__fsub_rn(PH(0, i + 1), PH(0, i - 1)) * inv2dr * ig2;
+                ez = -(double)__fsub_rn(PH(1, i), PH(0, i)) / dz * ig2;
+            } else if (j == nz - 1) {
+                ex = -(double)__fsub_rn(PH(nz - 1, i + 1), PH(nz - 1, i - 1)) * inv2dr * ig2;
+                ez = -(double)__fsub_rn(PH(nz - 1, i), PH(nz - 2, i)) / dz * ig2;
+            } else {
+                ex = -(double)__fsub_rn(PH(j, i + 1), PH(j, i - 1)) * inv2dr * ig2;
+                ez = -(double)__fsub_rn(PH(j + 1, i), PH(j - 1, i)) * inv2dz * ig2;
+            }
+#undef PH
+            Ex[cube0 + e] = (float)ex;
+            Ez[cube0 + e] = (float)ez;
+        }
+    }
+}
+
+// grids the fused solve is instantiated for: square, 32 / 64 / 128
+bool fused_grid(int nx, int nz) { return nx == nz && (nx == 32 || nx == 64 || nx == 128); }
+
+template <int NX, int NZ, bool HOCK>
+cudaError_t launch_fused_t(const unsigned long long *acc, const SCState *st, int ns, const float *gk, float *rho,
+                           float *phi, float *ex, float *ez, cudaStream_t s)
+{
+    constexpr size_t smem = solve_smem<NX, NZ, HOCK>();
+    static_assert(smem <= 227 * 1024, "slice does not fit in shared memory");
+    const cudaError_t e = cudaFuncSetAttribute(sc_solve_fused<NX, NZ, HOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+    if (e != cudaSuccess) return e;
+    sc_solve_fused<NX, NZ, HOCK><<<ns, SOLVE_TB, smem, s>>>(acc, st, gk, rho, phi, ex, ez);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fused(int n, bool hockney, const unsigned long long *acc, const SCState *st, int ns,
+                         const float *gk, float *rho, float *phi, float *ex, float *ez, cudaStream_t s)
+{
+    if (!hockney) {
+        switch (n) {
+        case 32: return launch_fused_t<32, 32, false>(acc, st, ns, gk, rho, phi, ex, ez, s);
+        case 64: return launch_fused_t<64, 64, false>(acc, st, ns, gk, rho, phi, ex, ez, s);
+        default: return launch_fused_t<128, 128, false>(acc, st, ns, gk, rho, phi, ex, ez, s);
+        }
+    }
+    switch (n) {
+    case 32: return launch_fused_t<64, 64, true>(acc, st, ns, gk, rho, phi, ex, ez, s);
+    case 64: return launch_fused_t<128, 128, true>(acc, st, ns, gk, rho, phi, ex, ez, s);
+    default: return launch_fused_t<256, 256, true>(acc, st, ns, gk, rho, phi, ex, ez, s);
+    }
+}
+
+// ------------------------------------- batched line FFTs (other grid sizes)
+
+// fixed point -> float32 charge cube, and the complex work cube of the
 // solver (the reference copies rho into a complex64 array, imaginary 0)
 __global__ void sc_convert(const unsigned long long *acc, ffa_sc_desc d, const SCState *st, float *rho,
                            float2 *work, int NZ, int NX)
 {
-    const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
     const int64_t wsz = (int64_t)d.ns * NZ * NX;
     const double q = st->diag.q_density / FIX_SCALE;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < wsz; e += (int64_t)gridDim.x * blockDim.x) {
@@ -347,32 +835,22 @@ __global__ void sc_convert(const unsigned long long *acc, ffa_sc_desc d, const S
         }
         work[e] = make_float2(v, 0.0f);
     }
-    (void)cube;
 }
 
-// ---------------------------------------------------------------- FFTs
-
-template <typename T> struct C2;
-template <> struct C2<float> { using t = float2; };
-template <> struct C2<double> { using t = double2; };
-
-// Batched radix-2 transforms of complete lines in shared memory.
-// Lines run along x (axis 1, contiguous) or z (axis 0, stride NX); a CTA
-// holds LINES lines of length n (bit-reversed on load, in-place butterflies,
-// one barrier per stage).  Loads and stores are coalesced for both axes:
-// along x consecutive threads read consecutive elements of a line, along z
-// consecutive threads read the same element of consecutive lines.
+// Batched radix-2 transforms of complete lines in shared memory, one kernel
+// per axis.  Lines run along x (axis 1, contiguous) or z (axis 0, stride NX);
+// a CTA holds LINES lines of length n (bit-reversed on load, in-place
+// butterflies, one barrier per stage) and forms the n / 2 twiddles
+// exp(-2 pi i k / n) itself.  Loads and stores are coalesced for both axes.
 // Forward: exp(-2 pi i jk/n); inverse: exp(+2 pi i jk/n), unnormalised.
-template <typename T, int LINES>
-__global__ void __launch_bounds__(256) fft_axis(typename C2<T>::t *data, int nslices, int NZ, int NX, int axis,
-                                                int logn, const typename C2<T>::t *tw, int inverse)
+template <int LINES>
+__global__ void __launch_bounds__(256) fft_axis(float2 *data, int NZ, int NX, int axis, int logn, int inverse)
 {
-    using V = typename C2<T>::t;
-    extern __shared__ unsigned char smraw[];
-    V *sm = reinterpret_cast<V *>(smraw);
+    extern __shared__ float2 smf[];
+    float2 *sm = smf;
     const int n = 1 << logn;
     const int ld = n + 1;  // padded line pitch
-    V *base;
+    float2 *base;
     int64_t lstride, estride;
     if (axis == 1) {
         const int64_t line0 = (int64_t)blockIdx.x * LINES;  // over nslices * NZ rows
@@ -395,26 +873,29 @@ __global__ void __launch_bounds__(256) fft_axis(typename C2<T>::t *data, int nsl
         const unsigned rk = __brev((unsigned)k) >> (32 - logn);
         sm[l * ld + rk] = base[l * lstride + (int64_t)k * estride];
     }
-    // twiddles exp(-2 pi i k / n), k < n / 2, staged once per block
-    V *tws = sm + LINES * ld;
-    for (int k = threadIdx.x; k < (n >> 1); k += blockDim.x) tws[k] = tw[k];
+    float2 *tws = sm + LINES * ld;
+    for (int k = threadIdx.x; k < (n >> 1); k += blockDim.x) {
+        double sv, cv;
+        sincospi(2.0 * (double)k / (double)n, &sv, &cv);
+        tws[k] = make_float2((float)cv, (float)(-sv));
+    }
     __syncthreads();
-    const T sgn = inverse ? (T)1 : (T)-1;
-    const int hb = logn - 1;                  // log2(n / 2)
+    const float sgn = inverse ? 1.0f : -1.0f;
+    const int hb = logn - 1;
     for (int s = 1; s <= logn; ++s) {
         const int half = 1 << (s - 1);
-        const int twshift = logn - s;         // twiddle index j * (n >> s)
+        const int twshift = logn - s;
         for (int b = threadIdx.x; b < LINES * (n >> 1); b += blockDim.x) {
             const int l = b >> hb;
             const int bb = b & ((n >> 1) - 1);
             const int grp = bb >> (s - 1);
             const int j = bb & (half - 1);
             const int i0 = grp * (half << 1) + j, i1 = i0 + half;
-            const V w = tws[j << twshift];
-            const T wr = w.x, wi = sgn * (-w.y);  // table holds exp(-2 pi i k/n)
-            V *p = sm + l * ld;
-            const V a = p[i0], c = p[i1];
-            const T xr = c.x * wr - c.y * wi, xi = c.x * wi + c.y * wr;
+            const float2 w = tws[j << twshift];
+            const float wr = w.x, wi = sgn * (-w.y);  // table holds exp(-2 pi i k/n)
+            float2 *p = sm + l * ld;
+            const float2 a = p[i0], c = p[i1];
+            const float xr = c.x * wr - c.y * wi, xi = c.x * wi + c.y * wr;
             p[i1].x = a.x - xr;
             p[i1].y = a.y - xi;
             p[i0].x = a.x + xr;
@@ -454,47 +935,21 @@ __global__ void sc_mul_periodic(float2 *work, ffa_sc_desc d, const SCState *st)
     }
 }
 
-// Open-boundary Green's function on the doubled (NZ, NX) grid, float64:
-// G = -ln(x^2 + z^2) / (4 pi eps0), the cell average at the origin.
-__global__ void sc_green_fill(double2 *g, int NZ, int NX, const SCState *st)
+// multiply by the Green transform (first-quadrant table, even in both indices)
+__global__ void sc_mul_green(float2 *work, int ns, int NZ, int NX, const float *gk, const SCState *st)
 {
     if (st->bad) return;
-    const double dx = st->diag.dx, dz = st->diag.dz;
-    const double K = -1.0 / (4.0 * PI * EPS0);
-    const int nx = NX / 2, nz = NZ / 2;
-    const int64_t tot = (int64_t)NZ * NX;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        const int j = (int)(e / NX), i = (int)(e - (int64_t)j * NX);
-        const double z = dz * (double)(j <= nz ? j : NZ - j);
-        const double x = dx * (double)(i <= nx ? i : NX - i);
-        double v;
-        if (i == 0 && j == 0) {
-            const double a = 0.5 * dx, b = 0.5 * dz;
-            const double F = a * b * (log(a * a + b * b) - 3.0) + a * a * atan(b / a) + b * b * atan(a / b);
-            v = K * (F / (a * b));
-        } else {
-            v = K * log(x * x + z * z);
-        }
-        g[e] = make_double2(v * dx * dz, 0.0);
-    }
-}
-
-__global__ void sc_green_finish(const double2 *g, float *gk, int64_t tot, const SCState *st)
-{
-    if (st->bad) return;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x)
-        gk[e] = (float)g[e].x;  // real and even: the transform is real
-}
-
-__global__ void sc_mul_green(float2 *work, int ns, int64_t plane, const float *gk, const SCState *st)
-{
-    if (st->bad) return;
+    const int64_t plane = (int64_t)NZ * NX;
     const int64_t tot = (int64_t)ns * plane;
+    const int hx = NX / 2;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
-        const float k = gk[e % plane];
+        const int64_t rem = e % plane;
+        const int j = (int)(rem / NX), i = (int)(rem - (int64_t)j * NX);
+        const int jj = j <= NZ / 2 ? j : NZ - j, ii = i <= hx ? i : NX - i;
+        const float k = gk[(int64_t)jj * (hx + 1) + ii];
         float2 v = work[e];
-        v.x *= k;
-        v.y *= k;
+        v.x = __fmul_rn(v.x, k);
+        v.y = __fmul_rn(v.y, k);
         work[e] = v;
     }
 }
@@ -512,8 +967,7 @@ __global__ void sc_potential(const float2 *work, ffa_sc_desc d, int NZ, int NX, 
     }
 }
 
-// compute_field_from_potential_numba_SBS for every cell (each cell takes the
-// value of the last loop of the reference that writes it)
+// compute_field_from_potential_numba_SBS for every cell
 __global__ void sc_field(const float *phi, ffa_sc_desc d, const SCState *st, float *Ex, float *Ez)
 {
     if (st->degenerate) return;
@@ -553,52 +1007,83 @@ __global__ void sc_field(const float *phi, ffa_sc_desc d, const SCState *st, flo
     }
 }
 
-__global__ void __launch_bounds__(SC_TB) sc_gather(ffa_state_soa S, int64_t n, ffa_sc_desc d, const double *x,
-                                                   const double *pr0, const int32_t *slice, const SCState *st,
-                                                   const float *Ex, const float *Ez)
+cudaError_t fft2d(float2 *data, int nslices, int NZ, int NX, int lognz, int lognx, int inverse, cudaStream_t s)
 {
-    if (st->degenerate) return;
-    const int nx = d.nx, nz = d.nz;
-    const double x0 = st->diag.xmin, z0 = st->diag.zmin, dx = st->diag.dx, dz = st->diag.dz;
-    const bool bad = st->bad != 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int s = slice[i];
-        if (s < 0) continue;
-        if (bad) { S.esc_r[i] = 0.0; S.esc_z[i] = 0.0; S.esc_fi[i] = 0.0; continue; }
-        const float *EX = Ex + (int64_t)s * nz * nx, *EZ = Ez + (int64_t)s * nz * nx;
-        const double t = (x[i] - x0) / dx, u = (S.z[i] - z0) / dz;
-        int64_t i0 = (int64_t)floor(t), j0 = (int64_t)floor(u);
-        if (i0 < 0) i0 = 0; else if (i0 > nx - 2) i0 = nx - 2;
-        if (j0 < 0) j0 = 0; else if (j0 > nz - 2) j0 = nz - 2;
-        const double al = t - (double)i0, be = u - (double)j0;
-        const double w00 = (1.0 - al) * (1.0 - be), w10 = al * (1.0 - be), w01 = (1.0 - al) * be, w11 = al * be;
-        const double er = w00 * EX[j0 * nx + i0] + w10 * EX[j0 * nx + i0 + 1] + w01 * EX[(j0 + 1) * nx + i0] +
-                          w11 * EX[(j0 + 1) * nx + i0 + 1];
-        const double ez = w00 * EZ[j0 * nx + i0] + w10 * EZ[j0 * nx + i0 + 1] + w01 * EZ[(j0 + 1) * nx + i0] +
-                          w11 * EZ[(j0 + 1) * nx + i0 + 1];
-        const double p = pr0[i];
-        const double rt = sqrt(1 + p * p);
-        S.esc_r[i] = er * (1 / rt);
-        S.esc_z[i] = ez;
-        S.esc_fi[i] = er * (-p / rt);
+    constexpr int LINES = 16;
+    // lines (padded pitch) + the n / 2 twiddles
+    const size_t smx = sizeof(float2) * (LINES * (NX + 1) + NX / 2), smz = sizeof(float2) * (LINES * (NZ + 1) + NZ / 2);
+    const cudaError_t e = cudaFuncSetAttribute(fft_axis<LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)(smx > smz ? smx : smz));
+    if (e != cudaSuccess) return e;
+    const unsigned gx = (unsigned)((int64_t)nslices * NZ / LINES), gz = (unsigned)((int64_t)nslices * (NX / LINES));
+    if (!inverse) {
+        fft_axis<LINES><<<gx, 256, smx, s>>>(data, NZ, NX, 1, lognx, 0);
+        fft_axis<LINES><<<gz, 256, smz, s>>>(data, NZ, NX, 0, lognz, 0);
+    } else {
+        fft_axis<LINES><<<gz, 256, smz, s>>>(data, NZ, NX, 0, lognz, 1);
+        fft_axis<LINES><<<gx, 256, smx, s>>>(data, NZ, NX, 1, lognx, 1);
     }
+    return cudaGetLastError();
 }
 
-// extrapolation endpoints after an update (src/FFAG_track.py:341-400)
-__global__ void sc_roll(ffa_state_soa S, int64_t n, int first)
+// ------------------------------------------------------- gather + roll
+
+// Bilinear field at each live particle, projected on the closed-orbit
+// direction; then, when `roll`, the extrapolation endpoints after the update
+// (src/FFAG_track.py:341-400): pre <- the new field for live particles,
+// pp <- the old pre, and the masks likewise.
+__global__ void __launch_bounds__(SC_TB) sc_gather_roll(ffa_state_soa S, int64_t n, ffa_sc_desc d, const double *x,
+                                                        const double *pr0, const int32_t *slice, const SCState *st,
+                                                        const float *Ex, const float *Ez, int roll, int first)
 {
+    const int nx = d.nx, nz = d.nz;
+    const int degenerate = st->degenerate, bad = st->bad;
+    const double x0 = st->diag.xmin, z0 = st->diag.zmin, dx = st->diag.dx, dz = st->diag.dz;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int s = slice[i];
+        double er = 0.0, ez = 0.0, ef = 0.0;
+        bool fresh = false;
+        if (!degenerate && s >= 0) {
+            if (!bad) {
+                const float *EX = Ex + (int64_t)s * nz * nx, *EZ = Ez + (int64_t)s * nz * nx;
+                const double t = (x[i] - x0) / dx, u = (S.z[i] - z0) / dz;
+                int64_t i0 = (int64_t)floor(t), j0 = (int64_t)floor(u);
+                if (i0 < 0) i0 = 0; else if (i0 > nx - 2) i0 = nx - 2;
+                if (j0 < 0) j0 = 0; else if (j0 > nz - 2) j0 = nz - 2;
+                const double al = t - (double)i0, be = u - (double)j0;
+                const double w00 = (1.0 - al) * (1.0 - be), w10 = al * (1.0 - be), w01 = (1.0 - al) * be, w11 = al * be;
+                const double gr = w00 * EX[j0 * nx + i0] + w10 * EX[j0 * nx + i0 + 1] + w01 * EX[(j0 + 1) * nx + i0] +
+                                  w11 * EX[(j0 + 1) * nx + i0 + 1];
+                const double gz = w00 * EZ[j0 * nx + i0] + w10 * EZ[j0 * nx + i0 + 1] + w01 * EZ[(j0 + 1) * nx + i0] +
+                                  w11 * EZ[(j0 + 1) * nx + i0 + 1];
+                const double p = pr0[i];
+                const double rt = sqrt(1 + p * p);
+                er = gr * (1 / rt);
+                ez = gz;
+                ef = gr * (-p / rt);
+            }
+            S.esc_r[i] = er;
+            S.esc_z[i] = ez;
+            S.esc_fi[i] = ef;
+            fresh = true;
+        }
+        if (!roll) continue;
         const uint8_t alive = S.surv[i] != 0;
+        if (alive && !fresh) { er = S.esc_r[i]; ez = S.esc_z[i]; ef = S.esc_fi[i]; }
         if (first) {
             S.sc_pre[i] = alive;
             S.sc_pp[i] = 0;
-            if (alive) { S.e_pre_r[i] = S.esc_r[i]; S.e_pre_z[i] = S.esc_z[i]; S.e_pre_fi[i] = S.esc_fi[i]; }
-            S.e_pp_r[i] = S.e_pre_r[i]; S.e_pp_z[i] = S.e_pre_z[i]; S.e_pp_fi[i] = S.e_pre_fi[i];
+            if (alive) {
+                S.e_pre_r[i] = er; S.e_pre_z[i] = ez; S.e_pre_fi[i] = ef;
+                S.e_pp_r[i] = er; S.e_pp_z[i] = ez; S.e_pp_fi[i] = ef;
+            } else {
+                S.e_pp_r[i] = S.e_pre_r[i]; S.e_pp_z[i] = S.e_pre_z[i]; S.e_pp_fi[i] = S.e_pre_fi[i];
+            }
         } else {
             S.sc_pp[i] = S.sc_pre[i];
             S.sc_pre[i] = alive;
             S.e_pp_r[i] = S.e_pre_r[i]; S.e_pp_z[i] = S.e_pre_z[i]; S.e_pp_fi[i] = S.e_pre_fi[i];
-            if (alive) { S.e_pre_r[i] = S.esc_r[i]; S.e_pre_z[i] = S.esc_z[i]; S.e_pre_fi[i] = S.esc_fi[i]; }
+            if (alive) { S.e_pre_r[i] = er; S.e_pre_z[i] = ez; S.e_pre_fi[i] = ef; }
         }
     }
 }
@@ -610,24 +1095,81 @@ int ilog2(int v)
     return (1 << l) == v ? l : -1;
 }
 
+// Device buffers of one update.  `acc` holds cells + 1 values: the slot after
+// the charge cube is pass1's block counter, cleared with the cube.
+struct SCBufs {
+    double *x, *pr0;
+    int32_t *slice;
+    int64_t *cell;
+    Partial *part;
+    SCState *st;
+    unsigned long long *acc;
+    float *rho, *phi, *ex, *ez;
+    float2 *work;         // batched-FFT path only
+    double *gT;           // open boundary: Green row sums, (NZ/2 + 1) x (NX/2 + 1)
+    float *gk;            // open boundary: Green transform quadrant
+};
+
+// The whole update on one stream, no host synchronisation.
+int run_update(const ffa_sc_desc &d, const SCBufs &b, ffa_state_soa *S, int64_t n, int roll, int first,
+               cudaStream_t s, int64_t *status, ffa_sc_diag *diag)
+{
+    const int NX = d.hockney ? 2 * d.nx : d.nx, NZ = d.hockney ? 2 * d.nz : d.nz;
+    const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
+    const unsigned ew = 148 * 8;  // elementwise grids
+    FFA_CHECK_CUDA(cudaMemsetAsync(b.acc, 0, sizeof(unsigned long long) * (cube + 1), s));
+    sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.part, b.acc + cube, b.st, status);
+    sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.slice, b.cell, b.st, b.acc);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    if (d.hockney) {
+        sc_green_rows<<<NZ / 2 + 1, 256, sizeof(double) * (NX / 2 + 1 + NX), s>>>(NZ, NX, b.st, b.gT);
+        sc_green_cols<<<NZ / 2 + 1, 256, sizeof(double) * NZ, s>>>(NZ, NX, b.st, b.gT, b.gk);
+        FFA_CHECK_CUDA(cudaGetLastError());
+    }
+    if (fused_grid(d.nx, d.nz)) {
+        FFA_CHECK_CUDA(launch_fused(d.nx, d.hockney != 0, b.acc, b.st, d.ns, b.gk, b.rho, b.phi, b.ex, b.ez, s));
+    } else {
+        const int lx = ilog2(NX), lz = ilog2(NZ);
+        sc_convert<<<ew, 256, 0, s>>>(b.acc, d, b.st, b.rho, b.work, NZ, NX);
+        FFA_CHECK_CUDA(cudaGetLastError());
+        FFA_CHECK_CUDA(fft2d(b.work, d.ns, NZ, NX, lz, lx, 0, s));
+        if (d.hockney) sc_mul_green<<<ew, 256, 0, s>>>(b.work, d.ns, NZ, NX, b.gk, b.st);
+        else sc_mul_periodic<<<ew, 256, 0, s>>>(b.work, d, b.st);
+        FFA_CHECK_CUDA(fft2d(b.work, d.ns, NZ, NX, lz, lx, 1, s));
+        sc_potential<<<ew, 256, 0, s>>>(b.work, d, NZ, NX, b.st, b.phi);
+        sc_field<<<ew, 256, 0, s>>>(b.phi, d, b.st, b.ex, b.ez);
+    }
+    sc_gather_roll<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.slice, b.st, b.ex, b.ez, roll ? 1 : 0,
+                                               first ? 1 : 0);
+    FFA_CHECK_CUDA(cudaGetLastError());
+    if (diag) FFA_CHECK_CUDA(cudaMemcpyAsync(diag, &b.st->diag, sizeof(ffa_sc_diag), cudaMemcpyDeviceToDevice, s));
+    return FFA_OK;
+}
+
+int check_state(const ffa_state_soa *S, int64_t n, int32_t roll)
+{
+    if (!S || !S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r || !S->esc_z ||
+        !S->esc_fi || n < 0)
+        return FFA_ERR_INVALID;
+    if (roll && (!S->sc_pre || !S->sc_pp || !S->e_pre_r || !S->e_pre_z || !S->e_pre_fi || !S->e_pp_r ||
+                 !S->e_pp_z || !S->e_pp_fi))
+        return FFA_ERR_INVALID;
+    return FFA_OK;
+}
+
+int check_desc(const ffa_sc_desc &d)
+{
+    if (d.ns < 2 || d.nx < 16 || d.nz < 16 || d.nE < 2 || d.nfi < 2 || !d.seo_Ek || !d.seo_r || !d.seo_pr ||
+        !d.seo_perimeter || !(d.dEk > 0) || !(d.dfi > 0))
+        return FFA_ERR_INVALID;
+    return FFA_OK;
+}
+
 }  // namespace
 
 struct ffa_sc_plan {
     ffa_sc_desc d;
-    int NZ, NX;           // solver grid (doubled for Hockney)
-    int lognz, lognx;
-    double *x, *pr0;
-    int32_t *slice;
-    int64_t *cell;
-    Partial1 *p1;
-    Partial2 *p2;
-    SCState *st;
-    unsigned long long *acc;
-    float *rho, *phi, *ex, *ez;
-    float2 *work;
-    float2 *twx32, *twz32;
-    double2 *gwork, *twx64, *twz64;
-    float *gk;
+    SCBufs b;
 };
 
 namespace {
@@ -635,45 +1177,11 @@ namespace {
 void free_plan(ffa_sc_plan *p)
 {
     if (!p) return;
-    void *ptrs[] = {p->x, p->pr0, p->slice, p->cell, p->p1, p->p2, p->st, p->acc, p->rho, p->phi, p->ex, p->ez,
-                    p->work, p->twx32, p->twz32, p->gwork, p->twx64, p->twz64, p->gk};
+    void *ptrs[] = {p->b.x, p->b.pr0, p->b.slice, p->b.cell, p->b.part, p->b.st, p->b.acc, p->b.rho, p->b.phi,
+                    p->b.ex, p->b.ez, p->b.work, p->b.gT, p->b.gk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     free(p);
-}
-
-template <typename V>
-int upload_twiddles(int n, V **out)
-{
-    V *h = (V *)malloc(sizeof(V) * (n / 2));
-    if (!h) return FFA_ERR_NOMEM;
-    for (int k = 0; k < n / 2; ++k) {
-        const double a = -2.0 * PI * (double)k / (double)n;
-        h[k].x = (decltype(h[k].x))cos(a);
-        h[k].y = (decltype(h[k].y))sin(a);
-    }
-    if (cudaMalloc(out, sizeof(V) * (n / 2)) != cudaSuccess) { free(h); return FFA_ERR_NOMEM; }
-    const cudaError_t e = cudaMemcpy(*out, h, sizeof(V) * (n / 2), cudaMemcpyHostToDevice);
-    free(h);
-    return e == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
-}
-
-template <typename T, int LINES>
-cudaError_t fft2d(typename C2<T>::t *data, int nslices, int NZ, int NX, int lognz, int lognx,
-                  const typename C2<T>::t *twz, const typename C2<T>::t *twx, int inverse, cudaStream_t s)
-{
-    using V = typename C2<T>::t;
-    // lines (padded pitch) + the n / 2 twiddles
-    const size_t smx = sizeof(V) * (LINES * (NX + 1) + NX / 2), smz = sizeof(V) * (LINES * (NZ + 1) + NZ / 2);
-    cudaFuncSetAttribute(fft_axis<T, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(smx > smz ? smx : smz));
-    if (!inverse) {
-        fft_axis<T, LINES><<<(unsigned)((int64_t)nslices * NZ / LINES), 256, smx, s>>>(data, nslices, NZ, NX, 1, lognx, twx, 0);
-        fft_axis<T, LINES><<<(unsigned)((int64_t)nslices * (NX / LINES)), 256, smz, s>>>(data, nslices, NZ, NX, 0, lognz, twz, 0);
-    } else {
-        fft_axis<T, LINES><<<(unsigned)((int64_t)nslices * (NX / LINES)), 256, smz, s>>>(data, nslices, NZ, NX, 0, lognz, twz, 1);
-        fft_axis<T, LINES><<<(unsigned)((int64_t)nslices * NZ / LINES), 256, smx, s>>>(data, nslices, NZ, NX, 1, lognx, twx, 1);
-    }
-    return cudaGetLastError();
 }
 
 }  // namespace
@@ -686,45 +1194,36 @@ int ffa_sc_plan_create(const ffa_sc_desc *desc, void *stream, ffa_sc_plan **out)
     if (!desc || !out) return FFA_ERR_INVALID;
     *out = nullptr;
     const ffa_sc_desc &d = *desc;
-    if (d.ns < 2 || d.nx < 16 || d.nz < 16 || d.n_max < 0 || d.nE < 2 || d.nfi < 2 || !d.seo_Ek || !d.seo_r ||
-        !d.seo_pr || !d.seo_perimeter || !(d.dEk > 0) || !(d.dfi > 0))
-        return FFA_ERR_INVALID;
+    if (check_desc(d) != FFA_OK || d.n_max < 0) return FFA_ERR_INVALID;
     const int lx = ilog2(d.nx), lz = ilog2(d.nz);
     if (lx < 0 || lz < 0 || d.nx > 512 || d.nz > 512) return FFA_ERR_UNSUPPORTED;  // powers of two, <= 512
     ffa_sc_plan *p = (ffa_sc_plan *)calloc(1, sizeof(ffa_sc_plan));
     if (!p) return FFA_ERR_NOMEM;
     p->d = d;
-    p->NX = d.hockney ? 2 * d.nx : d.nx;
-    p->NZ = d.hockney ? 2 * d.nz : d.nz;
-    p->lognx = ilog2(p->NX);
-    p->lognz = ilog2(p->NZ);
+    const int NX = d.hockney ? 2 * d.nx : d.nx, NZ = d.hockney ? 2 * d.nz : d.nz;
     const int64_t n = d.n_max > 0 ? d.n_max : 1;
     const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
-    const int64_t wsz = (int64_t)d.ns * p->NZ * p->NX;
-    bool ok = cudaMalloc(&p->x, sizeof(double) * n) == cudaSuccess &&
-              cudaMalloc(&p->pr0, sizeof(double) * n) == cudaSuccess &&
-              cudaMalloc(&p->slice, sizeof(int32_t) * n) == cudaSuccess &&
-              cudaMalloc(&p->cell, sizeof(int64_t) * n) == cudaSuccess &&
-              cudaMalloc(&p->p1, sizeof(Partial1) * SC_BLOCKS) == cudaSuccess &&
-              cudaMalloc(&p->p2, sizeof(Partial2) * SC_BLOCKS) == cudaSuccess &&
-              cudaMalloc(&p->st, sizeof(SCState)) == cudaSuccess &&
-              cudaMalloc(&p->acc, sizeof(unsigned long long) * cube) == cudaSuccess &&
-              cudaMalloc(&p->rho, sizeof(float) * cube) == cudaSuccess &&
-              cudaMalloc(&p->phi, sizeof(float) * cube) == cudaSuccess &&
-              cudaMalloc(&p->ex, sizeof(float) * cube) == cudaSuccess &&
-              cudaMalloc(&p->ez, sizeof(float) * cube) == cudaSuccess &&
-              cudaMalloc(&p->work, sizeof(float2) * wsz) == cudaSuccess;
-    if (ok && d.hockney)
-        ok = cudaMalloc(&p->gwork, sizeof(double2) * (int64_t)p->NZ * p->NX) == cudaSuccess &&
-             cudaMalloc(&p->gk, sizeof(float) * (int64_t)p->NZ * p->NX) == cudaSuccess;
+    SCBufs &b = p->b;
+    bool ok = cudaMalloc(&b.x, sizeof(double) * n) == cudaSuccess &&
+              cudaMalloc(&b.pr0, sizeof(double) * n) == cudaSuccess &&
+              cudaMalloc(&b.slice, sizeof(int32_t) * n) == cudaSuccess &&
+              cudaMalloc(&b.cell, sizeof(int64_t) * n) == cudaSuccess &&
+              cudaMalloc(&b.part, sizeof(Partial) * SC_BLOCKS) == cudaSuccess &&
+              cudaMalloc(&b.st, sizeof(SCState)) == cudaSuccess &&
+              cudaMalloc(&b.acc, sizeof(unsigned long long) * (cube + 1)) == cudaSuccess &&
+              cudaMalloc(&b.rho, sizeof(float) * cube) == cudaSuccess &&
+              cudaMalloc(&b.phi, sizeof(float) * cube) == cudaSuccess &&
+              cudaMalloc(&b.ex, sizeof(float) * cube) == cudaSuccess &&
+              cudaMalloc(&b.ez, sizeof(float) * cube) == cudaSuccess;
+    if (ok && !fused_grid(d.nx, d.nz)) ok = cudaMalloc(&b.work, sizeof(float2) * d.ns * (int64_t)NZ * NX) == cudaSuccess;
+    if (ok && d.hockney) {
+        const int64_t quad = (int64_t)(NZ / 2 + 1) * (NX / 2 + 1);
+        ok = cudaMalloc(&b.gT, sizeof(double) * quad) == cudaSuccess &&
+             cudaMalloc(&b.gk, sizeof(float) * quad) == cudaSuccess;
+    }
     if (!ok) { free_plan(p); return FFA_ERR_NOMEM; }
-    int rc = upload_twiddles(p->NX, &p->twx32);
-    if (rc == FFA_OK) rc = upload_twiddles(p->NZ, &p->twz32);
-    if (rc == FFA_OK && d.hockney) rc = upload_twiddles(p->NX, &p->twx64);
-    if (rc == FFA_OK && d.hockney) rc = upload_twiddles(p->NZ, &p->twz64);
-    if (rc != FFA_OK) { free_plan(p); return rc; }
-    if (cudaMemset(p->st, 0, sizeof(SCState)) != cudaSuccess || cudaMemset(p->slice, 0xff, sizeof(int32_t) * n) != cudaSuccess ||
-        cudaMemset(p->cell, 0xff, sizeof(int64_t) * n) != cudaSuccess) {
+    if (cudaMemset(b.st, 0, sizeof(SCState)) != cudaSuccess || cudaMemset(b.slice, 0xff, sizeof(int32_t) * n) != cudaSuccess ||
+        cudaMemset(b.cell, 0xff, sizeof(int64_t) * n) != cudaSuccess) {
         free_plan(p);
         return FFA_ERR_CUDA;
     }
@@ -741,55 +1240,23 @@ int ffa_sc_plan_destroy(ffa_sc_plan *plan)
 int ffa_sc_step(ffa_sc_plan *p, ffa_state_soa *S, int64_t n, int32_t roll, int32_t first, void *stream,
                 int64_t *status, ffa_sc_diag *diag)
 {
-    if (!p || !S || !S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r || !S->esc_z ||
-        !S->esc_fi || n < 0)
-        return FFA_ERR_INVALID;
+    if (!p) return FFA_ERR_INVALID;
+    const int rc = check_state(S, n, roll);
+    if (rc != FFA_OK) return rc;
     if (n > p->d.n_max) return FFA_ERR_INVALID;
-    if (roll && (!S->sc_pre || !S->sc_pp || !S->e_pre_r || !S->e_pre_z || !S->e_pre_fi || !S->e_pp_r ||
-                 !S->e_pp_z || !S->e_pp_fi))
-        return FFA_ERR_INVALID;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const ffa_sc_desc &d = p->d;
-    const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
-    const int64_t wsz = (int64_t)d.ns * p->NZ * p->NX;
-    const unsigned ew = 148 * 8;  // elementwise grids
-    FFA_CHECK_CUDA(cudaMemsetAsync(p->acc, 0, sizeof(unsigned long long) * cube, s));
-    sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->pr0, p->slice, p->cell, p->p1);
-    sc_reduce1<<<1, SC_TB, 0, s>>>(p->p1, SC_BLOCKS, d, p->st);
-    sc_pass2<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->slice, p->st, p->p2);
-    sc_reduce2<<<1, SC_TB, 0, s>>>(p->p2, SC_BLOCKS, d, p->st, status);
-    sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->slice, p->cell, p->st, p->acc);
-    sc_convert<<<ew, 256, 0, s>>>(p->acc, d, p->st, p->rho, p->work, p->NZ, p->NX);
-    FFA_CHECK_CUDA(cudaGetLastError());
-    if (d.hockney) {
-        sc_green_fill<<<ew, 256, 0, s>>>(p->gwork, p->NZ, p->NX, p->st);
-        FFA_CHECK_CUDA((fft2d<double, 8>(p->gwork, 1, p->NZ, p->NX, p->lognz, p->lognx, p->twz64, p->twx64, 0, s)));
-        sc_green_finish<<<ew, 256, 0, s>>>(p->gwork, p->gk, (int64_t)p->NZ * p->NX, p->st);
-    }
-    FFA_CHECK_CUDA((fft2d<float, 16>(p->work, d.ns, p->NZ, p->NX, p->lognz, p->lognx, p->twz32, p->twx32, 0, s)));
-    if (d.hockney) sc_mul_green<<<ew, 256, 0, s>>>(p->work, d.ns, (int64_t)p->NZ * p->NX, p->gk, p->st);
-    else sc_mul_periodic<<<ew, 256, 0, s>>>(p->work, d, p->st);
-    FFA_CHECK_CUDA((fft2d<float, 16>(p->work, d.ns, p->NZ, p->NX, p->lognz, p->lognx, p->twz32, p->twx32, 1, s)));
-    sc_potential<<<ew, 256, 0, s>>>(p->work, d, p->NZ, p->NX, p->st, p->phi);
-    sc_field<<<ew, 256, 0, s>>>(p->phi, d, p->st, p->ex, p->ez);
-    sc_gather<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, p->x, p->pr0, p->slice, p->st, p->ex, p->ez);
-    if (roll) sc_roll<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, first);
-    FFA_CHECK_CUDA(cudaGetLastError());
-    if (diag) FFA_CHECK_CUDA(cudaMemcpyAsync(diag, &p->st->diag, sizeof(ffa_sc_diag), cudaMemcpyDeviceToDevice, s));
-    (void)wsz;
-    return FFA_OK;
+    return run_update(p->d, p->b, S, n, roll, first, reinterpret_cast<cudaStream_t>(stream), status, diag);
 }
 
 int ffa_sc_buffers(const ffa_sc_plan *p, const float **rho, const float **phi, const float **ex, const float **ez,
                    const int32_t **slice_idx, const int64_t **cell_idx)
 {
     if (!p) return FFA_ERR_INVALID;
-    if (rho) *rho = p->rho;
-    if (phi) *phi = p->phi;
-    if (ex) *ex = p->ex;
-    if (ez) *ez = p->ez;
-    if (slice_idx) *slice_idx = p->slice;
-    if (cell_idx) *cell_idx = p->cell;
+    if (rho) *rho = p->b.rho;
+    if (phi) *phi = p->b.phi;
+    if (ex) *ex = p->b.ex;
+    if (ez) *ez = p->b.ez;
+    if (slice_idx) *slice_idx = p->b.slice;
+    if (cell_idx) *cell_idx = p->b.cell;
     return FFA_OK;
 }
 
@@ -814,13 +1281,14 @@ int ffa_sc_buffers(const ffa_sc_plan *p, const float **rho, const float **phi, c
 // count) or FFA_ERR_UNSUPPORTED (grid, open boundary) before anything runs.
 //
 // The array is shared by every call on a device and keeps the previous
-// call's contents; the charge accumulator is cleared at the start of each
-// call, every other region is fully rewritten before it is read.  Calls
-// whose work overlaps on the GPU (different streams, or host threads)
-// race on the array and must be serialised by the caller.
-// The first call on a device looks up the array's device address (with that
-// device current) and fills the FFT twiddle tables; make that first call
-// before capturing any stream.
+// call's contents; the charge accumulator (and the block counter after it)
+// is cleared at the start of each call, every other region is fully
+// rewritten before it is read, and the FFT twiddles are formed inside the
+// kernels, so no table outlives a call.  Calls whose work overlaps on the
+// GPU (different streams, or host threads) race on the array and must be
+// serialised by the caller.  Every call asks the runtime for the array's
+// address on the current device (cudaGetSymbolAddress, which allocates
+// nothing), so nothing cached can go stale after a device reset.
 // ------------------------------------------------------------------------
 namespace {
 
@@ -833,36 +1301,15 @@ constexpr size_t ST_OFF_X = 0;
 constexpr size_t ST_OFF_PR0 = ST_OFF_X + a256(sizeof(double) * ST_MAX_N);
 constexpr size_t ST_OFF_SLICE = ST_OFF_PR0 + a256(sizeof(double) * ST_MAX_N);
 constexpr size_t ST_OFF_CELL = ST_OFF_SLICE + a256(sizeof(int32_t) * ST_MAX_N);
-constexpr size_t ST_OFF_P1 = ST_OFF_CELL + a256(sizeof(int64_t) * ST_MAX_N);
-constexpr size_t ST_OFF_P2 = ST_OFF_P1 + a256(sizeof(Partial1) * SC_BLOCKS);
-constexpr size_t ST_OFF_STATE = ST_OFF_P2 + a256(sizeof(Partial2) * SC_BLOCKS);
+constexpr size_t ST_OFF_PART = ST_OFF_CELL + a256(sizeof(int64_t) * ST_MAX_N);
+constexpr size_t ST_OFF_STATE = ST_OFF_PART + a256(sizeof(Partial) * SC_BLOCKS);
 constexpr size_t ST_OFF_ACC = ST_OFF_STATE + a256(sizeof(SCState));
-constexpr size_t ST_OFF_RHO = ST_OFF_ACC + a256(sizeof(unsigned long long) * ST_MAX_CELLS);
+constexpr size_t ST_OFF_RHO = ST_OFF_ACC + a256(sizeof(unsigned long long) * (ST_MAX_CELLS + 1));
 constexpr size_t ST_OFF_PHI = ST_OFF_RHO + a256(sizeof(float) * ST_MAX_CELLS);
 constexpr size_t ST_OFF_EX = ST_OFF_PHI + a256(sizeof(float) * ST_MAX_CELLS);
 constexpr size_t ST_OFF_EZ = ST_OFF_EX + a256(sizeof(float) * ST_MAX_CELLS);
 constexpr size_t ST_OFF_WORK = ST_OFF_EZ + a256(sizeof(float) * ST_MAX_CELLS);
-constexpr size_t ST_OFF_TWX = ST_OFF_WORK + a256(sizeof(float2) * ST_MAX_CELLS);
-constexpr size_t ST_OFF_TWZ = ST_OFF_TWX + a256(sizeof(float2) * ST_MAX_GRID / 2);
-constexpr size_t ST_BYTES = ST_OFF_TWZ + a256(sizeof(float2) * ST_MAX_GRID / 2);
-
-// Twiddles exp(-2 pi i k / n) of both axes, one set per device; the table of
-// an axis is rebuilt when a call uses a different length.
-struct StaticDev {
-    unsigned char *base;  // device address of the array (from cudaGetSymbolAddress)
-    int twx_n, twz_n;
-};
-
-constexpr int ST_MAX_DEVICES = 64;
-StaticDev g_static_dev[ST_MAX_DEVICES];
-
-__global__ void st_twiddles(float2 *tw, int n)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n / 2) return;
-    const double a = -2.0 * PI * (double)k / (double)n;
-    tw[k] = make_float2((float)cos(a), (float)sin(a));
-}
+constexpr size_t ST_BYTES = ST_OFF_WORK + a256(sizeof(float2) * ST_MAX_CELLS);
 
 }  // namespace
 
@@ -871,76 +1318,33 @@ static __device__ __align__(256) unsigned char ffa_sc_static_scratch[ST_BYTES];
 extern "C" int ffa_sc_step_static(const ffa_sc_desc *desc, ffa_state_soa *S, int64_t n, int32_t roll,
                                   int32_t first, void *stream, int64_t *status, ffa_sc_diag *diag)
 {
-    if (!desc || !S || !S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r ||
-        !S->esc_z || !S->esc_fi || n < 0)
-        return FFA_ERR_INVALID;
+    if (!desc) return FFA_ERR_INVALID;
+    int rc = check_state(S, n, roll);
+    if (rc != FFA_OK) return rc;
     const ffa_sc_desc &d = *desc;
-    if (d.ns < 2 || d.nx < 16 || d.nz < 16 || d.nE < 2 || d.nfi < 2 || !d.seo_Ek || !d.seo_r || !d.seo_pr ||
-        !d.seo_perimeter || !(d.dEk > 0) || !(d.dfi > 0))
-        return FFA_ERR_INVALID;
+    if (check_desc(d) != FFA_OK) return FFA_ERR_INVALID;
     if (n > ST_MAX_N) return FFA_ERR_INVALID;  // more particles than the static scratch holds
     const int lx = ilog2(d.nx), lz = ilog2(d.nz);
     if (d.hockney || lx < 0 || lz < 0 || d.nx > ST_MAX_GRID || d.nz > ST_MAX_GRID ||
         (int64_t)d.ns * d.nz * d.nx > ST_MAX_CELLS)
         return FFA_ERR_UNSUPPORTED;
-    if (roll && (!S->sc_pre || !S->sc_pp || !S->e_pre_r || !S->e_pre_z || !S->e_pre_fi || !S->e_pp_r ||
-                 !S->e_pp_z || !S->e_pp_fi))
-        return FFA_ERR_INVALID;
-    int dev = 0;
-    FFA_CHECK_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= ST_MAX_DEVICES) return FFA_ERR_UNSUPPORTED;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    StaticDev &sd = g_static_dev[dev];
-    if (!sd.base) {
-        // host code must not use the array's name as a device address: ask
-        // the runtime for the address on this (current) device once
-        void *ptr = nullptr;
-        FFA_CHECK_CUDA(cudaGetSymbolAddress(&ptr, ffa_sc_static_scratch));
-        sd.base = static_cast<unsigned char *>(ptr);
-        sd.twx_n = sd.twz_n = 0;
-    }
-    unsigned char *b = sd.base;
-    double *x = reinterpret_cast<double *>(b + ST_OFF_X);
-    double *pr0 = reinterpret_cast<double *>(b + ST_OFF_PR0);
-    int32_t *slice = reinterpret_cast<int32_t *>(b + ST_OFF_SLICE);
-    int64_t *cell = reinterpret_cast<int64_t *>(b + ST_OFF_CELL);
-    Partial1 *p1 = reinterpret_cast<Partial1 *>(b + ST_OFF_P1);
-    Partial2 *p2 = reinterpret_cast<Partial2 *>(b + ST_OFF_P2);
-    SCState *st = reinterpret_cast<SCState *>(b + ST_OFF_STATE);
-    unsigned long long *acc = reinterpret_cast<unsigned long long *>(b + ST_OFF_ACC);
-    float *rho = reinterpret_cast<float *>(b + ST_OFF_RHO);
-    float *phi = reinterpret_cast<float *>(b + ST_OFF_PHI);
-    float *ex = reinterpret_cast<float *>(b + ST_OFF_EX);
-    float *ez = reinterpret_cast<float *>(b + ST_OFF_EZ);
-    float2 *work = reinterpret_cast<float2 *>(b + ST_OFF_WORK);
-    float2 *twx = reinterpret_cast<float2 *>(b + ST_OFF_TWX);
-    float2 *twz = reinterpret_cast<float2 *>(b + ST_OFF_TWZ);
-    if (sd.twx_n != d.nx) {
-        st_twiddles<<<1, 64, 0, s>>>(twx, d.nx);
-        sd.twx_n = d.nx;
-    }
-    if (sd.twz_n != d.nz) {
-        st_twiddles<<<1, 64, 0, s>>>(twz, d.nz);
-        sd.twz_n = d.nz;
-    }
-    const int64_t cube = (int64_t)d.ns * d.nz * d.nx;
-    const unsigned ew = 148 * 8;
-    FFA_CHECK_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * cube, s));
-    sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, pr0, slice, cell, p1);
-    sc_reduce1<<<1, SC_TB, 0, s>>>(p1, SC_BLOCKS, d, st);
-    sc_pass2<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, st, p2);
-    sc_reduce2<<<1, SC_TB, 0, s>>>(p2, SC_BLOCKS, d, st, status);
-    sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, slice, cell, st, acc);
-    sc_convert<<<ew, 256, 0, s>>>(acc, d, st, rho, work, d.nz, d.nx);
-    FFA_CHECK_CUDA(cudaGetLastError());
-    FFA_CHECK_CUDA((fft2d<float, 16>(work, d.ns, d.nz, d.nx, lz, lx, twz, twx, 0, s)));
-    sc_mul_periodic<<<ew, 256, 0, s>>>(work, d, st);
-    FFA_CHECK_CUDA((fft2d<float, 16>(work, d.ns, d.nz, d.nx, lz, lx, twz, twx, 1, s)));
-    sc_potential<<<ew, 256, 0, s>>>(work, d, d.nz, d.nx, st, phi);
-    sc_field<<<ew, 256, 0, s>>>(phi, d, st, ex, ez);
-    sc_gather<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, x, pr0, slice, st, ex, ez);
-    if (roll) sc_roll<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, first);
-    FFA_CHECK_CUDA(cudaGetLastError());
-    if (diag) FFA_CHECK_CUDA(cudaMemcpyAsync(diag, &st->diag, sizeof(ffa_sc_diag), cudaMemcpyDeviceToDevice, s));
-    return FFA_OK;
+    // host code must not use the array's name as a device address: ask the
+    // runtime for its address on the current device
+    void *ptr = nullptr;
+    FFA_CHECK_CUDA(cudaGetSymbolAddress(&ptr, ffa_sc_static_scratch));
+    unsigned char *base = static_cast<unsigned char *>(ptr);
+    SCBufs b{};
+    b.x = reinterpret_cast<double *>(base + ST_OFF_X);
+    b.pr0 = reinterpret_cast<double *>(base + ST_OFF_PR0);
+    b.slice = reinterpret_cast<int32_t *>(base + ST_OFF_SLICE);
+    b.cell = reinterpret_cast<int64_t *>(base + ST_OFF_CELL);
+    b.part = reinterpret_cast<Partial *>(base + ST_OFF_PART);
+    b.st = reinterpret_cast<SCState *>(base + ST_OFF_STATE);
+    b.acc = reinterpret_cast<unsigned long long *>(base + ST_OFF_ACC);
+    b.rho = reinterpret_cast<float *>(base + ST_OFF_RHO);
+    b.phi = reinterpret_cast<float *>(base + ST_OFF_PHI);
+    b.ex = reinterpret_cast<float *>(base + ST_OFF_EX);
+    b.ez = reinterpret_cast<float *>(base + ST_OFF_EZ);
+    b.work = reinterpret_cast<float2 *>(base + ST_OFF_WORK);
+    return run_update(d, b, S, n, roll, first, reinterpret_cast<cudaStream_t>(stream), status, diag);
 }

@@ -688,6 +688,66 @@ def plain_track(frame, tracker, phys, turns, record=False):
     return res
 
 
+# ------------------------------------------- the time-domain plain pushers
+def phys_to_boris(phys, conv=None) -> np.ndarray:
+    """States at a sector entrance, phys (n, 5) r, pr, z, pz, P (pr, pz the
+    transverse momenta over P, P in kg m/s), as the Boris pushers' N x 16
+    matrix at fi = 0: vr = pr v, vz = pz v, dfi/dt = sqrt(1 - pr^2 - pz^2) v / r,
+    all injected and alive."""
+    from .constants import FFAG_ConversionTools
+    conv = conv or FFAG_ConversionTools()
+    ph = np.asarray(phys.cpu().numpy() if hasattr(phys, "cpu") else phys, np.float64)
+    E = np.sqrt((ph[:, 4] * conv.c) ** 2 + conv.E0 ** 2)
+    v = ph[:, 4] * conv.c ** 2 / E
+    m = np.zeros((ph.shape[0], 16))
+    m[:, 0] = ph[:, 0]
+    m[:, 1] = ph[:, 1] * v
+    m[:, 2] = ph[:, 2]
+    m[:, 3] = ph[:, 3] * v
+    m[:, 5] = np.sqrt(1.0 - ph[:, 1] ** 2 - ph[:, 3] ** 2) * v / ph[:, 0]
+    m[:, 7] = 1.0
+    m[:, 8] = 1.0
+    m[:, 15] = np.arange(ph.shape[0])
+    return m
+
+
+def boris_record(frame, gp, phys, turns, dt, precision="fp64", device=None):
+    """The time-domain Boris pusher on the states `phys` (sector entrance,
+    fi = 0) for enough steps that every state makes `turns` turns; the
+    normalised transverse coordinates where each state crosses fi = 0,
+    turn by turn (turns + 1, n, 4) as LearnedSectorMap.track records them
+    (NaN for a state lost before)."""
+    import os
+    import tempfile
+    torch = _torch()
+    from . import diagnostics
+    from .bunch import FFAG_Bunch
+    from .dump import Dumps, PositionDumpBunch
+    from .track import FFAG_RungeKutta
+    m = phys_to_boris(phys)
+    n = m.shape[0]
+    t_rev = (2 * np.pi / m[:, 5]).max()            # the slowest state's revolution time, roughly
+    nsteps = int(np.ceil((turns + 0.5) * t_rev / dt))
+    b = FFAG_Bunch(m, BunchType="Boris", device=device)
+    d = PositionDumpBunch(0.0, -dt, (nsteps + 1) * dt, save_folder=os.path.join(tempfile.mkdtemp(), "x"))
+    dumps = Dumps()
+    dumps.add_dump(d)
+    lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+          "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": dumps}
+    FFAG_RungeKutta(precision=precision, verbose=False).rk4_solve_dt_bunch3_withSC_boris(None, 0.0, b, gp, lp)
+    tab = diagnostics.crossing_table(d.crossing_records, n, dt)[: turns + 1]
+    rec = np.full((turns + 1, n, 4), np.nan, np.float32)
+    P = np.asarray(phys[:, 4].cpu().numpy() if hasattr(phys, "cpu") else phys[:, 4], np.float64)
+    for t in range(tab.shape[0]):
+        ok = np.isfinite(tab[t, :, 0])
+        if not ok.any():
+            continue
+        spd = tab[t, ok, 4]
+        ph = np.stack([tab[t, ok, 0], tab[t, ok, 1] / spd, tab[t, ok, 2], tab[t, ok, 3] / spd, P[ok]], 1)
+        rec[t, ok] = frame.to_norm(torch.as_tensor(ph, dtype=torch.float64))[:, :4].float().numpy()
+    return rec
+
+
 # ------------------------------------------------------------- persistence
 def save(path, params, frame):
     """Writes a trained network and its coordinate frame to one .npz file."""

@@ -232,3 +232,56 @@ def test_host_matrix_entry_point_matches_device_push(full_lattice, precision):
 def _lib_status_lost():
     from pyffa_b200 import _lib
     return _lib.STATUS_LOST
+
+
+def test_c0_hundred_turns_vs_oracle():
+    """Workload c0: plain float64 Boris, no RF, no space charge, the full
+    1301 x 6000 map with z-Taylor order 2, a 1e4-particle seeded 6D Gaussian
+    bunch, 100 turns of 720 steps.  The whole bunch is pushed on the GPU one
+    turn per launch; after every turn a 512-particle subset is compared with
+    the oracle's run of the same particles, per element, at 1e-12 per turn or
+    ten times the dynamics' own rounding sensitivity over the same turns (the
+    oracle against itself with r nudged by one ulp), whichever is larger."""
+    import os
+    import tempfile
+    from oracle import oracle as O
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools, FFAG_GlobalParameters
+    from pyffa_b200.fields import FFAG_Bfield_analytical, FFAG_EField_new
+    from pyffa_b200.track import Pusher, StepClock, _EphemeralBunch
+    cfg = synthetic.lattice_bmap()
+    gp = FFAG_GlobalParameters()
+    gp.AddBMap(FFAG_Bfield_analytical(config=cfg, max_order=2, stacks=synthetic.taylor_stacks(cfg, 2)))
+    gp.AddEMap(FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=False))
+    gp.AddAperture(7.5, 9.5, -0.1, 0.1)
+    n, turns, spt = 10_000, 100, 720
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(synthetic.centred_bunch(n, seed=5))
+    v[:, 7] = 1.0
+    v[:, 8] = 1.0
+    dt = synthetic.design_dt(300.0, spt)
+    idx = np.sort(np.random.Generator(np.random.PCG64(1)).choice(n, 512, replace=False))
+    dev = torch.device("cuda", 0)
+    b = _EphemeralBunch(v.copy(), "Boris", dev)
+    pu = Pusher(b, gp, "Boris", "fp64")
+    clock = StepClock(0.0, dt, gp.Emap, "Boris", dev)
+    clock.ensure(turns * spt)
+    S = O.Setup(gp.Bmap, gp.Emap, gp)
+    ref = v[idx].copy()
+    nudged = ref.copy()
+    nudged[:, 0] = np.nextafter(nudged[:, 0], np.inf)
+    worst = []
+    for t in range(1, turns + 1):
+        pu.push(clock, (t - 1) * spt, spt, 0)
+        torch.cuda.synchronize()
+        got = b.matrix()[idx]
+        O.track(S, "Boris", ref, clock.t[(t - 1) * spt], dt, spt)
+        O.track(S, "Boris", nudged, clock.t[(t - 1) * spt], dt, spt)
+        floor = coord_errors(nudged, ref)
+        assert np.array_equal(got[:, 7:9], ref[:, 7:9]), f"flags differ after turn {t}"
+        for c, err in coord_errors(got, ref).items():
+            tol = max(1e-12 * t, 10 * floor[c])
+            assert err <= tol, f"turn {t}, column {c}: relative error {err:.3g} > {tol:.3g}"
+        worst.append(max(coord_errors(got, ref)[c] for c in ELEMENTWISE))
+    assert (ref[:, 8] == 1).sum() > 256
+    print("\nc0: largest per-element error of r, fi, dfi/dt, RF phase after turns 1, 10, 100:",
+          worst[0], worst[9], worst[-1])
