@@ -13,6 +13,11 @@ main_track forces 1, examples/main_track.py:5-6).  The oracle's C port
 particles over the same steps.  One JSON line: particle-steps/s and
 particle-turns/s of both, the host's core count and CPU model.
 
+With --c3, it times instead the reference's closed-orbit and tune search per
+energy (FFAG_SearchSEO: SearchSEOUsingInitialEkVect + the one-turn track +
+GetQrQz, src/FFAG_track.py:1245-1371 and 1441-1481) on the scan's lattice at
+a few energies of 300-600 MeV, and extrapolates to the 256-energy scan.
+
 Test infrastructure: needs the reference checkout (--ref PATH or
 PYFFA_REFERENCE) and numba; it is not part of the library.
 """
@@ -50,9 +55,12 @@ def main():
     ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"))
     ap.add_argument("--n", type=int, default=100_000)
     ap.add_argument("--steps", type=int, default=144)
+    ap.add_argument("--c3", action="store_true")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
+    if args.c3:
+        return time_c3(args)
     sys.path.insert(0, os.path.join(REPO, "tests", "golden", "shims"))
     sys.path.insert(0, os.path.join(args.ref, "src"))
     import numba
@@ -136,6 +144,46 @@ def main():
         "port_over_reference": ref_s / port_s,
         "port_vs_reference_max_rel_r": float(dr.max()),
     }))
+
+
+def time_c3(args, energies=(300.0, 400.0, 500.0, 600.0), n_scan=256):
+    sys.path.insert(0, os.path.join(REPO, "tests", "golden", "shims"))
+    sys.path.insert(0, os.path.join(args.ref, "src"))
+    import numba
+    numba.set_num_threads(os.cpu_count())
+    from FFAG_Field import FFAG_Bfield_analytical, FFAG_BField_Error
+    from FFAG_ParasAndConversion import FFAG_GlobalParameters
+    from FFAG_track import FFAG_SearchSEO
+
+    from pyffa_b200 import synthetic
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = synthetic.lattice_bmap(r_range=(7.5, 9.5, 0.01), theta_step_deg=0.05)
+        cfg["config"]["folder"] = tmp
+        path = os.path.join(tmp, "config_Bmap.json")
+        with open(path, "w") as f:
+            json.dump(cfg, f)
+        FFAG_Bfield_analytical(path, 0, AddNumricalMap=False).UpdataConfig()   # as main_SEO does
+        gp = FFAG_GlobalParameters()
+        gp.AddBMap(FFAG_Bfield_analytical(path, 0, AddNumricalMap=False))
+        gp.AddBHarmonics(FFAG_BField_Error([], False))
+        finder = FFAG_SearchSEO(gp)
+        per = []
+        tunes = []
+        for k, Ek in enumerate(energies):
+            t0 = time.perf_counter()
+            r0, pr0, _ = finder.SearchSEOUsingInitialEkVect(Ek, 0.001, 0.0, verbose=False)
+            finder.TrackAParticle(r0, pr0, Ek, np.pi * 2, 0.001)
+            Qr, Qz, *_ = finder.GetQrQz(r0, pr0, Ek, 0.001)
+            el = time.perf_counter() - t0
+            if k > 0 or len(energies) == 1:      # the first includes Numba's compilation
+                per.append(el)
+            tunes.append([float(Qr), float(Qz)])
+    s_per = sum(per) / len(per)
+    print(json.dumps({"workload": "c3 closed-orbit / tune search per energy, the scan's lattice (analytic field)",
+                      "energies_timed": list(energies[1:]), "s_per_energy": s_per,
+                      "scan_energies": n_scan, "scan_s_estimate": s_per * n_scan,
+                      "tunes": tunes, "cores": os.cpu_count(), "cpu": cpu_model(),
+                      "numba_threads": numba.get_num_threads()}))
 
 
 if __name__ == "__main__":
