@@ -392,6 +392,7 @@ def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=
     vb32 = vb.copy()
     vb32[:, 0] *= 1 + 2.0 ** -24
     cases = {"fp64_boris": ("Boris", "fp64", vb), "fp32c_boris": ("Boris", "fp32c", vb),
+             "fp32_boris": ("Boris", "fp32", vb),
              "fp64_rk4": ("RK4", "fp64", vr), "fp64_boris_r_1_2e-24": ("Boris", "fp64", vb32)}
     last, tun, alive = {}, {}, {}
     for name, (solver, prec, m) in cases.items():
@@ -404,7 +405,7 @@ def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=
         last[name + "_s"] = time.perf_counter() - t0
     out = {"particles": n, "turns": turns, "steps_per_turn": STEPS_PER_TURN, "rf": "2 gaps, last-gap semantics",
            "vs": "fp64_boris", "tune_particles": tune_n, "alive": alive}
-    for name in ("fp32c_boris", "fp64_rk4", "fp64_boris_r_1_2e-24"):
+    for name in ("fp32c_boris", "fp32_boris", "fp64_rk4", "fp64_boris_r_1_2e-24"):
         e = D.azimuth_errors(last["fp64_boris"], last[name])
         dq = np.abs(tun[name] - tun["fp64_boris"])
         dq = np.minimum(dq, 1.0 - dq)
@@ -947,6 +948,22 @@ def main():
             vt = v32
         tuned.update({"value": vt, "speedup_vs_fp64": vt / value})
         fp32c["autotuned"] = tuned
+        # the float32 pusher (float32 push, float64 accumulation of r, fi, z)
+        pu32f = Pusher(b, gp, "Boris", "fp32")
+        for k in range(args.warmup):
+            restore()
+            pu32f.push(clock, k * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        msf = timed_turns(pu32f, args.steps)
+        tf = torch.tensor([sum(msf)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tf, op=dist.ReduceOp.MAX)
+        vf = n * world * args.steps / (float(tf.item()) * 1e-3)
+        fp32c["fp32_push"] = {"value": vf, "unit": "particle-turns/s", "ms_per_step": float(tf.item()) / args.steps,
+                              "speedup_vs_fp64": vf / value,
+                              "dtype": "f32 field and push, f64 accumulation of r, fi, z and the RF phase"}
     clocks = cs.summary()
 
     # end to end through the host-buffer API: host matrix in, one turn, host matrix out

@@ -51,6 +51,8 @@ enum ffa_push_flags {
     FFA_FP64 = 0,                 /* all arithmetic in float64 */
     FFA_FP32C = 2,                /* Boris: float32 field exponentials and map lookup, float64 push */
     FFA_RF_PHYSICAL_SUM = 4,      /* sum every RF gap (reference: last gap wins) */
+    FFA_FP32 = 8,                 /* Boris: float32 field and push, r / fi / z / RF phase accumulated in
+                                     float64 (no space charge, no field-error harmonics) */
     /* Launch shape of the Boris pushers, bits 8-11 (0: the default shape).
      * Bits 8-9: threads per block 32 << v (32, 64, 128, 256).  Bits 10-11:
      * register cap per thread 80, 72, 64, 56; caps below 80 are built for the

@@ -22,6 +22,7 @@ FFA_BORIS = 0
 FFA_RK4 = 1
 FFA_FP64 = 0
 FFA_FP32C = 2
+FFA_FP32 = 8
 FFA_RF_PHYSICAL_SUM = 4
 FFA_SHAPE_TB_SHIFT = 8
 FFA_SHAPE_NREG_SHIFT = 10

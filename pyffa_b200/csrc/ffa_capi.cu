@@ -190,6 +190,17 @@ int ffa_fieldmap_create(const ffa_field_desc *d, void *stream, ffa_fieldmap **ou
         }
         k.pw_tlim = lo;
     }
+    k.B0f = (float)k.B0;
+    k.c1f = (float)k.c1;
+    k.kc1f = (float)k.kc1;
+    k.km1f = (float)k.km1;
+    for (int j = 0; j < d->n_convex; ++j) {
+        k.seg_x0f[j] = (float)k.seg_x0[j];
+        k.seg_x1f[j] = (float)k.seg_x1[j];
+        k.seg_kf[j] = (float)k.seg_k[j];
+        k.seg_yf[j] = (float)k.seg_y[j];
+        k.seg_ykf[j] = (float)(k.seg_y[j] * k.seg_k[j]);
+    }
     for (int j = 0; j < d->n_convex; ++j) {
         k.seg_yk[j] = k.seg_y[j] * k.seg_k[j];
         const double hc = 0.5 * k.seg_k[j] * (k.seg_x1[j] - k.seg_x0[j]);
@@ -275,8 +286,11 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     if (sc_step > 0 && st->sc_pre &&
         (!st->sc_pp || !st->e_pre_r || !st->e_pre_z || !st->e_pre_fi || !st->e_pp_r || !st->e_pp_z || !st->e_pp_fi))
         return FFA_ERR_INVALID;
-    if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_RF_PHYSICAL_SUM | FFA_SHAPE_MASK)) return FFA_ERR_INVALID;
+    if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_FP32 | FFA_RF_PHYSICAL_SUM | FFA_SHAPE_MASK)) return FFA_ERR_INVALID;
     if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
+    if ((flags & FFA_FP32) && ((flags & (FFA_RK4 | FFA_FP32C)) || (sc_step > 0 && st->sc_pre) ||
+                               fm->k.n_harm > 0))
+        return FFA_ERR_UNSUPPORTED;
     const int tb_sel = (flags >> FFA_SHAPE_TB_SHIFT) & 3, nreg_sel = (flags >> FFA_SHAPE_NREG_SHIFT) & 3;
     if ((flags & FFA_RK4) && (tb_sel | nreg_sel)) return FFA_ERR_UNSUPPORTED;
     if (nreg_sel && (!(flags & FFA_FP32C) || (sc_step > 0 && st->sc_pre) || fm->k.n_harm > 0))
@@ -339,6 +353,7 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     }
     cudaError_t e;
     if (flags & FFA_RK4) e = launch_rk4_f64(p, as_stream(stream));
+    else if (flags & FFA_FP32) e = launch_boris_f32(p, as_stream(stream), 32 << tb_sel);
     else if (flags & FFA_FP32C) e = launch_boris_f32c(p, as_stream(stream), 32 << tb_sel, nreg_sel);
     else e = launch_boris_f64(p, as_stream(stream), 32 << tb_sel);
     return e == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;

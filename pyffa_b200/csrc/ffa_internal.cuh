@@ -52,6 +52,9 @@ struct FieldK {
     // rmin <= r <= rmax (fi unwrapped)
     int32_t n_harm, pad2;
     const double *harm;
+    // float32 copies for the float32 pusher
+    float B0f, c1f, kc1f, km1f;
+    float seg_x0f[FFA_MAX_SEG], seg_x1f[FFA_MAX_SEG], seg_kf[FFA_MAX_SEG], seg_yf[FFA_MAX_SEG], seg_ykf[FFA_MAX_SEG];
 };
 
 struct RFK {
@@ -106,6 +109,7 @@ namespace ffa {
 cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s, int tb);
 cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s);
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel);
+cudaError_t launch_boris_f32(const PushK &p, cudaStream_t s, int tb);
 cudaError_t push_occupancy(bool rk4, bool f32, int max_order, bool xing, int tb, int nreg_sel, int *blocks);
 cudaError_t launch_theta_track(const FieldK &f, const ffa_theta_track_desc &d, cudaStream_t s);
 cudaError_t launch_pack_nodes(const ffa_field_desc &d, int npad, double *n64, float *n32, cudaStream_t s);

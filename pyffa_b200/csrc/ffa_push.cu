@@ -603,6 +603,218 @@ __global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
     status_add(p.status, lost, !(isfinite(r) && isfinite(fi) && isfinite(z)), oob);
 }
 
+// ------------------------------------------------------ Boris, float32 push
+//
+// The float32 pusher: field and Boris update in float32, the positions (r,
+// fi, z) and the RF phase accumulated in float64 from float32 increments.
+// It carries the normalised momentum u = gamma v / c across the launch
+// (float32) and converts from and to the float64 state once per launch.
+// Each step the radius increment comes from
+//   r' - r = (2 r dx + dx^2 + dy^2) / (r' + r)
+// (dx, dy the local-frame displacement, formed in float32, so the increment
+// keeps float32's relative accuracy instead of the radius), the azimuth
+// increment from the arcsine series of dy / r'.  The RF gap test runs in
+// float64 inside the gap's angular window.  Velocities keep float32
+// precision: their rounding (~6e-8 of |u| per step) walks over a run, which
+// is what limits this pusher's accuracy.  Not built with space charge,
+// crossing capture of the steps' states is.
+
+template <int MAXO>
+__device__ __forceinline__ void field_f32(const FieldK &f, double r, double fim, float z, float &Bz, float &Br,
+                                          float &Bfi, int &clamped)
+{
+    float hz = 0.0f, hf = 0.0f, hr = 0.0f;
+    if constexpr (MAXO >= 1) {
+        const double qx = (r - f.r_min) * f.inv_r_step;
+        const double qy = (fim - f.fi_min) * f.inv_fi_step;
+        const int nr = (int)f.r_size, nf = (int)f.fi_size;
+        int i = trunc_index(qx), jj = trunc_index(qy);
+        if (i < 0) { i = 0; ++clamped; } else if (i >= nr - 1) { i = nr - 2; ++clamped; }
+        if (jj < 0) { jj = 0; ++clamped; } else if (jj >= nf - 1) { jj = nf - 2; ++clamped; }
+        const float tx = (float)(qx - (double)i), ty = (float)(qy - (double)jj);
+        const float w[4] = {(1.0f - tx) * (1.0f - ty), (1.0f - tx) * ty, tx * (1.0f - ty), tx * ty};
+        constexpr int NP = (3 * MAXO <= 4) ? 4 : ((3 * MAXO <= 8) ? 8 : 12);
+        constexpr int NV = 3 * MAXO;
+        const float *nd[4];
+        nd[0] = f.nodes32 + (i * nf + jj) * NP;
+        nd[1] = nd[0] + NP;
+        nd[2] = nd[0] + nf * NP;
+        nd[3] = nd[2] + NP;
+        float acc[NV];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int a = 0; a < NV; a += 4) {
+                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+            }
+        }
+        const float z2 = z * z;
+        float ze = z2, zo = z2 * z;
+#pragma unroll
+        for (int n = 0; n < MAXO; ++n) {
+            hz += acc[3 * n] * ze;
+            hf += acc[3 * n + 1] * zo;
+            hr += acc[3 * n + 2] * zo;
+            ze *= z2;
+            zo *= z2;
+        }
+    }
+    float spiral_p = 0.0f;
+    double fs = fim;
+    if (!f.spiral_zero) {   // as in analytic_b64, in float64 (spiral lattices only)
+        double spiral = 0.0, sp = 0.0;
+        for (int a = 0; a < f.n_spoly; ++a) spiral = spiral * r + f.spoly[a];
+        for (int a = 0; a < f.n_spolyp; ++a) sp = sp * r + f.spolyp[a];
+        spiral_p = (float)sp;
+        fs = fim - spiral;
+        fs -= f.period * floor(fs * f.inv_period);
+    }
+    const float rf = (float)r;
+    float B0r, B0r_p;
+    if (f.k == 0.0) {
+        B0r = f.B0f;
+        B0r_p = 0.0f;
+    } else {
+        const float eps = (float)((r - f.r_ref) * f.inv_r_ref);
+        const float g = expf(f.km1f * log1pf(eps));
+        B0r_p = f.kc1f * g;
+        B0r = f.c1f * g * rf;
+    }
+    const float fsf = (float)fs;
+    float F = 0.0f, Fp = 0.0f;
+    for (int j = 0; j < f.n_seg; ++j) {
+        const float a1 = f.seg_kf[j] * (fsf - f.seg_x0f[j]);
+        const float a2 = f.seg_kf[j] * (fsf - f.seg_x1f[j]);
+        float e1 = 0.0f, e2 = 0.0f;   // as in field_mixed
+        if (a1 < 24.0f) e1 = expf(fminf(-a1, 80.0f));
+        if (a2 > -24.0f) e2 = expf(fminf(a2, 80.0f));
+        const float s1 = __frcp_rn(1.0f + e1), s2 = __frcp_rn(1.0f + e2);
+        const float ss = s1 * s2;
+        const float dd = e1 * s1 - e2 * s2;
+        F += f.seg_yf[j] * ss;
+        Fp += f.seg_ykf[j] * (ss * dd);
+    }
+    Bz = B0r * F + hz;
+    Bfi = B0r * Fp * __frcp_rn(rf) * z + hf;
+    Br = (B0r_p * F - B0r * Fp * spiral_p) * z + hr;
+}
+
+template <int MAXO, bool XING>
+__global__ void __launch_bounds__(128) boris_f32_kernel(const PushK p)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const FieldK &f = p.f;
+    const ffa_state_soa &S = p.st;
+    const double c = p.cs.c;
+    double r = S.r[i], z = S.z[i], fi = S.fi[i], rfph = S.rf[i];
+    float ux, uy, uz;
+    {
+        const double vr = S.vr[i], vf = r * S.f5[i], vz = S.vz[i];
+        const double g = 1.0 / sqrt(1.0 - (vr * vr + vf * vf + vz * vz) * p.inv_cc);
+        ux = (float)(g * vr / c);
+        uy = (float)(g * vf / c);
+        uz = (float)(g * vz / c);
+    }
+    const double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
+    int inj = S.inj[i], surv = S.surv[i];
+    const int32_t injs = S.inj_step ? S.inj_step[i] : -1;
+    const float aE = (float)(p.hq / (p.cs.m0 * c));   // q dt / (2 m c): E [V/m] -> du
+    const float aB = (float)p.hqm;                     // q dt / (2 m): B [T] -> gamma t
+    const float cdt = (float)(c * p.dt);
+    const float esrf = (float)esr, eszf = (float)esz, esff = (float)esf;
+    int lost = 0, oob = 0;
+    // vr, vz and dfi/dt of the current momentum in float64 (crossing records)
+    auto vstate = [&](double rr, double out[3]) {
+        const double ig = 1.0 / sqrt(1.0 + (double)ux * ux + (double)uy * uy + (double)uz * uz);
+        out[0] = (double)ux * ig * c;
+        out[1] = (double)uz * ig * c;
+        out[2] = (double)uy * ig * c / rr;
+    };
+
+    for (int s = 0; s < p.nsteps; ++s) {
+        const int64_t gs = p.step0 + s;
+        if (injs == gs) { inj = 1; surv = 1; }
+        const double drf = __ldg(p.drf + gs);
+        double pre[7];
+        const int surv0 = surv;
+        if constexpr (XING) {
+            double v[3];
+            vstate(r, v);
+            pre[0] = r; pre[1] = v[0]; pre[2] = z; pre[3] = v[1]; pre[4] = fi; pre[5] = v[2]; pre[6] = rfph;
+        }
+        if ((inj == 1) && (surv == 1)) {
+            const double acc = __ldg(p.acc + gs);
+            const double fim = fi - f.period * floor(fi * f.inv_period);
+            float Bz, Br, Bfi;
+            field_f32<MAXO>(f, r, fim, (float)z, Bz, Br, Bfi, oob);
+            double Erd, Efid;
+            rf_field64(p.rf, acc, r, fi, rfph, Erd, Efid);
+            const float Er = (float)Erd + esrf, Efi = (float)Efid + esff, Ez = eszf;
+            if (p.ap.enable && (r > p.ap.rmax || r < p.ap.rmin || z > p.ap.zmax || z < p.ap.zmin)) {
+                surv = 0;
+                ++lost;
+            }
+            // local frame, B negated as in the float64 pusher
+            const float Bx = -Br, By = -Bfi, Bzc = -Bz;
+            ux += aE * Er;
+            uy += aE * Efi;
+            uz += aE * Ez;
+            const float cb = aB * rsqrtf(1.0f + ux * ux + uy * uy + uz * uz);
+            const float tx = cb * Bx, ty = cb * By, tz = cb * Bzc;
+            const float upx = ux + (uy * tz - uz * ty);
+            const float upy = uy + (uz * tx - ux * tz);
+            const float upz = uz + (ux * ty - uy * tx);
+            const float sb = 2.0f * __frcp_rn(1.0f + tx * tx + ty * ty + tz * tz);
+            const float sx = sb * tx, sy = sb * ty, sz = sb * tz;
+            ux += (upy * sz - upz * sy);
+            uy += (upz * sx - upx * sz);
+            uz += (upx * sy - upy * sx);
+            ux += aE * Er;
+            uy += aE * Efi;
+            uz += aE * Ez;
+            const float k = cdt * rsqrtf(1.0f + ux * ux + uy * uy + uz * uz);
+            const float dx = ux * k, dy = uy * k, dz = uz * k;
+            const float rf = (float)r;
+            const float xn = rf + dx;
+            const float rn2 = xn * xn + dy * dy;
+            const float irn = rsqrtf(rn2);
+            const float rn = rn2 * irn;
+            const float dr = (2.0f * rf * dx + dx * dx + dy * dy) * __frcp_rn(rn + rf);
+            const float sn = dy * irn, cn = xn * irn;
+            const float s2 = sn * sn;
+            const float dfi = sn * (1.0f + s2 * (1.0f / 6 + s2 * (3.0f / 40 + s2 * (5.0f / 112))));
+            r += (double)dr;
+            fi += (double)dfi;
+            z += (double)dz;
+            const float nux = ux * cn + uy * sn;
+            uy = -ux * sn + uy * cn;
+            ux = nux;
+        }
+        rfph += drf;
+        if constexpr (XING) {
+            if (surv0 == 1) {
+                double v[3];
+                vstate(r, v);
+                const double post[7] = {r, v[0], z, v[1], fi, v[2], rfph};
+                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+            }
+        }
+    }
+    const double ig = 1.0 / sqrt(1.0 + (double)ux * ux + (double)uy * uy + (double)uz * uz);
+    S.r[i] = r; S.z[i] = z; S.fi[i] = fi; S.rf[i] = rfph;
+    S.vr[i] = (double)ux * ig * c;
+    S.vz[i] = (double)uz * ig * c;
+    S.f5[i] = (double)uy * ig * c / r;
+    S.inj[i] = (uint8_t)inj;
+    S.surv[i] = (uint8_t)surv;
+    status_add(p.status, lost, !(isfinite(r) && isfinite(fi) && isfinite(z)), oob);
+}
+
 // -------------------------------------------------------------- RK4 fp64
 
 struct Y7 {
@@ -900,6 +1112,26 @@ static void boris32_launch(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
 {
     FFA_DISPATCH(boris32_launch, p, s, tb, nreg_sel);
+    return cudaGetLastError();
+}
+
+template <int MAXO, bool SC>
+static void boris_f32_launch(const PushK &p, cudaStream_t s, int tb, int)
+{
+    const unsigned g = (unsigned)((p.n + tb - 1) / tb);
+    if (p.xing.buf) boris_f32_kernel<MAXO, true><<<g, tb, 0, s>>>(p);
+    else boris_f32_kernel<MAXO, false><<<g, tb, 0, s>>>(p);
+}
+
+cudaError_t launch_boris_f32(const PushK &p, cudaStream_t s, int tb)
+{
+    switch (p.f.max_order) {
+    case 0: boris_f32_launch<0, false>(p, s, tb, 0); break;
+    case 1: boris_f32_launch<1, false>(p, s, tb, 0); break;
+    case 2: boris_f32_launch<2, false>(p, s, tb, 0); break;
+    case 3: boris_f32_launch<3, false>(p, s, tb, 0); break;
+    default: boris_f32_launch<4, false>(p, s, tb, 0); break;
+    }
     return cudaGetLastError();
 }
 

@@ -187,6 +187,6 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="B200 tracking driver (config_track.json)")
     ap.add_argument("config", nargs="?", default="./config_track.json")
     ap.add_argument("-r", "--restart", default=None)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c", "fp32"])
     a = ap.parse_args()
     main(a.config, a.restart, precision=a.precision)

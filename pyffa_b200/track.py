@@ -117,10 +117,12 @@ class Pusher:
         # and set on it before each push, since maps are shared between pushers
         self.harmonics = getattr(gp, "BHarmonics", None)
         self.flags = _lib.FFA_RK4 if solver == "RK4" else _lib.FFA_BORIS
-        if precision == "fp32c":
+        if precision in ("fp32c", "fp32"):
             if solver == "RK4":
-                raise NotImplementedError("the compensated float32 pusher is Boris-only")
-            self.flags |= _lib.FFA_FP32C
+                raise NotImplementedError("the float32 pushers are Boris-only")
+            self.flags |= _lib.FFA_FP32C if precision == "fp32c" else _lib.FFA_FP32
+        elif precision != "fp64":
+            raise ValueError(f"precision must be fp64, fp32c or fp32, not {precision!r}")
         if getattr(gp.Emap, "physical_sum", False):
             self.flags |= _lib.FFA_RF_PHYSICAL_SUM
         self.stream = torch.cuda.current_stream(bunch.device)

@@ -28,8 +28,10 @@ def test_shape_constants_match_header():
 
 def _dummy_push_args(sc=False):
     """Descriptors that pass the argument checks; n = 0, so nothing is
-    launched and no pointer is dereferenced."""
-    keep = ctypes.create_string_buffer(64)
+    launched.  The field map is a zeroed host block larger than the library's
+    map object, which the checks read (a map without field-error harmonics);
+    no other pointer is dereferenced."""
+    keep = ctypes.create_string_buffer(1 << 16)
     fake = ctypes.addressof(keep)
     rf = _lib.RFDesc()
     rf.ngaps = 1

@@ -161,3 +161,31 @@ def test_fp32c_single_turn_close_to_fp64():
         scale = np.max(np.abs(f(ar) - f(a64)) / np.abs(f(a64)))
         print(f"\none turn, {name}: fp32c {err:.3g}, fp64 response to r * (1 + 2^-24) {scale:.3g}")
         assert err <= 1e-7 and err <= max(4 * scale, 1e-12), (name, err, scale)
+
+
+def test_fp32_push_single_turn():
+    """The float32 pusher (float32 field and push, r, fi, z and the RF phase
+    accumulated in float64), one turn at 720 steps/turn against float64:
+    flags exact, radius, azimuth and speed within 1e-5 (its float32
+    velocities round at ~6e-8 per step), and visibly not float64."""
+    from pyffa_b200 import synthetic
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.track import Pusher
+    from pyffa_b200.bunch import FFAG_Bunch
+    gp = _lattice(True)
+    p = synthetic.centred_bunch(4096, seed=17)
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek_boris(p)
+    dt = synthetic.design_dt(300.0, 720)
+    a64, _ = _track(gp, v, dt, 720, "fp64")
+    a32, _ = _track(gp, v, dt, 720, "fp32")
+    assert np.array_equal(a64[:, 7:9], a32[:, 7:9])
+    al = a64[:, 8] == 1
+    speed = lambda a: np.sqrt(a[:, 1] ** 2 + a[:, 3] ** 2 + (a[:, 0] * a[:, 5]) ** 2)
+    errs = {}
+    for name, f in (("r", lambda a: a[al, 0]), ("fi", lambda a: a[al, 4]), ("v", lambda a: speed(a[al]))):
+        errs[name] = float(np.max(np.abs(f(a32) - f(a64)) / np.abs(f(a64))))
+    print("\none turn, fp32 push vs fp64:", errs)
+    assert all(np.isfinite(a32[al, c]).all() for c in range(6))
+    assert max(errs.values()) <= 1e-5 and max(errs.values()) > 1e-12, errs
+    with pytest.raises(NotImplementedError):
+        Pusher(FFAG_Bunch(v.copy(), BunchType="RK4"), gp, "RK4", "fp32")
