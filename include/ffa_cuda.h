@@ -314,6 +314,48 @@ int ffa_sc_buffers(const ffa_sc_plan *plan, const float **rho, const float **phi
                    const float **ex, const float **ez, const int32_t **slice_idx,
                    const int64_t **cell_idx);
 
+/* ------------------------------------------------------ bunch generation
+ * One sub-bunch of GenerateInitDistributionDtInjNew
+ * (src/FFAG_Distribution.py:1152-1345) written on the device: n rows of the
+ * reference's p-format matrix (r, pr, z, pz, fi, Ek [MeV], inj_t [ns],
+ * flags 0, RF phase 0, space-charge fields 0, Bunch_ID, Local_ID, Global_ID),
+ * drawn from the distribution shapes of src/FFAG_Distribution.py:76-1149
+ * through the Twiss transformation of TwissContainer (:16-73).  Random
+ * numbers: Philox4x32-10, counter (particle id0 + i, draw group, sub_bunch)
+ * under the key `seed`, so the rows do not depend on the launch or on how a
+ * bunch is split over calls.  `twiss` holds (alpha, beta, emittance) of the
+ * horizontal, vertical and longitudinal planes as the reference's
+ * generator receives them; each shape applies its own emittance factor
+ * (KV2D 4x, water-bag 2D 6x, KV1D 2x, water-bag 1D 4x).  Rejection shapes
+ * (Gauss with a cut-off, hollow water-bag 2D) try FFA_BUNCH_MAX_ATTEMPTS
+ * times; particles that never pass keep the last draw and are counted in
+ * *rejected (device, may be NULL). */
+#define FFA_BUNCH_MAX_ATTEMPTS 64
+enum ffa_dist_type {
+    FFA_DIST_GAUSS = 0,
+    FFA_DIST_KV = 1,
+    FFA_DIST_WATERBAG = 2,
+    FFA_DIST_HOLLOW_WATERBAG = 3,
+    FFA_DIST_UNIFORM_GAUSS = 4     /* longitudinal only: t uniform, dE normal */
+};
+typedef struct ffa_bunch_desc {
+    int64_t n;                    /* rows */
+    int64_t id0;                  /* Local_ID / Global_ID of the first row */
+    uint64_t seed;
+    int64_t sub_bunch;            /* painting index (Bunch_ID's stream) */
+    int32_t transverse, longitudinal;
+    double cut_off;               /* Gauss cut-off in rms units, <= 0: none */
+    double twiss[3][3];           /* (alpha, beta, emittance) of x, z, longitudinal */
+    double uniform_length;        /* FFA_DIST_UNIFORM_GAUSS: t span [ns] */
+    double uniform_sigma;         /* FFA_DIST_UNIFORM_GAUSS: rms of dE [MeV] */
+    double centre[6];             /* added: r, pr, z, pz, Ek, inj_t */
+    double fi;                    /* injection azimuth [rad] */
+    double bunch_id;
+    double *out;                  /* device, n x 16 */
+} ffa_bunch_desc;
+
+int ffa_bunch_sample(const ffa_bunch_desc *desc, unsigned long long *rejected, void *stream);
+
 /* ------------------------------------------------------ closed-orbit tracks
  * Tracks of the closed-orbit search (FunctionForSEO through rk4_solve /
  * rk4_solve_vect, src/FFAG_track.py:582-640 and 1698-1740): m trajectories

@@ -15,12 +15,14 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libffa_oracle.so")
+LIB_FMA = os.path.join(HERE, "libffa_oracle_fma.so")
 MAXG, MAXSEG, MAXPOLY, MAXHARM = 8, 16, 16, 16
 
 
 def build(force: bool = False) -> str:
     srcs = [os.path.join(HERE, f) for f in ("ffa_oracle.c", "ffa_oracle_sc.c", "Makefile")]
-    if force or not os.path.exists(LIB) or any(os.path.getmtime(s) > os.path.getmtime(LIB) for s in srcs):
+    if force or not all(os.path.exists(x) for x in (LIB, LIB_FMA)) or \
+            any(os.path.getmtime(s) > min(os.path.getmtime(LIB), os.path.getmtime(LIB_FMA)) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "all"], check=True)
     return LIB
 
@@ -73,29 +75,44 @@ class OrcSCDiag(C.Structure):
 
 
 _lib = None
+_lib_fma = None
+
+
+def _bind(path):
+    L = C.CDLL(path)
+    L.orc_boris_step.argtypes = [C.c_double, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]
+    L.orc_rk4_step.argtypes = [C.c_double, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_track.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_void_p,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_track.restype = C.c_double
+    L.orc_inject.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
+    L.orc_theta_track.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
+                                  C.c_double, C.c_void_p, C.c_void_p, C.c_int]
+    L.orc_sc_step.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.orc_sc_step.restype = C.c_int
+    L.orc_num_threads.restype = C.c_int
+    L.orc_set_num_threads.argtypes = [C.c_int]
+    return L
 
 
 def lib():
     global _lib
     if _lib is None:
         build()
-        L = C.CDLL(LIB)
-        L.orc_boris_step.argtypes = [C.c_double, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_void_p,
-                                     C.c_void_p, C.c_void_p]
-        L.orc_rk4_step.argtypes = [C.c_double, C.c_void_p, C.c_int64, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.orc_track.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_void_p,
-                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.orc_track.restype = C.c_double
-        L.orc_inject.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
-        L.orc_theta_track.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
-                                      C.c_double, C.c_void_p, C.c_void_p, C.c_int]
-        L.orc_sc_step.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-        L.orc_sc_step.restype = C.c_int
-        L.orc_num_threads.restype = C.c_int
-        L.orc_set_num_threads.argtypes = [C.c_int]
-        _lib = L
+        _lib = _bind(LIB)
     return _lib
+
+
+def lib_fma():
+    """The same oracle built with fused multiply-adds (a second, differently
+    rounded float64 build; see oracle/Makefile)."""
+    global _lib_fma
+    if _lib_fma is None:
+        build()
+        _lib_fma = _bind(LIB_FMA)
+    return _lib_fma
 
 
 def _orc_field(bmap, keep):
@@ -211,11 +228,12 @@ def rk4_step(setup: Setup, mat, t, dt):
                        C.byref(setup.cs))
 
 
-def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0):
-    """Injection + push loop without space charge; returns (t_end, head)."""
+def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0, fused=False):
+    """Injection + push loop without space charge; returns (t_end, head).
+    fused: run the build with fused multiply-adds (lib_fma)."""
     _mat(mat)
     h = C.c_int64(head)
-    t = lib().orc_track(1 if solver == "Boris" else 0, mat.ctypes.data, mat.shape[0], t_start, dt, nsteps,
+    t = (lib_fma() if fused else lib()).orc_track(1 if solver == "Boris" else 0, mat.ctypes.data, mat.shape[0], t_start, dt, nsteps,
                         C.byref(h), C.byref(setup.field), C.byref(setup.emap), C.byref(setup.ap),
                         C.byref(setup.cs))
     return t, h.value

@@ -163,6 +163,16 @@ class SCDesc(C.Structure):
     ]
 
 
+class BunchDesc(C.Structure):
+    _fields_ = [("n", C.c_int64), ("id0", C.c_int64), ("seed", C.c_uint64), ("sub_bunch", C.c_int64),
+                ("transverse", C.c_int32), ("longitudinal", C.c_int32), ("cut_off", C.c_double),
+                ("twiss", (C.c_double * 3) * 3), ("uniform_length", C.c_double), ("uniform_sigma", C.c_double),
+                ("centre", C.c_double * 6), ("fi", C.c_double), ("bunch_id", C.c_double), ("out", C.c_void_p)]
+
+
+DIST_TYPES = {"gauss": 0, "kv": 1, "waterbag": 2, "hollow_waterbag": 3, "UniformGauss": 4}
+
+
 class SCDiag(C.Structure):
     _fields_ = [(name, C.c_double) for name in (
         "fi_s", "fi_e", "slice_step", "mean_gamma_m1", "mean_x", "mean_z", "sigma_x", "sigma_z",
@@ -171,6 +181,7 @@ class SCDiag(C.Structure):
 
 
 EXPORTS = {
+    "ffa_bunch_sample": [C.POINTER(BunchDesc), d_p, d_p],
     "ffa_fieldmap_create": [C.POINTER(FieldDesc), d_p, C.POINTER(d_p)],
     "ffa_fieldmap_destroy": [d_p],
     "ffa_fieldmap_set_harmonics": [d_p, C.c_int32, d_p, d_p, d_p, d_p, d_p],

@@ -14,7 +14,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO_DIR = os.path.dirname(PKG_DIR)
 CSRC = os.path.join(PKG_DIR, "csrc")
 LIB_PATH = os.path.join(PKG_DIR, "libffa_cuda.so")
-SOURCES = ["ffa_push.cu", "ffa_capi.cu", "ffa_sc.cu", "ffa_mapgen.cu", "ffa_mlp.cu"]
+SOURCES = ["ffa_push.cu", "ffa_capi.cu", "ffa_sc.cu", "ffa_mapgen.cu", "ffa_mlp.cu", "ffa_bunch.cu"]
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -325,9 +325,13 @@ def GetInitRAndFiForInjection(SEO_R, SEO_Pr, InjectCL, Ek):
 def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit, num_points, InjTimeNanoSec,
                                      LongitudeAlpha, LongitudeBeta, LongitudeT, acc_U0=100.0e3, acc_phi0=0.0,
                                      TwissParams=None, dist_types=("gauss", "gauss"), dx_xp_y_yp=(0.0, 0.0, 0.0, 0.0),
-                                     Bunch_ID=0.0, bucket_obj=None, rng=None):
+                                     Bunch_ID=0.0, bucket_obj=None, rng=None, device_out=None, seed=0):
     """One sub-bunch (src/FFAG_Distribution.py:1152-1345): returns (p-format
-    matrix, distribution, centre (r, pr, z, pz, Ek, t), bucket_obj)."""
+    matrix, distribution, centre (r, pr, z, pz, Ek, t), bucket_obj).
+    device_out: a device float64 tensor of num_points x 16 rows; the rows are
+    then drawn on the GPU (ffa_bunch_sample, Philox keyed by `seed` and the
+    sub-bunch index Bunch_ID) and written there, and the returned matrix is
+    that tensor."""
     from .seo import LoadSEOParams
     rng = rng if rng is not None else _default_rng
     eR, eZ, eFi = Emit[0] / 1000.0 / 1000.0, Emit[1] / 1000.0 / 1000.0, Emit[2]
@@ -354,12 +358,18 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
     dist = CustomDist3D(create_distribution(ttype, twiss_transverse=(TwissContainer(aR, bR, eR),
                                                                        TwissContainer(aZ, bZ, eZ))),
                         create_distribution(ltype, twiss_longitudinal=tw_fi))
+    rc, prc, zc, pzc = r_c + dx_xp_y_yp[0], pr_c + dx_xp_y_yp[1], dx_xp_y_yp[2], dx_xp_y_yp[3]
+    if device_out is not None:
+        _sample_on_device(device_out, num_points, ttype, ltype, ((aR, bR, eR), (aZ, bZ, eZ),
+                          (LongitudeAlpha, LongitudeBeta, eFi)), LongitudeT,
+                          math.sqrt(eFi / LongitudeBeta), (rc, prc, zc, pzc, Ek_c, InjTimeNanoSec), fi_c,
+                          Bunch_ID, seed)
+        return device_out, dist, (rc, prc, zc, pzc, Ek_c, InjTimeNanoSec), bucket_obj
     r, pr, z, pz, t_inj, Ek = dist.sample(num_points, rng)
     if ltype == "UniformGauss":
         sigma = math.sqrt(eFi / LongitudeBeta)
         t_inj = rng.uniform(-0.5 * LongitudeT, 0.5 * LongitudeT, num_points)
         Ek = rng.normal(0.0, sigma, num_points)
-    rc, prc, zc, pzc = r_c + dx_xp_y_yp[0], pr_c + dx_xp_y_yp[1], dx_xp_y_yp[2], dx_xp_y_yp[3]
     a = np.zeros((num_points, 16))
     a[:, COLUMNS["r"]] = r + rc
     a[:, COLUMNS["vr"]] = pr + prc
@@ -374,6 +384,34 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
     return a, dist, (rc, prc, zc, pzc, Ek_c, InjTimeNanoSec), bucket_obj
 
 
+def _sample_on_device(out, n, ttype, ltype, twiss, length, sigma, centre, fi, bunch_id, seed, id0=0):
+    """One ffa_bunch_sample call writing n p-format rows into `out` (device
+    float64, n x 16, contiguous)."""
+    import ctypes
+    import torch
+    from . import _lib
+    if out.dtype != torch.float64 or not out.is_cuda or not out.is_contiguous() or tuple(out.shape) != (n, 16):
+        raise ValueError("device_out must be a contiguous CUDA float64 tensor of shape (num_points, 16)")
+    for t, kind in ((ttype, "transverse"), (ltype, "longitudinal")):
+        if t not in _lib.DIST_TYPES or (kind == "transverse" and t == "UniformGauss"):
+            raise ValueError(f"{kind} distribution {t!r} is not built on the device")
+    d = _lib.BunchDesc()
+    d.n, d.id0, d.seed, d.sub_bunch = int(n), int(id0), int(seed) & ((1 << 64) - 1), int(bunch_id)
+    d.transverse, d.longitudinal = _lib.DIST_TYPES[ttype], _lib.DIST_TYPES[ltype]
+    d.cut_off = -1.0
+    for p in range(3):
+        for k in range(3):
+            d.twiss[p][k] = float(twiss[p][k])
+    d.uniform_length, d.uniform_sigma = float(length), float(sigma)
+    for k in range(6):
+        d.centre[k] = float(centre[k])
+    d.fi, d.bunch_id, d.out = float(fi), float(bunch_id), out.data_ptr()
+    with torch.cuda.device(out.device):
+        _lib.check(_lib.lib().ffa_bunch_sample(ctypes.byref(d), None,
+                                                torch.cuda.current_stream(out.device).cuda_stream),
+                   "ffa_bunch_sample")
+
+
 def _emap_paint_params(path):
     with open(path) as f:
         content = f.read()
@@ -381,13 +419,23 @@ def _emap_paint_params(path):
     return get("gap_azimuth"), get("acc_phi_paint"), get("acc_voltage_paint")
 
 
-def GenerateBunches(BunchPara, rng=None):
+def GenerateBunches(BunchPara, rng=None, device=None):
     """All painted sub-bunches, stacked (src/FFAG_Distribution.py:1542-1640).
     BunchPara holds the reference's keys (SEO, InjectEk, InjPosition,
     ParticleNum, TransverseREmit, TransverseZEmit, LongitudeT, LongitudeDEk,
     InjTimeNanoSec, TransverseDistType, LongitudeDistType, PaintEnable,
     PaintMaxNum, PaintTimeInterval, PaintCurve, EmapPATHName) and optionally
-    Seed."""
+    Seed.  device: draw the particles on that GPU (ffa_bunch_sample) and
+    return a device float64 tensor; the host side (SEO tables, painting
+    offsets) is the same."""
+    if device is not None:
+        import torch
+        num = int(BunchPara["ParticleNum"])
+        curve_n = 1
+        if BunchPara["PaintEnable"]:
+            c_ = np.loadtxt(BunchPara["PaintCurve"], skiprows=1)
+            curve_n = int(min(np.floor(np.max(c_[:, 0]) / BunchPara["PaintTimeInterval"]), BunchPara["PaintMaxNum"]))
+        out_dev = torch.empty((curve_n * num, 16), dtype=torch.float64, device=device)
     if rng is None:
         rng = np.random.default_rng(BunchPara.get("Seed"))
     _, acc_phi0, acc_V0 = _emap_paint_params(BunchPara["EmapPATHName"])
@@ -410,6 +458,8 @@ def GenerateBunches(BunchPara, rng=None):
             [BunchPara["TransverseREmit"], BunchPara["TransverseZEmit"], LT * LdE / 16], BunchPara["ParticleNum"],
             t_inj, 0.0, LT / LdE, LT, acc_U0=acc_V0, acc_phi0=acc_phi0,
             dist_types=(BunchPara["TransverseDistType"], BunchPara["LongitudeDistType"]), dx_xp_y_yp=off,
-            Bunch_ID=i, bucket_obj=bucket, rng=rng)
+            Bunch_ID=i, bucket_obj=bucket, rng=rng,
+            device_out=None if device is None else out_dev[i * num:(i + 1) * num],
+            seed=int(BunchPara.get("Seed") or 0))
         out.append(sub)
-    return np.vstack(out)
+    return out_dev if device is not None else np.vstack(out)

@@ -78,3 +78,51 @@ def test_bunch_matches_reference_in_distribution(gb, key):
             sd = r[:, c].std()
             assert abs(m[:, c].mean() - r[:, c].mean()) <= 6 * sd / np.sqrt(n) + 1e-15, (b, c)
             assert abs(m[:, c].std() / sd - 1) <= 0.06, (b, c)
+
+
+# ------------------------------------------------ the GPU generator's oracle
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors (counter, key -> output) of its
+    published description, through the oracle's restatement."""
+    from oracle import bunch as OB
+    M = 0xFFFFFFFF
+    for ctr, key, want in (((0, 0, 0, 0), 0, (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+                           ((M, M, M, M), (M << 32) | M, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+                           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0x299f31d0 << 32) | 0xa4093822,
+                            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))):
+        got = [int(x) for x in OB.philox4x32_10(*ctr, key)]
+        assert got == list(want)
+
+
+@pytest.mark.parametrize("kind,ltype", [("gauss", "gauss"), ("kv", "kv"), ("waterbag", "waterbag"),
+                                        ("hollow_waterbag", "hollow_waterbag"), ("gauss", "UniformGauss")])
+def test_device_sampler_oracle_matches_host_generator_in_distribution(kind, ltype):
+    """The restated device sampler (Philox draws) against the host numpy
+    generator of the same shapes: means, rms sizes and rms emittances of
+    every plane agree within sampling error."""
+    from oracle import bunch as OB
+    from pyffa_b200 import _lib
+    tw = ((-0.8, 2.5, 1.2e-6), (0.4, 5.0, 0.7e-6), (0.1, 40.0, 3e-3))
+    n = 200_000
+    # the longitudinal emittance as GenerateInitDistributionDtInjNew hands it
+    # to the shapes (doubled for KV)
+    lt = tw[2][2] * (2 if ltype == "kv" else 1)
+    got = OB.sample(n, 77, 3, _lib.DIST_TYPES[kind], _lib.DIST_TYPES[ltype], (tw[0], tw[1], (tw[2][0], tw[2][1], lt)),
+                    (8.5, 0.01, 0.0, 0.0, 300.0, 5.0), 0.2, 3.0, uniform_length=100.0, uniform_sigma=0.05)
+    dist = D.CustomDist3D(D.create_distribution(kind, twiss_transverse=(D.TwissContainer(*tw[0]),
+                                                                        D.TwissContainer(*tw[1]))),
+                          D.create_distribution(ltype, twiss_longitudinal=D.TwissContainer(tw[2][0], tw[2][1], lt)))
+    r, pr, z, pz, t, E = dist.sample(n, np.random.default_rng(5))
+    if ltype == "UniformGauss":
+        t, E = np.random.default_rng(6).uniform(-50.0, 50.0, n), np.random.default_rng(7).normal(0.0, 0.05, n)
+    ref = np.stack([r + 8.5, pr + 0.01, z, pz, E + 300.0, t + 5.0], 1)
+    mine = got[:, [0, 1, 2, 3, 5, 6]]
+    assert np.all(got[:, 4] == 0.2) and np.all(got[:, 13] == 3.0) and np.array_equal(got[:, 14], np.arange(n))
+    for c in range(6):
+        sd = ref[:, c].std()
+        assert abs(mine[:, c].mean() - ref[:, c].mean()) <= 6 * sd / np.sqrt(n), c
+        assert abs(mine[:, c].std() / sd - 1) <= 0.02, c
+    for a, b in ((0, 1), (2, 3)):
+        e = lambda m: np.sqrt(np.cov(m[:, a], m[:, b]).diagonal().prod() - np.cov(m[:, a], m[:, b])[0, 1] ** 2)
+        assert abs(e(mine) / e(ref) - 1) <= 0.02

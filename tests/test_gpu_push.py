@@ -240,8 +240,14 @@ def test_c0_hundred_turns_vs_oracle():
     bunch, 100 turns of 720 steps.  The whole bunch is pushed on the GPU one
     turn per launch; after every turn a 512-particle subset is compared with
     the oracle's run of the same particles, per element, at 1e-12 per turn or
-    ten times the dynamics' own rounding sensitivity over the same turns (the
-    oracle against itself with r nudged by one ulp), whichever is larger."""
+    ten times the dynamics' own rounding sensitivity over the same turns,
+    whichever is larger.  That sensitivity is the larger of two measures: the
+    oracle against itself with r nudged by one ulp, and the oracle against
+    its build with fused multiply-adds (a second correct float64 build that
+    rounds differently at every contracted operation, as the GPU build
+    does).  At 720 steps per turn the large-amplitude motion is weakly
+    chaotic, so the sensitivity itself grows from 1e-14 to ~1e-7 of the
+    vertical amplitude over the run."""
     import os
     import tempfile
     from oracle import oracle as O
@@ -269,6 +275,7 @@ def test_c0_hundred_turns_vs_oracle():
     ref = v[idx].copy()
     nudged = ref.copy()
     nudged[:, 0] = np.nextafter(nudged[:, 0], np.inf)
+    fused = ref.copy()
     worst = []
     for t in range(1, turns + 1):
         pu.push(clock, (t - 1) * spt, spt, 0)
@@ -276,7 +283,9 @@ def test_c0_hundred_turns_vs_oracle():
         got = b.matrix()[idx]
         O.track(S, "Boris", ref, clock.t[(t - 1) * spt], dt, spt)
         O.track(S, "Boris", nudged, clock.t[(t - 1) * spt], dt, spt)
-        floor = coord_errors(nudged, ref)
+        O.track(S, "Boris", fused, clock.t[(t - 1) * spt], dt, spt, fused=True)
+        fn, ff = coord_errors(nudged, ref), coord_errors(fused, ref)
+        floor = {c: max(fn[c], ff[c]) for c in fn}
         assert np.array_equal(got[:, 7:9], ref[:, 7:9]), f"flags differ after turn {t}"
         for c, err in coord_errors(got, ref).items():
             tol = max(1e-12 * t, 10 * floor[c])
