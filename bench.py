@@ -112,6 +112,15 @@ class ClockSampler:
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait (at most 5 s) for its
+        # first sample so that the timed region is covered
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            self.fh.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):

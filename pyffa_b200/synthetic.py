@@ -288,11 +288,26 @@ def design_dt(Ek=300.0, steps_per_turn=720, cfg=None):
 
 
 def centred_bunch(n, seed=0, Ek=300.0, cfg=None, kind="gauss", **kw):
-    """Bunch centred on the closed orbit at fi = 0 (p-format pr = atan(pr0))."""
+    """Bunch centred on the closed orbit (p-format pr = atan(pr0)).  A bunch
+    spread in azimuth (the KV bunch's sigma_t) has every particle centred on
+    the closed orbit at its own azimuth: the orbit is scalloped, so one
+    radius for all would start the particles far from their local orbit
+    with large radial oscillations."""
     d = design(Ek, cfg)
     if kind == "gauss":
         a = gaussian_bunch(n, seed=seed, Ek=Ek, r0=d["r0"], **kw)
     else:
         a = kv_bunch(n, seed=seed, Ek=Ek, r0=d["r0"], **kw)
-    a[:, 1] += np.arctan(d["pr0"])
+    fm = np.mod(a[:, 4], 2 * np.pi)
+    if np.any(fm != 0.0):
+        from . import orbit
+        key = ("orbit_table", json.dumps(cfg if cfg is not None else lattice_bmap(), sort_keys=True), float(Ek))
+        if key not in _design_cache:
+            t = orbit.seo_tables(cfg if cfg is not None else lattice_bmap(), np.array([float(Ek)]), nfi=721)
+            _design_cache[key] = (t["fi_axis"], t["r"][0], t["pr"][0])
+        fi_axis, r_co, pr_co = _design_cache[key]
+        a[:, 0] += np.interp(fm, fi_axis, r_co) - d["r0"]
+        a[:, 1] += np.arctan(np.interp(fm, fi_axis, pr_co))
+    else:
+        a[:, 1] += np.arctan(d["pr0"])
     return a
