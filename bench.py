@@ -526,9 +526,10 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     (RF off), 200 turns of the slowest instance per iteration, float64
     one-turn-map fit and fixed-point update per instance; the push's launch
     shape picked by the autotuner on the scan's bunch first; each iteration
-    one push launch over all its steps (crossing records in one device
-    buffer); iteration 1 direct, iteration 2 captured as a CUDA graph, later
-    ones replays.  2880 steps per
+    one push launch over all its steps, the kernel adding every crossing to
+    its instance's normal equations (no crossing records); iteration 1
+    direct, iteration 2 captured as a CUDA graph, later ones replays.  2880
+    steps per
     turn of the fastest instance: at 720 the 2.8-degree D magnet gets five
     steps and the motion is not regular enough for a tune."""
     import torch
@@ -547,8 +548,7 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
     scan = coscan.BatchedOrbitScan(gp2, E, counts, r_sc + 1e-4, np.full(n_instances, np.arctan(d["pr0"])),
                                    d["perimeter"] * scale, sigma=0.5e-3, turns=turns, seed=seed, device=dev,
                                    steps_per_turn=steps_per_turn)
-    # iteration 1 direct (per-launch record counts), iteration 2 the
-    # fixed-shape accumulation, captured as a CUDA graph, then replays
+    # iteration 1 direct, iteration 2 captured as a CUDA graph, then replays
     recs = [scan.iterate(graph=False)] + [scan.iterate(graph=True) for _ in range(iterations)]
     torch.cuda.synchronize(dev)
     pt = sum(r["particle_turns"] for r in recs)
@@ -561,14 +561,17 @@ def coscan_bench(gp, dev, n_instances=256, turns=200, iterations=2, seed=0, step
             "ms_per_iteration": [r["ms"] for r in recs], "modes": [r["mode"] for r in recs],
             "push_launches_per_iteration": recs[-1]["launches"],
             "steps_per_launch": scan._dev_state.L,
-            "crossing_buffer_gb": scan._dev_state.cap.buf.numel() * 8 / 1e9,
+            "accumulate": scan.accumulate,
+            "fit_memory_mb": sum(t.numel() * t.element_size() for t in
+                                 (scan._dev_state.sums, scan._dev_state.fit_last, scan._dev_state.fit_has,
+                                  scan._dev_state.fit_inst)) / 1e6,
             "max_abs_dr_m": [r["max_abs_dr"] for r in recs],
             "orbit_vs_scaling_law_m": float(np.abs(scan.r - r_sc).max()),
             "Qr_frac_range": [float(np.nanmin(q[:, 0])), float(np.nanmax(q[:, 0]))],
             "Qz_frac_range": [float(np.nanmin(q[:, 1])), float(np.nanmax(q[:, 1]))],
             "padding_waste": scan.padding(), "valid_instances": int(recs[-1]["good"].sum()),
             "dtype": "f32c push, f64 fit and update",
-            "graph": "iteration 1 direct; iteration 2 fixed-shape and captured as one CUDA graph; iteration 3 a replay",
+            "graph": "iteration 1 direct; iteration 2 captured as one CUDA graph; iteration 3 a replay",
             "autotune": None if scan.tuning is None else
             {"shape": scan.tuning.report()["chosen"], "speedup_vs_default_shape": scan.tuning.speedup,
              "tune_steps": scan.tune_steps, "rtol": scan.tune_rtol, "candidates": _tune_rows(scan.tuning)}}

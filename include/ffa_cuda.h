@@ -159,9 +159,31 @@ typedef struct ffa_step_table {
  *   [18] post-step survival flag, [19] injection flag,
  *   [20..22] the space-charge field the step used (Esc r, z, fi).
  * Records come in no particular order.  `count` (device int64) is advanced
- * atomically; records past `capacity` are counted but not written. */
+ * atomically; records past `capacity` are counted but not written.
+ *
+ * One-turn-map sums instead of records (fit_sums != NULL; one target): the
+ * closed-orbit and tune fits of many instances (groups of particles, one
+ * energy each) need, per instance and transverse plane, only the normal
+ * equations of the least-squares map x' = M x + b between a particle's
+ * successive crossings (the reference fits that map one trajectory at a
+ * time: FFAG_SearchSEO / GetQrQz, src/FFAG_track.py:1142-1371).  At each
+ * crossing the kernel interpolates the step as a cubic Hermite curve in
+ * Cartesian coordinates rotated by the target (positions and velocities at
+ * both ends, the crossing time by three Newton steps from the linear
+ * estimate, velocities linear in time) to s = (r, vr, z, vz) at the target,
+ * forms u = (s - fit_centre[k]) * fit_scale[k] for the particle's instance
+ * k = fit_instance[i], and, when fit_has[i] is set, adds with float64
+ * atomics to fit_sums[k * FFA_FIT_SUMS + 12 p + j], plane p (0: r, vr;
+ * 1: z, vz), f = (w_p0, w_p1, 1) of the previous crossing w = fit_last[i]:
+ *   j = 0..5:  f0 f0, f0 f1, f0, f1 f1, f1, 1     (f f^T, upper triangle)
+ *   j = 6..11: u_p0 f0, u_p0 f1, u_p0, u_p1 f0, u_p1 f1, u_p1   (u' f^T)
+ * and adds 1 to fit_sums[k * FFA_FIT_SUMS + 24] for every crossing; then
+ * fit_last[i] = u, fit_has[i] = 1.  Memory is O(instances + particles),
+ * whatever the number of turns; buf, capacity and count are not used.  The
+ * sums depend on the order of the atomics at the rounding level. */
 #define FFA_CROSSING_RECORD 23
 #define FFA_MAX_CROSSING_TARGETS 8
+#define FFA_FIT_SUMS 25
 typedef struct ffa_crossing {
     int32_t ntargets;             /* 1 .. FFA_MAX_CROSSING_TARGETS */
     int32_t pad;
@@ -169,6 +191,12 @@ typedef struct ffa_crossing {
     double *buf;                  /* device, capacity * FFA_CROSSING_RECORD */
     int64_t capacity;
     int64_t *count;               /* device */
+    const int32_t *fit_instance;  /* device, n; NULL unless fit_sums */
+    const double *fit_centre;     /* device, (instances, 4) */
+    const double *fit_scale;      /* device, (instances, 4) */
+    double *fit_last;             /* device, (n, 4) */
+    uint8_t *fit_has;             /* device, n */
+    double *fit_sums;             /* device, (instances, FFA_FIT_SUMS); NULL: records */
 } ffa_crossing;
 
 /* ffa_push with azimuth-crossing capture (all three pushers).  Replaces the

@@ -109,9 +109,14 @@ CROSSING_RECORD = 23
 MAX_CROSSING_TARGETS = 8
 
 
+FIT_SUMS = 25
+
+
 class Crossing(C.Structure):
     _fields_ = [("ntargets", C.c_int32), ("pad", C.c_int32), ("target", C.c_double * MAX_CROSSING_TARGETS),
-                ("buf", d_p), ("capacity", C.c_int64), ("count", d_p)]
+                ("buf", d_p), ("capacity", C.c_int64), ("count", d_p),
+                ("fit_instance", d_p), ("fit_centre", d_p), ("fit_scale", d_p), ("fit_last", d_p),
+                ("fit_has", d_p), ("fit_sums", d_p)]
 
 
 class ThetaTrackDesc(C.Structure):

@@ -7,9 +7,10 @@ load of small and large instances is balanced particle by particle.  Per
 iteration the bunch is pushed for `turns` turns of the slowest instance, the
 azimuth-0 crossings of every particle (ffa_push_crossing; the state at the
 azimuth from a cubic Hermite interpolation of the step in Cartesian
-coordinates) are paired turn to turn on the device, and for every instance
-and transverse plane the least-squares one-turn map x' = M x + b over all of
-its particles and turns is formed in float64.  Its fixed point
+coordinates) are paired turn to turn inside the push kernel, which adds each
+pair to its instance's normal equations of the least-squares one-turn map
+x' = M x + b (per transverse plane, over all of the instance's particles and
+turns, float64); the map is solved on the host.  Its fixed point
 (I - M)^-1 b is the Newton update of the closed orbit; the phase advance of
 M (trace, with the sign of M12 fixing the half plane) is the fractional tune.
 The next iteration restarts the instances around the updated orbits.
@@ -146,6 +147,25 @@ def accumulate_crossings_fixed(rec, count, dt, gv, inst_ext, nsteps, last, has, 
     has.index_fill_(0, idx, True)
 
 
+def unpack_fit_sums(sums):
+    """S (2, I, 3, 3) and Y (2, I, 2, 3) of accumulate_crossings, and the
+    crossing counts (I,), from the (I, 25) sums a push accumulates at
+    crossing time (ffa_crossing.fit_sums): per plane the upper triangle of
+    f f^T (f0 f0, f0 f1, f0, f1 f1, f1, 1) then x' f^T row by row; the
+    crossings last."""
+    sums = np.asarray(sums, np.float64)
+    I = sums.shape[0]
+    S = np.empty((2, I, 3, 3))
+    Y = np.empty((2, I, 2, 3))
+    for pl in (0, 1):
+        q = sums[:, 12 * pl:12 * pl + 12]
+        S[pl, :, 0, 0], S[pl, :, 0, 1], S[pl, :, 0, 2] = q[:, 0], q[:, 1], q[:, 2]
+        S[pl, :, 1, 1], S[pl, :, 1, 2], S[pl, :, 2, 2] = q[:, 3], q[:, 4], q[:, 5]
+        S[pl, :, 1, 0], S[pl, :, 2, 0], S[pl, :, 2, 1] = q[:, 1], q[:, 2], q[:, 4]
+        Y[pl] = q[:, 6:12].reshape(I, 2, 3)
+    return S, Y, sums[:, 24].copy()
+
+
 def fit_one_turn(S, Y, cond_max=1e14):
     """float64 least-squares one-turn map per instance and plane from the sums
     of accumulate_crossings: returns the fixed point offsets (I, 4), the
@@ -190,17 +210,27 @@ class BatchedOrbitScan:
     whose states differ from the default's by more than tune_rtol (relative)
     on the tuning run are not chosen.  The scan fits maps to many crossings,
     so rounding-level differences (1e-11) are accepted by default.
-    persistent: the whole iteration is one push launch, its crossing records
-    held in one device buffer (about 1.8 KB per particle and turn-bound of
-    crossings: 10 GB for 162k particles over 200 turns), when that buffer and
-    the accumulation's temporaries (taken as 3x the buffer) fit in half the
-    free device memory; otherwise, and with persistent=False, launches of the
-    longest length whose records fit that memory (at most 5 records per
-    particle without `persistent`)."""
+    accumulate="kernel": the push kernel itself adds each crossing to its
+    instance's normal equations (ffa_crossing.fit_sums), so the whole
+    iteration is one push launch whose memory is 25 doubles per instance and
+    4 doubles + 1 byte per particle, whatever the number of turns.
+    accumulate="records": the crossing records are written to a device
+    buffer and reduced into the same sums by accumulate_crossings_fixed
+    (kept to check the kernel's sums); persistent: the whole iteration is one
+    push launch, its records held in one buffer (about 1.8 KB per particle
+    and turn-bound of crossings: 10 GB for 162k particles over 200 turns),
+    when that buffer and the accumulation's temporaries (taken as 3x the
+    buffer) fit in half the free device memory; otherwise, and with
+    persistent=False, launches of the longest length whose records fit that
+    memory (at most 5 records per particle without `persistent`)."""
 
     def __init__(self, gp, energies, counts, r0, pr0, perimeter, sigma=0.5e-3, steps_per_turn=720, turns=200,
-                 seed=0, device=None, autotune=True, tune_steps=1000, tune_rtol=1e-9, persistent=True):
+                 seed=0, device=None, autotune=True, tune_steps=1000, tune_rtol=1e-9, persistent=True,
+                 accumulate="kernel"):
         import torch
+        if accumulate not in ("kernel", "records"):
+            raise ValueError(f"accumulate must be 'kernel' or 'records', not {accumulate!r}")
+        self.accumulate = accumulate
         self.gp = gp
         self.persistent = bool(persistent)
         self.autotune = bool(autotune)
@@ -268,10 +298,6 @@ class BatchedOrbitScan:
         st.pusher.stream = st.stream
         st.clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
         st.clock.ensure(self.steps + 1)
-        st.cap = CrossingCapture(st.bunch, [0.0], self.gp, self.dt)
-        st.L = self._launch_steps(st.cap)
-        st.xing = st.cap.prepare(st.L)
-        st.rows = st.cap.buf.view(-1, 23)[:st.cap.x.capacity]
         unit = np.ones((self.I + 1, 4))
         unit[:self.I, 0] = unit[:self.I, 2] = 1e-3
         unit[:self.I, 1] = unit[:self.I, 3] = 1e-3 * self.conv.Ek2v(self.E)
@@ -285,6 +311,29 @@ class BatchedOrbitScan:
         st.Y = torch.zeros((2, self.I + 1, 2, 3), **f64)
         st.crossings = torch.zeros(self.I + 1, **f64)
         st.maxk = torch.zeros(1, dtype=torch.int64, device=dev)
+        if self.accumulate == "kernel":
+            from . import _lib
+            st.cap = None
+            st.L = self.steps
+            st.fit_inst = torch.as_tensor(self.inst.astype(np.int32), device=dev)
+            st.fit_last = torch.zeros((self.N, 4), **f64)
+            st.fit_has = torch.zeros(self.N, dtype=torch.uint8, device=dev)
+            st.sums = torch.zeros((self.I, _lib.FIT_SUMS), **f64)
+            x = _lib.Crossing()
+            x.ntargets = 1
+            x.target[0] = 0.0
+            x.fit_instance = st.fit_inst.data_ptr()
+            x.fit_centre = st.gv.data_ptr()
+            x.fit_scale = st.scale.data_ptr()
+            x.fit_last = st.fit_last.data_ptr()
+            x.fit_has = st.fit_has.data_ptr()
+            x.fit_sums = st.sums.data_ptr()
+            st.xing = x
+        else:
+            st.cap = CrossingCapture(st.bunch, [0.0], self.gp, self.dt)
+            st.L = self._launch_steps(st.cap)
+            st.xing = st.cap.prepare(st.L)
+            st.rows = st.cap.buf.view(-1, 23)[:st.cap.x.capacity]
         st.launches = len(range(0, self.steps, st.L))
         self._dev_state = st
         if self.autotune:
@@ -302,8 +351,12 @@ class BatchedOrbitScan:
         def reset():
             _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()),
                                                  st.stream.cuda_stream), "ffa_aos_to_soa")
+            if st.cap is None:
+                for t in (st.sums, st.fit_last, st.fit_has):
+                    t.zero_()
         res = autotune.tune_push(st.pusher, st.clock, 0, min(st.L, self.tune_steps, self.steps), xing=st.xing,
-                                 reset=reset, count=st.cap.count, rtol=self.tune_rtol)
+                                 reset=reset, count=None if st.cap is None else st.cap.count,
+                                 rtol=self.tune_rtol)
         st.pusher.shape = res.best
         self.tuning = res
 
@@ -330,14 +383,20 @@ class BatchedOrbitScan:
 
     def _body(self):
         """The work of one iteration, enqueued on the scan's stream: AoS ->
-        SoA, then for every launch the push with crossing capture and the
-        accumulation of its records."""
+        SoA, then the push with the kernel's own accumulation, or for every
+        launch the push with crossing capture and the accumulation of its
+        records."""
         import ctypes
         from . import _lib
         st = self._dev_state
         b = st.bunch
         _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), st.stream.cuda_stream),
                    "ffa_aos_to_soa")
+        if st.cap is None:
+            for t in (st.sums, st.fit_last, st.fit_has):
+                t.zero_()
+            st.pusher.push(st.clock, 0, self.steps, 0, xing=st.xing)
+            return
         for t in (st.S, st.Y, st.crossings, st.last, st.has, st.maxk):
             t.zero_()
         for s0 in range(0, self.steps, st.L):
@@ -354,6 +413,9 @@ class BatchedOrbitScan:
         import ctypes
         from . import _lib
         st = self._dev_state
+        if st.cap is None:
+            self._body()
+            return
         b = st.bunch
         _lib.check(_lib.lib().ffa_aos_to_soa(b.aos.data_ptr(), b.n, ctypes.byref(b.soa()), st.stream.cuda_stream),
                    "ffa_aos_to_soa")
@@ -374,13 +436,14 @@ class BatchedOrbitScan:
     def iterate(self, graph=True):
         """One push of all instances and the float64 update; returns the
         iteration record (orbit change, tunes, particle-turns, device time).
-        graph=False: the launches run directly, each launch's records counted
-        on the host and accumulated ("direct").  graph=True: the fixed-shape
-        accumulation over the whole record buffer, which has no host
-        read-back; the first such iteration runs directly (it is also the
-        warm-up, "captured") and is captured as one CUDA graph, which later
-        iterations replay after uploading their starting states and guesses
-        ("graph")."""
+        With accumulate="kernel" an iteration is one push launch either way.
+        With "records", graph=False: the launches run directly, each launch's
+        records counted on the host and accumulated ("direct"); graph=True:
+        the fixed-shape accumulation over the whole record buffer, which has
+        no host read-back.  With graph=True the first iteration runs directly
+        (it is also the warm-up, "captured") and is captured as one CUDA
+        graph, which later iterations replay after uploading their starting
+        states and guesses ("graph")."""
         import torch
         if self._dev_state is None:
             self._setup()
@@ -402,11 +465,14 @@ class BatchedOrbitScan:
             e1.record(st.stream)
         st.stream.synchronize()
         ms = e0.elapsed_time(e1)
-        if int(st.maxk.item()) > st.cap.x.capacity:
-            raise RuntimeError(f"crossing records overflowed: {int(st.maxk.item())} > {st.cap.x.capacity}")
-        S = st.S[:, :self.I].cpu().numpy()
-        Y = st.Y[:, :self.I].cpu().numpy()
-        crossings = st.crossings[:self.I].cpu().numpy()
+        if st.cap is None:
+            S, Y, crossings = unpack_fit_sums(st.sums.cpu().numpy())
+        else:
+            if int(st.maxk.item()) > st.cap.x.capacity:
+                raise RuntimeError(f"crossing records overflowed: {int(st.maxk.item())} > {st.cap.x.capacity}")
+            S = st.S[:, :self.I].cpu().numpy()
+            Y = st.Y[:, :self.I].cpu().numpy()
+            crossings = st.crossings[:self.I].cpu().numpy()
         gvn = st.gv[:self.I].cpu().numpy()
         if graph and self._graph is None:
             g = torch.cuda.CUDAGraph()

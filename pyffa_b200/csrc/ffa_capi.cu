@@ -344,9 +344,16 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     }
     p.status = status;
     if (xing) {
-        if (!xing->buf || !xing->count || xing->capacity < 0 || xing->ntargets < 1 ||
-            xing->ntargets > FFA_MAX_CROSSING_TARGETS)
+        if (xing->ntargets < 1 || xing->ntargets > FFA_MAX_CROSSING_TARGETS) return FFA_ERR_INVALID;
+        if (xing->fit_sums) {
+            // the fit reads f5 as d(phi)/dt, the Boris state; one target
+            if (!xing->fit_instance || !xing->fit_centre || !xing->fit_scale || !xing->fit_last ||
+                !xing->fit_has || xing->ntargets != 1)
+                return FFA_ERR_INVALID;
+            if (flags & FFA_RK4) return FFA_ERR_UNSUPPORTED;
+        } else if (!xing->buf || !xing->count || xing->capacity < 0) {
             return FFA_ERR_INVALID;
+        }
         for (int t = 0; t < xing->ntargets; ++t)
             if (!(xing->target[t] >= 0.0) || !(xing->target[t] < 2.0 * ffa::PI)) return FFA_ERR_INVALID;
         p.xing = *xing;

@@ -84,7 +84,7 @@ struct PushK {
     int32_t nsteps, sc_step;
     double dt;
     int64_t *status;
-    ffa_crossing xing;  // records.buf == NULL: no crossing capture
+    ffa_crossing xing;  // buf and fit_sums both NULL: no crossing capture
     // Boris constants, formed on the host so the kernel reads them from the
     // parameter bank instead of holding them in registers
     double hq;          // (0.5 dt) q
@@ -93,6 +93,11 @@ struct PushK {
     double inv_cc;      // 1 / c^2
     double inv_mmcc;    // 1 / (m^2 c^2)
 };
+
+inline __host__ __device__ bool xing_on(const PushK &p)
+{
+    return p.xing.buf != nullptr || p.xing.fit_sums != nullptr;
+}
 
 }  // namespace ffa
 

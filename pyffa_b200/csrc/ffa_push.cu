@@ -291,9 +291,76 @@ __device__ __forceinline__ double mod_2pi(double a)
     return __dsub_rn(a, __dmul_rn(tw, floor(a / tw)));
 }
 
+// sin and cos of a small angle (|d| below a push step's azimuth advance, a
+// few 1e-3 rad) by their Taylor series to d^9 / 9! and d^8 / 8!: truncation
+// below 1e-22 for |d| < 0.02.
+__device__ __forceinline__ void sincos_small(double d, double &s, double &c)
+{
+    const double d2 = d * d;
+    s = d * (1.0 - d2 * (1.0 / 6 - d2 * (1.0 / 120 - d2 * (1.0 / 5040 - d2 * (1.0 / 362880)))));
+    c = 1.0 - d2 * (0.5 - d2 * (1.0 / 24 - d2 * (1.0 / 720 - d2 * (1.0 / 40320))));
+}
+
+// One-turn-map sums at a crossing (the fit_sums form of ffa_crossing).  d0
+// and d1: the step's start and end azimuth relative to the target (d0 <= 0
+// <= d1, reduced mod 2 pi).
+__device__ __forceinline__ void fit_accumulate(const ffa_crossing &xc, int64_t i, double dt, double d0, double d1,
+                                               const double pre[7], const double post[7])
+{
+    // Cartesian state in the frame whose x axis points at the target azimuth
+    double s0, c0, s1, c1;
+    sincos_small(d0, s0, c0);
+    sincos_small(d1, s1, c1);
+    const double r0 = pre[0], vf0 = r0 * pre[5], r1 = post[0], vf1 = r1 * post[5];
+    const double X0 = r0 * c0, Y0 = r0 * s0, VX0 = pre[1] * c0 - vf0 * s0, VY0 = pre[1] * s0 + vf0 * c0;
+    const double X1 = r1 * c1, Y1 = r1 * s1, VX1 = post[1] * c1 - vf1 * s1, VY1 = post[1] * s1 + vf1 * c1;
+    double tau = Y0 / (Y0 - Y1);
+    for (int it = 0; it < 3; ++it) {
+        const double t2 = tau * tau, t3 = t2 * tau;
+        const double y = (2 * t3 - 3 * t2 + 1) * Y0 + (t3 - 2 * t2 + tau) * VY0 * dt + (3 * t2 - 2 * t3) * Y1 +
+                         (t3 - t2) * VY1 * dt;
+        const double dy = (6 * t2 - 6 * tau) * Y0 + (3 * t2 - 4 * tau + 1) * VY0 * dt + (6 * tau - 6 * t2) * Y1 +
+                          (3 * t2 - 2 * tau) * VY1 * dt;
+        tau = tau - y / dy;
+    }
+    const double t2 = tau * tau, t3 = t2 * tau;
+    const double h00 = 2 * t3 - 3 * t2 + 1, h10 = t3 - 2 * t2 + tau, h01 = 3 * t2 - 2 * t3, h11 = t3 - t2;
+    const int k = xc.fit_instance[i];
+    const double *ce = xc.fit_centre + 4 * k, *sc = xc.fit_scale + 4 * k;
+    double u[4];
+    u[0] = h00 * X0 + h10 * VX0 * dt + h01 * X1 + h11 * VX1 * dt;
+    u[1] = VX0 + tau * (VX1 - VX0);
+    u[2] = h00 * pre[2] + h10 * pre[3] * dt + h01 * post[2] + h11 * post[3] * dt;
+    u[3] = pre[3] + tau * (post[3] - pre[3]);
+    for (int c = 0; c < 4; ++c) u[c] = (u[c] - ce[c]) * sc[c];
+    double *acc = xc.fit_sums + (int64_t)k * FFA_FIT_SUMS;
+    double *w = xc.fit_last + 4 * i;
+    if (xc.fit_has[i]) {
+        for (int pl = 0; pl < 2; ++pl) {
+            const double f0 = w[2 * pl], f1 = w[2 * pl + 1], a = u[2 * pl], b = u[2 * pl + 1];
+            double *q = acc + 12 * pl;
+            atomicAdd(q + 0, f0 * f0);
+            atomicAdd(q + 1, f0 * f1);
+            atomicAdd(q + 2, f0);
+            atomicAdd(q + 3, f1 * f1);
+            atomicAdd(q + 4, f1);
+            atomicAdd(q + 5, 1.0);
+            atomicAdd(q + 6, a * f0);
+            atomicAdd(q + 7, a * f1);
+            atomicAdd(q + 8, a);
+            atomicAdd(q + 9, b * f0);
+            atomicAdd(q + 10, b * f1);
+            atomicAdd(q + 11, b);
+        }
+    }
+    atomicAdd(acc + 24, 1.0);
+    for (int c = 0; c < 4; ++c) w[c] = u[c];
+    xc.fit_has[i] = 1;
+}
+
 __device__ __forceinline__ void xing_check(const ffa_crossing &xc, int64_t i, int64_t gs, const double pre[7],
                                            const double post[7], int surv_after, int inj, double esr, double esz,
-                                           double esf)
+                                           double esf, double dt)
 {
     const double tw = 2.0 * PI;
     const double a = mod_2pi(pre[4]), b = mod_2pi(post[4]);
@@ -312,6 +379,15 @@ __device__ __forceinline__ void xing_check(const ffa_crossing &xc, int64_t i, in
             }
         }
         if (!hit) continue;
+        if (xc.fit_sums) {
+            double d0 = a - target, d1 = b - target;
+            if (b < a) {
+                if (target >= a) d1 += tw;
+                else d0 -= tw;
+            }
+            fit_accumulate(xc, i, dt, d0, d1, pre, post);
+            continue;
+        }
         const unsigned long long k = atomicAdd((unsigned long long *)xc.count, 1ull);
         if ((int64_t)k >= xc.capacity) continue;
         double *rec = xc.buf + (int64_t)k * FFA_CROSSING_RECORD;
@@ -472,7 +548,7 @@ constexpr int BORIS_TB = 32;
 // (more resident warps, more spills) for the launch-shape autotuner.  The
 // cap changes register allocation only, not the arithmetic.
 template <int MAXO, bool SC, bool XING, bool F32, int NREG = 80, bool HARM = false>
-__global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
+__global__ void __maxnreg__(NREG) boris_f64_kernel(const __grid_constant__ PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -591,7 +667,7 @@ __global__ void __maxnreg__(NREG) boris_f64_kernel(const PushK p)
         if constexpr (XING) {
             if (surv0 == 1) {
                 const double post[7] = {r, rdot, z, zdot, fi, fidot, rfph};
-                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf, p.dt);
             }
         }
     }
@@ -704,7 +780,7 @@ __device__ __forceinline__ void field_f32(const FieldK &f, double r, double fim,
 }
 
 template <int MAXO, bool XING>
-__global__ void __launch_bounds__(128) boris_f32_kernel(const PushK p)
+__global__ void __launch_bounds__(128) boris_f32_kernel(const __grid_constant__ PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -801,7 +877,7 @@ __global__ void __launch_bounds__(128) boris_f32_kernel(const PushK p)
                 double v[3];
                 vstate(r, v);
                 const double post[7] = {r, v[0], z, v[1], fi, v[2], rfph};
-                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+                xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf, p.dt);
             }
         }
     }
@@ -856,7 +932,7 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
 }
 
 template <int MAXO, bool SC, bool XING, bool HARM = false>
-__global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
+__global__ void __launch_bounds__(128) rk4_f64_kernel(const __grid_constant__ PushK p)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
@@ -886,7 +962,7 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
                 if (surv == 1) {
                     const double pre[7] = {y0.r, y0.vr, y0.z, y0.vz, y0.fi, y0.E, y0.rf};
                     const double post[7] = {y.r, y.vr, y.z, y.vz, y.fi, y.E, y.rf};
-                    xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+                    xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf, p.dt);
                 }
             }
             continue;
@@ -915,7 +991,7 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const PushK p)
         if constexpr (XING) {
             const double pre[7] = {y0.r, y0.vr, y0.z, y0.vz, y0.fi, y0.E, y0.rf};
             const double post[7] = {y.r, y.vr, y.z, y.vz, y.fi, y.E, y.rf};
-            xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf);
+            xing_check(p.xing, i, gs, pre, post, surv, inj, esr, esz, esf, p.dt);
         }
     }
     S.r[i] = y.r; S.vr[i] = y.vr; S.z[i] = y.z; S.vz[i] = y.vz; S.fi[i] = y.fi; S.f5[i] = y.E;
@@ -1031,7 +1107,7 @@ template <int MAXO, bool SC, bool F32>
 static void boris_default(const PushK &p, cudaStream_t s, int tb)
 {
     const unsigned g = (unsigned)((p.n + tb - 1) / tb);
-    const bool x = p.xing.buf != nullptr;
+    const bool x = xing_on(p);
     if (p.f.n_harm > 0) {
         if (x) boris_f64_kernel<MAXO, SC, true, F32, 80, true><<<g, tb, 0, s>>>(p);
         else boris_f64_kernel<MAXO, SC, false, F32, 80, true><<<g, tb, 0, s>>>(p);
@@ -1052,7 +1128,7 @@ static void rk4_launch(const PushK &p, cudaStream_t s)
 {
     const int tb = 128;
     const unsigned g = (unsigned)((p.n + tb - 1) / tb);
-    const bool x = p.xing.buf != nullptr;
+    const bool x = xing_on(p);
     if (p.f.n_harm > 0) {
         if (x) rk4_f64_kernel<MAXO, SC, true, true><<<g, tb, 0, s>>>(p);
         else rk4_f64_kernel<MAXO, SC, false, true><<<g, tb, 0, s>>>(p);
@@ -1097,7 +1173,7 @@ static void boris32_launch(const PushK &p, cudaStream_t s, int tb, int nreg_sel)
 {
     if constexpr (!SC) {
         if (nreg_sel != 0) {   // the caller has checked: no space charge, no harmonics
-            const bool x = p.xing.buf != nullptr;
+            const bool x = xing_on(p);
             switch (nreg_sel) {
             case 1: x ? boris32_shaped<MAXO, true, 72>(p, s, tb) : boris32_shaped<MAXO, false, 72>(p, s, tb); break;
             case 2: x ? boris32_shaped<MAXO, true, 64>(p, s, tb) : boris32_shaped<MAXO, false, 64>(p, s, tb); break;
@@ -1119,7 +1195,7 @@ template <int MAXO, bool SC>
 static void boris_f32_launch(const PushK &p, cudaStream_t s, int tb, int)
 {
     const unsigned g = (unsigned)((p.n + tb - 1) / tb);
-    if (p.xing.buf) boris_f32_kernel<MAXO, true><<<g, tb, 0, s>>>(p);
+    if (xing_on(p)) boris_f32_kernel<MAXO, true><<<g, tb, 0, s>>>(p);
     else boris_f32_kernel<MAXO, false><<<g, tb, 0, s>>>(p);
 }
 

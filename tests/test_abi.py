@@ -38,11 +38,11 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "ffa_cuda.h"
-int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d %d %d %d %d\n", sizeof(ffa_field_desc),
+int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %d %d %d %d %d %d\n", sizeof(ffa_field_desc),
  sizeof(ffa_rf_desc), sizeof(ffa_aperture), sizeof(ffa_consts), sizeof(ffa_state_soa), sizeof(ffa_step_table),
  sizeof(ffa_sc_desc), sizeof(ffa_sc_diag), sizeof(ffa_crossing), sizeof(ffa_mapgen_desc), sizeof(ffa_theta_track_desc),
  sizeof(ffa_mlp_train_desc), sizeof(ffa_mlp_infer_desc), sizeof(void*), FFA_CROSSING_RECORD, FFA_MLP_HIDDEN,
- FFA_MLP_PARAMS, FFA_MLP_WPACK_BYTES, FFA_MLP_SPLIT_WORK); return 0;}
+ FFA_MLP_PARAMS, FFA_MLP_WPACK_BYTES, FFA_MLP_SPLIT_WORK, FFA_FIT_SUMS); return 0;}
 '''
     d = tempfile.mkdtemp()
     with open(os.path.join(d, "s.c"), "w") as f:
@@ -55,7 +55,7 @@ int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %
                                      _lib.StepTable, _lib.SCDesc, _lib.SCDiag, _lib.Crossing,
                                      _lib.MapgenDesc, _lib.ThetaTrackDesc, _lib.MlpTrainDesc, _lib.MlpInferDesc)] + \
         [ctypes.sizeof(ctypes.c_void_p), _lib.CROSSING_RECORD, _lib.MLP_HIDDEN, _lib.MLP_PARAMS, _lib.MLP_WPACK_BYTES,
-                                               _lib.MLP_SPLIT_WORK]
+                                               _lib.MLP_SPLIT_WORK, _lib.FIT_SUMS]
     assert sizes == py
 
 

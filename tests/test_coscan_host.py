@@ -203,3 +203,40 @@ def test_fixed_shape_accumulation_equals_direct():
     assert torch.allclose(last2[:N], last1, rtol=1e-15, atol=0)
     # (turns - 1) pairs per particle in the normal equations' constant term
     assert S1[0, :, 2, 2].tolist() == [float((turns - 1) * c) for c in counts]
+
+
+def test_fit_sums_layout_unpacks_to_normal_equations():
+    """The per-instance sums in the layout the push kernel accumulates
+    (ffa_crossing.fit_sums: per plane f0 f0, f0 f1, f0, f1 f1, f1, 1, then
+    u'_0 f0, u'_0 f1, u'_0, u'_1 f0, u'_1 f1, u'_1; the crossing count last)
+    unpack to the S, Y and counts of accumulate_crossings for the same
+    crossings."""
+    from pyffa_b200 import _lib
+    rng = np.random.default_rng(9)
+    I, counts, turns = 3, [2, 5, 4], 7
+    inst = np.repeat(np.arange(I), counts)
+    N = len(inst)
+    u = rng.standard_normal((turns, N, 4))          # scaled crossing states, turn by turn
+    sums = np.zeros((I, _lib.FIT_SUMS))
+    for t in range(turns):
+        for p in range(N):
+            k = inst[p]
+            if t > 0:
+                for pl in (0, 1):
+                    f0, f1 = u[t - 1, p, 2 * pl], u[t - 1, p, 2 * pl + 1]
+                    a, b = u[t, p, 2 * pl], u[t, p, 2 * pl + 1]
+                    sums[k, 12 * pl:12 * pl + 12] += [f0 * f0, f0 * f1, f0, f1 * f1, f1, 1.0,
+                                                      a * f0, a * f1, a, b * f0, b * f1, b]
+            sums[k, 24] += 1.0
+    S, Y, c = coscan.unpack_fit_sums(sums)
+    f64 = dict(dtype=torch.float64)
+    S1, Y1, c1 = torch.zeros((2, I, 3, 3), **f64), torch.zeros((2, I, 2, 3), **f64), torch.zeros(I, **f64)
+    last, has = torch.zeros((N, 4), **f64), torch.zeros(N, dtype=torch.bool)
+    p = torch.as_tensor(np.tile(np.arange(N), turns))
+    step = torch.as_tensor(np.repeat(np.arange(turns), N) * 1000)
+    coscan.accumulate_crossings(p, step, torch.as_tensor(u.reshape(-1, 4)), torch.zeros((I, 4), **f64),
+                                torch.as_tensor(inst), 1000 * turns, last, has, S1, Y1, c1)
+    np.testing.assert_allclose(S, S1.numpy(), rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(Y, Y1.numpy(), rtol=1e-13, atol=1e-13)
+    np.testing.assert_array_equal(c, c1.numpy())
+    assert np.array_equal(S, S.transpose(0, 1, 3, 2))
