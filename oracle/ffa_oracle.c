@@ -511,6 +511,46 @@ double orc_track(int solver /*1 Boris, 0 RK4*/, double *mat, int64_t N, double t
     return t;
 }
 
+/* splitmix64 (Steele, Lea and Flood, OOPSLA 2014) as a hash */
+static uint64_t mix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+/* orc_track with rounding noise (test infrastructure): after every step the
+ * last bit of r, vr, z, vz, fi and f5 of every particle is flipped or kept,
+ * as a hash of (seed, step0 + step, particle, column) decides -- a model of
+ * a second float64 implementation whose roundings differ from this one's
+ * at every step.  How far the dynamics carries that noise over many steps
+ * is the scale against which two correct implementations are compared. */
+double orc_track_noisy(int solver, double *mat, int64_t N, double t_start, double dt, int64_t nsteps,
+                       int64_t *head, const orc_field *f, const orc_emap *em, const orc_aperture *ap,
+                       const orc_consts *cs, uint64_t seed, int64_t step0)
+{
+    double t = t_start;
+    for (int64_t s = 0; s < nsteps; ++s) {
+        orc_inject(mat, N, t, dt, head);
+        if (solver == 1) orc_boris_step(t, mat, N, dt, f, em, ap, cs);
+        else orc_rk4_step(t, mat, N, dt, f, em, cs);
+        t = t + dt;
+        const uint64_t key = mix64(seed ^ mix64((uint64_t)(step0 + s)));
+        for (int64_t i = 0; i < N; ++i) {
+            const uint64_t h = mix64(key ^ (uint64_t)i);
+            for (int c = 0; c < 6; ++c) {
+                double *x = mat + i * NCOL + c;
+                uint64_t u;
+                memcpy(&u, x, 8);
+                u ^= (h >> c) & 1ull;
+                memcpy(x, &u, 8);
+            }
+        }
+    }
+    return t;
+}
+
 /* FunctionForSEO (src/FFAG_track.py:1698-1740): d/dtheta of (r, pr, z, pz)
  * at fixed momentum P, mid-plane field and its z-linear terms. */
 static void seo_rhs(const orc_field *f, double t, const double *x, double P, double q, double *d)

@@ -86,6 +86,8 @@ def _bind(path):
     L.orc_track.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_void_p,
                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_track.restype = C.c_double
+    L.orc_track_noisy.argtypes = L.orc_track.argtypes + [C.c_uint64, C.c_int64]
+    L.orc_track_noisy.restype = C.c_double
     L.orc_inject.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.c_void_p]
     L.orc_theta_track.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_double,
                                   C.c_double, C.c_void_p, C.c_void_p, C.c_int]
@@ -228,14 +230,20 @@ def rk4_step(setup: Setup, mat, t, dt):
                        C.byref(setup.cs))
 
 
-def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0, fused=False):
+def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0, fused=False, noise=None):
     """Injection + push loop without space charge; returns (t_end, head).
-    fused: run the build with fused multiply-adds (lib_fma)."""
+    fused: run the build with fused multiply-adds (lib_fma).  noise: (seed,
+    first step) -- flip or keep the last bit of every state value after every
+    step (orc_track_noisy), a model of per-step rounding differences."""
     _mat(mat)
     h = C.c_int64(head)
-    t = (lib_fma() if fused else lib()).orc_track(1 if solver == "Boris" else 0, mat.ctypes.data, mat.shape[0], t_start, dt, nsteps,
-                        C.byref(h), C.byref(setup.field), C.byref(setup.emap), C.byref(setup.ap),
-                        C.byref(setup.cs))
+    L = lib_fma() if fused else lib()
+    args = (1 if solver == "Boris" else 0, mat.ctypes.data, mat.shape[0], t_start, dt, nsteps,
+            C.byref(h), C.byref(setup.field), C.byref(setup.emap), C.byref(setup.ap), C.byref(setup.cs))
+    if noise is None:
+        t = L.orc_track(*args)
+    else:
+        t = L.orc_track_noisy(*args, int(noise[0]), int(noise[1]))
     return t, h.value
 
 

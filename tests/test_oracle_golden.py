@@ -152,3 +152,22 @@ def test_space_charge_loop(golden, setup):
     for c in (10, 11, 12):
         d = np.abs(m[:, c] - ref[:, c]) / np.abs(ref[:, c]).max()
         assert np.quantile(d, 0.99) <= 5e-3 and d.max() <= 0.2, c
+
+
+def test_rounding_noise_run(golden, setup):
+    """orc_track_noisy (the rounding-sensitivity measure of the long GPU
+    parity tests): one step is the plain step with each of r, vr, z, vz, fi
+    and f5 at most one ulp away, flags and the other columns untouched; the
+    same seed and first step repeat exactly, another seed differs."""
+    ts, dt, _ = golden["borisloop_t"]
+    m0 = golden["borisloop_in"].copy()
+    plain, a, b, c = m0.copy(), m0.copy(), m0.copy(), m0.copy()
+    O.track(setup, "Boris", plain, ts, dt, 1)
+    O.track(setup, "Boris", a, ts, dt, 1, noise=(7, 0))
+    O.track(setup, "Boris", b, ts, dt, 1, noise=(7, 0))
+    O.track(setup, "Boris", c, ts, dt, 1, noise=(8, 0))
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    assert np.array_equal(a[:, 6:], plain[:, 6:])
+    d = a[:, :6] != plain[:, :6]
+    assert 0.3 < d.mean() < 0.7
+    assert np.array_equal(np.nextafter(plain[:, :6], a[:, :6])[d], a[:, :6][d])
