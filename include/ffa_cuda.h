@@ -98,7 +98,21 @@ typedef struct ffa_field_desc {
     const double *br_stack;
 } ffa_field_desc;
 
-/* Fixed RF gaps (src/FFAG_Field.py:167-306, src/FFAG_Utils.py:984-1036). */
+/* RF gaps.  Fixed rectangles (spiral_nodes == NULL; FFAG_EField_new,
+ * src/FFAG_Field.py:167-306, emap_kernel src/FFAG_Utils.py:984-1036): the
+ * last gap's rectangle decides (or every gap's, FFA_RF_PHYSICAL_SUM), field
+ * acc * (cos, sin)(theta_n - fi).
+ * Spiral gaps (spiral_nodes != NULL; FFAG_EField_spiral, src/FFAG_Field.py:
+ * 379-550, interpolate_spiral_emap_unique_gap_kernel src/FFAG_MathTools.py:
+ * 1042-1114): one (r, phi) map of Er, Ez / z and Ephi shared by the gaps,
+ * each gap placed at gap_azimuth[g].  For g = 0, 1, ... the local azimuth
+ * phi = d + k 2 pi, d = fi - gap_azimuth[g], k = rint((phi_c - d) / 2 pi),
+ * phi_c the middle of the phi axis; the first g with phi on the axis
+ * [phi0, phi0 + dphi (nphi - 1)] is the particle's gap (none: no field).
+ * Bilinear interpolation at (r, phi) with floor indices clamped to
+ * [0, n - 2] and weights from the unclamped offsets (linear extrapolation
+ * outside the r axis), field acc * (Er, Ez/z * z, Ephi) * sin(RF phase +
+ * rf_shift[g]).  physical_sum does not apply (one gap per point). */
 typedef struct ffa_rf_desc {
     int32_t enable;               /* Emap EnableFlag */
     int32_t ngaps;                /* 1..FFA_MAX_GAPS */
@@ -108,6 +122,12 @@ typedef struct ffa_rf_desc {
     double box[FFA_MAX_GAPS][4];  /* x_min, x_max, y_min, y_max */
     double theta_n[FFA_MAX_GAPS]; /* gap azimuth + pi/2 */
     double rf_shift[FFA_MAX_GAPS];
+    /* spiral gaps */
+    const double *spiral_nodes;   /* device, nr * nphi nodes of 4 doubles (Er, Ez/z, Ephi, 0), phi fastest */
+    int32_t spiral_nr, spiral_nphi;   /* >= 2 each */
+    double spiral_r0, spiral_dr;      /* r axis [m] */
+    double spiral_phi0, spiral_dphi;  /* phi axis [rad], relative to the gap azimuth */
+    double gap_azimuth[FFA_MAX_GAPS]; /* rad */
 } ffa_rf_desc;
 
 typedef struct ffa_aperture {

@@ -75,6 +75,12 @@ typedef struct {
     int64_t fc_n;
     const double *fc_freq;
     const double *fc_volt;
+    /* spiral gaps (FFAG_EField_spiral, src/FFAG_Field.py:379-550); er_map
+     * NULL: fixed gaps.  Maps (nr, nphi), row-major. */
+    const double *er_map, *ezc_map, *ephi_map;
+    int64_t nr, nphi;
+    double r0, dr, phi0, dphi;
+    double gap_az[MAXG];
 } orc_emap;
 
 typedef struct {
@@ -219,17 +225,85 @@ static int gap_field(const orc_emap *em, int g, double acc_Etot, double r, doubl
     return 1;
 }
 
+/* Spiral gaps: interpolate_spiral_emap_unique_gap_kernel (src/FFAG_MathTools.py:
+ * 1042-1114) for one point -- the first gap whose shifted azimuth
+ * (shift_to_nearest_window, :1118-1135) lies on the map's phi axis, then
+ * Bilinear_interp_2D_vect_uniform_3fields (:940-1039) with rf_amp = V0 /
+ * gap_width.  Returns the gap (-1: none, and no field). */
+int orc_spiral_lookup(const orc_emap *em, double rf_amp, double r, double fi, double z, double *Er, double *Ez,
+                      double *Efi)
+{
+    const double twopi = 2.0 * M_PI;
+    const double phi_min = em->phi0;
+    const double phi_max = em->phi0 + em->dphi * (double)(em->nphi - 1);
+    const double phi_center = 0.5 * (phi_min + phi_max);
+    int hit = -1;
+    double phl = 0.0;
+    *Er = 0.0;
+    *Ez = 0.0;
+    *Efi = 0.0;
+    for (int g = 0; g < em->ngaps; ++g) {
+        double phi = fi - em->gap_az[g];
+        double k = nearbyint((phi_center - phi) / twopi);
+        double local = phi + k * twopi;
+        if (local >= phi_min && local <= phi_max) {
+            hit = g;
+            phl = local;
+            break;
+        }
+    }
+    if (hit < 0) return -1;
+    int64_t i = (int64_t)floor((r - em->r0) / em->dr);
+    int64_t j = (int64_t)floor((phl - em->phi0) / em->dphi);
+    if (i < 0) i = 0;
+    else if (i >= em->nr - 1) i = em->nr - 2;
+    if (j < 0) j = 0;
+    else if (j >= em->nphi - 1) j = em->nphi - 2;
+    double xx0 = em->r0 + (double)i * em->dr;
+    double yy0 = em->phi0 + (double)j * em->dphi;
+    double tx = (r - xx0) / em->dr;
+    double ty = (phl - yy0) / em->dphi;
+    double w00 = (1.0 - tx) * (1.0 - ty), w01 = (1.0 - tx) * ty, w10 = tx * (1.0 - ty), w11 = tx * ty;
+    const int64_t a = i * em->nphi + j, b = a + em->nphi;
+    double er = w00 * em->er_map[a] + w01 * em->er_map[a + 1] + w10 * em->er_map[b] + w11 * em->er_map[b + 1];
+    double ez = w00 * em->ezc_map[a] + w01 * em->ezc_map[a + 1] + w10 * em->ezc_map[b] + w11 * em->ezc_map[b + 1];
+    double ef = w00 * em->ephi_map[a] + w01 * em->ephi_map[a + 1] + w10 * em->ephi_map[b] +
+                w11 * em->ephi_map[b + 1];
+    *Er = rf_amp * er;
+    *Ez = rf_amp * ez * z;
+    *Efi = rf_amp * ef;
+    return hit;
+}
+
+/* The spiral field times the RF factor of cylindrical_to_cartesian
+ * (src/FFAG_MathTools.py:1984) with the hit gap's rf_shift. */
+static void spiral_field(const orc_emap *em, double rf_amp, double r, double fi, double z, double rf_phase,
+                         double *Er, double *Ez, double *Efi)
+{
+    int hit = orc_spiral_lookup(em, rf_amp, r, fi, z, Er, Ez, Efi);
+    if (hit < 0) return;
+    double s = sin(rf_phase + em->rf_shift[hit]);
+    *Er = *Er * s;
+    *Ez = *Ez * s;
+    *Efi = *Efi * s;
+}
+
 /* Interpolation2D_EMap (src/FFAG_Field.py:284-306) followed by the RF factor of
  * cylindrical_to_cartesian / RK4_equations_of_motion_njit:
  *   E_cyl = E_gap * sin(RF_phase + rf_shift[gap]).
  * Reference semantics: each gap's call overwrites E, so only the last gap's
  * field survives (E = 0 outside the last gap).  physical_sum adds every gap. */
-static void rf_field(const orc_emap *em, double acc_Etot, double r, double fi, double rf_phase,
-                     double *Er, double *Efi)
+static void rf_field(const orc_emap *em, double acc_Etot, double r, double fi, double z, double rf_phase,
+                     double *Er, double *Ez, double *Efi)
 {
     *Er = 0.0;
+    *Ez = 0.0;
     *Efi = 0.0;
     if (!em->enable) return;
+    if (em->er_map) {
+        spiral_field(em, acc_Etot, r, fi, z, rf_phase, Er, Ez, Efi);
+        return;
+    }
     if (!em->physical_sum) {
         int g = em->ngaps - 1;
         double er = 0.0, ef = 0.0;
@@ -284,9 +358,8 @@ void orc_boris_step(double t, double *mat, int64_t N, double dt,
             if (f->max_order >= 1) high_order_B(f, r, fi_mod, z, &Bz, &Bfi, &Br);
         }
         if (f->n_harm > 0) Bz += harmonics_Bz(f, r, fi);   /* src/FFAG_track.py:1007 */
-        double Er = 0.0, Efi = 0.0;
-        rf_field(em, acc_Etot, r, fi, row[9], &Er, &Efi);
-        double Ez = 0.0;
+        double Er = 0.0, Ez = 0.0, Efi = 0.0;
+        rf_field(em, acc_Etot, r, fi, z, row[9], &Er, &Ez, &Efi);
         Ez += row[11];
         Er += row[10];
         Efi += row[12];
@@ -383,9 +456,8 @@ static void rk4_rhs_row(const double *row, double dRF_rate, double acc_Etot,
     analytic_B(f, r, fi_mod, z, &Bz, &Br, &Bfi);
     if (f->max_order >= 1) high_order_B(f, r, fi_mod, z, &Bz, &Bfi, &Br);
     if (f->n_harm > 0) Bz += harmonics_Bz(f, r, fi);       /* src/FFAG_track.py:1782 */
-    double Er = 0.0, Efi = 0.0;
-    rf_field(em, acc_Etot, r, fi, row[9], &Er, &Efi);
-    double Ez = 0.0;
+    double Er = 0.0, Ez = 0.0, Efi = 0.0;
+    rf_field(em, acc_Etot, r, fi, z, row[9], &Er, &Ez, &Efi);
     Ez += row[11];
     Er += row[10];
     Efi += row[12];

@@ -48,7 +48,10 @@ class OrcEmap(C.Structure):
                 ("box", (C.c_double * 4) * MAXG), ("theta_n", C.c_double * MAXG),
                 ("rf_shift", C.c_double * MAXG), ("acc_Etot_uniform", C.c_double),
                 ("fc_x0", C.c_double), ("fc_dx", C.c_double), ("fc_n", C.c_int64),
-                ("fc_freq", C.c_void_p), ("fc_volt", C.c_void_p)]
+                ("fc_freq", C.c_void_p), ("fc_volt", C.c_void_p),
+                ("er_map", C.c_void_p), ("ezc_map", C.c_void_p), ("ephi_map", C.c_void_p),
+                ("nr", C.c_int64), ("nphi", C.c_int64), ("r0", C.c_double), ("dr", C.c_double),
+                ("phi0", C.c_double), ("dphi", C.c_double), ("gap_az", C.c_double * MAXG)]
 
 
 class OrcAperture(C.Structure):
@@ -94,6 +97,9 @@ def _bind(path):
     L.orc_sc_step.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.orc_sc_step.restype = C.c_int
+    L.orc_spiral_lookup.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
+    L.orc_spiral_lookup.restype = C.c_int
     L.orc_num_threads.restype = C.c_int
     L.orc_set_num_threads.argtypes = [C.c_int]
     return L
@@ -165,7 +171,8 @@ class ThetaTracker:
 
 class Setup:
     """Oracle parameter blocks built from the product's host-side objects
-    (FFAG_Bfield_analytical, FFAG_EField_new, FFAG_GlobalParameters)."""
+    (FFAG_Bfield_analytical, FFAG_EField_new or FFAG_EField_spiral,
+    FFAG_GlobalParameters)."""
 
     def __init__(self, bmap, emap, gp):
         self._keep = []
@@ -185,13 +192,23 @@ class Setup:
         e.enable = 1 if emap.EnableFlag else 0
         e.ngaps = len(emap.gap_azimuths)
         e.physical_sum = 1 if getattr(emap, "physical_sum", False) else 0
-        for g, (region, theta, box) in enumerate(zip(emap.acc_regions, emap.gap_azimuths, emap.box_bounds)):
-            for j in range(4):
-                e.poly_x[g][j] = float(region[j, 0])
-                e.poly_y[g][j] = float(region[j, 1])
-                e.box[g][j] = float(box[j])
-            e.theta_n[g] = float(theta + np.pi / 2.0)
-            e.rf_shift[g] = float(emap.rf_shift[g]) if g < len(emap.rf_shift) else 0.0
+        if getattr(emap, "GapType", "fixed") == "spiral":
+            maps = [np.ascontiguousarray(m, dtype=np.float64) for m in (emap.Er_map, emap.Ezcoef_map, emap.Ephi_map)]
+            self._keep += maps
+            e.er_map, e.ezc_map, e.ephi_map = (m.ctypes.data for m in maps)
+            e.nr, e.nphi = int(emap.nr), int(emap.nphi)
+            e.r0, e.dr, e.phi0, e.dphi = float(emap.r0), float(emap.dr), float(emap.phi0), float(emap.dphi)
+            for g, az in enumerate(emap.gap_azimuths):
+                e.gap_az[g] = float(az)
+                e.rf_shift[g] = float(emap.rf_shift[g]) if g < len(emap.rf_shift) else 0.0
+        else:
+            for g, (region, theta, box) in enumerate(zip(emap.acc_regions, emap.gap_azimuths, emap.box_bounds)):
+                for j in range(4):
+                    e.poly_x[g][j] = float(region[j, 0])
+                    e.poly_y[g][j] = float(region[j, 1])
+                    e.box[g][j] = float(box[j])
+                e.theta_n[g] = float(theta + np.pi / 2.0)
+                e.rf_shift[g] = float(emap.rf_shift[g]) if g < len(emap.rf_shift) else 0.0
         e.acc_Etot_uniform = float(emap.acc_Etot_uniform)
         fc = emap.freq_curve
         e.fc_x0 = float(fc[0, 0])
@@ -245,6 +262,21 @@ def track(setup: Setup, solver, mat, t_start, dt, nsteps, head=0, fused=False, n
     else:
         t = L.orc_track_noisy(*args, int(noise[0]), int(noise[1]))
     return t, h.value
+
+
+def spiral_lookup(setup: Setup, rf_amp, r, fi, z):
+    """Spiral-gap field without the RF factor at points (r, fi, z): Er, Ez,
+    Efi and the hit gap (-1: none), as the reference's Interpolation2D_EMap
+    of FFAG_EField_spiral returns them (orc_spiral_lookup)."""
+    r, fi, z = (np.asarray(x, np.float64).ravel() for x in (r, fi, z))
+    out = np.zeros((len(r), 3))
+    hit = np.zeros(len(r), np.int32)
+    er, ez, ef = C.c_double(), C.c_double(), C.c_double()
+    for k in range(len(r)):
+        hit[k] = lib().orc_spiral_lookup(C.byref(setup.emap), float(rf_amp), r[k], fi[k], z[k], C.byref(er),
+                                         C.byref(ez), C.byref(ef))
+        out[k] = er.value, ez.value, ef.value
+    return out[:, 0], out[:, 1], out[:, 2], hit
 
 
 def detect_azimuth_crossing(pre_fi, post_fi, survive, target):

@@ -65,6 +65,9 @@ class RFDesc(C.Structure):
         ("poly_x", (C.c_double * 4) * MAX_GAPS), ("poly_y", (C.c_double * 4) * MAX_GAPS),
         ("box", (C.c_double * 4) * MAX_GAPS),
         ("theta_n", C.c_double * MAX_GAPS), ("rf_shift", C.c_double * MAX_GAPS),
+        ("spiral_nodes", d_p), ("spiral_nr", C.c_int32), ("spiral_nphi", C.c_int32),
+        ("spiral_r0", C.c_double), ("spiral_dr", C.c_double), ("spiral_phi0", C.c_double),
+        ("spiral_dphi", C.c_double), ("gap_azimuth", C.c_double * MAX_GAPS),
     ]
 
 

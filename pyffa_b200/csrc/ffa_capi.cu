@@ -282,6 +282,10 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
     if (!fm || !rf || !ap || !cs || !tab || !state_ok(st) || n < 0 || nsteps < 0 || step0 < 0) return FFA_ERR_INVALID;
     if (!tab->drf || !tab->acc || step0 + nsteps > tab->nsteps) return FFA_ERR_INVALID;
     if (rf->ngaps < 1 || rf->ngaps > FFA_MAX_GAPS) return FFA_ERR_INVALID;
+    if (rf->spiral_nodes &&
+        (rf->spiral_nr < 2 || rf->spiral_nphi < 2 || !(rf->spiral_dr > 0.0) || !(rf->spiral_dphi > 0.0) ||
+         (int64_t)rf->spiral_nr * rf->spiral_nphi >= ((int64_t)1 << 31)))
+        return FFA_ERR_INVALID;
     if (sc_step < 0) return FFA_ERR_INVALID;
     if (sc_step > 0 && st->sc_pre &&
         (!st->sc_pp || !st->e_pre_r || !st->e_pre_z || !st->e_pre_fi || !st->e_pp_r || !st->e_pp_z || !st->e_pp_fi))
@@ -322,6 +326,20 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
         }
         p.rf.win_center[g] = c0;
         p.rf.win_half[g] = half < 1.0 ? half + 1e-9 : 4.0;  // wide gaps: no shortcut
+    }
+    if (rf->spiral_nodes) {
+        p.rf.sp = rf->spiral_nodes;
+        p.rf.sp_nr = rf->spiral_nr;
+        p.rf.sp_nphi = rf->spiral_nphi;
+        p.rf.sp_r0 = rf->spiral_r0;
+        p.rf.sp_dr = rf->spiral_dr;
+        p.rf.sp_phi0 = rf->spiral_phi0;
+        p.rf.sp_dphi = rf->spiral_dphi;
+        // phi_max and the window centre as shift_to_nearest_window forms them
+        // (src/FFAG_MathTools.py:1072-1073, 1131)
+        p.rf.sp_phimax = rf->spiral_phi0 + rf->spiral_dphi * (double)(rf->spiral_nphi - 1);
+        p.rf.sp_phic = 0.5 * (rf->spiral_phi0 + p.rf.sp_phimax);
+        memcpy(p.rf.gap_az, rf->gap_azimuth, sizeof(p.rf.gap_az));
     }
     p.ap = *ap;
     p.cs = *cs;

@@ -70,6 +70,12 @@ struct RFK {
     // test (win_half = pi disables the shortcut).
     double win_center[FFA_MAX_GAPS];
     double win_half[FFA_MAX_GAPS];
+    // spiral gaps (sp != NULL): the shared (r, phi) map, its axes, the
+    // middle and end of the phi axis, and each gap's azimuth
+    const double *sp;
+    int32_t sp_nr, sp_nphi;
+    double sp_r0, sp_dr, sp_phi0, sp_dphi, sp_phimax, sp_phic;
+    double gap_az[FFA_MAX_GAPS];
 };
 
 struct PushK {

@@ -221,15 +221,68 @@ __device__ __forceinline__ bool in_window(const RFK &rf, int g, double fi)
     return fabs(d) <= rf.win_half[g];
 }
 
-// RF field (cylindrical r, fi components) times sin(RF phase + rf_shift[gap]).
-// Reference semantics: every gap's emap_kernel call overwrites the field, so
-// only the last gap contributes; physical_sum adds all gaps.
-__device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double r, double fi, double rfph,
-                                           double &Er, double &Efi)
+// Spiral gaps (interpolate_spiral_emap_unique_gap_kernel, src/FFAG_MathTools.py:
+// 1042-1114, with shift_to_nearest_window :1118-1135 and
+// Bilinear_interp_2D_vect_uniform_3fields :940-1039): the first gap whose
+// window holds the particle, the bilinear map value, the RF factor.  The
+// roundings are the reference's, one operation at a time (no contraction).
+__device__ __forceinline__ double3 rf_spiral64(const RFK &rf, double acc, double r, double fi, double z, double rfph)
+{
+    const double tw = 2.0 * PI;
+    int hit = -1;
+    double phl = 0.0;
+    for (int g = 0; g < rf.ngaps; ++g) {
+        const double d = fi - rf.gap_az[g];
+        const double k = rint((rf.sp_phic - d) / tw);
+        const double l = __dadd_rn(d, __dmul_rn(k, tw));
+        if (l >= rf.sp_phi0 && l <= rf.sp_phimax) {
+            hit = g;
+            phl = l;
+            break;
+        }
+    }
+    if (hit < 0) return make_double3(0.0, 0.0, 0.0);
+    int i = (int)floor((r - rf.sp_r0) / rf.sp_dr);
+    int j = (int)floor((phl - rf.sp_phi0) / rf.sp_dphi);
+    i = i < 0 ? 0 : (i >= rf.sp_nr - 1 ? rf.sp_nr - 2 : i);
+    j = j < 0 ? 0 : (j >= rf.sp_nphi - 1 ? rf.sp_nphi - 2 : j);
+    const double tx = (r - __dadd_rn(rf.sp_r0, __dmul_rn((double)i, rf.sp_dr))) / rf.sp_dr;
+    const double ty = (phl - __dadd_rn(rf.sp_phi0, __dmul_rn((double)j, rf.sp_dphi))) / rf.sp_dphi;
+    const double w00 = (1.0 - tx) * (1.0 - ty), w01 = (1.0 - tx) * ty, w10 = tx * (1.0 - ty), w11 = tx * ty;
+    // node (i, j): Er, Ez/z as one 16-byte load, Ephi in the next
+    const double2 *nd = reinterpret_cast<const double2 *>(rf.sp);
+    const int64_t b0 = 2 * ((int64_t)i * rf.sp_nphi + j), b1 = b0 + 2 * (int64_t)rf.sp_nphi;
+    const double2 a00 = __ldg(nd + b0), a01 = __ldg(nd + b0 + 2), a10 = __ldg(nd + b1), a11 = __ldg(nd + b1 + 2);
+    const double f00 = __ldg(rf.sp + 2 * b0 + 2), f01 = __ldg(rf.sp + 2 * b0 + 6);
+    const double f10 = __ldg(rf.sp + 2 * b1 + 2), f11 = __ldg(rf.sp + 2 * b1 + 6);
+    const double er = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(w00, a00.x), __dmul_rn(w01, a01.x)),
+                                          __dmul_rn(w10, a10.x)), __dmul_rn(w11, a11.x));
+    const double ez = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(w00, a00.y), __dmul_rn(w01, a01.y)),
+                                          __dmul_rn(w10, a10.y)), __dmul_rn(w11, a11.y));
+    const double ef = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(w00, f00), __dmul_rn(w01, f01)),
+                                          __dmul_rn(w10, f10)), __dmul_rn(w11, f11));
+    const double s = sin(rfph + rf.rf_shift[hit]);
+    return make_double3((acc * er) * s, ((acc * ez) * z) * s, (acc * ef) * s);   // Er, Ez, Efi
+}
+
+// RF field (cylindrical r, z, fi components) times sin(RF phase +
+// rf_shift[gap]).  Fixed gaps, reference semantics: every gap's emap_kernel
+// call overwrites the field, so only the last gap contributes (no Ez);
+// physical_sum adds all gaps.  Spiral gaps: rf_spiral64.
+__device__ __forceinline__ void rf_field64(const RFK &rf, double acc, double r, double fi, double z, double rfph,
+                                           double &Er, double &Ez, double &Efi)
 {
     Er = 0.0;
+    Ez = 0.0;
     Efi = 0.0;
     if (!rf.enable) return;
+    if (rf.sp) {
+        const double3 e = rf_spiral64(rf, acc, r, fi, z, rfph);
+        Er = e.x;
+        Ez = e.y;
+        Efi = e.z;
+        return;
+    }
     const int g0 = rf.physical_sum ? 0 : rf.ngaps - 1;
     for (int g = g0; g < rf.ngaps; ++g) {
         if (!in_window(rf, g, fi)) continue;
@@ -598,9 +651,8 @@ __global__ void __maxnreg__(NREG) boris_f64_kernel(const __grid_constant__ PushK
                 Br += hr;
             }
             if constexpr (HARM) Bz += harmonics_bz(f.harm, f.n_harm, r, fi);
-            double Er, Efi;
-            rf_field64(p.rf, acc, r, fi, rfph, Er, Efi);
-            double Ez = 0.0;
+            double Er, Ez, Efi;
+            rf_field64(p.rf, acc, r, fi, z, rfph, Er, Ez, Efi);
             Ez += esz;
             Er += esr;
             Efi += esf;
@@ -828,9 +880,9 @@ __global__ void __launch_bounds__(128) boris_f32_kernel(const __grid_constant__ 
             const double fim = fi - f.period * floor(fi * f.inv_period);
             float Bz, Br, Bfi;
             field_f32<MAXO>(f, r, fim, (float)z, Bz, Br, Bfi, oob);
-            double Erd, Efid;
-            rf_field64(p.rf, acc, r, fi, rfph, Erd, Efid);
-            const float Er = (float)Erd + esrf, Efi = (float)Efid + esff, Ez = eszf;
+            double Erd, Ezd, Efid;
+            rf_field64(p.rf, acc, r, fi, z, rfph, Erd, Ezd, Efid);
+            const float Er = (float)Erd + esrf, Efi = (float)Efid + esff, Ez = (float)Ezd + eszf;
             if (p.ap.enable && (r > p.ap.rmax || r < p.ap.rmin || z > p.ap.zmax || z < p.ap.zmin)) {
                 surv = 0;
                 ++lost;
@@ -909,9 +961,8 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     analytic_b64(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi);
     if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
     if constexpr (HARM) Bz += harmonics_bz(f.harm, f.n_harm, y.r, y.fi);
-    double Er, Efi;
-    rf_field64(p.rf, acc, y.r, y.fi, y.rf, Er, Efi);
-    double Ez = 0.0;
+    double Er, Ez, Efi;
+    rf_field64(p.rf, acc, y.r, y.fi, y.z, y.rf, Er, Ez, Efi);
     Ez += esz;
     Er += esr;
     Efi += esf;

@@ -340,7 +340,9 @@ class FFAG_EField_new:
         zi = Z[i] + (xi - x0) / (x1 - x0) * (Z[i + 1] - Z[i])
         return yi, zi
 
-    def rf_desc(self) -> "_lib.RFDesc":
+    def rf_desc(self, device=None) -> "_lib.RFDesc":
+        """The push kernels' description of the gaps (device: unused, the
+        fixed gaps need no device table)."""
         d = _lib.RFDesc()
         d.enable = 1 if self.EnableFlag else 0
         d.ngaps = len(self.gap_azimuths)
@@ -352,6 +354,97 @@ class FFAG_EField_new:
                 d.box[g][j] = float(box[j])
             d.theta_n[g] = float(theta + np.pi / 2.0)
             d.rf_shift[g] = float(self.rf_shift[g] if g < len(self.rf_shift) else 0.0)
+        return d
+
+
+def load_spiral_map(path):
+    """A spiral E-map file: first row the phi axis (from column 1), first
+    column the r axis (from row 1), the rest the (nr, nphi) values
+    (FFAG_EField_spiral.LoadSpiralMap, src/FFAG_Field.py:458-463)."""
+    raw = np.loadtxt(path)
+    return raw[1:, 1:].astype(np.float64), raw[1:, 0].astype(np.float64), raw[0, 1:].astype(np.float64)
+
+
+class FFAG_EField_spiral:
+    """Spiral RF gaps (src/FFAG_Field.py:379-550): one (r, phi) map of Er,
+    Ez / z and Ephi, placed at every gap azimuth, driven by the frequency /
+    voltage curve.  The push kernels evaluate it (interpolate_spiral_emap_
+    unique_gap_kernel, src/FFAG_MathTools.py:1042-1114: the first gap whose
+    window holds the particle, bilinear in (r, phi), E = V0 / gap_width *
+    map * sin(RF phase + rf_shift)); the map goes to the device with the
+    first rf_desc on a device.  Ek_gap / r_gap / phi_gap tables give the gap
+    crossing of the closed orbit per energy (r_gap_interp,
+    phi_gap_interp_unwrapped: linear interpolation, as np.interp)."""
+
+    GapType = "spiral"
+
+    def __init__(self, freq_curve_path=None, EnableFlag=True, header=None, data=None):
+        if header is None:
+            header, data = parse_emap_file(freq_curve_path)
+        self.header = header
+        self.acc_phi0 = np.deg2rad(float(header["acc_phi_paint"]))
+        self.gap_azimuths = np.deg2rad(np.atleast_1d(header["gap_azimuth"]).astype(np.float64))
+        if len(self.gap_azimuths) > _lib.MAX_GAPS:
+            raise ValueError(f"at most {_lib.MAX_GAPS} RF gaps are supported")
+        self.gap_width = float(header["gap_width"])
+        self.freq_curve = np.asarray(data, dtype=np.float64)
+        self.harmonic = int(header["harmonic"])
+        self.EnableFlag = EnableFlag
+        self.rf_shift = np.deg2rad(np.atleast_1d(header["rf_shift"]).astype(np.float64))
+        folder = os.path.dirname(os.path.abspath(freq_curve_path)) if freq_curve_path else "."
+        self.Er_map, self.r_axis, self.phi_axis = load_spiral_map(
+            os.path.join(folder, header.get("Er_map_file", "Er_coef.txt")))
+        self.Ezcoef_map = load_spiral_map(os.path.join(folder, header.get("Ez_map_file", "Ez_coef.txt")))[0]
+        self.Ephi_map = load_spiral_map(os.path.join(folder, header.get("Ephi_map_file", "Ephi_coef.txt")))[0]
+        if not (self.Er_map.shape == self.Ezcoef_map.shape == self.Ephi_map.shape):
+            raise ValueError("the three spiral maps differ in shape")
+        self.r0, self.dr, self.nr = self.r_axis[0], self.r_axis[1] - self.r_axis[0], len(self.r_axis)
+        self.phi0, self.dphi, self.nphi = self.phi_axis[0], self.phi_axis[1] - self.phi_axis[0], len(self.phi_axis)
+        self.map_rmin, self.map_rmax = self.r_axis[0], self.r_axis[-1]
+        self.map_phimin, self.map_phimax = self.phi_axis[0], self.phi_axis[-1]
+        self.acc_Etot_uniform = 1.0 / self.gap_width
+        order = np.argsort(np.atleast_1d(header["Ek_gap"]).astype(np.float64))
+        self.Ek_gap = np.atleast_1d(header["Ek_gap"]).astype(np.float64)[order]
+        self.r_gap = np.atleast_1d(header["r_gap"]).astype(np.float64)[order]
+        self.phi_gap = np.deg2rad(np.atleast_1d(header["phi_gap_deg"]).astype(np.float64))[order]
+        self.phi_gap_unwrapped = np.deg2rad(np.atleast_1d(header["phi_gap_unwrapped_deg"]).astype(np.float64))[order]
+        self.physical_sum = False
+        self._nodes = {}
+
+    def r_gap_interp(self, Ek):
+        return np.interp(np.asarray(Ek, np.float64), self.Ek_gap, self.r_gap)
+
+    def phi_gap_interp_unwrapped(self, Ek):
+        return np.interp(np.asarray(Ek, np.float64), self.Ek_gap, self.phi_gap_unwrapped)
+
+    Interpolation1D_freq_curve = FFAG_EField_new.Interpolation1D_freq_curve
+
+    def device_nodes(self, device):
+        """The (nr, nphi, 4) float64 node table on `device`: Er, Ez / z,
+        Ephi, 0 per node (kept for the object's lifetime)."""
+        import torch
+        key = str(torch.device(device))
+        if key not in self._nodes:
+            t = np.stack([self.Er_map, self.Ezcoef_map, self.Ephi_map, np.zeros_like(self.Er_map)], axis=-1)
+            self._nodes[key] = torch.as_tensor(np.ascontiguousarray(t), device=device)
+        return self._nodes[key]
+
+    def rf_desc(self, device=None) -> "_lib.RFDesc":
+        """The push kernels' description of the gaps, with the node table
+        on `device` (default: the current CUDA device)."""
+        import torch
+        if device is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        d = _lib.RFDesc()
+        d.enable = 1 if self.EnableFlag else 0
+        d.ngaps = len(self.gap_azimuths)
+        for g, az in enumerate(self.gap_azimuths):
+            d.gap_azimuth[g] = float(az)
+            d.rf_shift[g] = float(self.rf_shift[g] if g < len(self.rf_shift) else 0.0)
+        d.spiral_nodes = self.device_nodes(device).data_ptr()
+        d.spiral_nr, d.spiral_nphi = int(self.nr), int(self.nphi)
+        d.spiral_r0, d.spiral_dr = float(self.r0), float(self.dr)
+        d.spiral_phi0, d.spiral_dphi = float(self.phi0), float(self.dphi)
         return d
 
 

@@ -9,9 +9,9 @@ pyffa_b200.track.  ``Tracker.from_json(path, restart=None).run()`` is the same
 as an object.
 
 Differences from the reference driver: the bunch generator is seeded
-(``BunchPara.Seed``, default 0); the 'match' longitudinal distribution and
-spiral RF gaps (FFAG_EField_spiral) are rejected; there is no MPI split (one process tracks the whole bunch; see bunch.divide_variables
-for the reference's split).
+(``BunchPara.Seed``, default 0); the 'match' longitudinal distribution is
+rejected; there is no MPI split (one process tracks the whole bunch; see
+bunch.divide_variables for the reference's split).
 """
 from __future__ import annotations
 
@@ -24,7 +24,8 @@ from .bunch import FFAG_Bunch
 from .constants import COLUMNS, FFAG_ConversionTools, FFAG_GlobalParameters
 from .distribution import GenerateBunches
 from .dump import Dumps, PositionDump, PositionDumpBunch, StepDump, StepDumpBunch
-from .fields import FFAG_Bfield_analytical, FFAG_BField_Error, FFAG_EField_new, parse_emap_file
+from .fields import (FFAG_Bfield_analytical, FFAG_BField_Error, FFAG_EField_new, FFAG_EField_spiral,
+                     parse_emap_file)
 from .seo import LoadSEOParams
 from .track import FFAG_RungeKutta
 
@@ -40,11 +41,16 @@ def wrap_0_2pi(x):
 
 def calc_injection_rf_phase(EMap, Azimuth_start, t_start, T0, Ek_inj, gap_idx=0):
     """RF phase of the bunch at t_start such that the gap is crossed at the
-    accelerating phase (examples/main_track.py:26-45, fixed gaps)."""
+    accelerating phase (examples/main_track.py:26-45): the gap azimuth, for
+    spiral gaps where the closed orbit of the injection energy meets gap 0,
+    shifted by the gap's offset from gap 0."""
     phi_start = wrap_0_2pi(Azimuth_start)
-    if EMap.GapType != "fixed":
-        raise NotImplementedError("only fixed RF gaps are supported")
-    phi_gap = EMap.gap_azimuths[gap_idx]
+    if EMap.GapType == "fixed":
+        phi_gap = EMap.gap_azimuths[gap_idx]
+    elif EMap.GapType == "spiral":
+        phi_gap = EMap.phi_gap_interp_unwrapped(Ek_inj) + (EMap.gap_azimuths[gap_idx] - EMap.gap_azimuths[0])
+    else:
+        raise ValueError("EMap.type must be 'fixed' or 'spiral'")
     dphi_orbit = phi_gap - phi_start
     return EMap.acc_phi0 - EMap.harmonic * dphi_orbit - EMap.harmonic * 2.0 * np.pi * (0.0 - t_start) / T0
 
@@ -132,9 +138,13 @@ class Tracker:
         gp = FFAG_GlobalParameters()
         gp.AddBMap(FFAG_Bfield_analytical(os.path.join(bmap_path, "config_Bmap.json"), max_order))
         header, _ = parse_emap_file(emap_path)
-        if str(header.get("gap_model", "fixed")).strip().lower() != "fixed":
-            raise NotImplementedError("spiral RF gaps are not supported")
-        emap = FFAG_EField_new(emap_path, cfg["Emap"]["enable"])
+        gap_type = str(header.get("gap_model", "fixed")).strip().lower()
+        if gap_type == "fixed":
+            emap = FFAG_EField_new(emap_path, cfg["Emap"]["enable"])
+        elif gap_type == "spiral":
+            emap = FFAG_EField_spiral(emap_path, cfg["Emap"]["enable"])
+        else:
+            raise ValueError(f"Unknown Emap gap type: {gap_type!r}")
         gp.AddEMap(emap)
         gp.AddSEOInfo(SEO_info)
         seo_cfg = os.path.join(seo_dir, "config_SEO.json")

@@ -201,6 +201,75 @@ def emap_file(path: str, gap_azimuth_deg=(3.75, 183.75), rf_shift_deg=(0.0, 0.0)
     return path
 
 
+def spiral_emap_folder(folder: str, alpha_deg=40.0, r_ref=8.5, s_ref_deg=0.0, r_axis=(7.9, 9.3, 141),
+                       pad_deg=1.0, nphi=241, sigma=0.03, gap_azimuth_deg=(3.75, 183.75), rf_shift_deg=(0.0, 0.0),
+                       voltage=100e3, gap_width=0.2, harmonic=1, acc_phi_deg=30.0, Ek_ramp=(300.0, 310.0),
+                       ramp_turns=1000, t_start=-200e-9, npts=2001, lattice=LATTICE) -> str:
+    """A spiral RF gap in the reference's file layout (FFAG_EField_spiral,
+    src/FFAG_Field.py:379-463; written as examples/main_Emap.py:752-800,
+    960-980 write theirs): emap.txt (header with gap_model = spiral, the gap
+    crossing tables Ek_gap / r_gap / phi_gap_deg / phi_gap_unwrapped_deg and
+    the map file names, then the frequency curve) and Er_coef.txt,
+    Ez_coef.txt, Ephi_coef.txt ((nr + 1) x (nphi + 1): phi axis in the first
+    row, r axis in the first column).  The gap follows the logarithmic spiral
+    phi_s(r) = s_ref + tan(alpha) ln(r / r_ref); its field has a Gaussian
+    profile of width sigma across the line, Eh = gap_width / (sigma
+    sqrt(2 pi)) exp(-d^2 / 2 sigma^2) with d = r (phi - phi_s(r)) cos(alpha)
+    (so V0 / gap_width * Eh integrates to V0 across the gap), directed along
+    the line's normal (Er, Ephi) = Eh (-sin alpha, cos alpha); Ez / z =
+    -(Er / r + dEr/dr + dEphi/dphi / r) by central differences.  Returns the
+    emap.txt path."""
+    os.makedirs(folder, exist_ok=True)
+    al = math.radians(alpha_deg)
+    s_ref = math.radians(s_ref_deg)
+    r = np.linspace(r_axis[0], r_axis[1], int(r_axis[2]))
+
+    def phi_s(rr):
+        return s_ref + math.tan(al) * np.log(np.asarray(rr, np.float64) / r_ref)
+    pad = math.radians(pad_deg)
+    phi = np.linspace(float(phi_s(r).min()) - pad, float(phi_s(r).max()) + pad, int(nphi))
+    R, PHI = np.meshgrid(r, phi, indexing="ij")
+    d = R * (PHI - phi_s(R)) * math.cos(al)
+    Eh = gap_width / (sigma * math.sqrt(2 * math.pi)) * np.exp(-0.5 * (d / sigma) ** 2)
+    Er, Ephi = -math.sin(al) * Eh, math.cos(al) * Eh
+    Ezc = -(Er / R + np.gradient(Er, r, axis=0) + np.gradient(Ephi, phi, axis=1) / R)
+    names = {"Er_map_file": "Er_coef.txt", "Ez_map_file": "Ez_coef.txt", "Ephi_map_file": "Ephi_coef.txt"}
+    for key, data in (("Er_map_file", Er), ("Ez_map_file", Ezc), ("Ephi_map_file", Ephi)):
+        table = np.zeros((len(r) + 1, len(phi) + 1))
+        table[0, 1:] = phi
+        table[1:, 0] = r
+        table[1:, 1:] = data
+        np.savetxt(os.path.join(folder, names[key]), table, fmt="%.17e")
+    Ek_gap = np.linspace(Ek_ramp[0] - 50.0, Ek_ramp[1] + 50.0, 11)
+    r_gap = orbit_radius(Ek_gap, lattice)
+    phi_gap_unwrapped = np.degrees(math.radians(gap_azimuth_deg[0]) + phi_s(r_gap))
+    T0 = float(revolution_time(Ek_ramp[0], lattice))
+    t = np.linspace(t_start, t_start + ramp_turns * T0 * 1.05, npts)
+    frac = np.clip(t / (ramp_turns * T0), 0.0, 1.0)
+    Ek = Ek_ramp[0] + (Ek_ramp[1] - Ek_ramp[0]) * frac
+    f = harmonic / revolution_time(Ek, lattice)
+    header = [
+        "gap_model = spiral",
+        f"Ngap = {len(gap_azimuth_deg)}",
+        f"acc_phi_paint = {float(acc_phi_deg)}",
+        f"acc_phi_acc = {float(acc_phi_deg)}",
+        f"gap_azimuth = {[float(a) for a in gap_azimuth_deg]}",
+        f"rf_shift = {[float(a) for a in rf_shift_deg]}",
+        f"gap_width = {float(gap_width)}",
+        f"harmonic = {int(harmonic)}",
+        f"Ek_gap = {[float(x) for x in Ek_gap]}",
+        f"r_gap = {[float(x) for x in r_gap]}",
+        f"phi_gap_deg = {[float(x % 360.0) for x in phi_gap_unwrapped]}",
+        f"phi_gap_unwrapped_deg = {[float(x) for x in phi_gap_unwrapped]}",
+        f"dt_uniform = {float(t[1] - t[0]):.6e}",
+    ] + [f"{k} = {v}" for k, v in names.items()] + ["#Time (s)        Frequency (Hz)    V0 (V)    Energy (MeV)"]
+    path = os.path.join(folder, "emap.txt")
+    with open(path, "w") as fh:
+        fh.write("\n".join(header) + "\n")
+        np.savetxt(fh, np.column_stack([t, f, np.full_like(t, voltage), Ek]), fmt="%.12e", delimiter="\t")
+    return path
+
+
 def seo_tables(Ek_axis=None, nfi=361, lattice=LATTICE):
     """Closed-orbit tables r0(Ek, fi), pr0(Ek, fi) and perimeter(Ek) from the
     scaling law (pr0 = 0; fi axis over [0, 2 pi])."""

@@ -110,7 +110,7 @@ class Pusher:
         self.gp = gp
         self.solver = solver
         self.fm = gp.Bmap.device_map(bunch.device)
-        self.rf = gp.Emap.rf_desc()
+        self.rf = gp.Emap.rf_desc(device=bunch.device)
         self.ap = _aperture(gp)
         self.cs = _consts(gp)
         # field-error harmonics (FFAG_BField_Error): carried by the device map

@@ -15,6 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "golden_tracking.npz")
 GOLDEN_HARMONICS = os.path.join(HERE, "golden", "golden_harmonics.npz")
+GOLDEN_SPIRAL = os.path.join(HERE, "golden", "golden_spiral.npz")
 
 
 class Golden:
@@ -59,6 +60,25 @@ class Golden:
         return g
 
 
+class SpiralGolden(Golden):
+    """The spiral-gap fixture (tests/golden/make_golden.py --spiral): the
+    tracking fixture's lattice with the spiral RF gap files it stores."""
+
+    def __init__(self, path=None):
+        z = np.load(path or GOLDEN_SPIRAL)
+        self.z = {k: z[k] for k in z.files}
+        self.cfg = json.loads(bytes(self.z["cfg_json"]).decode())
+        self.aperture = tuple(self.z["aperture"].tolist())
+        self.folder = tempfile.mkdtemp()
+        for name in ("emap", "Er_coef", "Ez_coef", "Ephi_coef"):
+            with open(os.path.join(self.folder, name + ".txt"), "w") as f:
+                f.write(bytes(self.z["file_" + name]).decode())
+
+    def emap(self, enable=True):
+        from pyffa_b200.fields import FFAG_EField_spiral
+        return FFAG_EField_spiral(os.path.join(self.folder, "emap.txt"), enable)
+
+
 _cache = {}
 
 
@@ -74,6 +94,13 @@ def load_golden_harmonics():
     if "h" not in _cache:
         _cache["h"] = Golden(GOLDEN_HARMONICS)
     return _cache["h"]
+
+
+def load_golden_spiral():
+    """The spiral RF gap fixture: field lookups, single steps and loops."""
+    if "s" not in _cache:
+        _cache["s"] = SpiralGolden()
+    return _cache["s"]
 
 
 def rel_err(a, b, scale=None):

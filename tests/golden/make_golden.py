@@ -8,6 +8,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py --seo --ref REFERENCE_CHECKOUT        # closed orbits
     python tests/golden/make_golden.py --bunch --ref REFERENCE_CHECKOUT      # injected bunches
     python tests/golden/make_golden.py --harmonics --ref REFERENCE_CHECKOUT  # field-error harmonics
+    python tests/golden/make_golden.py --spiral --ref REFERENCE_CHECKOUT     # spiral RF gaps
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -538,17 +539,151 @@ def harmonics_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+# Spiral RF gap of the spiral fixture (synthetic.spiral_emap_folder): two gaps
+# whose windows overlap, so the first-gap rule is exercised
+SPIRAL = dict(alpha_deg=40.0, r_ref=8.2, r_axis=(7.95, 8.55, 61), pad_deg=1.0, nphi=121, sigma=0.02,
+              gap_azimuth_deg=(1.0, 4.0), rf_shift_deg=(0.0, 25.0), voltage=150e3, gap_width=0.2,
+              acc_phi_deg=30.0, ramp_turns=20, npts=201)
+
+
+def spiral_main(ref):
+    """Spiral RF gaps (FFAG_EField_spiral): the reference's own field lookup
+    (Interpolation2D_EMap) on scattered points, Boris and RK4 single steps
+    and tracking loops through the gaps, on the tracking fixture's lattice."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    import FFAG_track
+    from FFAG_Bunch import FFAG_Bunch
+    from FFAG_dump import Dumps
+    from FFAG_Field import FFAG_EField_spiral
+    from FFAG_MathTools import RK4_Post_Step_njit
+    from FFAG_ParasAndConversion import FFAG_ConversionTools
+
+    conv = FFAG_ConversionTools()
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg_path, emap_fixed = build_inputs(tmp)
+        sp_dir = os.path.join(tmp, "spiral")
+        emap_path = synthetic.spiral_emap_folder(sp_dir, **SPIRAL)
+        aperture = (8.02, 8.48, -0.006, 0.006)
+        dt = synthetic.design_dt(300.0, 720)
+        t0 = 1.0e-9
+
+        def gp_s():
+            gp = ref_objects(cfg_path, emap_fixed, aperture)
+            gp.AddEMap(FFAG_EField_spiral(emap_path, True))
+            return gp
+
+        # ---- the field lookup itself on scattered points
+        rng = np.random.Generator(np.random.PCG64(41))
+        n = 4000
+        r = rng.uniform(7.9, 8.6, n)                        # beyond both ends of the map's r axis too
+        fi = np.concatenate([rng.uniform(-4 * np.pi, 4 * np.pi, n // 2),
+                             np.deg2rad(rng.uniform(-3.0, 9.0, n // 2)) + 2 * np.pi * rng.integers(-3, 4, n // 2)])
+        z = rng.uniform(-0.01, 0.01, n)
+        em = FFAG_EField_spiral(emap_path, True)
+        Er, Ez, Efi = np.zeros(n), np.zeros(n), np.zeros(n)
+        hit = np.zeros(n, dtype=np.int32)
+        em.Interpolation2D_EMap(r, fi, z, Er, Ez, Efi, hit, v0_volt=1.3e5)
+        out["lookup_in"] = np.stack([r, fi, z], 1)
+        out["lookup_out"] = np.stack([Er, Ez, Efi], 1)
+        out["lookup_hit"] = hit
+        out["lookup_v0"] = np.array([1.3e5])
+
+        # ---- single steps with particles across both gap windows
+        pa = p_bunch(64, seed=43)
+        pa[:40, 4] = np.deg2rad(np.linspace(-2.0, 7.0, 40))
+        pa[40:48, 0] = np.linspace(8.03, 8.47, 8)
+        pa[40:48, 4] = np.deg2rad(2.5)
+        va = conv.ConvertPrzek2Vrzek_boris(pa)
+        va[:, 9] = 0.3
+        va[:, 7] = 1.0
+        va[:, 8] = 1.0
+        va[60:, 7] = 0.0
+        va[60:, 8] = 0.0
+        bunch = FFAG_Bunch(va.copy(), BunchType="Boris")
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        FFAG_track.FFAG_RungeKutta().Boris_solve(
+            t0, m, dt, bunch.Malloc_x_cart, bunch.Malloc_y_cart, bunch.Malloc_z_cart,
+            bunch.Malloc_vx_cart, bunch.Malloc_vy_cart, bunch.Malloc_vz_cart,
+            bunch.Malloc_Ex_cart, bunch.Malloc_Ey_cart, bunch.Malloc_Ez_cart,
+            bunch.Malloc_Bx_cart, bunch.Malloc_By_cart, bunch.Malloc_Bz_cart,
+            bunch.Malloc_RF_phase, bunch.Malloc_mod_fi,
+            bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+            bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+            bunch.Step_SurviveFlag, bunch.Malloc_RF_shift,
+            bunch.SurvivedNum_Local, bunch.LostNum_Local, gp_s())
+        out["boris1_in"], out["boris1_out"], out["boris1_t"] = m_in, m.copy(), np.array([t0, dt])
+
+        vr = conv.ConvertPrzek2Vrzek(pa)
+        vr[:, 9] = 0.3
+        vr[:, 7] = 1.0
+        vr[:, 8] = 1.0
+        vr[60:, 7] = 0.0
+        vr[60:, 8] = 0.0
+        bunch = FFAG_Bunch(vr.copy(), BunchType="RK4")
+        m = bunch.LocalBunch
+        m_in = m.copy()
+        dr, _, _, _ = FFAG_track.FFAG_RungeKutta().rk4_step_malloc(
+            FFAG_track.FunctionForAccelerationBunch_dt, t0, m, dt, gp_s(),
+            bunch.Malloc_Bz_interp, bunch.Malloc_Br_interp, bunch.Malloc_Bf_interp,
+            bunch.Malloc_Ez_interp, bunch.Malloc_Er_interp, bunch.Malloc_Ef_interp,
+            bunch.Malloc_mod_fi, bunch.Malloc_RF_shift, bunch.Malloc_RK_dxdt,
+            bunch.SurvivedNum_Local, bunch.LostNum_Local)
+        RK4_Post_Step_njit(m, dr)
+        out["rk41_in"], out["rk41_out"] = m_in, m.copy()
+
+        # ---- loops that carry the bunch through both gaps
+        for solver, nsteps in (("Boris", 240), ("RK4", 120)):
+            pl = p_bunch(64, seed=47, inj_spread_ns=4 * dt * 1e9)
+            pl[:, 4] = np.deg2rad(rng.uniform(-4.0, 0.0, 64))
+            v = conv.ConvertPrzek2Vrzek_boris(pl) if solver == "Boris" else conv.ConvertPrzek2Vrzek(pl)
+            v[:, 9] = 0.3
+            v[:, 15] = np.arange(v.shape[0])
+            b = FFAG_Bunch(v.copy(), BunchType=solver)
+            lp = {"stop_condition": {"max_stepsN": nsteps, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+                  "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+            v_in = b.LocalBunch.copy()
+            ts = -0.5 * dt
+            if solver == "Boris":
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC_boris(None, ts, b, gp_s(), lp)
+            else:
+                FFAG_track.FFAG_RungeKutta().rk4_solve_dt_bunch3_withSC(FFAG_track.FunctionForAccelerationBunch_dt,
+                                                                       ts, b, gp_s(), lp)
+            key = "borisloop" if solver == "Boris" else "rk4loop"
+            out[key + "_in"], out[key + "_out"], out[key + "_t"] = v_in, b.LocalBunch.copy(), np.array([ts, dt, nsteps])
+
+        with open(cfg_path) as f:
+            out["cfg_json"] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+        for name in ("emap.txt", "Er_coef.txt", "Ez_coef.txt", "Ephi_coef.txt"):
+            with open(os.path.join(sp_dir, name)) as f:
+                out["file_" + name.replace(".txt", "")] = np.frombuffer(f.read().encode(), dtype=np.uint8)
+        stacks = {}
+        for comp in ("Bz", "Bfi", "Br"):
+            stacks[comp] = np.stack([np.load(os.path.join(os.path.dirname(cfg_path), f"{comp}_order_{n}.npz"))
+                                     [f"{comp}_Taylor_coeff"] for n in range(MAX_ORDER + 1)])
+            out[f"stack_{comp}"] = stacks[comp][1:]
+        out["aperture"] = np.array(aperture)
+        out["spiral_json"] = np.frombuffer(json.dumps(SPIRAL).encode(), dtype=np.uint8)
+    path = os.path.join(HERE, "golden_spiral.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="Generate golden vectors by running the reference's own code.")
     ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"),
                     help="checkout of the reference project (or set PYFFA_REFERENCE)")
     kind = ap.add_mutually_exclusive_group()
-    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics"):
+    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics", "spiral"):
         kind.add_argument("--" + k, action="store_true")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
-    if args.harmonics:
+    if args.spiral:
+        spiral_main(args.ref)
+    elif args.harmonics:
         harmonics_main(args.ref)
     elif args.bunch:
         bunch_main(args.ref)
