@@ -155,6 +155,12 @@ typedef struct ffa_state_soa {
     double *e_pre_r, *e_pre_z, *e_pre_fi;
     double *e_pp_r, *e_pp_z, *e_pp_fi;
     uint8_t *sc_pre, *sc_pp;
+    /* Optional (NULL: identity): thread t of a push launch advances particle
+     * order[t], a permutation of 0 .. n-1.  Every particle's arithmetic is
+     * the same in any order; an order in which the 32 particles of a warp
+     * are close in (r, vr, azimuth, energy) lets their z-Taylor node loads
+     * share cache lines. */
+    const int32_t *order;
 } ffa_state_soa;
 
 /* Per-step host-precomputed scalars (device arrays indexed by absolute step).

@@ -87,7 +87,7 @@ class StateSoA(C.Structure):
         ("inj", d_p), ("surv", d_p), ("inj_step", d_p),
         ("e_pre_r", d_p), ("e_pre_z", d_p), ("e_pre_fi", d_p),
         ("e_pp_r", d_p), ("e_pp_z", d_p), ("e_pp_fi", d_p),
-        ("sc_pre", d_p), ("sc_pp", d_p),
+        ("sc_pre", d_p), ("sc_pp", d_p), ("order", d_p),
     ]
 
 
@@ -99,6 +99,8 @@ def soa_offset(st: "StateSoA", start: int) -> "StateSoA":
     pointer advanced by start elements)."""
     out = StateSoA()
     for name, _ in StateSoA._fields_:
+        if name == "order":         # a permutation of the whole range: not carried over
+            continue
         p = getattr(st, name)
         setattr(out, name, None if not p else p + start * _SOA_ELEM.get(name, 8))
     return out

@@ -295,6 +295,7 @@ class BatchedOrbitScan:
         st.stream = torch.cuda.Stream(dev)
         st.bunch = _EphemeralBunch(self._vformat(), "Boris", dev)
         st.pusher = Pusher(st.bunch, self.gp, "Boris", "fp32c")
+        st.pusher.order_every = 0     # one thread order for the scan's life (graph replays read it)
         st.pusher.stream = st.stream
         st.clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", dev)
         st.clock.ensure(self.steps + 1)

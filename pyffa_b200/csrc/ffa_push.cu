@@ -123,6 +123,21 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
 // clamp applies anyway, and a NaN coordinate truncates to node 0.
 __device__ __forceinline__ int trunc_index(double q) { return __double2int_rz(q); }
 
+// 32-byte read-only global loads (sm_100): four doubles, eight floats; the
+// address must be 32-byte aligned
+__device__ __forceinline__ void ldg_v4(const double *p, double t[4])
+{
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(t[0]), "=d"(t[1]), "=d"(t[2]), "=d"(t[3]) : "l"(p));
+}
+
+__device__ __forceinline__ void ldg_v8(const float *p, float t[8])
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(t[0]), "=f"(t[1]), "=f"(t[2]), "=f"(t[3]), "=f"(t[4]), "=f"(t[5]), "=f"(t[6]), "=f"(t[7])
+        : "l"(p));
+}
+
 template <int MAXO>
 __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double y, double z,
                                                double &Bz, double &Bfi, double &Br, int &clamped)
@@ -153,20 +168,19 @@ __device__ __forceinline__ void high_order_b64(const FieldK &f, double x, double
     nd[3] = nd[2] + NP;                       // (i+1, j+1)
     const double w[4] = {w00, w01, w10, w11};
     // accumulate node by node in the reference's order w00, w01, w10, w11;
-    // a node's coefficients are 16 B aligned pairs
+    // a node (32, 64 or 96 B) is read in 32-byte loads: half the load
+    // instructions of 16-byte pairs, and the L1 throughput they take is the
+    // kernel's bound
     double acc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
 #pragma unroll
-        for (int a = 0; a < NV; a += 2) {
-            const double2 t = __ldg(reinterpret_cast<const double2 *>(nd[k] + a));
-            if (k == 0) {
-                acc[a] = w[0] * t.x;
-                if (a + 1 < NV) acc[a + 1] = w[0] * t.y;
-            } else {
-                acc[a] += w[k] * t.x;
-                if (a + 1 < NV) acc[a + 1] += w[k] * t.y;
-            }
+        for (int a = 0; a < NV; a += 4) {
+            double t[4];
+            ldg_v4(nd[k] + a, t);
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * t[b] : acc[a + b] + w[k] * t[b];
         }
     }
     const double z2 = z * z;
@@ -519,13 +533,20 @@ __device__ __forceinline__ void field_mixed(const FieldK &f, double r, double ir
         float acc[NV];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            if constexpr (NP == 8) {   // 32-byte nodes: one 32-byte load each
+                float tv[8];
+                ldg_v8(nd[k], tv);
 #pragma unroll
-            for (int a = 0; a < NV; a += 4) {
-                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
-                const float tv[4] = {t.x, t.y, t.z, t.w};
+                for (int b = 0; b < NV; ++b) acc[b] = (k == 0) ? w[0] * tv[b] : acc[b] + w[k] * tv[b];
+            } else {
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+                for (int a = 0; a < NV; a += 4) {
+                    const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                    const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+                }
             }
         }
         const double z2 = z * z;
@@ -603,8 +624,9 @@ constexpr int BORIS_TB = 32;
 template <int MAXO, bool SC, bool XING, bool F32, int NREG = 80, bool HARM = false>
 __global__ void __maxnreg__(NREG) boris_f64_kernel(const __grid_constant__ PushK p)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+    const int64_t t_ = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t_ >= p.n) return;
+    const int64_t i = p.st.order ? (int64_t)__ldg(p.st.order + t_) : t_;   // the particle this thread advances
     const FieldK &f = p.f;
     const ffa_state_soa &S = p.st;
     double r = S.r[i], rdot = S.vr[i], z = S.z[i], zdot = S.vz[i], fi = S.fi[i], fidot = S.f5[i];
@@ -771,13 +793,20 @@ __device__ __forceinline__ void field_f32(const FieldK &f, double r, double fim,
         float acc[NV];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            if constexpr (NP == 8) {   // 32-byte nodes: one 32-byte load each
+                float tv[8];
+                ldg_v8(nd[k], tv);
 #pragma unroll
-            for (int a = 0; a < NV; a += 4) {
-                const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
-                const float tv[4] = {t.x, t.y, t.z, t.w};
+                for (int b = 0; b < NV; ++b) acc[b] = (k == 0) ? w[0] * tv[b] : acc[b] + w[k] * tv[b];
+            } else {
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+                for (int a = 0; a < NV; a += 4) {
+                    const float4 t = __ldg(reinterpret_cast<const float4 *>(nd[k] + a));
+                    const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        if (a + b < NV) acc[a + b] = (k == 0) ? w[0] * tv[b] : acc[a + b] + w[k] * tv[b];
+                }
             }
         }
         const float z2 = z * z;
@@ -834,8 +863,9 @@ __device__ __forceinline__ void field_f32(const FieldK &f, double r, double fim,
 template <int MAXO, bool XING>
 __global__ void __launch_bounds__(128) boris_f32_kernel(const __grid_constant__ PushK p)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+    const int64_t t_ = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t_ >= p.n) return;
+    const int64_t i = p.st.order ? (int64_t)__ldg(p.st.order + t_) : t_;   // the particle this thread advances
     const FieldK &f = p.f;
     const ffa_state_soa &S = p.st;
     const double c = p.cs.c;
@@ -985,8 +1015,9 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
 template <int MAXO, bool SC, bool XING, bool HARM = false>
 __global__ void __launch_bounds__(128) rk4_f64_kernel(const __grid_constant__ PushK p)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= p.n) return;
+    const int64_t t_ = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t_ >= p.n) return;
+    const int64_t i = p.st.order ? (int64_t)__ldg(p.st.order + t_) : t_;   // the particle this thread advances
     const ffa_state_soa &S = p.st;
     Y7 y{S.r[i], S.vr[i], S.z[i], S.vz[i], S.fi[i], S.f5[i], S.rf[i]};
     double esr = S.esc_r[i], esz = S.esc_z[i], esf = S.esc_fi[i];
