@@ -38,14 +38,17 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <cooperative_groups.h>
+
 #include "ffa_internal.cuh"
 
 namespace {
 
+namespace cg = cooperative_groups;
 using ffa::PI;
 
 constexpr int SC_TB = 256;
-constexpr int SC_BLOCKS = 592;             // 4 per SM on 148 SMs; fixed for determinism
+constexpr int SC_BLOCKS = 444;             // pass1: 3 per SM on 148 SMs (one wave); fixed for determinism
 constexpr double FIX_SCALE = 1099511627776.0;  // 2^40
 constexpr double EPS0 = 8.854187817e-12;
 
@@ -71,16 +74,6 @@ __device__ __forceinline__ double py_mod(double a, double b)
     double r = fmod(a, b);
     if (r != 0.0 && ((r < 0.0) != (b < 0.0))) r += b;
     return r;
-}
-
-__device__ __forceinline__ double gamma_of(const ffa_state_soa &S, int64_t i, int boris, double c, double E0_J)
-{
-    if (boris) {
-        const double rd = S.r[i] * S.f5[i];
-        const double v2 = S.vr[i] * S.vr[i] + S.vz[i] * S.vz[i] + rd * rd;
-        return 1.0 / sqrt(1.0 - v2 / (c * c));
-    }
-    return S.f5[i] / E0_J;
 }
 
 // Bilinear_interp_2D_vect_uniform (src/FFAG_MathTools.py:828-936) for one point
@@ -232,23 +225,29 @@ __device__ void finalize_state(const Partial *part, int nblk, const ffa_sc_desc 
 
 // `done` counts finished blocks; it must be zero at launch (it sits in the
 // slot after the charge accumulator, which is cleared before every update).
-__global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ffa_sc_desc d, double *x_out,
-                                                  double *pr0_out, Partial *part, unsigned long long *done,
-                                                  SCState *st, int64_t *status)
+__global__ void __launch_bounds__(SC_TB, 3) sc_pass1(ffa_state_soa S, int64_t n, ffa_sc_desc d, double *x_out,
+                                                     double *pr0_out, Partial *part, unsigned long long *done,
+                                                     SCState *st, int64_t *status)
 {
     const double shifts[4] = {0.0, PI, PI * 0.5, PI * 1.5};
     Partial p;
     p.sum_gamma = 0.0; p.sx = p.sz = p.sx2 = p.sz2 = 0.0; p.count = 0;
     for (int k = 0; k < 4; ++k) { p.amin[k] = 1e30; p.amax[k] = -1e30; }
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (S.surv[i] == 0) continue;
-        const double g = gamma_of(S, i, d.boris, d.speed_c, d.E0_J);
-        const double fi = S.fi[i];
+    // one live particle into the partial sums, in the thread's fixed order
+    auto take = [&](int64_t i, double r, double vr, double z, double vz, double fi, double f5) {
+        double g;
+        if (d.boris) {
+            const double rd = r * f5;
+            const double v2 = vr * vr + vz * vz + rd * rd;
+            g = 1.0 / sqrt(1.0 - v2 / (d.speed_c * d.speed_c));
+        } else {
+            g = f5 / d.E0_J;
+        }
         const double fm = fi - 2 * PI * floor(fi / (2 * PI));
         const double Ek = (g - 1) * d.E0_rest_MeV;
         const double r0 = seo_lookup(d.seo_r, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
         pr0_out[i] = seo_lookup(d.seo_pr, d.Ek0, d.dEk, d.nE, d.fi0, d.dfi, d.nfi, Ek, fm);
-        const double xi = S.r[i] - r0, zi = S.z[i];
+        const double xi = r - r0, zi = z;
         x_out[i] = xi;
         p.sum_gamma += g;
         ++p.count;
@@ -262,6 +261,12 @@ __global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ff
         p.sz += zi;
         p.sx2 += xi * xi;
         p.sz2 += zi * zi;
+    };
+    // every load of a particle issued before its survival test
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t a = S.surv[i];
+        const double r = S.r[i], vr = S.vr[i], z = S.z[i], vz = S.vz[i], fi = S.fi[i], f5 = S.f5[i];
+        if (a != 0) take(i, r, vr, z, vz, fi, f5);
     }
     const Partial b = block_partial(p);
     __shared__ int last;
@@ -276,7 +281,10 @@ __global__ void __launch_bounds__(SC_TB) sc_pass1(ffa_state_soa S, int64_t n, ff
     finalize_state(part, gridDim.x, d, st, status);
 }
 
-// slice index of every live particle (-1 otherwise), then the CIC deposit
+// slice index of every live particle (-1 otherwise), then the CIC deposit.
+// The integer sums do not depend on the order of the atomics, so any grid
+// gives the same cube; two particles per pass keep two particles' loads in
+// flight per thread.
 __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, ffa_sc_desc d, const double *x,
                                                     int32_t *slice, int64_t *cell, const SCState *st,
                                                     unsigned long long *acc)
@@ -285,13 +293,12 @@ __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, 
     const double fi_s = st->diag.fi_s, step = st->diag.slice_step;
     const double xmin = st->diag.xmin, zmin = st->diag.zmin, inv_dx = st->inv_dx, inv_dz = st->inv_dz;
     const int nx = d.nx, nz = d.nz;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (S.surv[i] == 0) {
+    auto one = [&](int64_t i, uint8_t alive, double fi, double xi, double zi) {
+        if (alive == 0) {
             slice[i] = -1;
             cell[i] = -1;
-            continue;
+            return;
         }
-        double fi = S.fi[i];
         fi = fi - 2 * PI * floor(fi / (2 * PI));
         if (fi < fi_s) fi += 2 * PI;
         int64_t s = (int64_t)((fi - fi_s) / step);
@@ -299,9 +306,9 @@ __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, 
         slice[i] = (int32_t)s;
         if (bad) {
             cell[i] = -1;
-            continue;
+            return;
         }
-        const double rx = (x[i] - xmin) * inv_dx, rz = (S.z[i] - zmin) * inv_dz;
+        const double rx = (xi - xmin) * inv_dx, rz = (zi - zmin) * inv_dz;
         int64_t ix = (int64_t)floor(rx), iz = (int64_t)floor(rz);
         double fx = rx - (double)ix, fz = rz - (double)iz;
         if (ix < 0) { ix = 0; fx = 0.0; } else if (ix >= nx - 1) { ix = nx - 2; fx = 1.0; }
@@ -312,6 +319,14 @@ __global__ void __launch_bounds__(SC_TB) sc_deposit(ffa_state_soa S, int64_t n, 
         atomicAdd(acc + c0 + 1, (unsigned long long)llrint(fx * (1.0 - fz) * FIX_SCALE));
         atomicAdd(acc + c0 + nx, (unsigned long long)llrint((1.0 - fx) * fz * FIX_SCALE));
         atomicAdd(acc + c0 + nx + 1, (unsigned long long)llrint(fx * fz * FIX_SCALE));
+    };
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+        const int64_t k = i + stride < n ? i + stride : i;
+        const uint8_t a0 = S.surv[i], a1 = S.surv[k];
+        const double f0 = S.fi[i], f1 = S.fi[k], x0 = x[i], x1 = x[k], z0 = S.z[i], z1 = S.z[k];
+        one(i, a0, f0, x0, z0);
+        if (k != i) one(k, a1, f1, x1, z1);
     }
 }
 
@@ -340,40 +355,77 @@ __device__ __forceinline__ double green_point(int j, int i, double dx, double dz
     return v * dx * dz;
 }
 
+// Both sums are small dense products, (hz + 1) x (hx + 1) outputs of
+// hx + 1 (rows) or hz + 1 (columns) terms, tiled: a block computes 32 x 32
+// outputs (each thread one kx and four rows j or kz), with the shared
+// operand staged in GT-term chunks through shared memory and the cosine
+// table of the summed axis in shared memory; every output is summed over
+// increasing i (or j) as one chain of multiply-adds.
+constexpr int GT = 64;
+
 __global__ void __launch_bounds__(256) sc_green_rows(int NZ, int NX, const SCState *st, double *T)
 {
     if (st->bad) return;
-    extern __shared__ double gsh[];
-    const int hx = NX / 2;
-    double *g = gsh;                 // hx + 1 weighted values of row j
-    double *c = gsh + (hx + 1);      // cos(2 pi m / NX), m < NX
-    const int j = blockIdx.x;        // 0 .. NZ / 2
+    __shared__ double g[GT][32];     // w_i G[j][i] for a chunk of i and the block's 32 rows j
+    extern __shared__ double cx[];   // cos(2 pi m / NX), m < NX
+    const int hx = NX / 2, hz = NZ / 2;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int kx = blockIdx.x * 32 + tx, jb = blockIdx.y * 32;
     const double dx = st->diag.dx, dz = st->diag.dz;
-    for (int i = threadIdx.x; i <= hx; i += blockDim.x)
-        g[i] = ((i == 0 || i == hx) ? 1.0 : 2.0) * green_point(j, i, dx, dz);
-    for (int m = threadIdx.x; m < NX; m += blockDim.x) c[m] = cospi(2.0 * (double)m / (double)NX);
-    __syncthreads();
-    for (int kx = threadIdx.x; kx <= hx; kx += blockDim.x) {
-        double a = 0.0;
-        for (int i = 0; i <= hx; ++i) a += g[i] * c[(i * kx) & (NX - 1)];
-        T[(int64_t)j * (hx + 1) + kx] = a;
+    for (int m = threadIdx.x; m < NX; m += blockDim.x) cx[m] = cospi(2.0 * (double)m / (double)NX);
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i0 = 0; i0 <= hx; i0 += GT) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < GT * 32; e += blockDim.x) {
+            const int ii = e >> 5, jj = e & 31, i = i0 + ii, j = jb + jj;
+            g[ii][jj] = (i <= hx && j <= hz) ? ((i == 0 || i == hx) ? 1.0 : 2.0) * green_point(j, i, dx, dz) : 0.0;
+        }
+        __syncthreads();
+        const int in = min(GT, hx + 1 - i0);
+        for (int ii = 0; ii < in; ++ii) {
+            const double c = cx[((i0 + ii) * kx) & (NX - 1)];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] += g[ii][ty * 4 + q] * c;
+        }
+    }
+    if (kx > hx) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = jb + ty * 4 + q;
+        if (j <= hz) T[(int64_t)j * (hx + 1) + kx] = a[q];
     }
 }
 
 __global__ void __launch_bounds__(256) sc_green_cols(int NZ, int NX, const SCState *st, const double *T, float *gk)
 {
     if (st->bad) return;
-    extern __shared__ double gsh[];
+    __shared__ double t[GT][32];     // w_j T[j][kx] for a chunk of j and the block's 32 columns kx
+    extern __shared__ double cz[];   // cos(2 pi m / NZ), m < NZ
     const int hx = NX / 2, hz = NZ / 2;
-    double *c = gsh;                 // cos(2 pi m / NZ), m < NZ
-    const int kz = blockIdx.x;       // 0 .. NZ / 2
-    for (int m = threadIdx.x; m < NZ; m += blockDim.x) c[m] = cospi(2.0 * (double)m / (double)NZ);
-    __syncthreads();
-    for (int kx = threadIdx.x; kx <= hx; kx += blockDim.x) {
-        double a = 0.0;
-        for (int j = 0; j <= hz; ++j)
-            a += ((j == 0 || j == hz) ? 1.0 : 2.0) * T[(int64_t)j * (hx + 1) + kx] * c[(j * kz) & (NZ - 1)];
-        gk[(int64_t)kz * (hx + 1) + kx] = (float)a;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int kx = blockIdx.x * 32 + tx, kzb = blockIdx.y * 32 + ty * 4;
+    for (int m = threadIdx.x; m < NZ; m += blockDim.x) cz[m] = cospi(2.0 * (double)m / (double)NZ);
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j0 = 0; j0 <= hz; j0 += GT) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < GT * 32; e += blockDim.x) {
+            const int jj = e >> 5, xx = e & 31, j = j0 + jj, x = blockIdx.x * 32 + xx;
+            t[jj][xx] = (j <= hz && x <= hx) ? ((j == 0 || j == hz) ? 1.0 : 2.0) * T[(int64_t)j * (hx + 1) + x] : 0.0;
+        }
+        __syncthreads();
+        const int jn = min(GT, hz + 1 - j0);
+        for (int jj = 0; jj < jn; ++jj) {
+            const double v = t[jj][tx];
+            const int j = j0 + jj;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] += v * cz[(j * (kzb + q)) & (NZ - 1)];
+        }
+    }
+    if (kx > hx) return;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int kz = kzb + q;
+        if (kz <= hz) gk[(int64_t)kz * (hx + 1) + kx] = (float)a[q];
     }
 }
 
@@ -552,7 +604,8 @@ constexpr size_t solve_smem()
     return sizeof(float2) * (size_t)(nz * P + NX + NZ + (GX > GZ ? GX : GZ));
 }
 
-// One block per slice.  Charge rows (2p, 2p + 1) are the real and imaginary
+// One cluster of two blocks per slice (block 2 s + r, r = 0, 1; each pass
+// over lines gives line 2 m + r to block r).  Charge rows (2p, 2p + 1) are the real and imaginary
 // parts of one complex line; their x transforms give the two half spectra
 // (kx = 0 .. NX/2).  Each half-spectrum column then goes through the z
 // transform, the kernel and the inverse z transform in registers, and row
@@ -562,10 +615,15 @@ constexpr size_t solve_smem()
 // potential (scaled by 1 / (NX NZ) as the normalised inverse does) and the
 // field cubes; the charge cube as float32 on the way in.
 template <int NX, int NZ, bool HOCK>
-__global__ void __launch_bounds__(SOLVE_TB, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(SOLVE_TB, 1)
     sc_solve_fused(const unsigned long long *__restrict__ acc, const SCState *st, const float *__restrict__ gk,
                    float *__restrict__ rho, float *__restrict__ phi, float *__restrict__ Ex, float *__restrict__ Ez)
 {
+    // a cluster of two CTAs per slice: each holds the whole half spectrum,
+    // transforms every second line of each pass, and stores its results in
+    // its own and its partner's shared memory
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
     constexpr int nx = HOCK ? NX / 2 : NX, nz = HOCK ? NZ / 2 : NZ;
     constexpr int P = NX / 2 + 1;     // half-spectrum pitch (float2)
     constexpr int NCOL = NX / 2 + 1;
@@ -576,11 +634,12 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
     float2 *twx = spec + nz * P;
     float2 *twz = twx + NX;
     float2 *scr = twz + NZ;
+    float2 *peer = cluster.map_shared_rank(spec, rank ^ 1);
     const int tid = threadIdx.x;
-    const int64_t cube0 = (int64_t)blockIdx.x * nz * nx;
+    const int64_t cube0 = (int64_t)(blockIdx.x >> 1) * nz * nx;
     const int degenerate = st->degenerate, bad = st->bad;
-    if (bad) {
-        for (int e = tid; e < nz * nx; e += SOLVE_TB) {
+    if (bad) {   // the same for both CTAs: neither touches the other's memory
+        for (int e = tid + rank * SOLVE_TB; e < nz * nx; e += 2 * SOLVE_TB) {
             rho[cube0 + e] = 0.0f;
             phi[cube0 + e] = 0.0f;
             if (!degenerate) { Ex[cube0 + e] = 0.0f; Ez[cube0 + e] = 0.0f; }
@@ -598,15 +657,15 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
         sincospi(2.0 * (double)m / (double)NZ, &sv, &cv);
         twz[m] = make_float2((float)cv, (float)(-sv));
     }
-    __syncthreads();
+    cluster.sync();   // both CTAs running (and twiddles ready) before any store to the partner
 
     // (1) forward row transforms, two real rows per complex line
     {
         const Grp<X1> g;
         float2 *S = scr + g.gid * SX;
         constexpr int NPAIR = nz / 2, G = SOLVE_TB / X1;
-        for (int base = 0; base < NPAIR; base += G) {
-            const int p = base + g.line;
+        for (int base = 0; base < (NPAIR + 1) / 2; base += G) {
+            const int p = 2 * (base + g.line) + rank;
             const bool act = p < NPAIR;
             float2 v[X2];
 #pragma unroll
@@ -634,13 +693,17 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
             if (act) {
                 for (int k = g.t; k <= NX / 2; k += X1) {
                     const float2 zk = S[k], zn = S[(NX - k) & (NX - 1)];
-                    spec[(2 * p) * P + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-                    spec[(2 * p + 1) * P + k] = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+                    const float2 A = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+                    const float2 B = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+                    spec[(2 * p) * P + k] = A;
+                    spec[(2 * p + 1) * P + k] = B;
+                    peer[(2 * p) * P + k] = A;
+                    peer[(2 * p + 1) * P + k] = B;
                 }
             }
         }
     }
-    __syncthreads();
+    cluster.sync();
 
     // (2) per half-spectrum column: z transform, kernel, inverse z transform
     {
@@ -652,8 +715,8 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
             dkx = (float)(2.0 * PI / (nx * st->diag.dx));
             dkz = (float)(2.0 * PI / (nz * st->diag.dz));
         }
-        for (int base = 0; base < NCOL; base += G) {
-            const int c = base + g.line;
+        for (int base = 0; base < (NCOL + 1) / 2; base += G) {
+            const int c = 2 * (base + g.line) + rank;
             const bool act = c < NCOL;
             float2 v[Z2];
 #pragma unroll
@@ -690,12 +753,15 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
 #pragma unroll
                 for (int n2 = 0; n2 < Z2; ++n2) {
                     const int row = g.t + Z1 * n2;
-                    if (row < nz) spec[row * P + c] = v[n2];
+                    if (row < nz) {
+                        spec[row * P + c] = v[n2];
+                        peer[row * P + c] = v[n2];
+                    }
                 }
             }
         }
     }
-    __syncthreads();
+    cluster.sync();
 
     // (3) inverse row transforms: half spectra A (row 2p), B (row 2p + 1)
     // -> Z[k] = A[k] + i B[k] over all k (Hermitian extension) -> a + i b
@@ -704,8 +770,8 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
         float2 *S = scr + g.gid * SX;
         constexpr int NPAIR = nz / 2, G = SOLVE_TB / X1;
         const float scale = (float)(1.0 / ((double)NX * (double)NZ));
-        for (int base = 0; base < NPAIR; base += G) {
-            const int p = base + g.line;
+        for (int base = 0; base < (NPAIR + 1) / 2; base += G) {
+            const int p = 2 * (base + g.line) + rank;
             const bool act = p < NPAIR;
             float2 v[X2];
 #pragma unroll
@@ -730,6 +796,8 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
             if (act) {
                 float *pa = reinterpret_cast<float *>(spec + (2 * p) * P);
                 float *pb = reinterpret_cast<float *>(spec + (2 * p + 1) * P);
+                float *qa = reinterpret_cast<float *>(peer + (2 * p) * P);
+                float *qb = reinterpret_cast<float *>(peer + (2 * p + 1) * P);
 #pragma unroll
                 for (int n2 = 0; n2 < X2; ++n2) {
                     const int nn = g.t + X1 * n2;
@@ -737,6 +805,8 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
                         const float fa = __fmul_rn(v[n2].x, scale), fb = __fmul_rn(v[n2].y, scale);
                         pa[nn] = fa;
                         pb[nn] = fb;
+                        qa[nn] = fa;
+                        qb[nn] = fb;
                         phi[cube0 + (int64_t)(2 * p) * nx + nn] = fa;
                         phi[cube0 + (int64_t)(2 * p + 1) * nx + nn] = fb;
                     }
@@ -744,7 +814,7 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
             }
         }
     }
-    __syncthreads();
+    cluster.sync();   // the last stores to the partner: phase 4 reads local memory only
 
     // (4) compute_field_from_potential_numba_SBS for every cell (each cell
     // takes the value of the last loop of the reference that writes it)
@@ -754,7 +824,7 @@ __global__ void __launch_bounds__(SOLVE_TB, 1)
         const double ig2 = 1.0 / (gm * gm);
         const double inv2dr = 0.5 / dr, inv2dz = 0.5 / dz;
         const bool zero = (dr == 0.0 || dz == 0.0 || BL == 0);
-        for (int e = tid; e < nz * nx; e += SOLVE_TB) {
+        for (int e = tid + rank * SOLVE_TB; e < nz * nx; e += 2 * SOLVE_TB) {
             if (zero) { Ex[cube0 + e] = 0.0f; Ez[cube0 + e] = 0.0f; continue; }
             const int j = e / nx, i = e - j * nx;
 #define PH(jj, ii) reinterpret_cast<const float *>(spec + (jj) * P)[(ii)]
@@ -793,7 +863,7 @@ cudaError_t launch_fused_t(const unsigned long long *acc, const SCState *st, int
     const cudaError_t e = cudaFuncSetAttribute(sc_solve_fused<NX, NZ, HOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)smem);
     if (e != cudaSuccess) return e;
-    sc_solve_fused<NX, NZ, HOCK><<<ns, SOLVE_TB, smem, s>>>(acc, st, gk, rho, phi, ex, ez);
+    sc_solve_fused<NX, NZ, HOCK><<<2 * ns, SOLVE_TB, smem, s>>>(acc, st, gk, rho, phi, ex, ez);   // 2-CTA clusters
     return cudaGetLastError();
 }
 
@@ -1039,14 +1109,13 @@ __global__ void __launch_bounds__(SC_TB) sc_gather_roll(ffa_state_soa S, int64_t
     const int nx = d.nx, nz = d.nz;
     const int degenerate = st->degenerate, bad = st->bad;
     const double x0 = st->diag.xmin, z0 = st->diag.zmin, dx = st->diag.dx, dz = st->diag.dz;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int s = slice[i];
+    auto one = [&](int64_t i, int s, double xi, double zi, double p, uint8_t surv) {
         double er = 0.0, ez = 0.0, ef = 0.0;
         bool fresh = false;
         if (!degenerate && s >= 0) {
             if (!bad) {
                 const float *EX = Ex + (int64_t)s * nz * nx, *EZ = Ez + (int64_t)s * nz * nx;
-                const double t = (x[i] - x0) / dx, u = (S.z[i] - z0) / dz;
+                const double t = (xi - x0) / dx, u = (zi - z0) / dz;
                 int64_t i0 = (int64_t)floor(t), j0 = (int64_t)floor(u);
                 if (i0 < 0) i0 = 0; else if (i0 > nx - 2) i0 = nx - 2;
                 if (j0 < 0) j0 = 0; else if (j0 > nz - 2) j0 = nz - 2;
@@ -1056,7 +1125,6 @@ __global__ void __launch_bounds__(SC_TB) sc_gather_roll(ffa_state_soa S, int64_t
                                   w11 * EX[(j0 + 1) * nx + i0 + 1];
                 const double gz = w00 * EZ[j0 * nx + i0] + w10 * EZ[j0 * nx + i0 + 1] + w01 * EZ[(j0 + 1) * nx + i0] +
                                   w11 * EZ[(j0 + 1) * nx + i0 + 1];
-                const double p = pr0[i];
                 const double rt = sqrt(1 + p * p);
                 er = gr * (1 / rt);
                 ez = gz;
@@ -1067,8 +1135,8 @@ __global__ void __launch_bounds__(SC_TB) sc_gather_roll(ffa_state_soa S, int64_t
             S.esc_fi[i] = ef;
             fresh = true;
         }
-        if (!roll) continue;
-        const uint8_t alive = S.surv[i] != 0;
+        if (!roll) return;
+        const uint8_t alive = surv != 0;
         if (alive && !fresh) { er = S.esc_r[i]; ez = S.esc_z[i]; ef = S.esc_fi[i]; }
         if (first) {
             S.sc_pre[i] = alive;
@@ -1085,7 +1153,25 @@ __global__ void __launch_bounds__(SC_TB) sc_gather_roll(ffa_state_soa S, int64_t
             S.e_pp_r[i] = S.e_pre_r[i]; S.e_pp_z[i] = S.e_pre_z[i]; S.e_pp_fi[i] = S.e_pre_fi[i];
             if (alive) { S.e_pre_r[i] = er; S.e_pre_z[i] = ez; S.e_pre_fi[i] = ef; }
         }
+    };
+    // two particles per pass, their first loads issued together
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+        const int64_t k = i + stride < n ? i + stride : i;
+        const int s0 = slice[i], s1 = slice[k];
+        const double xa = x[i], xb = x[k], za = S.z[i], zb = S.z[k], pa = pr0[i], pb = pr0[k];
+        const uint8_t va = S.surv[i], vb = S.surv[k];
+        one(i, s0, xa, za, pa, va);
+        if (k != i) one(k, s1, xb, zb, pb, vb);
     }
+}
+
+// Blocks of the per-particle passes whose results do not depend on the
+// grid (deposit, gather): two particles per thread, at most 16 blocks per SM
+unsigned particle_blocks(int64_t n)
+{
+    const int64_t b = (n + 2 * SC_TB - 1) / (2 * SC_TB);
+    return (unsigned)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
 }
 
 int ilog2(int v)
@@ -1119,11 +1205,12 @@ int run_update(const ffa_sc_desc &d, const SCBufs &b, ffa_state_soa *S, int64_t 
     const unsigned ew = 148 * 8;  // elementwise grids
     FFA_CHECK_CUDA(cudaMemsetAsync(b.acc, 0, sizeof(unsigned long long) * (cube + 1), s));
     sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.part, b.acc + cube, b.st, status);
-    sc_deposit<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.slice, b.cell, b.st, b.acc);
+    sc_deposit<<<particle_blocks(n), SC_TB, 0, s>>>(*S, n, d, b.x, b.slice, b.cell, b.st, b.acc);
     FFA_CHECK_CUDA(cudaGetLastError());
     if (d.hockney) {
-        sc_green_rows<<<NZ / 2 + 1, 256, sizeof(double) * (NX / 2 + 1 + NX), s>>>(NZ, NX, b.st, b.gT);
-        sc_green_cols<<<NZ / 2 + 1, 256, sizeof(double) * NZ, s>>>(NZ, NX, b.st, b.gT, b.gk);
+        const dim3 gg((NX / 2 + 32) / 32, (NZ / 2 + 32) / 32);
+        sc_green_rows<<<gg, 256, sizeof(double) * NX, s>>>(NZ, NX, b.st, b.gT);
+        sc_green_cols<<<gg, 256, sizeof(double) * NZ, s>>>(NZ, NX, b.st, b.gT, b.gk);
         FFA_CHECK_CUDA(cudaGetLastError());
     }
     if (fused_grid(d.nx, d.nz)) {
@@ -1139,8 +1226,8 @@ int run_update(const ffa_sc_desc &d, const SCBufs &b, ffa_state_soa *S, int64_t 
         sc_potential<<<ew, 256, 0, s>>>(b.work, d, NZ, NX, b.st, b.phi);
         sc_field<<<ew, 256, 0, s>>>(b.phi, d, b.st, b.ex, b.ez);
     }
-    sc_gather_roll<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.slice, b.st, b.ex, b.ez, roll ? 1 : 0,
-                                               first ? 1 : 0);
+    sc_gather_roll<<<particle_blocks(n), SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.slice, b.st, b.ex, b.ez,
+                                                        roll ? 1 : 0, first ? 1 : 0);
     FFA_CHECK_CUDA(cudaGetLastError());
     if (diag) FFA_CHECK_CUDA(cudaMemcpyAsync(diag, &b.st->diag, sizeof(ffa_sc_diag), cudaMemcpyDeviceToDevice, s));
     return FFA_OK;
