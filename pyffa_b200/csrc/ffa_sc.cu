@@ -363,22 +363,35 @@ __device__ __forceinline__ double green_point(int j, int i, double dx, double dz
 // increasing i (or j) as one chain of multiply-adds.
 constexpr int GT = 64;
 
-__global__ void __launch_bounds__(256) sc_green_rows(int NZ, int NX, const SCState *st, double *T)
+// w_i G[j][i] over the first quadrant (j <= NZ/2, i <= NX/2), row-major,
+// every point once
+__global__ void __launch_bounds__(256) sc_green_points(int NZ, int NX, const SCState *st, double *G)
 {
     if (st->bad) return;
-    __shared__ double g[GT][32];     // w_i G[j][i] for a chunk of i and the block's 32 rows j
+    const int hx = NX / 2, hz = NZ / 2;
+    const double dx = st->diag.dx, dz = st->diag.dz;
+    const int64_t tot = (int64_t)(hz + 1) * (hx + 1);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / (hx + 1)), i = (int)(e - (int64_t)j * (hx + 1));
+        G[e] = ((i == 0 || i == hx) ? 1.0 : 2.0) * green_point(j, i, dx, dz);
+    }
+}
+
+__global__ void __launch_bounds__(256) sc_green_rows(int NZ, int NX, const SCState *st, const double *G, double *T)
+{
+    if (st->bad) return;
+    __shared__ double g[GT][33];     // w_i G[j][i] for a chunk of i and the block's 32 rows j (padded)
     extern __shared__ double cx[];   // cos(2 pi m / NX), m < NX
     const int hx = NX / 2, hz = NZ / 2;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int kx = blockIdx.x * 32 + tx, jb = blockIdx.y * 32;
-    const double dx = st->diag.dx, dz = st->diag.dz;
     for (int m = threadIdx.x; m < NX; m += blockDim.x) cx[m] = cospi(2.0 * (double)m / (double)NX);
     double a[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i0 = 0; i0 <= hx; i0 += GT) {
         __syncthreads();
         for (int e = threadIdx.x; e < GT * 32; e += blockDim.x) {
-            const int ii = e >> 5, jj = e & 31, i = i0 + ii, j = jb + jj;
-            g[ii][jj] = (i <= hx && j <= hz) ? ((i == 0 || i == hx) ? 1.0 : 2.0) * green_point(j, i, dx, dz) : 0.0;
+            const int ii = e & (GT - 1), jj = e / GT, i = i0 + ii, j = jb + jj;
+            g[ii][jj] = (i <= hx && j <= hz) ? G[(int64_t)j * (hx + 1) + i] : 0.0;
         }
         __syncthreads();
         const int in = min(GT, hx + 1 - i0);
@@ -1193,6 +1206,11 @@ struct SCBufs {
     float *rho, *phi, *ex, *ez;
     float2 *work;         // batched-FFT path only
     double *gT;           // open boundary: Green row sums, (NZ/2 + 1) x (NX/2 + 1)
+    double *gG;           // open boundary: weighted Green points, same shape
+    // open boundary with a plan: the Green transform runs on `side`,
+    // concurrently with the deposit (fork after pass1, join before the solve)
+    cudaStream_t side;
+    cudaEvent_t fork, join;
     float *gk;            // open boundary: Green transform quadrant
 };
 
@@ -1205,14 +1223,24 @@ int run_update(const ffa_sc_desc &d, const SCBufs &b, ffa_state_soa *S, int64_t 
     const unsigned ew = 148 * 8;  // elementwise grids
     FFA_CHECK_CUDA(cudaMemsetAsync(b.acc, 0, sizeof(unsigned long long) * (cube + 1), s));
     sc_pass1<<<SC_BLOCKS, SC_TB, 0, s>>>(*S, n, d, b.x, b.pr0, b.part, b.acc + cube, b.st, status);
+    if (d.hockney) {
+        const bool par = b.side != nullptr;
+        const cudaStream_t g = par ? b.side : s;
+        if (par) {
+            FFA_CHECK_CUDA(cudaEventRecord(b.fork, s));
+            FFA_CHECK_CUDA(cudaStreamWaitEvent(b.side, b.fork, 0));
+        }
+        const dim3 gg((NX / 2 + 32) / 32, (NZ / 2 + 32) / 32);
+        const int64_t quad = (int64_t)(NZ / 2 + 1) * (NX / 2 + 1);
+        sc_green_points<<<(unsigned)((quad + 255) / 256), 256, 0, g>>>(NZ, NX, b.st, b.gG);
+        sc_green_rows<<<gg, 256, sizeof(double) * NX, g>>>(NZ, NX, b.st, b.gG, b.gT);
+        sc_green_cols<<<gg, 256, sizeof(double) * NZ, g>>>(NZ, NX, b.st, b.gT, b.gk);
+        FFA_CHECK_CUDA(cudaGetLastError());
+        if (par) FFA_CHECK_CUDA(cudaEventRecord(b.join, b.side));
+    }
     sc_deposit<<<particle_blocks(n), SC_TB, 0, s>>>(*S, n, d, b.x, b.slice, b.cell, b.st, b.acc);
     FFA_CHECK_CUDA(cudaGetLastError());
-    if (d.hockney) {
-        const dim3 gg((NX / 2 + 32) / 32, (NZ / 2 + 32) / 32);
-        sc_green_rows<<<gg, 256, sizeof(double) * NX, s>>>(NZ, NX, b.st, b.gT);
-        sc_green_cols<<<gg, 256, sizeof(double) * NZ, s>>>(NZ, NX, b.st, b.gT, b.gk);
-        FFA_CHECK_CUDA(cudaGetLastError());
-    }
+    if (d.hockney && b.side) FFA_CHECK_CUDA(cudaStreamWaitEvent(s, b.join, 0));
     if (fused_grid(d.nx, d.nz)) {
         FFA_CHECK_CUDA(launch_fused(d.nx, d.hockney != 0, b.acc, b.st, d.ns, b.gk, b.rho, b.phi, b.ex, b.ez, s));
     } else {
@@ -1265,9 +1293,12 @@ void free_plan(ffa_sc_plan *p)
 {
     if (!p) return;
     void *ptrs[] = {p->b.x, p->b.pr0, p->b.slice, p->b.cell, p->b.part, p->b.st, p->b.acc, p->b.rho, p->b.phi,
-                    p->b.ex, p->b.ez, p->b.work, p->b.gT, p->b.gk};
+                    p->b.ex, p->b.ez, p->b.work, p->b.gT, p->b.gG, p->b.gk};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (p->b.fork) cudaEventDestroy(p->b.fork);
+    if (p->b.join) cudaEventDestroy(p->b.join);
+    if (p->b.side) cudaStreamDestroy(p->b.side);
     free(p);
 }
 
@@ -1306,7 +1337,11 @@ int ffa_sc_plan_create(const ffa_sc_desc *desc, void *stream, ffa_sc_plan **out)
     if (ok && d.hockney) {
         const int64_t quad = (int64_t)(NZ / 2 + 1) * (NX / 2 + 1);
         ok = cudaMalloc(&b.gT, sizeof(double) * quad) == cudaSuccess &&
-             cudaMalloc(&b.gk, sizeof(float) * quad) == cudaSuccess;
+             cudaMalloc(&b.gG, sizeof(double) * quad) == cudaSuccess &&
+             cudaMalloc(&b.gk, sizeof(float) * quad) == cudaSuccess &&
+             cudaStreamCreateWithFlags(&b.side, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b.join, cudaEventDisableTiming) == cudaSuccess;
     }
     if (!ok) { free_plan(p); return FFA_ERR_NOMEM; }
     if (cudaMemset(b.st, 0, sizeof(SCState)) != cudaSuccess || cudaMemset(b.slice, 0xff, sizeof(int32_t) * n) != cudaSuccess ||

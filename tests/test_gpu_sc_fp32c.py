@@ -10,10 +10,15 @@ charge step itself is identical in both runs (same kernels); what differs is
 the push, and through the positions, the fields of the later updates.
 
 Exact: injection and loss flags.  Stated against float64, with bars: the
-radius, azimuth and momentum of the surviving particles after the turn,
-each within 4 times the float64 run's own response to a float32-sized input
-change (every initial radius times 1 + 2^-24) and within the absolute bars
-below.
+radius, azimuth and momentum of the surviving particles after the turn, the
+largest error within 4 times the float64 run's own response to a
+float32-sized input change (every initial radius times 1 + 2^-24), and the
+median error within the absolute bars below.  The largest errors cannot have
+an absolute bar: the 2.5D model gives each particle the field of its slice,
+and a particle that the rounding moves across a slice boundary sees another
+slice's field, so the response itself reaches 2e-4 of r in one turn for the
+particles at the boundaries, while the median stays at the float32 field's
+level.
 """
 import numpy as np
 import pytest
@@ -65,12 +70,12 @@ def _turn(gp, seo, v, dt, precision):
     return b.LocalBunch
 
 
-def _errors(a, b, alive, c=2.99792458e8):
+def _errors(a, b, alive, c=2.99792458e8, stat=np.max):
     speed = lambda m: np.sqrt(m[:, 1] ** 2 + m[:, 3] ** 2 + (m[:, 0] * m[:, 5]) ** 2)
     mom = lambda m: speed(m) / np.sqrt(1.0 - (speed(m) / c) ** 2)
-    return {"r": float(np.max(np.abs(b[alive, 0] - a[alive, 0]) / a[alive, 0])),
-            "fi": float(np.max(np.abs(b[alive, 4] - a[alive, 4]) / np.abs(a[alive, 4]))),
-            "p": float(np.max(np.abs(mom(b[alive]) - mom(a[alive])) / mom(a[alive])))}
+    return {"r": float(stat(np.abs(b[alive, 0] - a[alive, 0]) / a[alive, 0])),
+            "fi": float(stat(np.abs(b[alive, 4] - a[alive, 4]) / np.abs(a[alive, 4]))),
+            "p": float(stat(np.abs(mom(b[alive]) - mom(a[alive])) / mom(a[alive])))}
 
 
 def test_c2_turn_fp32c_vs_fp64():
@@ -85,9 +90,11 @@ def test_c2_turn_fp32c_vs_fp64():
     alive = a64[:, 8] == 1
     assert alive.sum() > N // 4
     e = _errors(a64, a32, alive)
+    med = _errors(a64, a32, alive, stat=np.median)
     scale = _errors(a64, ar, alive & (ar[:, 8] == 1))
-    print("\nc2 turn, fp32c vs fp64:", e, "\nfp64 response to r * (1 + 2^-24):", scale,
+    print("\nc2 turn, fp32c vs fp64: max", e, "median", med, "\nfp64 response to r * (1 + 2^-24):", scale,
           "\nalive fraction:", float(alive.mean()))
     bars = {"r": 1e-6, "fi": 1e-7, "p": 1e-6}
     for k in ("r", "fi", "p"):
-        assert e[k] <= max(4 * scale[k], 1e-12) and e[k] <= bars[k], (k, e[k], scale[k])
+        assert e[k] <= max(4 * scale[k], 1e-12), (k, e[k], scale[k])
+        assert med[k] <= bars[k], (k, med[k])
