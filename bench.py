@@ -593,12 +593,12 @@ LEARNED_FLOP_PER_MAP = 2 * (5 * 256 + 2 * 256 * 256 + 256 * 4)
 LEARNED_MMA_FLOP_PER_MAP = 2 * (16 * 256 + 2 * 256 * 256 + 256 * 16)
 
 
-def same_lattice_push(gp_l, phys, dev, turns=2):
+def same_lattice_push(gp_l, phys, dev, turns=2, steps_per_turn=STEPS_PER_TURN):
     """The plain time-domain Boris pushers (FP64, FP32C) on the learned map's
     own lattice (analytic field, no z-Taylor map, no RF) and bunch (the
-    learned map's states as Boris states at fi = 0), 720 steps of the
-    300 MeV design dt per launch.  The bunch spans 300-600 MeV, so a launch
-    carries each particle through a different fraction of a turn: the
+    learned map's states as Boris states at fi = 0), `steps_per_turn` steps
+    of the 300 MeV design per launch.  The bunch spans 300-600 MeV, so a
+    launch carries each particle through a different fraction of a turn: the
     particle-turns are counted from each particle's azimuth advance."""
     import torch
     from pyffa_b200 import synthetic
@@ -610,21 +610,22 @@ def same_lattice_push(gp_l, phys, dev, turns=2):
     gp2.AddBMap(gp_l.Bmap)
     gp2.AddEMap(FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")), EnableFlag=False))
     m = phys_to_boris(phys)
-    dt = synthetic.design_dt(300.0, STEPS_PER_TURN)
-    out = {"particles": m.shape[0], "launches": turns, "steps_per_launch": STEPS_PER_TURN,
+    spt = int(steps_per_turn)
+    dt = synthetic.design_dt(300.0, spt)
+    out = {"particles": m.shape[0], "launches": turns, "steps_per_launch": spt,
            "lattice": "the learned map's: analytic field, no z-Taylor map, no RF"}
     for prec in ("fp64", "fp32c"):
         b = _EphemeralBunch(m, "Boris", dev)
         pu = Pusher(b, gp2, "Boris", prec)
         clock = StepClock(0.0, dt, gp2.Emap, "Boris", dev)
-        clock.ensure(STEPS_PER_TURN * (turns + 2))
-        pu.push(clock, 0, STEPS_PER_TURN, 0)
+        clock.ensure(spt * (turns + 2))
+        pu.push(clock, 0, spt, 0)
         torch.cuda.synchronize()
         fi0 = b.cols["fi"].clone()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(pu.stream)
         for k in range(turns):
-            pu.push(clock, (k + 1) * STEPS_PER_TURN, STEPS_PER_TURN, 0)
+            pu.push(clock, (k + 1) * spt, spt, 0)
         e1.record(pu.stream)
         torch.cuda.synchronize()
         pturns = float(((b.cols["fi"] - fi0) / (2 * np.pi)).sum().item())
@@ -636,13 +637,18 @@ def same_lattice_push(gp_l, phys, dev, turns=2):
     return out, gp2, dt
 
 
+LEARNED_STEPS_PER_TURN = 2880     # the learned map's plain tracker: Boris, 2880 steps per 300 MeV turn
+
+
 def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=10_000_000, turns_per_step=50,
                   steps=10, check_n=512, check_turns=1000):
     """Learned sector map: train on `samples` one-sector crossings of the
-    plain azimuth-domain tracker (300-600 MeV, amplitudes up to 10 mm / 5
-    mrad, uniform in normalised phase space), then track an n-particle bunch
-    with audits every 50 turns on 1% of the states (one step = 50 turns), and
-    compare a check bunch over 1000 turns with the FP64 plain tracker."""
+    plain FP32C time-domain Boris pusher (2880 steps per 300 MeV turn;
+    300-600 MeV, amplitudes up to 10 mm / 5 mrad, uniform in normalised
+    phase space), then track an n-particle bunch with audits every 50 turns
+    on 1% of the states against the same pusher (one step = 50 turns), and
+    compare a check bunch over 1000 turns with the FP64 Boris pusher at the
+    same step (and with the azimuth-domain RK4 tracker)."""
     import torch
     from pyffa_b200 import learned, synthetic
     from pyffa_b200.constants import FFAG_ConversionTools, FFAG_GlobalParameters
@@ -652,13 +658,16 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
     bm.UpdataConfig()
     gp = FFAG_GlobalParameters()
     gp.AddBMap(bm)
-    tracker = learned.SectorTracker(gp.Bmap, gp.q, steps_per_sector=128, device=dev)
+    dt_td = synthetic.design_dt(300.0, LEARNED_STEPS_PER_TURN)
+    tracker = learned.TimeDomainSectorTracker(gp, dt_td, "fp32c", device=dev)      # data, audits, fall-back
+    t64 = learned.TimeDomainSectorTracker(gp, dt_td, "fp64", device=dev)          # frame and reference
+    rk4 = learned.SectorTracker(gp.Bmap, gp.q, steps_per_sector=128, device=dev)  # azimuth-domain check
     d0 = synthetic.design(300.0)
     conv = FFAG_ConversionTools()
     nodes = np.cos(np.pi * (np.arange(17) + 0.5) / 17)[::-1]
     P = conv.Ek2P(450.0 + 150.0 * nodes)
     r_guess = d0["r0"] * (P / conv.Ek2P(300.0)) ** (1 / (cfg["Bmap"]["coefficients_tupel"][1] + 1))
-    frame = learned.SectorFrame.build(tracker, (300.0, 600.0), (10e-3, 5e-3), r_guess=r_guess, pr_guess=d0["pr0"])
+    frame = learned.SectorFrame.build(t64, (300.0, 600.0), (10e-3, 5e-3), r_guess=r_guess, pr_guess=d0["pr0"])
     t0 = time.perf_counter()
     X, T = learned.make_dataset(frame, tracker, samples, seed=1)
     Xv, Tv = learned.make_dataset(frame, tracker, 1 << 16, seed=2)
@@ -721,31 +730,33 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
         peaks = {"burst": 1590.0, "sustained": 1400.0,
                  "source": "fallback (MEASURED_PEAKS.json absent): 1.59 PF/s burst, 1.4 sustained"}
     ach = LEARNED_FLOP_PER_MAP * maps / k_s / 1e12
-    # the plain time-domain pushers on the same lattice and bunch
-    same, gp_same, dt_same = same_lattice_push(gp, phys, dev)
+    # the plain time-domain pushers on the same lattice and bunch: at the
+    # learned map's own step (the tracker it replaces) and at c1's
+    same, _, _ = same_lattice_push(gp, phys, dev, steps_per_turn=LEARNED_STEPS_PER_TURN)
     same["speedup_vs_fp64_same_lattice"] = value / same["fp64"]["value"]
     same["speedup_vs_fp32c_same_lattice"] = value / same["fp32c"]["value"]
+    same720, _, _ = same_lattice_push(gp, phys, dev, steps_per_turn=STEPS_PER_TURN)
+    same["at_720_steps_per_turn"] = {k: same720[k] for k in ("fp64", "fp32c")}
+    same["at_720_steps_per_turn"]["speedup_vs_fp64"] = value / same720["fp64"]["value"]
+    same["at_720_steps_per_turn"]["speedup_vs_fp32c"] = value / same720["fp32c"]["value"]
     del phys
     torch.cuda.empty_cache()
-    # accuracy: a check bunch over 1000 turns against the FP64 plain tracker
+    # accuracy: a check bunch over 1000 turns against the FP64 Boris pusher
+    # at the same step, and against the azimuth-domain RK4 tracker
     cb = bunch(check_n, 4)
-    ref = learned.plain_track(frame, tracker, cb, check_turns, record=True)
+    ref = learned.plain_track(frame, t64, cb, check_turns, record=True)
     got = learned.LearnedSectorMap(frame, tracker, p, audit_every=50, audit_frac=0.01,
                                    audit_tol=1e-5).track(cb, check_turns, record=True)
     dq = np.abs(learned.tunes(got["record"]) - learned.tunes(ref["record"]))
     de = np.abs(learned.betatron_emittance(frame, got["record"][-1]) /
                 learned.betatron_emittance(frame, ref["record"][-1]) - 1)
-    # and against the FP64 time-domain Boris pusher (60 steps per sector of
-    # the 300 MeV design), whose own truncation error shows as its
-    # difference from the azimuth-domain RK4
-    rb = learned.boris_record(frame, gp_same, cb, check_turns, dt_same, "fp64", dev)
-    ok = np.isfinite(rb).all(axis=(0, 2))
-    qb = learned.tunes(rb[:, ok])
-    dqb = np.abs(learned.tunes(got["record"][:, ok]) - qb)
-    dqbr = np.abs(learned.tunes(ref["record"][:, ok]) - qb)
-    eb = learned.betatron_emittance(frame, rb[-1][ok])
-    deb = np.abs(learned.betatron_emittance(frame, got["record"][-1][ok]) / eb - 1)
-    debr = np.abs(learned.betatron_emittance(frame, ref["record"][-1][ok]) / eb - 1)
+    rr = learned.plain_track(frame, rk4, cb, check_turns, record=True)
+    qr = learned.tunes(rr["record"])
+    er = learned.betatron_emittance(frame, rr["record"][-1])
+    dqr = np.abs(learned.tunes(got["record"]) - qr)
+    der = np.abs(learned.betatron_emittance(frame, got["record"][-1]) / er - 1)
+    dqbr = np.abs(learned.tunes(ref["record"]) - qr)
+    debr = np.abs(learned.betatron_emittance(frame, ref["record"][-1]) / er - 1)
     return {
         "value": value, "unit": "particle-turns/s",
         "speedup_vs_fp64": value / fp64_value if fp64_value else None,
@@ -762,15 +773,15 @@ def learned_bench(dev, fp64_value, fp32c_value, samples=20_000_000, epochs=8, n=
                                 "flop_per_map": LEARNED_FLOP_PER_MAP,
                                 "mma_flop_per_map": LEARNED_MMA_FLOP_PER_MAP,
                                 "peak_source": peaks["source"]}},
+        "plain_tracker": f"FP32C time-domain Boris, {LEARNED_STEPS_PER_TURN} steps per 300 MeV turn",
         "accuracy": {"check_bunch": check_n, "turns": check_turns, "tune_error_max": float(dq.max()),
                      "tune_error_rms": float(np.sqrt(np.mean(dq ** 2))),
-                     "emittance_error_max": float(de.max()), "vs": "FP64 azimuth-domain RK4 tracker, 128 steps/sector",
-                     "vs_fp64_boris": {"states": int(ok.sum()), "tune_error_max": float(dqb.max()),
-                                       "tune_error_rms": float(np.sqrt(np.mean(dqb ** 2))),
-                                       "emittance_error_max": float(deb.max()),
-                                       "rk4_vs_boris_tune_max": float(dqbr.max()),
-                                       "rk4_vs_boris_emittance_max": float(debr.max()),
-                                       "boris": "FP64 time-domain Boris, 720 steps per turn at 300 MeV"}},
+                     "emittance_error_max": float(de.max()),
+                     "vs": f"FP64 time-domain Boris, {LEARNED_STEPS_PER_TURN} steps per 300 MeV turn",
+                     "vs_azimuth_rk4": {"tune_error_max": float(dqr.max()), "emittance_error_max": float(der.max()),
+                                        "boris_vs_rk4_tune_max": float(dqbr.max()),
+                                        "boris_vs_rk4_emittance_max": float(debr.max()),
+                                        "rk4": "FP64 azimuth-domain RK4, 128 steps per sector"}},
         "same_lattice": same,
         "training": {"samples": samples, "epochs": epochs, "batch": 8192, "s": t_train, "data_s": t_data,
                      "steps": tr.t, "samples_per_s": tr.t * 8192 / t_train, "validation_mse": mse,

@@ -31,10 +31,12 @@ import numpy as np
 from .constants import FFAG_ConversionTools
 
 
-def crossing_states(rec, dt, iterations=3):
-    """States (k, 4) = r, vr, z, vz at azimuth 0 of crossing records (k, 23).
+def crossing_states(rec, dt, iterations=3, target=0.0):
+    """States (k, 4) = r, vr, z, vz at the azimuth `target` (rad) of crossing
+    records (k, 23).
 
-    The pre- and post-step states are taken to Cartesian coordinates and the
+    The pre- and post-step states are taken to Cartesian coordinates (x axis
+    along the target azimuth) and the
     step is interpolated as a cubic Hermite curve in time (positions and
     velocities at both ends), the crossing time found by Newton on y(tau) = 0
     from the linear estimate; velocities are interpolated linearly.  Near
@@ -45,7 +47,7 @@ def crossing_states(rec, dt, iterations=3):
 
     def cart(o):
         r, vr, z, vz, fi, f5 = (rec[:, o + j] for j in range(6))
-        c, s_ = torch.cos(fi), torch.sin(fi)
+        c, s_ = torch.cos(fi - target), torch.sin(fi - target)
         vf = r * f5
         return r * c, r * s_, z, vr * c - vf * s_, vr * s_ + vf * c, vz
 

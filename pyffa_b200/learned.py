@@ -137,6 +137,100 @@ class SectorTracker:
         return x1
 
 
+class TimeDomainSectorTracker:
+    """Whole sectors of the time-domain Boris pusher -- the tracking loop's
+    own plain pusher, the compensated float32 one by default -- behind
+    SectorTracker's interface: x0 (m, 5) = r, pr, z, pz, P at a sector
+    entrance -> (m, 4) at the entrance n_sectors later.  The lattice repeats
+    every sector, so every state starts at azimuth 0; all states are pushed
+    in one launch of steps dt (RF off, no aperture) until each azimuth has
+    passed n_sectors sector angles, the push kernels capture the crossing
+    step, and the state at that azimuth comes from a cubic Hermite
+    interpolation of the step in Cartesian coordinates
+    (coscan.crossing_states); pr, pz = vr / v, vz / v with the speed v of the
+    state's momentum (a static magnetic field keeps it).  gp: the lattice's
+    FFAG_GlobalParameters (its Bmap is used); chunk: states per launch."""
+
+    def __init__(self, gp, dt, precision="fp32c", device=None, chunk=1 << 21):
+        import os
+        import tempfile
+        torch = _torch()
+        from . import synthetic
+        from .constants import FFAG_GlobalParameters
+        from .fields import FFAG_EField_new
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.gp = FFAG_GlobalParameters()
+        self.gp.AddBMap(gp.Bmap)
+        self.gp.AddEMap(FFAG_EField_new(synthetic.emap_file(os.path.join(tempfile.mkdtemp(), "emap.txt")),
+                                        EnableFlag=False))
+        self.dt = float(dt)
+        self.precision = precision
+        self.nsectors = int(gp.Bmap.Nsectors)
+        self.period = 2 * np.pi / self.nsectors
+        self.chunk = int(chunk)
+        self.q = float(self.gp.q)
+        self.launches = 0
+        self._clock = None
+
+    def _clock_for(self, nsteps):
+        from .track import StepClock
+        if self._clock is None:
+            self._clock = StepClock(0.0, self.dt, self.gp.Emap, "Boris", self.dev)
+        self._clock.ensure(nsteps + 1)
+        return self._clock
+
+    def run(self, x0, n_sectors=1):
+        torch = _torch()
+        x0 = x0.to(self.dev, torch.float64).contiguous()
+        m = x0.shape[0]
+        if m == 0 or n_sectors == 0:
+            return x0[:, :4].clone()
+        out = torch.empty((m, 4), dtype=torch.float64, device=self.dev)
+        for a in range(0, m, self.chunk):
+            b = min(m, a + self.chunk)
+            out[a:b] = self._run(x0[a:b], int(n_sectors))
+        return out
+
+    def _run(self, x0, ns):
+        torch = _torch()
+        from .constants import FFAG_ConversionTools
+        from .coscan import crossing_states
+        from .track import CrossingCapture, Pusher, _EphemeralBunch
+        conv = FFAG_ConversionTools()
+        m = x0.shape[0]
+        P = x0[:, 4]
+        v = P * conv.c ** 2 / torch.sqrt((P * conv.c) ** 2 + conv.E0 ** 2)
+        mat = torch.zeros((m, 16), dtype=torch.float64, device=self.dev)
+        mat[:, 0], mat[:, 1], mat[:, 2], mat[:, 3] = x0[:, 0], x0[:, 1] * v, x0[:, 2], x0[:, 3] * v
+        mat[:, 5] = torch.sqrt(1.0 - x0[:, 1] ** 2 - x0[:, 3] ** 2) * v / x0[:, 0]
+        mat[:, 7] = 1.0
+        mat[:, 8] = 1.0
+        T = ns * self.period
+        w_min = float(mat[:, 5].min().item())
+        nsteps = int(math.ceil(1.25 * T / (w_min * self.dt))) + 4
+        b = _EphemeralBunch(mat, "Boris", self.dev)
+        pu = Pusher(b, self.gp, "Boris", self.precision)
+        cap = CrossingCapture(b, [T % (2 * np.pi)], self.gp, self.dt)
+        xing = cap.prepare(nsteps)
+        pu.push(self._clock_for(nsteps), 0, nsteps, 0, xing=xing)
+        self.launches += 1
+        k = int(cap.count.item())
+        if k > cap.x.capacity:
+            raise RuntimeError(f"crossing records overflowed: {k} > {cap.x.capacity}")
+        rec = cap.buf[:k * _lib.CROSSING_RECORD].view(k, _lib.CROSSING_RECORD)
+        rec = rec[(rec[:, 8] < T) & (rec[:, 15] >= T)]        # the step that passes T (unwrapped azimuth)
+        idx = rec[:, 1].long()
+        if idx.numel() != m or torch.unique(idx).numel() != m:
+            raise RuntimeError(f"{m - torch.unique(idx).numel()} of {m} states did not reach the sector entrance")
+        st = crossing_states(rec, self.dt, target=T)
+        out = torch.empty((m, 4), dtype=torch.float64, device=self.dev)
+        out[idx, 0] = st[:, 0]
+        out[idx, 1] = st[:, 1] / v[idx]
+        out[idx, 2] = st[:, 2]
+        out[idx, 3] = st[:, 3] / v[idx]
+        return out
+
+
 # ------------------------------------------------------------- the frame
 class SectorFrame:
     """Normalised coordinates at the sector entrance.

@@ -504,7 +504,7 @@ class _EphemeralBunch:
         self.device = dev
         self.n = a.shape[0]
         self._a = a
-        self.aos = torch.from_numpy(a).to(dev)
+        self.aos = a.to(dev, torch.float64).contiguous() if torch.is_tensor(a) else torch.from_numpy(a).to(dev)
         f64 = dict(dtype=torch.float64, device=dev)
         self.cols = {k: torch.empty(self.n, **f64) for k in ("r", "vr", "z", "vz", "fi", "f5", "rf",
                                                              "esc_r", "esc_z", "esc_fi")}
