@@ -306,12 +306,72 @@ def LoadSEOBetaFunc(SEOPATHName, Ek_c, fi_c):
     return tuple(out)
 
 
+def _segments(points):
+    """Polyline points (n, 2) -> segments (n - 1, 4) = x1, y1, x2, y2
+    (CentralLine2Segments, src/FFAG_Utils.py:278-286)."""
+    p = np.asarray(points, np.float64)
+    return np.column_stack([p[:-1], p[1:]])
+
+
+def _segment_crossings(A, B):
+    """Every segment of A against every segment of B (FindIntersectionVect,
+    src/FFAG_Utils.py:32-152): the crossing flags (a, b) -- bounding boxes
+    overlap and each segment's ends lie strictly on both sides of the other's
+    line -- and the signed distances of A's two ends from B's line (a, b)."""
+    A = np.atleast_2d(A)[:, None, :]
+    B = np.atleast_2d(B)[None, :, :]
+    A1x, A1y, A2x, A2y = A[..., 0], A[..., 1], A[..., 2], A[..., 3]
+    B1x, B1y, B2x, B2y = B[..., 0], B[..., 1], B[..., 2], B[..., 3]
+    apart = ((np.minimum(A1x, A2x) >= np.maximum(B1x, B2x)) | (np.maximum(A1x, A2x) <= np.minimum(B1x, B2x)) |
+             (np.minimum(A1y, A2y) >= np.maximum(B1y, B2y)) | (np.maximum(A1y, A2y) <= np.minimum(B1y, B2y)))
+    LB = np.sqrt((B2x - B1x) ** 2 + (B2y - B1y) ** 2)
+    cA1 = (B2x - B1x) * (A1y - B1y) - (B2y - B1y) * (A1x - B1x)
+    cA2 = (B2x - B1x) * (A2y - B1y) - (B2y - B1y) * (A2x - B1x)
+    cB1 = (A2x - A1x) * (B1y - A1y) - (A2y - A1y) * (B1x - A1x)
+    cB2 = (A2x - A1x) * (B2y - A1y) - (A2y - A1y) * (B2x - A1x)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        dA1 = np.where(LB != 0, cA1 / np.where(LB != 0, LB, 1.0), np.nan)
+        dA2 = np.where(LB != 0, cA2 / np.where(LB != 0, LB, 1.0), np.nan)
+    flag = ~apart & (cA1 * cA2 < 0) & (cB1 * cB2 < 0)
+    return flag, dA1, dA2
+
+
 def GetInitRAndFiForInjection(SEO_R, SEO_Pr, InjectCL, Ek):
-    """Injection point (azimuth, r, pr) on the closed orbit of energy Ek at the
-    azimuth InjectCL [deg] (src/FFAG_Distribution.py:1347-1414; the
-    central-line-file variant is not supported)."""
+    """Injection point (azimuth, r, pr) on the closed orbit of energy Ek
+    (src/FFAG_Distribution.py:1347-1414).  InjectCL a number: the azimuth in
+    deg, r and pr by 4 x 4 Lagrange interpolation of the tables.  InjectCL an
+    array (n, 2) of x, y points: the injection central line; the closed orbit
+    of Ek (the tables' rows linearly interpolated in energy, My1p5DInterp)
+    as a polyline over the azimuth axis, closed by repeating its second
+    point; the first crossing of its segments with the line's (in segment
+    order); the crossing point from the two ends' distances to the line's
+    segment; pr of the orbit segment's start.  (The reference's last line
+    indexes the scalar azimuth and raises for this branch; here the azimuth
+    is returned as computed.)"""
     if isinstance(InjectCL, np.ndarray):
-        raise NotImplementedError("injection along a central-line file is not supported; give the azimuth in deg")
+        Ek_axis, fi_axis = SEO_R[1:, 0], SEO_R[0, 1:]
+        R, Pr = SEO_R[1:, 1:], SEO_Pr[1:, 1:]
+        right = int(np.searchsorted(Ek_axis, Ek, side="right"))
+        i0, i1 = right - 1, right
+        if i0 < 0:
+            i0, i1 = 0, 1
+        if i1 > len(Ek_axis) - 1:
+            i0, i1 = len(Ek_axis) - 2, len(Ek_axis) - 1
+        x0, x1 = Ek_axis[i0], Ek_axis[i1]
+        r_fi = (Ek - x1) / (x0 - x1) * R[i0] + (Ek - x0) / (x1 - x0) * R[i1]
+        pr_fi = (Ek - x1) / (x0 - x1) * Pr[i0] + (Ek - x0) / (x1 - x0) * Pr[i1]
+        traj = np.column_stack((r_fi * np.cos(fi_axis), r_fi * np.sin(fi_axis)))
+        traj = np.vstack((traj, traj[1]))
+        seo_seg, cl_seg = _segments(traj), _segments(InjectCL)
+        flag, dA1, dA2 = _segment_crossings(seo_seg, cl_seg)
+        ii, jj = np.nonzero(flag)
+        if ii.size == 0:
+            raise ValueError("the injection central line does not cross the closed orbit of this energy")
+        i, j = ii[0], jj[0]
+        pre_len, post_len = abs(dA1[i, j]), abs(dA2[i, j])
+        total = pre_len + post_len
+        P = ((pre_len - total) / (0 - total) * seo_seg[i, 0:2] + (pre_len - 0) / (total - 0) * seo_seg[i, 2:4])
+        return float(np.arctan2(P[1], P[0])), float(np.hypot(P[0], P[1])), float(pr_fi[i])
     Ek_axis, fi_axis = SEO_R[1:, 0], SEO_R[0, 1:]
     theta = np.array([np.deg2rad(InjectCL)])
     r = Lagrange_interp_2D_vect(Ek_axis, fi_axis, SEO_R[1:, 1:], np.array([Ek]), theta)[0][0]
@@ -341,6 +401,8 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
     Ek_c = ini[0]
     if isinstance(InjectionPosition, dict):
         fi_c, r_c, pr_c = InjectionPosition["fi"], InjectionPosition["r"], InjectionPosition["pr"]
+    elif isinstance(InjectionPosition, str):           # a central-line file: x, y after one header line
+        fi_c, r_c, pr_c = GetInitRAndFiForInjection(SEO_R, SEO_Pr, np.loadtxt(InjectionPosition, skiprows=1), Ek_c)
     elif isinstance(InjectionPosition, (float, int)):
         fi_c, r_c, pr_c = GetInitRAndFiForInjection(SEO_R, SEO_Pr, float(InjectionPosition), Ek_c)
     else:

@@ -9,6 +9,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py --bunch --ref REFERENCE_CHECKOUT      # injected bunches
     python tests/golden/make_golden.py --harmonics --ref REFERENCE_CHECKOUT  # field-error harmonics
     python tests/golden/make_golden.py --spiral --ref REFERENCE_CHECKOUT     # spiral RF gaps
+    python tests/golden/make_golden.py --injection --ref REFERENCE_CHECKOUT  # central-line injection point
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -671,17 +672,82 @@ def spiral_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def injection_main(ref):
+    """The injection point on the closed orbit where an injection central line
+    crosses it (GetInitRAndFiForInjection, src/FFAG_Distribution.py:1347-1414,
+    central-line branch).  The reference's function raises at its last line
+    (it indexes the scalar azimuth, `theta_rad[0]`), so the fixture runs the
+    same steps through the reference's own helpers -- My1p5DInterp,
+    CentralLine2Segments, FindIntersectionVect, xy2rfi_m2p180 -- and stores
+    what the function computes before that line; it also records that the
+    function itself raises."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    from FFAG_Distribution import GetInitRAndFiForInjection
+    from FFAG_MathTools import FFAG_interpolation
+    from FFAG_ParasAndConversion import FFAG_ConversionTools
+    from FFAG_Utils import FFAG_GeometryCalc, FFAG_SegmentTools
+    from pyffa_b200 import orbit
+    tab = orbit.seo_tables(synthetic.lattice_bmap(), np.linspace(290.0, 310.0, 5), nfi=361)
+    fi, Ek_axis = tab["fi_axis"], tab["Ek_axis"]
+    SEO_R = np.zeros((len(Ek_axis) + 1, len(fi) + 1))
+    SEO_R[0, 1:], SEO_R[1:, 0], SEO_R[1:, 1:] = fi, Ek_axis, tab["r"]
+    SEO_Pr = SEO_R.copy()
+    SEO_Pr[1:, 1:] = tab["pr"]
+    rng = np.random.Generator(np.random.PCG64(53))
+    lines, cases = [], []
+    for k in range(8):
+        a = np.deg2rad(rng.uniform(0.0, 360.0))
+        tilt = np.deg2rad(rng.uniform(-20.0, 20.0))
+        rr = np.linspace(7.6, 8.9, 5 + k)
+        bend = 0.002 * rng.standard_normal(len(rr))
+        ang = a + np.tan(tilt) * (rr - 8.2) / 8.2 + bend
+        lines.append(np.column_stack([rr * np.cos(ang), rr * np.sin(ang)]))
+    out = {}
+    raised = 0
+    for k, CL in enumerate(lines):
+        Ek = float(rng.uniform(291.0, 309.0))
+        try:
+            GetInitRAndFiForInjection(SEO_R, SEO_Pr, CL, Ek)
+        except IndexError:
+            raised += 1
+        R, P = SEO_R[1:, 1:], SEO_Pr[1:, 1:]
+        r_fi, _ = FFAG_interpolation().My1p5DInterp(Ek_axis, R)(np.array([Ek]))
+        pr_fi, _ = FFAG_interpolation().My1p5DInterp(Ek_axis, P)(np.array([Ek]))
+        traj = np.column_stack((r_fi[0] * np.cos(fi), r_fi[0] * np.sin(fi)))
+        traj = np.vstack((traj, traj[1, :]))
+        seo_seg = FFAG_SegmentTools().CentralLine2Segments(traj)
+        cl_seg = FFAG_SegmentTools().CentralLine2Segments(CL)
+        flag, dA1, dA2, _, _ = FFAG_GeometryCalc().FindIntersectionVect(seo_seg, cl_seg)
+        ii, jj = np.where(flag)
+        i, j = ii[0], jj[0]
+        pre, post = abs(dA1[i, j]), abs(dA2[i, j])
+        tot = pre + post
+        point = (pre - tot) / (0 - tot) * seo_seg[i, 0:2] + (pre - 0) / (tot - 0) * seo_seg[i, 2:4]
+        th, r, _ = FFAG_ConversionTools().xy2rfi_m2p180(point[0], point[1])
+        cases.append([Ek, float(th), float(r), float(pr_fi[0, i]), float(i), float(j)])
+        out[f"line_{k}"] = CL
+    out["cases"] = np.array(cases)
+    out["seo_r"], out["seo_pr"] = SEO_R, SEO_Pr
+    out["reference_raised"] = np.array([raised])
+    path = os.path.join(HERE, "golden_injection.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes; the reference raised on", raised, "of", len(lines))
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="Generate golden vectors by running the reference's own code.")
     ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"),
                     help="checkout of the reference project (or set PYFFA_REFERENCE)")
     kind = ap.add_mutually_exclusive_group()
-    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics", "spiral"):
+    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics", "spiral", "injection"):
         kind.add_argument("--" + k, action="store_true")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
-    if args.spiral:
+    if args.injection:
+        injection_main(args.ref)
+    elif args.spiral:
         spiral_main(args.ref)
     elif args.harmonics:
         harmonics_main(args.ref)

@@ -126,3 +126,32 @@ def test_device_sampler_oracle_matches_host_generator_in_distribution(kind, ltyp
     for a, b in ((0, 1), (2, 3)):
         e = lambda m: np.sqrt(np.cov(m[:, a], m[:, b]).diagonal().prod() - np.cov(m[:, a], m[:, b])[0, 1] ** 2)
         assert abs(e(mine) / e(ref) - 1) <= 0.02
+
+
+def test_central_line_injection_point_matches_reference_steps():
+    """Injection along a central line (GetInitRAndFiForInjection, central-line
+    branch, src/FFAG_Distribution.py:1361-1406) against the values the
+    reference's own helpers give for 8 lines and energies
+    (tests/golden/golden_injection.npz; the reference function itself raises
+    at its last line, which the fixture records)."""
+    import os
+    from pyffa_b200.distribution import GetInitRAndFiForInjection
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_injection.npz"))
+    assert int(z["reference_raised"][0]) == 8
+    for k, (Ek, th, r, pr, i, j) in enumerate(z["cases"]):
+        got = GetInitRAndFiForInjection(z["seo_r"], z["seo_pr"], z[f"line_{k}"], Ek)
+        assert got == (th, r, pr), (k, got, (th, r, pr))
+
+
+def test_central_line_file_in_the_generator(tmp_path):
+    """A str InjectionPosition is read as a central-line file (x, y after one
+    header line), as the reference's generator does."""
+    import os
+    from pyffa_b200.distribution import GetInitRAndFiForInjection
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_injection.npz"))
+    p = tmp_path / "cl.txt"
+    np.savetxt(p, z["line_0"], header="x y", comments="")
+    line = np.loadtxt(str(p), skiprows=1)
+    assert np.array_equal(line, z["line_0"])
+    Ek = z["cases"][0, 0]
+    assert GetInitRAndFiForInjection(z["seo_r"], z["seo_pr"], line, Ek) == tuple(z["cases"][0, 1:4])
