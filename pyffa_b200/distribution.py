@@ -395,7 +395,7 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
     from .seo import LoadSEOParams
     rng = rng if rng is not None else _default_rng
     eR, eZ, eFi = Emit[0] / 1000.0 / 1000.0, Emit[1] / 1000.0 / 1000.0, Emit[2]
-    ini, _, _ = LoadSEOParams(os.path.join(SEOFileName, "SEO_ini.txt"), Ek_c)
+    ini, bmap_path, _ = LoadSEOParams(os.path.join(SEOFileName, "SEO_ini.txt"), Ek_c)
     SEO_R = np.loadtxt(os.path.join(SEOFileName, "SEO_r.txt"), skiprows=1)
     SEO_Pr = np.loadtxt(os.path.join(SEOFileName, "SEO_pr.txt"), skiprows=1)
     Ek_c = ini[0]
@@ -412,8 +412,9 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
     else:
         bZ, bR, aZ, aR = LoadSEOBetaFunc(SEOFileName, Ek_c, fi_c)
     ttype, ltype = dist_types
-    if ltype == "match":
-        raise NotImplementedError("the RF-bucket-matched longitudinal distribution (FFAG_bucket) is not built")
+    if ltype == "match" and bucket_obj is None:
+        from .bucket import FFAG_bucket
+        bucket_obj = FFAG_bucket(bmap_path, Ek0=Ek_c, fi0=acc_phi0, U0=acc_U0, step_t=20e-9, step_N=18000)
     if ltype == "kv":
         eFi *= 2
     tw_fi = TwissContainer(LongitudeAlpha, LongitudeBeta, eFi)
@@ -421,6 +422,14 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
                                                                        TwissContainer(aZ, bZ, eZ))),
                         create_distribution(ltype, twiss_longitudinal=tw_fi))
     rc, prc, zc, pzc = r_c + dx_xp_y_yp[0], pr_c + dx_xp_y_yp[1], dx_xp_y_yp[2], dx_xp_y_yp[3]
+    if device_out is not None and ltype == "match":
+        # the bucket's rejection sampling runs on the host; the rows go to the device
+        import torch
+        a, dist, centre, bucket_obj = GenerateInitDistributionDtInjNew(
+            SEOFileName, InjectionPosition, Ek_c, Emit, num_points, InjTimeNanoSec, LongitudeAlpha, LongitudeBeta,
+            LongitudeT, acc_U0, acc_phi0, TwissParams, dist_types, dx_xp_y_yp, Bunch_ID, bucket_obj, rng)
+        device_out.copy_(torch.from_numpy(a))
+        return device_out, dist, centre, bucket_obj
     if device_out is not None:
         _sample_on_device(device_out, num_points, ttype, ltype, ((aR, bR, eR), (aZ, bZ, eZ),
                           (LongitudeAlpha, LongitudeBeta, eFi)), LongitudeT,
@@ -432,6 +441,9 @@ def GenerateInitDistributionDtInjNew(SEOFileName, InjectionPosition, Ek_c, Emit,
         sigma = math.sqrt(eFi / LongitudeBeta)
         t_inj = rng.uniform(-0.5 * LongitudeT, 0.5 * LongitudeT, num_points)
         Ek = rng.normal(0.0, sigma, num_points)
+    elif ltype == "match":       # src/FFAG_Distribution.py:1270-1275
+        t_inj, Ek_MeV, _ = bucket_obj.scatter_filter_by_span(num_points, LongitudeT, rng=rng)
+        Ek = Ek_MeV - Ek_c
     a = np.zeros((num_points, 16))
     a[:, COLUMNS["r"]] = r + rc
     a[:, COLUMNS["vr"]] = pr + prc

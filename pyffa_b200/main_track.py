@@ -9,9 +9,8 @@ pyffa_b200.track.  ``Tracker.from_json(path, restart=None).run()`` is the same
 as an object.
 
 Differences from the reference driver: the bunch generator is seeded
-(``BunchPara.Seed``, default 0); the 'match' longitudinal distribution is
-rejected; there is no MPI split (one process tracks the whole bunch; see
-bunch.divide_variables for the reference's split).
+(``BunchPara.Seed``, default 0); there is no MPI split (one process tracks
+the whole bunch; see bunch.divide_variables for the reference's split).
 """
 from __future__ import annotations
 

@@ -10,6 +10,7 @@ Run in the development container, where the reference source is available:
     python tests/golden/make_golden.py --harmonics --ref REFERENCE_CHECKOUT  # field-error harmonics
     python tests/golden/make_golden.py --spiral --ref REFERENCE_CHECKOUT     # spiral RF gaps
     python tests/golden/make_golden.py --injection --ref REFERENCE_CHECKOUT  # central-line injection point
+    python tests/golden/make_golden.py --bucket --ref REFERENCE_CHECKOUT     # RF-bucket-matched distribution
 
 The reference imports mpi4py, pyfftw and matplotlib, which are not
 installed; tests/golden/shims/ provides single-rank / numpy.fft / no-op
@@ -735,17 +736,68 @@ def injection_main(ref):
     print("wrote", path, os.path.getsize(path), "bytes; the reference raised on", raised, "of", len(lines))
 
 
+def bucket_main(ref):
+    """The RF bucket of the 'match' longitudinal distribution (FFAG_bucket,
+    src/FFAG_bucket.py) with the generator's parameters (step 20 ns, 18000
+    steps) on a closed-orbit frequency table of the synthetic lattice: its
+    starting points, stability flags, box limits, H on the grid, the
+    centre-line H-span relation, thresholds for three bunch lengths and one
+    sample of its (unseeded) rejection draw."""
+    sys.path.insert(0, os.path.join(HERE, "shims"))
+    sys.path.insert(0, os.path.join(ref, "src"))
+    from FFAG_bucket import FFAG_bucket
+    from FFAG_MathTools import FFAG_interpolation
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "resultsSEO"))
+        Ek = np.linspace(250.0, 350.0, 21)
+        f = 1.0 / synthetic.revolution_time(Ek)
+        rows = np.column_stack([np.arange(len(Ek)), Ek, synthetic.orbit_radius(Ek), np.zeros(len(Ek)), f])
+        path = os.path.join(tmp, "resultsSEO", "SEO_ini.txt")
+        with open(path, "w") as fh:
+            fh.write("synthetic closed-orbit table\nidx Ek r pr f\n")
+            np.savetxt(fh, rows, fmt="%.17e")
+        out["seo_ini_text"] = np.frombuffer(open(path).read().encode(), dtype=np.uint8)
+        for k, (fi0, U0) in enumerate(((30.0, 100e3), (20.0, 150e3))):
+            b = FFAG_bucket(tmp, Ek0=300.0, fi0=fi0, U0=U0, step_t=20e-9, step_N=18000)
+            b.build_H()
+            H, L = b.compute_center_H_vs_span()
+            thr = []
+            for Lt in (30.0, 80.0, 1e4):
+                Lu = float(np.clip(Lt, L.min(), L.max()))
+                o = np.argsort(L)
+                thr.append(float(FFAG_interpolation().linear_interpolation(L[o], H[o])(Lu)))
+            t_ns, Ek_s, H_thr = b.scatter_filter_by_span(20000, 80.0, show=False)
+            assert abs(H_thr - thr[1]) == 0.0
+            out[f"b{k}_params"] = np.array([fi0, U0, b.G.Tc, b.G.w0, b.zd_u])
+            out[f"b{k}_X_in"] = b.X_in
+            out[f"b{k}_stable"] = np.stack([b.stable_fwd, b.stable_rev])
+            out[f"b{k}_limits"] = np.array([b.x_min_plot, b.x_max_plot, b.y_min_plot, b.y_max_plot,
+                                            b.x_min_sample, b.x_max_sample, b.y_min_sample, b.y_max_sample])
+            out[f"b{k}_tr_end"] = np.stack([b.tr_fwd[-1], b.tr_rev[-1]])
+            out[f"b{k}_H"] = np.stack([b.q_grid, b.p_grid, b.Hq_rel, b.Hp_rel])
+            out[f"b{k}_H0"] = np.array([b.H00, b.H_sep])
+            out[f"b{k}_HL"] = np.stack([H, L])
+            out[f"b{k}_thr"] = np.array(thr)
+            out[f"b{k}_sample"] = np.stack([t_ns, Ek_s], 1)
+    path = os.path.join(HERE, "golden_bucket.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser(description="Generate golden vectors by running the reference's own code.")
     ap.add_argument("--ref", default=os.environ.get("PYFFA_REFERENCE"),
                     help="checkout of the reference project (or set PYFFA_REFERENCE)")
     kind = ap.add_mutually_exclusive_group()
-    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics", "spiral", "injection"):
+    for k in ("bunch", "seo", "mapgen", "crossing", "harmonics", "spiral", "injection", "bucket"):
         kind.add_argument("--" + k, action="store_true")
     args = ap.parse_args()
     if not args.ref:
         ap.error("the reference checkout is required: --ref PATH or PYFFA_REFERENCE=PATH")
-    if args.injection:
+    if args.bucket:
+        bucket_main(args.ref)
+    elif args.injection:
         injection_main(args.ref)
     elif args.spiral:
         spiral_main(args.ref)

@@ -155,3 +155,26 @@ def test_central_line_file_in_the_generator(tmp_path):
     assert np.array_equal(line, z["line_0"])
     Ek = z["cases"][0, 0]
     assert GetInitRAndFiForInjection(z["seo_r"], z["seo_pr"], line, Ek) == tuple(z["cases"][0, 1:4])
+
+
+def test_match_longitudinal_draws_inside_the_bucket(gb):
+    """The 'match' longitudinal type (src/FFAG_Distribution.py:1270-1275):
+    energies and times from the RF bucket's rejection draw for the target
+    bunch length (FFAG_bucket, built from the closed-orbit table of the map
+    folder's resultsSEO), transverse rows as for the other types."""
+    import shutil
+    from pyffa_b200.bucket import FFAG_bucket
+    os.makedirs(os.path.join(gb["_dir"], "resultsSEO"), exist_ok=True)
+    shutil.copy(os.path.join(gb["_fold"], "SEO_ini.txt"), os.path.join(gb["_dir"], "resultsSEO", "SEO_ini.txt"))
+    rng = np.random.default_rng(7)
+    a, _, centre, bucket = D.GenerateInitDistributionDtInjNew(
+        gb["_fold"], 0.0, 300.0, (1.0, 1.0, 1e-3), 4000, 5.0, 0.0, 40.0, 60.0, acc_U0=100e3, acc_phi0=30.0,
+        dist_types=("gauss", "match"), rng=rng)
+    assert isinstance(bucket, FFAG_bucket)
+    Ek_c = centre[4]
+    t, E = a[:, 6] - 5.0, a[:, 5]
+    thr = bucket.threshold(60.0)
+    assert np.all(bucket.H_at(t * 1e-9, E - Ek_c) >= thr - 1e-12 * abs(thr))
+    assert bucket.x_min_sample <= t.min() and t.max() <= bucket.x_max_sample
+    assert bucket.y_min_sample <= E.min() and E.max() <= bucket.y_max_sample
+    assert a[:, 0].std() > 0 and np.all(a[:, 13] == 0)
