@@ -61,16 +61,9 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         double pk1;
         const double t = (ri - f.pw_r0) * f.pw_inv_r0;
         if (fabs(t) <= f.pw_tlim) {
-            // Estrin's scheme: four levels of independent multiply-adds
-            // instead of a 15-deep Horner chain (the step's longest
-            // dependent sequence when the SM has few warps to switch to)
-            const double t2 = t * t, t4 = t2 * t2, t8 = t4 * t4;
-            double q[8];
+            double P = f.pw_c[15];
 #pragma unroll
-            for (int a = 0; a < 8; ++a) q[a] = fma(f.pw_c[2 * a + 1], t, f.pw_c[2 * a]);
-            const double r0 = fma(q[1], t2, q[0]), r1 = fma(q[3], t2, q[2]);
-            const double r2 = fma(q[5], t2, q[4]), r3 = fma(q[7], t2, q[6]);
-            const double P = fma(fma(r3, t4, r2), t8, fma(r1, t4, r0));
+            for (int a = 14; a >= 0; --a) P = P * t + f.pw_c[a];
             pk1 = f.pw_r0m * P;
         } else {
             pk1 = exp(f.km1 * log(ri));
@@ -79,9 +72,6 @@ __device__ __forceinline__ void analytic_b64(const FieldK &f, double ri, double 
         B0r = f.B0 * (pk1 * ri);
     }
     double B0F = 0.0, B0Fp = 0.0;
-    // magnets in pairs: their exponential and division chains are
-    // independent and interleave
-#pragma unroll 2
     for (int j = 0; j < f.n_seg; ++j) {
         const double ks = f.seg_k[j];
         // Past 37.5 the exponential is below 2^-54, so 1 + e rounds to 1 and
@@ -331,11 +321,8 @@ __device__ __forceinline__ void step_rotation(double y, double x, double ir, dou
 {
     const double s0 = y * ir;
     if (x > 0.0 && fabs(s0) < 0.02) {
-        // Estrin's scheme in u = s^2: (1 + u/6) + u^2 (3/40 + 5u/112) + u^4 (35/1152 + 63u/2816)
-        const double s2 = s0 * s0, s4 = s2 * s2;
-        const double e0 = fma(1.0 / 6, s2, 1.0), e1 = fma(5.0 / 112, s2, 3.0 / 40);
-        const double e2 = fma(63.0 / 2816, s2, 35.0 / 1152);
-        a = s0 * fma(fma(e2, s4, e1), s4, e0);
+        const double s2 = s0 * s0;
+        a = s0 * (1.0 + s2 * (1.0 / 6 + s2 * (3.0 / 40 + s2 * (5.0 / 112 + s2 * (35.0 / 1152 + s2 * (63.0 / 2816))))));
         s = s0;
         c = x * ir;
     } else {
