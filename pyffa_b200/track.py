@@ -153,6 +153,7 @@ class Pusher:
         self.order_every = int(order_every)
         self.order_min = int(order_min)
         self._orders = {}
+        self._soa_views = {}
         self.bunch = bunch
         self.gp = gp
         self.solver = solver
@@ -187,7 +188,7 @@ class Pusher:
         n = b.n - start if count is None else count
         if start < 0 or n < 0 or start + n > b.n:
             raise ValueError(f"particle range [{start}, {start + n}) outside the bunch of {b.n}")
-        soa = b.soa() if start == 0 else _lib.soa_offset(b.soa(), start)
+        soa = b.soa() if start == 0 else self._soa_at(b.soa(), start)
         self.fm.set_harmonics(self.harmonics)
         st = self.stream if stream is None else stream
         s = st.cuda_stream
@@ -202,6 +203,15 @@ class Pusher:
         else:
             _lib.check(L.ffa_push_crossing(*args, ctypes.byref(xing)), "ffa_push_crossing")
 
+
+    def _soa_at(self, base, start):
+        """The SoA view of particles start.. (cached: the bunch's columns do
+        not move while it lives)."""
+        key = (start, base.r)
+        v = self._soa_views.get(key)
+        if v is None:
+            v = self._soa_views[key] = _lib.soa_offset(base, start)
+        return v
 
     def _order_for(self, start, n, stream):
         """The Morton permutation of particles [start, start + n), made on
@@ -564,6 +574,9 @@ class MatrixTracker:
         self.launches = 0
         self.spans = split_spans(n, chunks)
         self.streams = [torch.cuda.Stream(self.dev) for _ in self.spans] if len(self.spans) > 1 else []
+        self._soas = [_lib.soa_offset(self.b.soa(), a) for a, _ in self.spans]
+        self._ready = torch.cuda.Event()
+        self._done = [torch.cuda.Event() for _ in self.spans]
 
     def bind_clock(self, t_start, dt, nsteps_total):
         self.clock = StepClock(t_start, dt, self.gp.Emap, self.solver, self.dev)
@@ -586,12 +599,11 @@ class MatrixTracker:
             host_out.copy_(b.aos, non_blocking=True)
             self.launches += 3
             return
-        ready = torch.cuda.Event()
+        ready = self._ready
         ready.record(main)
         row = b.aos.stride(0) * b.aos.element_size()
-        for (a, e), st in zip(self.spans, self.streams):
+        for (a, e), st, soa, done in zip(self.spans, self.streams, self._soas, self._done):
             st.wait_event(ready)
-            soa = _lib.soa_offset(b.soa(), a)
             with torch.cuda.stream(st):
                 b.aos[a:e].copy_(host_in[a:e], non_blocking=True)
                 _lib.check(L.ffa_aos_to_soa(b.aos.data_ptr() + a * row, e - a, ctypes.byref(soa), st.cuda_stream),
@@ -600,7 +612,6 @@ class MatrixTracker:
                 _lib.check(L.ffa_soa_to_aos(ctypes.byref(soa), e - a, b.aos.data_ptr() + a * row, st.cuda_stream),
                            "ffa_soa_to_aos")
                 host_out[a:e].copy_(b.aos[a:e], non_blocking=True)
-            done = torch.cuda.Event()
             done.record(st)
             main.wait_event(done)
             self.launches += 3
