@@ -17,7 +17,9 @@
  *    thread-safe per object.  Kernels never trap: problems are counted in the
  *    caller's device status words (ffa_status_index).
  *  - Particle state is structure-of-arrays, float64, with the reference's
- *    meaning per array (src/FFAG_Bunch.py:23-74 column map).
+ *    meaning per array (src/FFAG_Bunch.py:23-74 column map).  An empty bunch
+ *    (n = 0) is valid with NULL columns: the calls do nothing (a space-charge
+ *    update then reports a degenerate grid).
  */
 #ifndef FFA_CUDA_H
 #define FFA_CUDA_H

@@ -11,10 +11,13 @@ namespace {
 
 cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
-bool state_ok(const ffa_state_soa *st)
+// the columns every kernel reads; an empty bunch (n = 0) may leave them NULL
+bool state_ok(const ffa_state_soa *st, int64_t n)
 {
-    return st && st->r && st->vr && st->z && st->vz && st->fi && st->f5 && st->rf && st->esc_r &&
-           st->esc_z && st->esc_fi && st->inj && st->surv;
+    if (!st) return false;
+    if (n == 0) return true;
+    return st->r && st->vr && st->z && st->vz && st->fi && st->f5 && st->rf && st->esc_r && st->esc_z &&
+           st->esc_fi && st->inj && st->surv;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -267,7 +270,7 @@ int ffa_fieldmap_destroy(ffa_fieldmap *fm)
 
 int ffa_inject(ffa_state_soa *st, int64_t n, int64_t step, void *stream)
 {
-    if (!state_ok(st) || !st->inj_step || n < 0) return FFA_ERR_INVALID;
+    if (n < 0 || !state_ok(st, n) || (n > 0 && !st->inj_step)) return FFA_ERR_INVALID;
     if (n == 0) return FFA_OK;
     inject_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(*st, n, step);
     FFA_CHECK_CUDA(cudaGetLastError());
@@ -279,7 +282,8 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
                      double dt, int32_t sc_step, int32_t flags, void *stream, int64_t *status,
                      const ffa_crossing *xing)
 {
-    if (!fm || !rf || !ap || !cs || !tab || !state_ok(st) || n < 0 || nsteps < 0 || step0 < 0) return FFA_ERR_INVALID;
+    if (!fm || !rf || !ap || !cs || !tab || n < 0 || !state_ok(st, n) || nsteps < 0 || step0 < 0)
+        return FFA_ERR_INVALID;
     if (!tab->drf || !tab->acc || step0 + nsteps > tab->nsteps) return FFA_ERR_INVALID;
     if (rf->ngaps < 1 || rf->ngaps > FFA_MAX_GAPS) return FFA_ERR_INVALID;
     if (rf->spiral_nodes &&
@@ -431,7 +435,7 @@ int ffa_push_crossing(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_a
 
 int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream)
 {
-    if (!aos || !state_ok(st) || n < 0) return FFA_ERR_INVALID;
+    if (n < 0 || !state_ok(st, n) || (n > 0 && !aos)) return FFA_ERR_INVALID;
     if (n == 0) return FFA_OK;
     aos_to_soa_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(aos, n, *st);
     FFA_CHECK_CUDA(cudaGetLastError());
@@ -440,7 +444,7 @@ int ffa_aos_to_soa(const double *aos, int64_t n, ffa_state_soa *st, void *stream
 
 int ffa_soa_to_aos(const ffa_state_soa *st, int64_t n, double *aos, void *stream)
 {
-    if (!aos || !state_ok(st) || n < 0) return FFA_ERR_INVALID;
+    if (n < 0 || !state_ok(st, n) || (n > 0 && !aos)) return FFA_ERR_INVALID;
     if (n == 0) return FFA_OK;
     soa_to_aos_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(*st, n, aos);
     FFA_CHECK_CUDA(cudaGetLastError());
@@ -449,7 +453,7 @@ int ffa_soa_to_aos(const ffa_state_soa *st, int64_t n, double *aos, void *stream
 
 int ffa_mean_fi(const ffa_state_soa *st, int64_t n, double *out, int64_t *count, void *stream)
 {
-    if (!st || !st->fi || !out || !count || n < 0) return FFA_ERR_INVALID;
+    if (!st || (n > 0 && !st->fi) || !out || !count || n < 0) return FFA_ERR_INVALID;
     cudaStream_t s = as_stream(stream);
     FFA_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
     FFA_CHECK_CUDA(cudaMemsetAsync(count, 0, sizeof(int64_t), s));

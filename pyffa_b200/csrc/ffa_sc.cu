@@ -1263,8 +1263,9 @@ int run_update(const ffa_sc_desc &d, const SCBufs &b, ffa_state_soa *S, int64_t 
 
 int check_state(const ffa_state_soa *S, int64_t n, int32_t roll)
 {
-    if (!S || !S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r || !S->esc_z ||
-        !S->esc_fi || n < 0)
+    if (!S || n < 0) return FFA_ERR_INVALID;
+    if (n == 0) return FFA_OK;      // an empty bunch: the update gives an empty (degenerate) grid
+    if (!S->r || !S->vr || !S->z || !S->vz || !S->fi || !S->f5 || !S->surv || !S->esc_r || !S->esc_z || !S->esc_fi)
         return FFA_ERR_INVALID;
     if (roll && (!S->sc_pre || !S->sc_pp || !S->e_pre_r || !S->e_pre_z || !S->e_pre_fi || !S->e_pp_r ||
                  !S->e_pp_z || !S->e_pp_fi))

@@ -137,3 +137,14 @@ def test_every_entry_point_cites_what_it_replaces():
         if not any(key in doc for key in ("src/", "examples/", "benchmarks/", "counterpart")):
             bad.append(m.group(1))
     assert not bad, bad
+
+
+def test_empty_bunch_accepted_without_columns():
+    """n = 0 with every column NULL: the conversions and the injection
+    return 0 without touching the device (argument checks come first)."""
+    st = _lib.StateSoA()
+    L = _lib.lib()
+    assert L.ffa_aos_to_soa(None, 0, ctypes.byref(st), None) == 0
+    assert L.ffa_soa_to_aos(ctypes.byref(st), 0, None, None) == 0
+    assert L.ffa_inject(ctypes.byref(st), 0, 0, None) == 0
+    assert L.ffa_aos_to_soa(None, 1, ctypes.byref(st), None) == 1      # a particle needs its columns
