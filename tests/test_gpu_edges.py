@@ -90,8 +90,10 @@ def test_lost_and_uninjected_particles_drift_like_the_oracle(golden):
     ref = m.copy()
     O.boris_step(S, ref, t0, dt)
     _close(got, ref, 1e-14)
-    assert st["lost"] == 0                                        # no live particle left the aperture
-    assert np.array_equal(got[:, 7:9], m[:, 7:9])
+    # the live particles that the oracle loses at the aperture (the fixture
+    # puts some outside it) are the ones counted; the others keep their flags
+    assert st["lost"] == int(((m[:, 7] == 1) & (m[:, 8] == 1) & (ref[:, 8] == 0)).sum()) > 0
+    assert np.array_equal(got[:, 7:9], ref[:, 7:9])
 
 
 def test_nan_particle_counted_neighbours_unchanged(golden):
