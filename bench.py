@@ -40,6 +40,12 @@ FP64_FLOP_PER_PARTICLE_STEP = 300.0
 # the kernel's executed float64 operations per particle-step (2 per DFMA, 1
 # per DADD / DMUL), counted by ncu on this workload: reported beside it
 FP64_EXEC_FLOP_PER_PARTICLE_STEP = 419.4
+# algorithmic float64 operations per particle-step of one RK4 step: four
+# right-hand sides (azimuth mod sector 3, analytic field 93, z-Taylor sum 77,
+# RF window test 4, equations of motion 40) and the stage arithmetic (k = h d,
+# the stage states and the weighted sum, seven components each: 112), i.e.
+# 4 x 217 + 112
+RK4_FLOP_PER_PARTICLE_STEP = 980.0
 # DRAM bytes (read + write) of one launch (one turn, 1e5 particles) from an
 # ncu capture of the same launch, L2 flushed before it
 BORIS_TRAFFIC_PER_LAUNCH = 19.571e6
@@ -323,10 +329,11 @@ def sc_bench(gp, dt, dev, hbm_peak, updates=20, warmup=3, turns=2):
     return out
 
 
-def rk4_bench(gp, dt, dev, steps, warmup, flush, n=N_PARTICLES, seed=7):
-    """c1 with the float64 RK4 pusher: the same lattice, RF and bunch (RK4
-    columns: f5 = total energy), 720 steps per turn, one turn per launch,
-    L2 flushed and the bunch restored between launches (outside the events)."""
+def rk4_bench(gp, dt, dev, steps, warmup, flush, n=N_PARTICLES, seed=7, precision="fp64"):
+    """c1 with the RK4 pusher (float64, or the FP32C field): the same
+    lattice, RF and bunch (RK4 columns: f5 = total energy), 720 steps per
+    turn, one turn per launch, L2 flushed and the bunch restored between
+    launches (outside the events)."""
     import torch
     from pyffa_b200 import synthetic
     from pyffa_b200.constants import FFAG_ConversionTools
@@ -336,7 +343,7 @@ def rk4_bench(gp, dt, dev, steps, warmup, flush, n=N_PARTICLES, seed=7):
     v[:, 8] = 1.0
     b = _EphemeralBunch(v, "RK4", dev)
     pristine = {k: t.clone() for k, t in b.cols.items()}
-    pu = Pusher(b, gp, "RK4", "fp64")
+    pu = Pusher(b, gp, "RK4", precision)
     clock = StepClock(0.0, dt, gp.Emap, "RK4", dev)
     clock.ensure(STEPS_PER_TURN * (warmup + steps + 1))
     stream = pu.stream
@@ -359,7 +366,7 @@ def rk4_bench(gp, dt, dev, steps, warmup, flush, n=N_PARTICLES, seed=7):
     torch.cuda.synchronize()
     ms = statistics.mean(a.elapsed_time(bb) for a, bb in ev)
     return {"value": n / (ms * 1e-3), "unit": "particle-turns/s", "ms_per_turn": ms, "particles": n,
-            "steps_per_turn": STEPS_PER_TURN, "launches": steps}
+            "steps_per_turn": STEPS_PER_TURN, "launches": steps, "precision": precision}
 
 
 def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=7):
@@ -367,7 +374,8 @@ def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=
     on by the float64 Boris pusher (the reference for the errors), the FP32C
     Boris pusher and the float64 RK4 pusher, and by the float64 Boris pusher
     from every radius times 1 + 2^-24 (the dynamics' own response to a
-    float32-sized input change).  Coordinates and rms emittances are compared
+    float32-sized input change); the RK4 pusher with the FP32C field beside
+    them.  Coordinates and rms emittances are compared
     where the particles cross the azimuth half a turn from the bunch in the
     last turn; tunes (FFT, the reference's estimator) from 1000 turns of
     crossings of the first `tune_n` particles."""
@@ -404,7 +412,8 @@ def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=
     vb32[:, 0] *= 1 + 2.0 ** -24
     cases = {"fp64_boris": ("Boris", "fp64", vb), "fp32c_boris": ("Boris", "fp32c", vb),
              "fp32_boris": ("Boris", "fp32", vb),
-             "fp64_rk4": ("RK4", "fp64", vr), "fp64_boris_r_1_2e-24": ("Boris", "fp64", vb32)}
+             "fp64_rk4": ("RK4", "fp64", vr), "fp32c_rk4": ("RK4", "fp32c", vr),
+             "fp64_boris_r_1_2e-24": ("Boris", "fp64", vb32)}
     last, tun, alive = {}, {}, {}
     for name, (solver, prec, m) in cases.items():
         t0 = time.perf_counter()
@@ -416,7 +425,7 @@ def c1_accuracy_bench(gp, dt, dev, n=N_PARTICLES, turns=1000, tune_n=1024, seed=
         last[name + "_s"] = time.perf_counter() - t0
     out = {"particles": n, "turns": turns, "steps_per_turn": STEPS_PER_TURN, "rf": "2 gaps, last-gap semantics",
            "vs": "fp64_boris", "tune_particles": tune_n, "alive": alive}
-    for name in ("fp32c_boris", "fp32_boris", "fp64_rk4", "fp64_boris_r_1_2e-24"):
+    for name in ("fp32c_boris", "fp32_boris", "fp64_rk4", "fp32c_rk4", "fp64_boris_r_1_2e-24"):
         e = D.azimuth_errors(last["fp64_boris"], last[name])
         dq = np.abs(tun[name] - tun["fp64_boris"])
         dq = np.minimum(dq, 1.0 - dq)
@@ -1060,6 +1069,13 @@ def main():
         rk4 = None
         if not args.no_rk4 and solo:
             rk4 = rk4_bench(gp, dt, dev, min(args.steps, 10), args.warmup, flush)
+            rk4["fp32c"] = rk4_bench(gp, dt, dev, min(args.steps, 10), args.warmup, flush, precision="fp32c")
+            rk4["fp32c"]["speedup_vs_fp64_rk4"] = rk4["fp32c"]["value"] / rk4["value"]
+            ach = RK4_FLOP_PER_PARTICLE_STEP * N_PARTICLES * STEPS_PER_TURN / (rk4["ms_per_turn"] * 1e-3) / 1e12
+            rk4["roofline"] = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                               "frac": ach / peak64, "flop_per_particle_step": RK4_FLOP_PER_PARTICLE_STEP,
+                               "flop_basis": "algorithmic",
+                               "peak_source": "measured live: float64 FMA probe kernel (libffa_probe.so)"}
         acc = None
         if not args.no_accuracy and solo:
             acc = c1_accuracy_bench(gp, dt, dev)

@@ -51,7 +51,8 @@ enum ffa_push_flags {
     FFA_BORIS = 0,                /* relativistic Boris (solver_type 1) */
     FFA_RK4 = 1,                  /* 4th-order Runge-Kutta (solver_type 0) */
     FFA_FP64 = 0,                 /* all arithmetic in float64 */
-    FFA_FP32C = 2,                /* Boris: float32 field exponentials and map lookup, float64 push */
+    FFA_FP32C = 2,                /* Boris and RK4: float32 field exponentials and map lookup, float64
+                                     push / RK4 stages */
     FFA_RF_PHYSICAL_SUM = 4,      /* sum every RF gap (reference: last gap wins) */
     FFA_FP32 = 8,                 /* Boris: float32 field and push, r / fi / z / RF phase accumulated in
                                      float64 (no space charge, no field-error harmonics) */

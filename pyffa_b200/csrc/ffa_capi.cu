@@ -295,7 +295,6 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
         (!st->sc_pp || !st->e_pre_r || !st->e_pre_z || !st->e_pre_fi || !st->e_pp_r || !st->e_pp_z || !st->e_pp_fi))
         return FFA_ERR_INVALID;
     if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_FP32 | FFA_RF_PHYSICAL_SUM | FFA_SHAPE_MASK)) return FFA_ERR_INVALID;
-    if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
     if ((flags & FFA_FP32) && ((flags & (FFA_RK4 | FFA_FP32C)) || (sc_step > 0 && st->sc_pre) ||
                                fm->k.n_harm > 0))
         return FFA_ERR_UNSUPPORTED;
@@ -381,7 +380,7 @@ static int push_impl(const ffa_fieldmap *fm, const ffa_rf_desc *rf, const ffa_ap
         p.xing = *xing;
     }
     cudaError_t e;
-    if (flags & FFA_RK4) e = launch_rk4_f64(p, as_stream(stream));
+    if (flags & FFA_RK4) e = launch_rk4_f64(p, as_stream(stream), (flags & FFA_FP32C) != 0);
     else if (flags & FFA_FP32) e = launch_boris_f32(p, as_stream(stream), 32 << tb_sel);
     else if (flags & FFA_FP32C) e = launch_boris_f32c(p, as_stream(stream), 32 << tb_sel, nreg_sel);
     else e = launch_boris_f64(p, as_stream(stream), 32 << tb_sel);
@@ -393,11 +392,10 @@ int ffa_push_occupancy(int32_t flags, int32_t max_order, int32_t crossing, int32
 {
     if (!blocks_per_sm || !threads_per_block || max_order < 0 || max_order > FFA_MAX_ORDER) return FFA_ERR_INVALID;
     if (flags & ~(FFA_RK4 | FFA_FP32C | FFA_RF_PHYSICAL_SUM | FFA_SHAPE_MASK)) return FFA_ERR_INVALID;
-    if ((flags & FFA_FP32C) && (flags & FFA_RK4)) return FFA_ERR_UNSUPPORTED;
     const int tb_sel = (flags >> FFA_SHAPE_TB_SHIFT) & 3, nreg_sel = (flags >> FFA_SHAPE_NREG_SHIFT) & 3;
     if ((flags & FFA_RK4) && (tb_sel | nreg_sel)) return FFA_ERR_UNSUPPORTED;
     if (nreg_sel && !(flags & FFA_FP32C)) return FFA_ERR_UNSUPPORTED;
-    const int tb = (flags & FFA_RK4) ? 128 : (32 << tb_sel);
+    const int tb = (flags & FFA_RK4) ? ffa::RK4_TB : (32 << tb_sel);
     int blocks = 0;
     if (push_occupancy((flags & FFA_RK4) != 0, (flags & FFA_FP32C) != 0, max_order, crossing != 0, tb, nreg_sel,
                        &blocks) != cudaSuccess)

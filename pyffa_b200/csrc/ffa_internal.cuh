@@ -118,7 +118,9 @@ struct ffa_fieldmap {
 namespace ffa {
 // tb: threads per block; nreg_sel: register cap 80, 72, 64, 56 (0..3)
 cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s, int tb);
-cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s);
+// RK4 (f32: the FP32C field) in blocks of RK4_TB threads
+constexpr int RK4_TB = 32;
+cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s, bool f32);
 cudaError_t launch_boris_f32c(const PushK &p, cudaStream_t s, int tb, int nreg_sel);
 cudaError_t launch_boris_f32(const PushK &p, cudaStream_t s, int tb);
 cudaError_t push_occupancy(bool rk4, bool f32, int max_order, bool xing, int tb, int nreg_sel, int *blocks);

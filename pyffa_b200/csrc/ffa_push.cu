@@ -980,7 +980,10 @@ struct Y7 {
 };
 
 // RK4_equations_of_motion_njit for one live particle at stage state y.
-template <int MAXO, bool HARM>
+// F32: the field of the FP32C Boris pusher (field_mixed: float32 flutter
+// exponentials and map lookup, float64 products with r and z); the
+// equations of motion and the RK4 stages stay float64.
+template <int MAXO, bool HARM, bool F32>
 __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double rate, double acc,
                                           double esr, double esz, double esf, Y7 &d, int &oob)
 {
@@ -988,8 +991,12 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     const double q = p.cs.q, c = p.cs.c, E0 = p.cs.E0;
     const double fim = y.fi - f.period * floor(y.fi / f.period);
     double Bz, Br, Bfi;
-    analytic_b64(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi);
-    if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
+    if constexpr (F32) {
+        field_mixed<MAXO>(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi, oob);
+    } else {
+        analytic_b64(f, y.r, 1.0 / y.r, fim, y.z, Bz, Br, Bfi);
+        if constexpr (MAXO >= 1) high_order_b64<MAXO>(f, y.r, fim, y.z, Bz, Bfi, Br, oob);
+    }
     if constexpr (HARM) Bz += harmonics_bz(f.harm, f.n_harm, y.r, y.fi);
     double Er, Ez, Efi;
     rf_field64(p.rf, acc, y.r, y.fi, y.z, y.rf, Er, Ez, Efi);
@@ -1012,8 +1019,14 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     d.rf = rate;
 }
 
-template <int MAXO, bool SC, bool XING, bool HARM = false>
-__global__ void __launch_bounds__(128) rk4_f64_kernel(const __grid_constant__ PushK p)
+// One-warp blocks, at most 80 registers (24 warps per SM, spills to L1): the
+// 3125 warps of a 1e5-particle bunch are resident in one wave.  Uncapped the
+// kernel takes 130 registers, 12 warps per SM, 1.76 waves (measured on c1:
+// 14.8 ms per 720-step turn uncapped, 12.4 ms at 80 registers in
+// 128-thread blocks).  Block size: RK4_TB.
+
+template <int MAXO, bool SC, bool XING, bool HARM = false, bool F32 = false>
+__global__ void __maxnreg__(80) rk4_f64_kernel(const __grid_constant__ PushK p)
 {
     const int64_t t_ = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t_ >= p.n) return;
@@ -1050,18 +1063,18 @@ __global__ void __launch_bounds__(128) rk4_f64_kernel(const __grid_constant__ Pu
             continue;
         }
         Y7 d, k1, k2, k3, k4, ys;
-        rk4_rhs64<MAXO, HARM>(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM, F32>(p, y, __ldg(rate + 0), __ldg(acc + 0), esr, esz, esf, d, oob);
         k1 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k1.r, y.vr + 0.5 * k1.vr, y.z + 0.5 * k1.z, y.vz + 0.5 * k1.vz,
               y.fi + 0.5 * k1.fi, y.E + 0.5 * k1.E, y.rf + 0.5 * k1.rf};
-        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM, F32>(p, ys, __ldg(rate + 1), __ldg(acc + 1), esr, esz, esf, d, oob);
         k2 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + 0.5 * k2.r, y.vr + 0.5 * k2.vr, y.z + 0.5 * k2.z, y.vz + 0.5 * k2.vz,
               y.fi + 0.5 * k2.fi, y.E + 0.5 * k2.E, y.rf + 0.5 * k2.rf};
-        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM, F32>(p, ys, __ldg(rate + 2), __ldg(acc + 2), esr, esz, esf, d, oob);
         k3 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         ys = {y.r + k3.r, y.vr + k3.vr, y.z + k3.z, y.vz + k3.vz, y.fi + k3.fi, y.E + k3.E, y.rf + k3.rf};
-        rk4_rhs64<MAXO, HARM>(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
+        rk4_rhs64<MAXO, HARM, F32>(p, ys, __ldg(rate + 3), __ldg(acc + 3), esr, esz, esf, d, oob);
         k4 = {h * d.r, h * d.vr, h * d.z, h * d.vz, h * d.fi, h * d.E, h * d.rf};
         y.r += (k1.r + 2 * k2.r + 2 * k3.r + k4.r) / 6;
         y.vr += (k1.vr + 2 * k2.vr + 2 * k3.vr + k4.vr) / 6;
@@ -1205,19 +1218,26 @@ static void boris_launch(const PushK &p, cudaStream_t s, int tb, int)
     boris_default<MAXO, SC, false>(p, s, tb);
 }
 
-template <int MAXO, bool SC>
-static void rk4_launch(const PushK &p, cudaStream_t s)
+template <int MAXO, bool SC, bool F32>
+static void rk4_launch_p(const PushK &p, cudaStream_t s)
 {
-    const int tb = 128;
+    const int tb = RK4_TB;
     const unsigned g = (unsigned)((p.n + tb - 1) / tb);
     const bool x = xing_on(p);
     if (p.f.n_harm > 0) {
-        if (x) rk4_f64_kernel<MAXO, SC, true, true><<<g, tb, 0, s>>>(p);
-        else rk4_f64_kernel<MAXO, SC, false, true><<<g, tb, 0, s>>>(p);
+        if (x) rk4_f64_kernel<MAXO, SC, true, true, F32><<<g, tb, 0, s>>>(p);
+        else rk4_f64_kernel<MAXO, SC, false, true, F32><<<g, tb, 0, s>>>(p);
     } else {
-        if (x) rk4_f64_kernel<MAXO, SC, true><<<g, tb, 0, s>>>(p);
-        else rk4_f64_kernel<MAXO, SC, false><<<g, tb, 0, s>>>(p);
+        if (x) rk4_f64_kernel<MAXO, SC, true, false, F32><<<g, tb, 0, s>>>(p);
+        else rk4_f64_kernel<MAXO, SC, false, false, F32><<<g, tb, 0, s>>>(p);
     }
+}
+
+template <int MAXO, bool SC>
+static void rk4_launch(const PushK &p, cudaStream_t s, bool f32)
+{
+    if (f32) rk4_launch_p<MAXO, SC, true>(p, s);
+    else rk4_launch_p<MAXO, SC, false>(p, s);
 }
 
 #define FFA_DISPATCH(FN, p, ...)                                                       \
@@ -1238,9 +1258,9 @@ cudaError_t launch_boris_f64(const PushK &p, cudaStream_t s, int tb)
     return cudaGetLastError();
 }
 
-cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s)
+cudaError_t launch_rk4_f64(const PushK &p, cudaStream_t s, bool f32)
 {
-    FFA_DISPATCH(rk4_launch, p, s);
+    FFA_DISPATCH(rk4_launch, p, s, f32);
     return cudaGetLastError();
 }
 
@@ -1297,7 +1317,8 @@ cudaError_t launch_boris_f32(const PushK &p, cudaStream_t s, int tb)
 template <int MAXO, bool X>
 static const void *push_kernel_fn(bool rk4, bool f32, int nreg_sel)
 {
-    if (rk4) return (const void *)rk4_f64_kernel<MAXO, false, X>;
+    if (rk4) return f32 ? (const void *)rk4_f64_kernel<MAXO, false, X, false, true>
+                        : (const void *)rk4_f64_kernel<MAXO, false, X>;
     if (!f32) return (const void *)boris_f64_kernel<MAXO, false, X, false>;
     switch (nreg_sel) {
     case 0: return (const void *)boris_f64_kernel<MAXO, false, X, true, 80>;

@@ -166,8 +166,8 @@ class Pusher:
         self.harmonics = getattr(gp, "BHarmonics", None)
         self.flags = _lib.FFA_RK4 if solver == "RK4" else _lib.FFA_BORIS
         if precision in ("fp32c", "fp32"):
-            if solver == "RK4":
-                raise NotImplementedError("the float32 pushers are Boris-only")
+            if solver == "RK4" and precision == "fp32":
+                raise NotImplementedError("the float32 push is Boris-only (RK4 takes fp64 or fp32c)")
             self.flags |= _lib.FFA_FP32C if precision == "fp32c" else _lib.FFA_FP32
         elif precision != "fp64":
             raise ValueError(f"precision must be fp64, fp32c or fp32, not {precision!r}")

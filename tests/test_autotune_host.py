@@ -59,6 +59,8 @@ def test_push_checks_shape_bits_before_any_cuda_call():
             assert _push(F | _lib.shape_flags(t, r)) == 0      # every shape, FP32C Boris
     assert _push(B | _lib.shape_flags(0, 1)) == 4              # register caps: FP32C only
     assert _push(R | _lib.shape_flags(1, 0)) == 4              # RK4 takes the default shape only
+    assert _push(R | F) == 0                                   # RK4 with the FP32C field
+    assert _push(R | _lib.FFA_FP32) == 4                       # the float32 push is Boris-only
     assert _push(F | _lib.shape_flags(0, 2), sc_step=5) == 4   # and not with space charge
     assert _push(F | _lib.shape_flags(1, 0), sc_step=5) == 0   # block size with space charge: fine
     assert _push(B | (1 << 12)) == 1                           # unknown bit

@@ -1,5 +1,6 @@
 """The FP32C Boris pusher (float32 field exponentials and map lookup,
-float64 push) against the float64 one.
+float64 push) against the float64 one; the RK4 pusher with the same field
+against float64 RK4.
 
 Both push the same seeded 6D Gaussian bunch through the full 1301 x 6000 map
 (z-Taylor order 2) for 1000 turns at 2880 steps per turn (at 720 steps/turn
@@ -161,6 +162,45 @@ def test_fp32c_single_turn_close_to_fp64():
         scale = np.max(np.abs(f(ar) - f(a64)) / np.abs(f(a64)))
         print(f"\none turn, {name}: fp32c {err:.3g}, fp64 response to r * (1 + 2^-24) {scale:.3g}")
         assert err <= 1e-7 and err <= max(4 * scale, 1e-12), (name, err, scale)
+
+
+def test_fp32c_rk4_single_turn_close_to_fp64():
+    """The RK4 pusher with the FP32C field (float32 flutter exponentials and
+    map lookup; equations of motion and RK4 stages in float64), one turn at
+    720 steps per turn with the RF on, against the float64 RK4 pusher:
+    flags exact; radius, azimuth and total energy within 1e-7 and within 4
+    times the float64 RK4 response to r * (1 + 2^-24); and not bit-equal to
+    float64 (the float32 field is the one in use)."""
+    from pyffa_b200 import synthetic
+    from pyffa_b200.bunch import FFAG_Bunch
+    from pyffa_b200.constants import FFAG_ConversionTools
+    from pyffa_b200.dump import Dumps
+    from pyffa_b200.track import FFAG_RungeKutta
+    gp = _lattice(True)
+    v = FFAG_ConversionTools().ConvertPrzek2Vrzek(synthetic.centred_bunch(4096, seed=19))
+    dt = synthetic.design_dt(300.0, 720)
+
+    def run(m, precision):
+        b = FFAG_Bunch(m.copy(), BunchType="RK4")
+        lp = {"stop_condition": {"max_stepsN": 720, "max_turn": 1e9, "max_time": 1e9}, "time_step": dt,
+              "enable_SC": False, "SC_type": 1, "SC_step": 20, "step_dumps": Dumps()}
+        FFAG_RungeKutta(precision=precision, verbose=False).rk4_solve_dt_bunch3_withSC(None, 0.0, b, gp, lp)
+        return b.LocalBunch
+
+    v32 = v.copy()
+    v32[:, 0] = v32[:, 0] * (1 + 2.0 ** -24)
+    a64, a32, ar = run(v, "fp64"), run(v, "fp32c"), run(v32, "fp64")
+    assert np.array_equal(a64[:, 7:9], a32[:, 7:9])
+    al = a64[:, 8] == 1
+    assert al.sum() > 4000
+    differs = False
+    for name, c in (("r", 0), ("fi", 4), ("E", 5)):
+        err = np.max(np.abs(a32[al, c] - a64[al, c]) / np.abs(a64[al, c]))
+        scale = np.max(np.abs(ar[al, c] - a64[al, c]) / np.abs(a64[al, c]))
+        print(f"\none RK4 turn, {name}: fp32c {err:.3g}, fp64 response to r * (1 + 2^-24) {scale:.3g}")
+        assert err <= 1e-7 and err <= max(4 * scale, 1e-12), (name, err, scale)
+        differs |= err > 0
+    assert differs
 
 
 def test_fp32_push_single_turn():
