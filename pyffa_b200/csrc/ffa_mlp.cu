@@ -882,6 +882,347 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (threadIdx.x == 0 && *abort_flag && error) atomicExch(error, 1);
 }
 
+// ------------------------------------------------ paired-tile inference
+// Two 128-state tiles per CTA in flight (slots 0 and 1), each with one
+// 256-column accumulator (D_s = tensor-memory columns 256 s .. 256 s + 255),
+// its own activation operand A_s and layer-1 input X_s in shared memory.
+// The epilogue warps alternate between the slots layer by layer,
+//   E(0, l)  E(1, l)  E(0, l + 1)  E(1, l + 1) ...
+// and the MMA thread issues in the same order, so the tensor cores run one
+// slot's layer while the epilogue converts the other slot's.  The MMAs of a
+// slot's next layer overwrite its accumulator: they wait for d_free[s], which
+// the epilogue warps signal once their last tensor-memory load of D_s has
+// completed (before the last chunk is converted), besides the A_s chunks.
+// W2 / W3 stream through a ring of two 32 KB slots, once per slot and layer.
+// A CTA's tiles are t, t + G (a pair), t + 2G, t + 3G, ... (G = grid size);
+// an unpaired last tile runs in slot 0 alone.
+constexpr int RING2 = 2;
+constexpr uint32_t S2_A = 0;                                   // A_0, A_1: 64 KB each
+constexpr uint32_t S2_RING = S2_A + 2 * 4 * A_CHUNK_BYTES;
+constexpr uint32_t S2_W4 = S2_RING + RING2 * W_CHUNK_BYTES;
+constexpr uint32_t S2_W1 = S2_W4 + 4 * W4_CHUNK_BYTES;
+constexpr uint32_t S2_X = S2_W1 + H * KIN * 2;                 // X_0, X_1: 4 KB each
+constexpr uint32_t S2_XB = TC_M * KIN * 2;
+constexpr uint32_t S2_BIAS = S2_X + 2 * S2_XB;
+constexpr uint32_t S2_TAIL = S2_BIAS + 3 * H * 4;
+constexpr uint32_t S2_BAR = S2_TAIL + 208 * 4;
+// x_ready[2], a_ready[2][4], d_full[2], d_free[2], full[RING2], empty[RING2], drain
+constexpr int NBAR2 = 2 + 8 + 2 + 2 + 2 * RING2 + 1;
+constexpr uint32_t S2_MISC = S2_BAR + NBAR2 * 8;
+constexpr uint32_t S2_TOTAL = S2_MISC + 16;
+constexpr size_t TC2_SMEM = S2_TOTAL + 1024;
+static_assert(TC2_SMEM <= 232448, "paired inference: shared memory per block");
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    mlp_infer_tc2_kernel(const float *__restrict__ P, const unsigned char *__restrict__ wp, float *__restrict__ state,
+                         int32_t *__restrict__ applied, int32_t *__restrict__ error, int64_t n, int n_apply,
+                         float radius2)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t s0 = smem_u32(sm);
+    float *sbias = reinterpret_cast<float *>(sm + S2_BIAS);
+    float *stail = reinterpret_cast<float *>(sm + S2_TAIL);   // b4[0..7], Ws[8..71], bs[72..79], Wq[80..207]
+    const uint32_t bar0 = s0 + S2_BAR;
+    const uint32_t BAR_X = bar0, BAR_A = bar0 + 16, BAR_D = bar0 + 80, BAR_F = bar0 + 96, BAR_FULL = bar0 + 112,
+                   BAR_EMPTY = BAR_FULL + 8 * RING2, BAR_DRAIN = BAR_EMPTY + 8 * RING2;
+    uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(sm + S2_MISC);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + S2_MISC + 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t ntiles = (n + TC_M - 1) / TC_M, G = gridDim.x;
+
+    for (int i = threadIdx.x; i < (int)(H * KIN * 2 / 16); i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + S2_W1)[i] = reinterpret_cast<const uint4 *>(wp + PK_W1)[i];
+    for (int i = threadIdx.x; i < (int)(4 * W4_CHUNK_BYTES / 16); i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm + S2_W4)[i] = reinterpret_cast<const uint4 *>(wp + PK_W4)[i];
+    for (int i = threadIdx.x; i < 3 * H; i += blockDim.x) sbias[i] = 0.5f * P[(i < H ? P_B1 : i < 2 * H ? P_B2 : P_B3) + (i % H)];
+    for (int i = threadIdx.x; i < 208; i += blockDim.x)
+        stail[i] = i < 8 ? P[P_B4 + i] : i < 72 ? P[P_WS + (i - 8)] : i < 80 ? P[P_BS + (i - 72)] : P[P_WQ + (i - 80)];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(BAR_X + 8 * s, 4);
+            for (int c = 0; c < 4; ++c) mbar_init(BAR_A + 8 * (4 * s + c), 16);
+            mbar_init(BAR_D + 8 * s, 1);
+            mbar_init(BAR_F + 8 * s, 16);
+        }
+        for (int r = 0; r < RING2; ++r) {
+            mbar_init(BAR_FULL + 8 * r, 1);
+            mbar_init(BAR_EMPTY + 8 * r, 1);
+        }
+        mbar_init(BAR_DRAIN, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *tmem_holder;
+
+    if (warp == 0) {
+        // ---------------------------------------------------- weight stream
+        // consumption order of the MMA thread: per map, W2 for slot 0, W2 for
+        // slot 1, W3 for slot 0, W3 for slot 1, four chunks each
+        if (lane == 0) {
+            uint32_t q = 0;
+            for (int64_t t0 = blockIdx.x; t0 < ntiles && !*abort_flag; t0 += 2 * G) {
+                const int ns = t0 + G < ntiles ? 2 : 1;
+                for (int it = 0; it < n_apply && !*abort_flag; ++it)
+                    for (int l = 0; l < 2; ++l)
+                        for (int s = 0; s < ns; ++s)
+                            for (int c = 0; c < 4; ++c, ++q) {
+                                const uint32_t slot = q % RING2, use = q / RING2;
+                                if (!mbar_wait(BAR_EMPTY + 8 * slot, (use & 1) ^ 1, abort_flag)) break;
+                                mbar_expect_tx(BAR_FULL + 8 * slot, W_CHUNK_BYTES);
+                                bulk_load(s0 + S2_RING + slot * W_CHUNK_BYTES,
+                                          wp + (l == 0 ? PK_W2 : PK_W3) + c * W_CHUNK_BYTES, W_CHUNK_BYTES,
+                                          BAR_FULL + 8 * slot);
+                            }
+            }
+            // drain: every issued copy has landed before the block exits
+            const uint32_t issued = q;
+            for (uint32_t r = issued > RING2 ? issued - RING2 : 0; r < issued; ++r)
+                if (!mbar_wait_bounded(BAR_FULL + 8 * (r % RING2), (r / RING2) & 1)) *abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------- MMA issue
+        if (lane == 0) {
+            const uint32_t ID256 = idesc_bf16(TC_M, H), ID16 = idesc_bf16(TC_M, 16);
+            uint32_t q = 0, nx[2] = {0, 0}, na[2] = {0, 0}, nb[2] = {0, 0};
+            bool ok = true;
+            for (int64_t t0 = blockIdx.x; t0 < ntiles && ok; t0 += 2 * G) {
+                const int ns = t0 + G < ntiles ? 2 : 1;
+                for (int it = 0; it < n_apply && ok; ++it)
+                    for (int layer = 0; layer < 4 && ok; ++layer)
+                        for (int s = 0; s < ns && ok; ++s) {
+                            const uint32_t D = tmem + 256 * s;
+                            // the accumulator's previous contents have been read
+                            if (nb[s] > 0) ok = mbar_wait(BAR_F + 8 * s, (nb[s] - 1) & 1, abort_flag);
+                            ++nb[s];
+                            if (!ok) break;
+                            if (layer == 0) {
+                                // layer 1: X_s (128 x 16) x W1^T -> D_s
+                                ok = mbar_wait(BAR_X + 8 * s, nx[s]++ & 1, abort_flag);
+                                if (!ok) break;
+                                tc_after_sync();
+                                umma(D, sdesc(s0 + S2_X + s * S2_XB, 128, 256, 0), sdesc(s0 + S2_W1, 128, 256, 0), ID256, 0);
+                            } else if (layer < 3) {
+                                // layers 2, 3: A_s (128 x 256) x W^T (streamed) -> D_s
+                                for (int c = 0; c < 4; ++c, ++q) {
+                                    const uint32_t slot = q % RING2, use = q / RING2;
+                                    ok = mbar_wait(BAR_A + 8 * (4 * s + c), na[s] & 1, abort_flag) &&
+                                         mbar_wait(BAR_FULL + 8 * slot, use & 1, abort_flag);
+                                    if (!ok) break;
+                                    tc_after_sync();
+                                    const uint32_t a0 = s0 + S2_A + (4 * s + c) * A_CHUNK_BYTES;
+                                    const uint32_t b0 = s0 + S2_RING + slot * W_CHUNK_BYTES;
+#pragma unroll
+                                    for (int kk = 0; kk < 4; ++kk)
+                                        umma(D, sdesc(a0 + 32 * kk, 16, 1024, 2), sdesc(b0 + 32 * kk, 16, 1024, 2),
+                                             ID256, (c | kk) != 0);
+                                    umma_commit(BAR_EMPTY + 8 * slot);
+                                }
+                                ++na[s];
+                            } else {
+                                // layer 4: A_s x W4^T (16 x 256, resident) -> D_s columns 0..15
+                                for (int c = 0; c < 4; ++c) {
+                                    ok = mbar_wait(BAR_A + 8 * (4 * s + c), na[s] & 1, abort_flag);
+                                    if (!ok) break;
+                                    tc_after_sync();
+                                    const uint32_t a0 = s0 + S2_A + (4 * s + c) * A_CHUNK_BYTES;
+                                    const uint32_t b0 = s0 + S2_W4 + c * W4_CHUNK_BYTES;
+#pragma unroll
+                                    for (int kk = 0; kk < 4; ++kk)
+                                        umma(D, sdesc(a0 + 32 * kk, 16, 1024, 2), sdesc(b0 + 32 * kk, 16, 1024, 2),
+                                             ID16, (c | kk) != 0);
+                                }
+                                ++na[s];
+                            }
+                            if (ok) umma_commit(BAR_D + 8 * s);
+                        }
+            }
+            // drain: every MMA issued has completed before tensor memory is freed
+            umma_commit(BAR_DRAIN);
+            if (!mbar_wait_bounded(BAR_DRAIN, 0)) *abort_flag = 1;
+        }
+    } else {
+        // ---------------------------------------------------- epilogue
+        // warps 2..17: tensor-memory lane quarter warp % 4, column quarter
+        // (warp - 2) / 4 of every 64-column chunk; the quarter-0 thread of a
+        // row owns that row's state in both slots
+        const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;          // column quarter 0..3
+        const int row = quarter * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + 16 * half;
+        uint32_t nd[2] = {0, 0};
+        bool ok = true;
+        // layer-1 input row of slot s (quarter-0 threads): the domain test, then
+        // s0..s5 split into bfloat16 high and low parts (columns 0..5 and 6..11;
+        // W1 is stacked twice), zero padding to 16
+        auto write_x = [&](const float *x, bool &act, int s) {
+            if (radius2 > 0.0f)
+                act = act && (x[0] * x[0] + x[1] * x[1] <= radius2) && (x[2] * x[2] + x[3] * x[3] <= radius2) &&
+                      (fabsf(x[4]) <= 1.0f);
+            float xl[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) xl[k] = x[k] - __bfloat162float(__float2bfloat16_rn(x[k]));
+            uint4 lo, hi;
+            lo.x = pack_bf16(x[0], x[1]);
+            lo.y = pack_bf16(x[2], x[3]);
+            lo.z = pack_bf16(x[4], x[5]);
+            lo.w = pack_bf16(xl[0], xl[1]);
+            hi.x = pack_bf16(xl[2], xl[3]);
+            hi.y = pack_bf16(xl[4], xl[5]);
+            hi.z = 0u;
+            hi.w = 0u;
+            unsigned char *xb = sm + S2_X + s * S2_XB;
+            *reinterpret_cast<uint4 *>(xb + core_off(row, 0)) = lo;
+            *reinterpret_cast<uint4 *>(xb + core_off(row, 8)) = hi;
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(BAR_X + 8 * s);
+        };
+        // layer 4 of slot s: the fitted outputs, the float32 skip connection
+        auto update = [&](float *x, bool act, int &cnt, const uint32_t *f) {
+            if (!act) return;
+            float y[4], q[15];
+            quad_features(x, q);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                float lin = stail[72 + c];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) lin = fmaf(x[k], stail[8 + k * NOUT + c], lin);
+#pragma unroll
+                for (int m = 0; m < 15; ++m) lin = fmaf(q[m], stail[80 + m * NOUT + c], lin);
+                y[c] = x[c] + (lin + (__uint_as_float(f[c]) + stail[c]));
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) x[c] = y[c];
+            ++cnt;
+        };
+        for (int64_t t0 = blockIdx.x; t0 < ntiles && ok; t0 += 2 * G) {
+            const int ns = t0 + G < ntiles ? 2 : 1;
+            const int64_t p0 = t0 * TC_M + row, p1 = (t0 + G) * TC_M + row;
+            float x0[NOUT], x1[NOUT];
+            bool act0 = p0 < n, act1 = ns == 2 && p1 < n;
+            int cnt0 = 0, cnt1 = 0;
+            if (half == 0) {
+#pragma unroll
+                for (int i = 0; i < NOUT; ++i) x0[i] = x1[i] = 0.0f;
+                if (act0) {
+                    const float4 u = reinterpret_cast<const float4 *>(state)[2 * p0];
+                    const float4 w = reinterpret_cast<const float4 *>(state)[2 * p0 + 1];
+                    x0[0] = u.x; x0[1] = u.y; x0[2] = u.z; x0[3] = u.w; x0[4] = w.x; x0[5] = w.y; x0[6] = w.z; x0[7] = w.w;
+                }
+                if (act1) {
+                    const float4 u = reinterpret_cast<const float4 *>(state)[2 * p1];
+                    const float4 w = reinterpret_cast<const float4 *>(state)[2 * p1 + 1];
+                    x1[0] = u.x; x1[1] = u.y; x1[2] = u.z; x1[3] = u.w; x1[4] = w.x; x1[5] = w.y; x1[6] = w.z; x1[7] = w.w;
+                }
+                write_x(x0, act0, 0);
+                if (ns == 2) write_x(x1, act1, 1);
+            }
+            for (int it = 0; it < n_apply && ok; ++it) {
+                // hidden layers 1..3 of slot 0, then slot 1
+                for (int l = 0; l < 3 && ok; ++l)
+                    for (int s = 0; s < ns && ok; ++s) {
+                        ok = __all_sync(0xffffffffu, mbar_wait(BAR_D + 8 * s, nd[s]++ & 1, abort_flag));
+                        if (!ok) break;
+                        tc_after_sync();
+                        const uint32_t src = lane_base + 256u * s;
+                        const float *hb = sbias + l * H + 16 * half;
+                        unsigned char *arow = sm + S2_A + s * (4 * A_CHUNK_BYTES) + row * 128;
+                        const uint32_t bar_a = BAR_A + 8 * (4 * s), bar_f = BAR_F + 8 * s;
+                        uint32_t va[16], vb[16];
+                        TMEM_LD16(src, va);
+                        tmem_wait_ld();
+                        REG_FENCE16(va);
+                        // chunk c is converted while chunk c + 1 is in flight; once
+                        // chunk 3 has landed, D_s is free for the next layer's MMAs
+#define EPI2_CHUNK(c, cur, nxt)                                                                          \
+    {                                                                                                    \
+        if ((c) < 3) TMEM_LD16(src + ((c) + 1) * TC_CHUNK, nxt);                                         \
+        _Pragma("unroll") for (int j = 0; j < 2; ++j)                                                    \
+        {                                                                                                \
+            const uint4 o = silu8(cur + 8 * j, hb + (c) * TC_CHUNK + 8 * j);                            \
+            *reinterpret_cast<uint4 *>(arow + (c) * A_CHUNK_BYTES + (((2 * half + j) ^ (row & 7)) << 4)) = o; \
+        }                                                                                                \
+        fence_async_smem();                                                                              \
+        if ((c) < 3) {                                                                                   \
+            tmem_wait_ld();                                                                              \
+            REG_FENCE16(nxt);                                                                            \
+        }                                                                                                \
+        tc_before_sync();                                                                                \
+        __syncwarp();                                                                                    \
+        if (lane == 0) {                                                                                 \
+            mbar_arrive(bar_a + 8 * (c));                                                                \
+            if ((c) == 2) mbar_arrive(bar_f);                                                            \
+        }                                                                                                \
+    }
+                        EPI2_CHUNK(0, va, vb)
+                        EPI2_CHUNK(1, vb, va)
+                        EPI2_CHUNK(2, va, vb)
+                        EPI2_CHUNK(3, vb, va)
+#undef EPI2_CHUNK
+                    }
+                if (!ok) break;
+                // layer 4 and the residual update per slot, then that slot's
+                // layer-1 input of the next map
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    if (s >= ns || !ok) break;
+                    ok = __all_sync(0xffffffffu, mbar_wait(BAR_D + 8 * s, nd[s]++ & 1, abort_flag));
+                    if (!ok) break;
+                    uint32_t f[16];
+                    if (half == 0) {
+                        tc_after_sync();
+                        TMEM_LD16(lane_base + 256u * s, f);
+                        tmem_wait_ld();
+                        REG_FENCE16(f);
+                    }
+                    tc_before_sync();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(BAR_F + 8 * s);
+                    if (half == 0) {
+                        if (s == 0) {
+                            update(x0, act0, cnt0, f);
+                            if (it + 1 < n_apply) write_x(x0, act0, 0);
+                        } else {
+                            update(x1, act1, cnt1, f);
+                            if (it + 1 < n_apply) write_x(x1, act1, 1);
+                        }
+                    }
+                }
+            }
+            if (half == 0 && ok) {
+                if (p0 < n) {
+                    reinterpret_cast<float4 *>(state)[2 * p0] = make_float4(x0[0], x0[1], x0[2], x0[3]);
+                    reinterpret_cast<float4 *>(state)[2 * p0 + 1] = make_float4(x0[4], x0[5], x0[6], x0[7]);
+                    if (applied) applied[p0] = cnt0;
+                }
+                if (ns == 2 && p1 < n) {
+                    reinterpret_cast<float4 *>(state)[2 * p1] = make_float4(x1[0], x1[1], x1[2], x1[3]);
+                    reinterpret_cast<float4 *>(state)[2 * p1 + 1] = make_float4(x1[4], x1[5], x1[6], x1[7]);
+                    if (applied) applied[p1] = cnt1;
+                }
+            }
+        }
+    }
+    // teardown: the MMA thread has drained its MMAs, the epilogue its loads
+    tc_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+    if (threadIdx.x == 0 && *abort_flag && error) atomicExch(error, 1);
+}
+
 // ------------------------------------------------- GEMM (training, tcgen05)
 // The training products of at least 128 x 128 x 64 on the 5th-generation
 // tensor cores: C[M][N] = op(A) op(B) (+ bias) with the operands and the
@@ -1278,9 +1619,19 @@ extern "C" int ffa_mlp_infer(const ffa_mlp_infer_desc *d, void *stream)
     FFA_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t tiles = (d->n + TC_M - 1) / TC_M;
     const int grid = (int)(tiles < sms ? tiles : sms);
-    FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-    mlp_infer_tc_kernel<<<grid, TC_THREADS, TC_SMEM, (cudaStream_t)stream>>>(
-        d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n, d->n_apply,
-        d->radius2);
+    if (tiles > sms) {
+        // more tiles than SMs: two tiles in flight per SM
+        FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TC2_SMEM));
+        mlp_infer_tc2_kernel<<<grid, TC_THREADS, TC2_SMEM, (cudaStream_t)stream>>>(
+            d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n,
+            d->n_apply, d->radius2);
+    } else {
+        FFA_CHECK_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)TC_SMEM));
+        mlp_infer_tc_kernel<<<grid, TC_THREADS, TC_SMEM, (cudaStream_t)stream>>>(
+            d->params, reinterpret_cast<const unsigned char *>(d->wpack), d->state, d->applied, d->error, d->n,
+            d->n_apply, d->radius2);
+    }
     return cudaGetLastError() == cudaSuccess ? FFA_OK : FFA_ERR_CUDA;
 }

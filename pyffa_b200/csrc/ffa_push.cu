@@ -1019,11 +1019,11 @@ __device__ __forceinline__ void rk4_rhs64(const PushK &p, const Y7 &y, double ra
     d.rf = rate;
 }
 
-// One-warp blocks, at most 80 registers (24 warps per SM, spills to L1): the
-// 3125 warps of a 1e5-particle bunch are resident in one wave.  Uncapped the
-// kernel takes 130 registers, 12 warps per SM, 1.76 waves (measured on c1:
-// 14.8 ms per 720-step turn uncapped, 12.4 ms at 80 registers in
-// 128-thread blocks).  Block size: RK4_TB.
+// One-warp blocks (RK4_TB), at most 80 registers (24 warps per SM, spills
+// to L1): the 3125 warps of a 1e5-particle bunch are resident in one wave.
+// Uncapped the kernel takes 130 registers, 12 warps per SM, 1.76 waves
+// (measured on c1: 14.8 ms per 720-step turn uncapped; at 80 registers
+// 12.4 ms in 128-thread blocks, 12.3 ms in 32-thread blocks).
 
 template <int MAXO, bool SC, bool XING, bool HARM = false, bool F32 = false>
 __global__ void __maxnreg__(80) rk4_f64_kernel(const __grid_constant__ PushK p)
