@@ -317,6 +317,7 @@ def sc_bench(gp, dt, dev, hbm_peak, updates=20, warmup=3, turns=2):
 
     cycle("fp32c", 1)                   # warm-up
     ms32, _ = cycle("fp32c", turns)
+    cycle("fp64", 1)                    # warm-up (the FP64 pusher's first particle order)
     ms64, _ = cycle("fp64", turns)
     out["cycle"] = "12 x (open-boundary update + 60 Boris FP32C steps) per turn"
     out["cycle_particle_turns_per_s"] = n * turns / (ms32 * 1e-3)

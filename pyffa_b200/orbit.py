@@ -31,7 +31,8 @@ class MidplaneField:
         self.N = bm["NSector"]
         self.P = 2 * np.pi / self.N
         if bm.get("SpiralAngle_deg", 0) != 0:
-            raise NotImplementedError("closed orbits are computed for a zero spiral angle")
+            raise NotImplementedError("this helper (synthetic inputs) takes a zero spiral angle; "
+                                      "spiral lattices: pyffa_b200.seo.FFAG_SearchSEO")
 
     def flutter(self, th):
         th = th - self.P * np.floor(th / self.P)

@@ -116,7 +116,9 @@ def morton_order(cols, start: int, n: int, period: float):
     the sector, f5), each quantised to 15 bits over the range's span:
     particles with nearby keys sit near each other in the coordinates that
     pick the z-Taylor nodes of the next steps.  Non-finite values count as
-    the span's low end."""
+    the span's low end.  Particles not in flight (not injected, or lost: the
+    push kernels take a different branch for them) come after all particles
+    in flight, so that warps do not mix the two branches."""
     import torch
     sl = slice(start, start + n)
     x = torch.stack([cols["r"][sl], cols["vr"][sl], torch.remainder(cols["fi"][sl], period), cols["f5"][sl]])
@@ -125,6 +127,9 @@ def morton_order(cols, start: int, n: int, period: float):
     span = (x.amax(1, keepdim=True) - lo).clamp_min(1e-300)
     q = ((x - lo) / span * 32767.0).to(torch.int64).clamp_(0, 32767)
     key = _part1by3(q[0]) | (_part1by3(q[1]) << 1) | (_part1by3(q[2]) << 2) | (_part1by3(q[3]) << 3)
+    if "inj" in cols and "surv" in cols:
+        idle = (cols["inj"][sl] != 1) | (cols["surv"][sl] != 1)
+        key |= idle.to(torch.int64) << 61
     return torch.argsort(key).to(torch.int32)
 
 

@@ -40,3 +40,24 @@ def test_morton_order_is_a_sorted_permutation():
         d_ord = np.median(np.linalg.norm(np.diff(x[p], axis=0), axis=1))
         d_given = np.median(np.linalg.norm(np.diff(x, axis=0), axis=1))
         assert d_ord < 0.3 * d_given, (d_ord, d_given)
+
+
+def test_particles_not_in_flight_come_last():
+    """Lost or not yet injected particles (the push kernels' other branch)
+    follow every particle in flight; each group keeps the Morton order."""
+    rng = np.random.default_rng(5)
+    n = 3000
+    cols = {"r": torch.as_tensor(8.1 + 3e-3 * rng.standard_normal(n)),
+            "vr": torch.as_tensor(2e5 * rng.standard_normal(n)),
+            "fi": torch.as_tensor(rng.uniform(-20, 20, n)),
+            "f5": torch.as_tensor(2.3e7 * (1 + 1e-3 * rng.standard_normal(n))),
+            "inj": torch.as_tensor((rng.uniform(size=n) > 0.1).astype(np.uint8)),
+            "surv": torch.as_tensor((rng.uniform(size=n) > 0.2).astype(np.uint8))}
+    p = morton_order(cols, 0, n, 2 * np.pi / 12).numpy()
+    assert np.array_equal(np.sort(p), np.arange(n))
+    live = ((cols["inj"] == 1) & (cols["surv"] == 1)).numpy()
+    k = int(live.sum())
+    assert live[p[:k]].all() and not live[p[k:]].any()
+    flat = {key: v for key, v in cols.items() if key not in ("inj", "surv")}
+    q = morton_order(flat, 0, n, 2 * np.pi / 12).numpy()
+    assert np.array_equal(p[:k], q[live[q]])        # the Morton order within the group
